@@ -1,0 +1,348 @@
+"""Benchmark: SOAP power spectrum with forces on one B200 (FP64 drop-in).
+
+Workload (one step): one periodic cubic box of 1000 atoms at number density
+0.1 A^-3 (L = 21.544 A), uniform positions rejection-sampled to a minimum
+pair distance of 0.9 A, 4 species (1, 6, 7, 8) drawn uniformly, seeded;
+hypers rc 5.5 A, ShiftedCosine 0.5 A, Gaussian width 0.3 A, GTO max_radial 7,
+max_angular 6, spline accuracy 1e-8.  Output: the power spectrum plus its
+positions and strain gradients, FP64 -- neighbour list, spherical expansion,
+contraction, every row materialised in featomic's TensorMap layout.
+
+* ``value``  atom-environments/s with positions resident in HBM and the
+  TensorMap left in HBM (featomic_b200_calculator_compute_device), CUDA
+  events on the launching stream, L2 flushed between steps.
+* ``e2e``    the same through featomic's C API (featomic_calculator_compute)
+  with host systems: host->device positions and device->host TensorMap
+  inside the timed region.
+* ``cpu_baseline`` / ``--impl reference``: featomic itself is Rust and cannot
+  be built here (no cargo / crates), so the CPU side is the FP64 C++
+  restatement in oracle/ (OpenMP, featomic's decomposition: spherical
+  expansion over systems, power spectrum over samples).
+
+Multi-GPU: the path has no exchange step; ``--gpus N`` runs N independent
+replicas (one process per GPU) and reports the aggregate rate.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SOAP power-spectrum atom-envs/s with forces, 1 B200, at stated error vs FP64"
+WORKLOAD = "random_box_1000_rho0.1_rc5.5_nmax7_lmax6_ps+positions+strain_fp64"
+GRADIENTS = ["positions", "strain"]
+N_ATOMS = 1000
+
+
+def workload():
+    from rascaline_b200 import workloads
+    system = workloads.random_box(N_ATOMS, density=0.1, min_distance=0.9, seed=2)
+    return system, workloads.hypers(5.5, 7, 6)
+
+
+def config(extra=None):
+    c = {
+        "workload": WORKLOAD,
+        "n_atoms": N_ATOMS,
+        "gradients": GRADIENTS,
+        "hypers": {"cutoff": 5.5, "max_radial": 7, "max_angular": 6, "gaussian_width": 0.3,
+                   "smoothing": "ShiftedCosine 0.5", "spline_accuracy": 1e-8},
+        "l2": "flushed between steps (256 MiB write); each step also writes 3.5 GB of output",
+        "parallelism": "replicas",
+    }
+    if extra:
+        c.update(extra)
+    return c
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fd:
+            data = json.load(fd)
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(smax)) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def cpu_baseline(system, hypers, seconds=20.0):
+    """The oracle (C++ FP64 restatement of featomic's path) on the host cores."""
+    from oracle import oracle
+    oracle.build()
+    threads = os.cpu_count() or 1
+    envs, elapsed, runs = 0, 0.0, 0
+    while elapsed < seconds or runs == 0:
+        t0 = time.perf_counter()
+        oracle.compute("soap_power_spectrum", hypers, [system], gradients=tuple(GRADIENTS), threads=threads)
+        elapsed += time.perf_counter() - t0
+        envs += N_ATOMS
+        runs += 1
+        if runs >= 3 and elapsed > seconds / 2:
+            break
+    return {
+        "value": envs / elapsed, "unit": "atom-envs/s", "cores": threads, "kind": "port",
+        "sample": f"{runs} full compute(s) of the {N_ATOMS}-atom box (PS + positions + strain gradients, FP64), "
+                  f"{elapsed:.1f} s; spherical expansion serial per system, power spectrum OpenMP over samples",
+    }
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args):
+    rank, world, _ = dist_setup(args.gpus)
+    if rank != 0:
+        barrier(world)
+        return
+    system, hypers = workload()
+    from oracle import oracle
+    oracle.build()
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.compute("soap_power_spectrum", hypers, [system], gradients=tuple(GRADIENTS), threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.compute("soap_power_spectrum", hypers, [system], gradients=tuple(GRADIENTS), threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1000.0 * float(np.mean(times))
+    value = N_ATOMS / (ms / 1000.0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "atom-envs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": config({"reference": "featomic is Rust and cannot be built here (no cargo/rustc, no crates); "
+                                       "timed: the C++ FP64 restatement in oracle/ with all host threads"}),
+        "cpu_baseline": {"value": value, "unit": "atom-envs/s", "cores": threads, "kind": "port",
+                         "sample": f"full {N_ATOMS}-atom compute per step"},
+        "e2e": {"value": value, "unit": "atom-envs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    barrier(world)
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--warmup", type=int, default=5)
+    parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank, world, local = dist_setup(args.gpus)
+    import torch
+    torch.cuda.set_device(local)
+    import rascaline_b200 as rb
+
+    system, hypers = workload()
+    calc = rb.SoapPowerSpectrum(**hypers)
+    stream = torch.cuda.current_stream()
+    positions = torch.tensor(system["positions"], device="cuda")
+    types = system["types"]
+    cells = system["cell"].reshape(1, 9)
+    sizes = [N_ATOMS]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        tm = calc.compute_device(positions, types, cells, sizes, gradients=GRADIENTS, stream=stream.cuda_stream)
+        return tm
+
+    for _ in range(max(3, args.warmup)):
+        tm = step()
+    torch.cuda.synchronize()
+
+    # output sizes, for the algorithmic byte counts
+    n_props = (6 + 1) * 8 * 8
+    grad_rows = sum(b.gradient("positions").shape[0] for b in tm.blocks())
+    samples = sum(b.shape[0] for b in tm.blocks())
+    del tm
+    n_pairs = len(rb.neighbor_list(system["positions"], system["cell"], 5.5)["first"])
+    K = 49 * 8
+    S = 4
+    out_bytes = 8 * (samples * n_props + grad_rows * 3 * n_props + samples * 9 * n_props)
+    pos_kernel_bytes = 8 * (grad_rows * 3 * n_props + N_ATOMS * S * K + n_pairs * 3 * K + N_ATOMS * S * 3 * K)
+
+    sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
+                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").isdigit() else local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kernel_ms = []
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        tm = step()
+        ends[k].record(stream)
+        kernel_ms.append(calc.timings())
+        del tm
+    torch.cuda.synchronize()
+    barrier(world)
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms_local = float(np.mean(step_ms))
+    ms = allreduce_max(ms_local, world)
+
+    # end to end through the C API with host buffers
+    host_system = rb.System.from_dict(system)
+    for _ in range(2):
+        calc.compute(host_system, gradients=GRADIENTS)
+    e2e_times = []
+    for _ in range(max(3, args.steps // 4)):
+        t0 = time.perf_counter()
+        out = calc.compute(host_system, gradients=GRADIENTS)
+        e2e_times.append(time.perf_counter() - t0)
+        del out
+    e2e_ms = allreduce_max(1000.0 * float(np.mean(e2e_times)), world)
+    clocks = sampler.stop()
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    pos_ms = float(np.mean([t["ps_positions"] for t in kernel_ms]))
+    achieved = pos_kernel_bytes / (pos_ms / 1000.0) / 1e9
+    phases = {name: float(np.mean([t[name] for t in kernel_ms])) for name in kernel_ms[0]}
+    line = {
+        "metric": METRIC,
+        "value": world * N_ATOMS / (ms / 1000.0),
+        "unit": "atom-envs/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded random box, no dataset)",
+        "config": config({"phase_ms": phases, "output_bytes_per_step": out_bytes, "pairs": n_pairs,
+                          "gradient_rows": grad_rows}),
+        "e2e": {
+            "value": world * N_ATOMS / (e2e_ms / 1000.0),
+            "unit": "atom-envs/s",
+            "h2d_bytes_per_step": N_ATOMS * (3 * 8 + 4),
+            "d2h_bytes_per_step": out_bytes + n_pairs * 8,
+        },
+        "roofline": {
+            "kernel": "ps_positions_kernel",
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": pos_kernel_bytes,
+            "traffic": profile_traffic("ps_positions_random_box_1000"),
+        },
+        "clocks": clocks,
+        "gpu_launches": 11 * args.steps,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(system, hypers)
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

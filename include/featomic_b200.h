@@ -1,0 +1,199 @@
+/* featomic-b200: B200-native SOAP spherical expansion / power spectrum behind
+ * featomic's C ABI.
+ *
+ * Every `featomic_*` entry point keeps the name, signature, status codes and
+ * ownership rules of featomic's C API (featomic/include/featomic.h, implemented
+ * in featomic/src/c_api/*.rs); the comment above each one cites the interface
+ * it replaces.  metatensor is not available, so the TensorMap returned by
+ * `featomic_calculator_compute` is this library's own minimal
+ * `mts_tensormap_t`, read through the `mts_*` accessors below (names and
+ * signatures follow metatensor's C API where one exists) and the
+ * `featomic_b200_block_values` accessor.
+ *
+ * Supported calculators: "spherical_expansion", "soap_power_spectrum"
+ * (Gaussian density, GTO radial basis, TensorProduct basis, ShiftedCosine or
+ * Step smoothing, optional Willatt2018 radial scaling).
+ */
+#ifndef FEATOMIC_B200_H
+#define FEATOMIC_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+/* featomic.h status codes */
+#define FEATOMIC_SUCCESS 0
+#define FEATOMIC_INVALID_PARAMETER_ERROR 1
+#define FEATOMIC_JSON_ERROR 2
+#define FEATOMIC_UTF8_ERROR 3
+#define FEATOMIC_SYSTEM_ERROR 128
+#define FEATOMIC_BUFFER_SIZE_ERROR 254
+#define FEATOMIC_INTERNAL_ERROR 255
+
+#define FEATOMIC_LOG_LEVEL_ERROR 1
+#define FEATOMIC_LOG_LEVEL_WARN 2
+#define FEATOMIC_LOG_LEVEL_INFO 3
+#define FEATOMIC_LOG_LEVEL_DEBUG 4
+#define FEATOMIC_LOG_LEVEL_TRACE 5
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t featomic_status_t;
+typedef int32_t mts_status_t;
+typedef struct featomic_calculator_t featomic_calculator_t;
+typedef struct mts_tensormap_t mts_tensormap_t;
+typedef struct mts_block_t mts_block_t;
+typedef void (*featomic_logging_callback_t)(int32_t level, const char* message);
+
+/* metatensor's mts_labels_t layout (metatensor.h): names, row-major int32
+ * values, `size` dimensions and `count` entries.  Labels handed out by this
+ * library are borrowed views into the TensorMap. */
+typedef struct mts_labels_t {
+    const void* internal_ptr_;
+    const char* const* names;
+    const int32_t* values;
+    uintptr_t size;
+    uintptr_t count;
+} mts_labels_t;
+
+/* featomic.h:114-120, same layout as featomic's Rust `Pair` */
+typedef struct featomic_pair_t {
+    uintptr_t first;
+    uintptr_t second;
+    double distance;
+    double vector[3];
+    int32_t cell_shift_indices[3];
+} featomic_pair_t;
+
+/* featomic.h:167-175 */
+typedef struct featomic_system_t {
+    void* user_data;
+    featomic_status_t (*size)(const void* user_data, uintptr_t* size);
+    featomic_status_t (*types)(const void* user_data, const int32_t** types);
+    featomic_status_t (*positions)(const void* user_data, const double** positions);
+    featomic_status_t (*cell)(const void* user_data, double* cell);
+    featomic_status_t (*compute_neighbors)(void* user_data, double cutoff);
+    featomic_status_t (*pairs)(const void* user_data, const featomic_pair_t** pairs, uintptr_t* count);
+    featomic_status_t (*pairs_containing)(const void* user_data, uintptr_t atom, const featomic_pair_t** pairs,
+                                          uintptr_t* count);
+} featomic_system_t;
+
+/* featomic.h:245-251 */
+typedef struct featomic_labels_selection_t {
+    const mts_labels_t* subset;
+    const mts_tensormap_t* predefined;
+} featomic_labels_selection_t;
+
+/* featomic.h:270-277 */
+typedef struct featomic_calculation_options_t {
+    const char* const* gradients;
+    uintptr_t gradients_count;
+    bool use_native_system;
+    featomic_labels_selection_t selected_samples;
+    featomic_labels_selection_t selected_properties;
+    const mts_labels_t* selected_keys;
+} featomic_calculation_options_t;
+
+/* ---- featomic C API -------------------------------------------------------- */
+
+/* featomic/src/c_api/status.rs:110-131 */
+const char* featomic_last_error(void);
+
+/* featomic/src/c_api/logging.rs:51 */
+featomic_status_t featomic_set_logging_callback(featomic_logging_callback_t callback);
+
+/* featomic/src/c_api/calculator.rs:54-84 */
+featomic_calculator_t* featomic_calculator(const char* name, const char* parameters);
+
+/* featomic/src/c_api/calculator.rs:95-105 */
+featomic_status_t featomic_calculator_free(featomic_calculator_t* calculator);
+
+/* featomic/src/c_api/calculator.rs:118-133 */
+featomic_status_t featomic_calculator_name(const featomic_calculator_t* calculator, char* name, uintptr_t bufflen);
+
+/* featomic/src/c_api/calculator.rs:146-161 */
+featomic_status_t featomic_calculator_parameters(const featomic_calculator_t* calculator, char* parameters,
+                                                 uintptr_t bufflen);
+
+/* featomic/src/c_api/calculator.rs:175-190 */
+featomic_status_t featomic_calculator_cutoffs(const featomic_calculator_t* calculator, const double** cutoffs,
+                                              uintptr_t* cutoffs_count);
+
+/* featomic/src/c_api/calculator.rs:392-461.  The returned TensorMap lives in
+ * host memory and is owned by the caller (free with mts_tensormap_free). */
+featomic_status_t featomic_calculator_compute(featomic_calculator_t* calculator, mts_tensormap_t** descriptor,
+                                              featomic_system_t* systems, uintptr_t systems_count,
+                                              featomic_calculation_options_t options);
+
+/* featomic/src/c_api/profiling.rs:17-91 */
+featomic_status_t featomic_profiling_clear(void);
+featomic_status_t featomic_profiling_enable(bool enabled);
+featomic_status_t featomic_profiling_get(const char* format, char* buffer, uintptr_t bufflen);
+
+/* ---- minimal metatensor accessors (metatensor/include/metatensor.h) --------- */
+
+/* mts_tensormap_free */
+mts_status_t mts_tensormap_free(mts_tensormap_t* tensor);
+/* mts_tensormap_keys: borrowed view */
+mts_status_t mts_tensormap_keys(const mts_tensormap_t* tensor, mts_labels_t* keys);
+/* mts_tensormap_block_by_id */
+mts_status_t mts_tensormap_block_by_id(mts_tensormap_t* tensor, mts_block_t** block, uintptr_t index);
+/* mts_block_labels: axis 0 = samples, 1..n = components, n+1 = properties */
+mts_status_t mts_block_labels(const mts_block_t* block, uintptr_t axis, mts_labels_t* labels);
+/* mts_block_gradient: NULL-free lookup, INVALID_PARAMETER if absent */
+mts_status_t mts_block_gradient(mts_block_t* block, const char* parameter, mts_block_t** gradient);
+/* mts_block_gradients_list */
+mts_status_t mts_block_gradients_list(const mts_block_t* block, const char* const** parameters, uintptr_t* count);
+/* mts_labels_free: no-op for the borrowed views handed out here */
+mts_status_t mts_labels_free(mts_labels_t* labels);
+
+/* ---- featomic-b200 extensions (no counterpart in featomic) ------------------- */
+
+/* Data of a block: a contiguous row-major float64 array of `shape`.  When the
+ * TensorMap lives on the GPU (featomic_b200_calculator_compute_device) `data`
+ * is a device pointer and `*on_device` is 1. */
+featomic_status_t featomic_b200_block_values(const mts_block_t* block, double** data, const uintptr_t** shape,
+                                             uintptr_t* shape_count, int32_t* on_device);
+
+/* Systems whose positions are already resident on the current CUDA device:
+ * atoms of all systems concatenated, `positions` a device pointer to
+ * [total atoms][3] float64; `types`, `cells` ([n_systems][9]) and
+ * `system_sizes` stay on the host. */
+typedef struct featomic_b200_device_systems_t {
+    uintptr_t n_systems;
+    const uintptr_t* system_sizes;
+    const int32_t* types;
+    const double* cells;
+    const double* positions;
+} featomic_b200_device_systems_t;
+
+/* Same calculation as featomic_calculator_compute, with device-resident
+ * positions and a TensorMap whose values stay in GPU memory, enqueued on
+ * `stream` (a cudaStream_t, NULL for the legacy default stream). */
+featomic_status_t featomic_b200_calculator_compute_device(featomic_calculator_t* calculator,
+                                                          mts_tensormap_t** descriptor,
+                                                          const featomic_b200_device_systems_t* systems,
+                                                          featomic_calculation_options_t options, void* stream);
+
+/* Half neighbour list of one system computed by the GPU cell list (the list
+ * featomic builds in featomic/src/systems/neighbors.rs:349-403), ordered by
+ * (first, second, cell shift).  `positions` [n_atoms][3] and `cell` [9] are
+ * host arrays.  Writes at most `capacity` pairs and always sets `*count`;
+ * returns FEATOMIC_BUFFER_SIZE_ERROR when `capacity` < `*count`. */
+featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t n_atoms, const double* cell,
+                                              double cutoff, featomic_pair_t* pairs, uintptr_t capacity,
+                                              uintptr_t* count);
+
+/* Per-phase device time (ms) of the last compute call of this calculator:
+ * [neighbours, host metadata, pair features, expansion, contraction,
+ *  device->host transfer, total wall, power-spectrum values kernel,
+ *  power-spectrum positions-gradient kernel, strain / cell kernels] */
+featomic_status_t featomic_b200_calculator_timings(const featomic_calculator_t* calculator, double* times,
+                                                   uintptr_t count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FEATOMIC_B200_H */

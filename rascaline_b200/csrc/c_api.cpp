@@ -1,0 +1,522 @@
+// featomic's C ABI on top of the B200 engine (see include/featomic_b200.h).
+//
+// Errors follow featomic/src/c_api/status.rs: every entry point catches
+// exceptions, stores the message in a thread-local buffer read by
+// featomic_last_error(), and returns the status code of the error kind.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <sstream>
+
+#include "../../include/featomic_b200.h"
+#include "engine.hpp"
+#include "host.hpp"
+
+using namespace fb200;
+
+struct featomic_calculator_t {
+    std::unique_ptr<CalculatorImpl> impl;
+};
+
+struct mts_block_t {
+    Block* block;
+    bool on_device = false;
+    std::vector<std::unique_ptr<mts_block_t>> gradient_handles;
+    std::vector<const char*> gradient_names;
+    // name pointer storage for labels
+    std::vector<std::vector<const char*>> name_ptrs;
+    std::vector<uintptr_t> shape;
+};
+
+struct mts_tensormap_t {
+    std::unique_ptr<TensorMap> tm;
+    std::vector<std::unique_ptr<mts_block_t>> handles;
+    std::vector<const char*> key_names;
+};
+
+namespace {
+
+thread_local std::string LAST_ERROR;
+
+std::mutex LOG_MUTEX;
+featomic_logging_callback_t LOG_CALLBACK = nullptr;
+
+void log_message(int32_t level, const std::string& msg) {
+    std::lock_guard<std::mutex> lock(LOG_MUTEX);
+    if (LOG_CALLBACK) LOG_CALLBACK(level, ("featomic_b200 -- " + msg).c_str());
+}
+
+template <typename F>
+featomic_status_t guarded(F&& f) {
+    try {
+        f();
+        return FEATOMIC_SUCCESS;
+    } catch (Error& e) {
+        LAST_ERROR = e.what();
+        return e.status;
+    } catch (std::bad_alloc&) {
+        LAST_ERROR = "out of memory";
+        return FEATOMIC_INTERNAL_ERROR;
+    } catch (std::exception& e) {
+        LAST_ERROR = std::string("internal error: ") + e.what();
+        return FEATOMIC_INTERNAL_ERROR;
+    } catch (...) {
+        LAST_ERROR = "internal error: unknown exception";
+        return FEATOMIC_INTERNAL_ERROR;
+    }
+}
+
+#define CHECK_POINTER(p)                                                                                   \
+    do {                                                                                                   \
+        if ((p) == nullptr)                                                                                \
+            throw invalid_parameter(std::string("got invalid NULL pointer for ") + #p + " at " + __FILE__ + \
+                                    ":" + std::to_string(__LINE__));                                       \
+    } while (0)
+
+void copy_str(const std::string& s, char* buffer, uintptr_t len) {
+    if (s.size() + 1 > len) {
+        throw Error(FEATOMIC_BUFFER_SIZE_ERROR, "string buffer is not big enough: got space for " + std::to_string(len) +
+                                                    " characters, but we need " + std::to_string(s.size() + 1));
+    }
+    std::memcpy(buffer, s.c_str(), s.size() + 1);
+}
+
+void check_system_status(featomic_status_t status, const char* what) {
+    if (status == FEATOMIC_SUCCESS) return;
+    std::string msg = std::string("error in C system callback `") + what + "`";
+    if (status < 0) throw Error(status, msg);
+    throw Error(FEATOMIC_SYSTEM_ERROR, msg);
+}
+
+struct Profile {
+    std::mutex mutex;
+    bool enabled = false;
+    std::map<std::string, std::pair<double, int64_t>> spans;  // name -> (total ms, calls)
+    void add(const std::string& name, double ms) {
+        if (!enabled) return;
+        auto& s = spans[name];
+        s.first += ms;
+        s.second++;
+    }
+};
+
+Profile& profile() {
+    static Profile p;
+    return p;
+}
+
+void record_profile(const PhaseTimes& t) {
+    Profile& p = profile();
+    std::lock_guard<std::mutex> lock(p.mutex);
+    p.add("Calculator::compute", t.total);
+    p.add("NeighborsList", t.neighbors);
+    p.add("Calculator::prepare", t.metadata);
+    p.add("SphericalExpansion::pair_features", t.features);
+    p.add("SphericalExpansion::compute", t.expansion);
+    p.add("SoapPowerSpectrum::compute", t.contraction);
+    p.add("TensorMap::to_host", t.transfer);
+}
+
+GradientOptions parse_options(const featomic_calculation_options_t& options) {
+    GradientOptions g;
+    if (options.gradients_count > 0) CHECK_POINTER(options.gradients);
+    for (uintptr_t k = 0; k < options.gradients_count; k++) {
+        CHECK_POINTER(options.gradients[k]);
+        std::string p = options.gradients[k];
+        if (p == "positions") g.positions = true;
+        else if (p == "strain") g.strain = true;
+        else if (p == "cell") g.cell = true;
+        else
+            throw invalid_parameter("unexpected gradient \"" + p +
+                                    "\", should be one of \"positions\", \"cell\", or \"strain\"");
+    }
+    if (options.selected_samples.subset || options.selected_samples.predefined || options.selected_properties.subset ||
+        options.selected_properties.predefined || options.selected_keys) {
+        throw invalid_parameter("samples / properties / keys selections are not supported by featomic-b200 yet");
+    }
+    if (g.cell && std::getenv("FEATOMIC_NO_WARN_CELL_GRADIENTS") == nullptr) {
+        log_message(FEATOMIC_LOG_LEVEL_WARN,
+                    "The meaning of \"cell\" gradients has changed recently, you likely want \"strain\" gradients "
+                    "instead. Please review the documentation carefully.");
+    }
+    return g;
+}
+
+mts_tensormap_t* wrap(std::unique_ptr<TensorMap> tm) {
+    auto* out = new mts_tensormap_t;
+    out->tm = std::move(tm);
+    for (auto& n : out->tm->keys.names) out->key_names.push_back(n.c_str());
+    for (auto& b : out->tm->blocks) {
+        auto h = std::make_unique<mts_block_t>();
+        h->block = b.get();
+        h->on_device = out->tm->on_device;
+        for (auto& g : b->gradients) {
+            auto gh = std::make_unique<mts_block_t>();
+            gh->block = g.second.get();
+            gh->on_device = out->tm->on_device;
+            h->gradient_names.push_back(g.first.c_str());
+            h->gradient_handles.push_back(std::move(gh));
+        }
+        out->handles.push_back(std::move(h));
+    }
+    return out;
+}
+
+void fill_labels(const Labels& l, std::vector<const char*>& names, mts_labels_t* out) {
+    names.clear();
+    for (auto& n : l.names) names.push_back(n.c_str());
+    out->internal_ptr_ = nullptr;
+    out->names = names.data();
+    out->values = l.values.data();
+    out->size = l.names.size();
+    out->count = l.count();
+}
+
+void warn_close_pairs(const std::vector<HostSystem>& systems) {
+    for (auto& s : systems)
+        for (auto& p : s.pairs)
+            if (p.distance * p.distance < 1e-3)
+                log_message(FEATOMIC_LOG_LEVEL_WARN, "atoms " + std::to_string(p.first) + " and " + std::to_string(p.second) +
+                                                         " are very close to one another (" + std::to_string(p.distance) + " A)");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* featomic_last_error(void) { return LAST_ERROR.c_str(); }
+
+featomic_status_t featomic_set_logging_callback(featomic_logging_callback_t callback) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lock(LOG_MUTEX);
+        LOG_CALLBACK = callback;
+    });
+}
+
+featomic_calculator_t* featomic_calculator(const char* name, const char* parameters) {
+    featomic_calculator_t* out = nullptr;
+    featomic_status_t status = guarded([&] {
+        CHECK_POINTER(name);
+        CHECK_POINTER(parameters);
+        auto impl = create_calculator(name, parameters);
+        out = new featomic_calculator_t{std::move(impl)};
+    });
+    if (status != FEATOMIC_SUCCESS) return nullptr;
+    return out;
+}
+
+featomic_status_t featomic_calculator_free(featomic_calculator_t* calculator) {
+    return guarded([&] { delete calculator; });
+}
+
+featomic_status_t featomic_calculator_name(const featomic_calculator_t* calculator, char* name, uintptr_t bufflen) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(name);
+        copy_str(calculator->impl->pretty_name, name, bufflen);
+    });
+}
+
+featomic_status_t featomic_calculator_parameters(const featomic_calculator_t* calculator, char* parameters,
+                                                 uintptr_t bufflen) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(parameters);
+        copy_str(calculator->impl->parameters, parameters, bufflen);
+    });
+}
+
+featomic_status_t featomic_calculator_cutoffs(const featomic_calculator_t* calculator, const double** cutoffs,
+                                              uintptr_t* cutoffs_count) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(cutoffs);
+        CHECK_POINTER(cutoffs_count);
+        *cutoffs = calculator->impl->cutoffs.data();
+        *cutoffs_count = calculator->impl->cutoffs.size();
+    });
+}
+
+featomic_status_t featomic_calculator_compute(featomic_calculator_t* calculator, mts_tensormap_t** descriptor,
+                                              featomic_system_t* systems, uintptr_t systems_count,
+                                              featomic_calculation_options_t options) {
+    return guarded([&] {
+        if (systems_count == 0) {
+            log_message(FEATOMIC_LOG_LEVEL_WARN, "0 systems given to featomic_calculator_compute, nothing to do");
+            return;
+        }
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(descriptor);
+        CHECK_POINTER(systems);
+        GradientOptions g = parse_options(options);
+        double cutoff = calculator->impl->hypers.cutoff;
+        std::vector<HostSystem> host(systems_count);
+        for (uintptr_t s = 0; s < systems_count; s++) {
+            featomic_system_t& sys = systems[s];
+            HostSystem& h = host[s];
+            if (!sys.size || !sys.types || !sys.positions || !sys.cell)
+                throw invalid_parameter("system callbacks (size, types, positions, cell) can not be NULL");
+            uintptr_t n = 0;
+            check_system_status(sys.size(sys.user_data, &n), "size");
+            h.n_atoms = (int64_t)n;
+            const int32_t* types = nullptr;
+            const double* positions = nullptr;
+            check_system_status(sys.types(sys.user_data, &types), "types");
+            check_system_status(sys.positions(sys.user_data, &positions), "positions");
+            check_system_status(sys.cell(sys.user_data, h.cell), "cell");
+            if (n > 0 && (!types || !positions)) throw Error(FEATOMIC_SYSTEM_ERROR, "system returned NULL types or positions");
+            h.types.assign(types, types + n);
+            h.positions.assign(positions, positions + 3 * n);
+            for (double x : h.positions)
+                if (!std::isfinite(x)) throw invalid_parameter("atomic positions must be finite");
+            if (!options.use_native_system) {
+                // the caller's own neighbour list (featomic/src/c_api/system.rs:248-320)
+                if (!sys.compute_neighbors || !sys.pairs)
+                    throw invalid_parameter("system callbacks `compute_neighbors` and `pairs` are required when use_native_system is false");
+                check_system_status(sys.compute_neighbors(sys.user_data, cutoff), "compute_neighbors");
+                const featomic_pair_t* pairs = nullptr;
+                uintptr_t count = 0;
+                check_system_status(sys.pairs(sys.user_data, &pairs, &count), "pairs");
+                h.has_pairs = true;
+                h.pairs.resize(count);
+                for (uintptr_t k = 0; k < count; k++) {
+                    h.pairs[k].first = pairs[k].first;
+                    h.pairs[k].second = pairs[k].second;
+                    h.pairs[k].distance = pairs[k].distance;
+                    for (int x = 0; x < 3; x++) {
+                        h.pairs[k].vector[x] = pairs[k].vector[x];
+                        h.pairs[k].shift[x] = pairs[k].cell_shift_indices[x];
+                    }
+                }
+            }
+        }
+        warn_close_pairs(host);
+        auto tm = compute(*calculator->impl, host, g, false, nullptr, nullptr);
+        record_profile(calculator->impl->engine->last_times());
+        *descriptor = wrap(std::move(tm));
+    });
+}
+
+featomic_status_t featomic_b200_calculator_compute_device(featomic_calculator_t* calculator,
+                                                          mts_tensormap_t** descriptor,
+                                                          const featomic_b200_device_systems_t* systems,
+                                                          featomic_calculation_options_t options, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(descriptor);
+        CHECK_POINTER(systems);
+        GradientOptions g = parse_options(options);
+        if (systems->n_systems == 0) {
+            log_message(FEATOMIC_LOG_LEVEL_WARN, "0 systems given to featomic_b200_calculator_compute_device, nothing to do");
+            return;
+        }
+        CHECK_POINTER(systems->system_sizes);
+        CHECK_POINTER(systems->cells);
+        std::vector<HostSystem> host(systems->n_systems);
+        int64_t off = 0;
+        for (uintptr_t s = 0; s < systems->n_systems; s++) {
+            host[s].n_atoms = (int64_t)systems->system_sizes[s];
+            if (host[s].n_atoms > 0) CHECK_POINTER(systems->types);
+            host[s].types.assign(systems->types + off, systems->types + off + host[s].n_atoms);
+            std::memcpy(host[s].cell, systems->cells + 9 * s, 9 * sizeof(double));
+            off += host[s].n_atoms;
+        }
+        if (off > 0) {
+            CHECK_POINTER(systems->positions);
+            cudaPointerAttributes attr;
+            if (cudaPointerGetAttributes(&attr, systems->positions) != cudaSuccess || attr.type != cudaMemoryTypeDevice) {
+                cudaGetLastError();
+                throw invalid_parameter("featomic_b200_calculator_compute_device expects device positions");
+            }
+        }
+        auto tm = compute(*calculator->impl, host, g, true, systems->positions, (cudaStream_t)stream);
+        record_profile(calculator->impl->engine->last_times());
+        *descriptor = wrap(std::move(tm));
+    });
+}
+
+featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t n_atoms, const double* cell,
+                                              double cutoff, featomic_pair_t* pairs, uintptr_t capacity,
+                                              uintptr_t* count) {
+    return guarded([&] {
+        CHECK_POINTER(cell);
+        CHECK_POINTER(count);
+        if (n_atoms > 0) CHECK_POINTER(positions);
+        if (!(cutoff > 0.0 && std::isfinite(cutoff))) throw invalid_parameter("cutoff must be positive and finite");
+        std::vector<Pair> out = neighbor_list(positions, (int64_t)n_atoms, cell, cutoff);
+        *count = out.size();
+        if (capacity < out.size()) {
+            throw Error(FEATOMIC_BUFFER_SIZE_ERROR, "pair buffer is too small: got space for " + std::to_string(capacity) +
+                                                        " pairs, need " + std::to_string(out.size()));
+        }
+        if (!out.empty()) CHECK_POINTER(pairs);
+        for (size_t k = 0; k < out.size(); k++) {
+            pairs[k].first = out[k].first;
+            pairs[k].second = out[k].second;
+            pairs[k].distance = out[k].distance;
+            for (int x = 0; x < 3; x++) {
+                pairs[k].vector[x] = out[k].vector[x];
+                pairs[k].cell_shift_indices[x] = out[k].shift[x];
+            }
+        }
+    });
+}
+
+featomic_status_t featomic_b200_calculator_timings(const featomic_calculator_t* calculator, double* times,
+                                                   uintptr_t count) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(times);
+        const PhaseTimes& t = calculator->impl->engine->last_times();
+        double all[10] = {t.neighbors, t.metadata,  t.features,     t.expansion,    t.contraction,
+                          t.transfer,  t.total,     t.ps_values,    t.ps_positions, t.ps_strain_cell};
+        for (uintptr_t k = 0; k < count && k < 10; k++) times[k] = all[k];
+    });
+}
+
+featomic_status_t featomic_profiling_clear(void) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lock(profile().mutex);
+        profile().spans.clear();
+    });
+}
+
+featomic_status_t featomic_profiling_enable(bool enabled) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lock(profile().mutex);
+        profile().enabled = enabled;
+    });
+}
+
+featomic_status_t featomic_profiling_get(const char* format, char* buffer, uintptr_t bufflen) {
+    return guarded([&] {
+        CHECK_POINTER(format);
+        std::string f = format;
+        std::ostringstream out;
+        std::lock_guard<std::mutex> lock(profile().mutex);
+        if (f == "json") {
+            out << "{";
+            bool first = true;
+            for (auto& kv : profile().spans) {
+                out << (first ? "" : ",") << "\"" << kv.first << "\":{\"total_ms\":" << kv.second.first
+                    << ",\"calls\":" << kv.second.second << "}";
+                first = false;
+            }
+            out << "}";
+        } else if (f == "table" || f == "short_table") {
+            out << "| span | calls | total (ms) | mean (ms) |\n|---|---|---|---|\n";
+            for (auto& kv : profile().spans)
+                out << "| " << kv.first << " | " << kv.second.second << " | " << kv.second.first << " | "
+                    << kv.second.first / (double)std::max<int64_t>(1, kv.second.second) << " |\n";
+        } else {
+            throw invalid_parameter("invalid data format in featomic_profiling_get: " + f +
+                                    ", expected 'table', 'short_table' or 'json'");
+        }
+        copy_str(out.str(), buffer, bufflen);
+    });
+}
+
+// ---- minimal metatensor accessors -------------------------------------------
+
+mts_status_t mts_tensormap_free(mts_tensormap_t* tensor) {
+    return guarded([&] { delete tensor; });
+}
+
+mts_status_t mts_tensormap_keys(const mts_tensormap_t* tensor, mts_labels_t* keys) {
+    return guarded([&] {
+        CHECK_POINTER(tensor);
+        CHECK_POINTER(keys);
+        keys->internal_ptr_ = nullptr;
+        keys->names = tensor->key_names.data();
+        keys->values = tensor->tm->keys.values.data();
+        keys->size = tensor->tm->keys.names.size();
+        keys->count = tensor->tm->keys.count();
+    });
+}
+
+mts_status_t mts_tensormap_block_by_id(mts_tensormap_t* tensor, mts_block_t** block, uintptr_t index) {
+    return guarded([&] {
+        CHECK_POINTER(tensor);
+        CHECK_POINTER(block);
+        if (index >= tensor->handles.size())
+            throw invalid_parameter("block index out of bounds: we have " + std::to_string(tensor->handles.size()) +
+                                    " blocks but the index is " + std::to_string(index));
+        *block = tensor->handles[index].get();
+    });
+}
+
+mts_status_t mts_block_labels(const mts_block_t* block, uintptr_t axis, mts_labels_t* labels) {
+    return guarded([&] {
+        CHECK_POINTER(block);
+        CHECK_POINTER(labels);
+        auto* b = const_cast<mts_block_t*>(block);
+        const Block& blk = *b->block;
+        size_t n_axes = blk.components.size() + 2;
+        if (axis >= n_axes) throw invalid_parameter("axis out of bounds for this block");
+        const Labels* l;
+        if (axis == 0) l = &blk.samples;
+        else if (axis == n_axes - 1) l = &blk.properties;
+        else l = &blk.components[axis - 1];
+        b->name_ptrs.emplace_back();
+        fill_labels(*l, b->name_ptrs.back(), labels);
+    });
+}
+
+mts_status_t mts_block_gradient(mts_block_t* block, const char* parameter, mts_block_t** gradient) {
+    return guarded([&] {
+        CHECK_POINTER(block);
+        CHECK_POINTER(parameter);
+        CHECK_POINTER(gradient);
+        for (size_t k = 0; k < block->gradient_names.size(); k++) {
+            if (std::strcmp(block->gradient_names[k], parameter) == 0) {
+                *gradient = block->gradient_handles[k].get();
+                return;
+            }
+        }
+        throw invalid_parameter(std::string("can not find gradients with respect to '") + parameter + "' in this block");
+    });
+}
+
+mts_status_t mts_block_gradients_list(const mts_block_t* block, const char* const** parameters, uintptr_t* count) {
+    return guarded([&] {
+        CHECK_POINTER(block);
+        CHECK_POINTER(parameters);
+        CHECK_POINTER(count);
+        *parameters = block->gradient_names.data();
+        *count = block->gradient_names.size();
+    });
+}
+
+mts_status_t mts_labels_free(mts_labels_t* labels) {
+    return guarded([&] {
+        if (labels) {
+            labels->names = nullptr;
+            labels->values = nullptr;
+            labels->count = 0;
+            labels->size = 0;
+        }
+    });
+}
+
+featomic_status_t featomic_b200_block_values(const mts_block_t* block, double** data, const uintptr_t** shape,
+                                             uintptr_t* shape_count, int32_t* on_device) {
+    return guarded([&] {
+        CHECK_POINTER(block);
+        CHECK_POINTER(data);
+        CHECK_POINTER(shape);
+        CHECK_POINTER(shape_count);
+        auto* b = const_cast<mts_block_t*>(block);
+        b->shape.assign(b->block->shape.begin(), b->block->shape.end());
+        *data = b->block->data;
+        *shape = b->shape.data();
+        *shape_count = b->shape.size();
+        if (on_device) *on_device = b->on_device ? 1 : 0;
+    });
+}
+
+}  // extern "C"

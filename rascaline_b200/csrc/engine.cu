@@ -1,0 +1,603 @@
+// Compute pipeline of one calculator on the GPU:
+//
+//   positions (H2D, or already resident)
+//     -> kernel (a) neighbour list            [neighbors.cu]
+//     -> D2H of the pair indices, host metadata (keys, samples, gradient
+//        samples, direction segments)         [plan.cpp]
+//     -> kernel (b) pair features + per-centre accumulation  [expansion.cu]
+//     -> kernel (c) power spectrum rows, or the spherical expansion blocks
+//                                            [power_spectrum.cu, expansion.cu]
+//     -> output TensorMap on the device, or D2H into pinned host memory
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "engine.hpp"
+#include "plan.hpp"
+
+namespace fb200 {
+
+// ---------------------------------------------------------------------------
+// DeviceArena
+// ---------------------------------------------------------------------------
+DeviceArena::~DeviceArena() { release(); }
+
+void DeviceArena::release() {
+    for (auto& kv : buffers_)
+        if (kv.second.ptr) cudaFree(kv.second.ptr);
+    buffers_.clear();
+}
+
+void* DeviceArena::alloc_bytes(const std::string& name, size_t bytes) {
+    auto& b = buffers_[name];
+    if (b.bytes >= bytes && b.ptr) return b.ptr;
+    if (b.ptr) {
+        // the previous buffer may still be read by queued work
+        CUDA_CHECK(cudaDeviceSynchronize());
+        CUDA_CHECK(cudaFree(b.ptr));
+        b.ptr = nullptr;
+    }
+    size_t grow = std::max(bytes, b.bytes + b.bytes / 4);
+    grow = (grow + 255) / 256 * 256;
+    CUDA_CHECK(cudaMalloc(&b.ptr, grow));
+    b.bytes = grow;
+    return b.ptr;
+}
+
+size_t DeviceArena::bytes_reserved() const {
+    size_t s = 0;
+    for (auto& kv : buffers_) s += kv.second.bytes;
+    return s;
+}
+
+void DeviceArena::exclusive_scan(const int32_t* in, int32_t* out, int64_t n, cudaStream_t stream) {
+    size_t temp = 0;
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, temp, in, out, (int)n, stream));
+    void* t = alloc_bytes("scan.temp", temp);
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(t, temp, in, out, (int)n, stream));
+}
+
+void DeviceArena::exclusive_scan(const int64_t* in, int64_t* out, int64_t n, cudaStream_t stream) {
+    size_t temp = 0;
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, temp, in, out, (int)n, stream));
+    void* t = alloc_bytes("scan.temp", temp);
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(t, temp, in, out, (int)n, stream));
+}
+
+// ---------------------------------------------------------------------------
+// Cell-list parameters (neighbors.rs:101-163, cell.rs:34-66 and :154-169,
+// matrix.rs:210-247).  This translation unit is compiled with
+// -ffp-contract=off so that the host arithmetic keeps the reference order.
+// ---------------------------------------------------------------------------
+namespace {
+
+double det3(const double* m) {
+    return m[0] * (m[4] * m[8] - m[7] * m[5]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+void cross3(const double* a, const double* b, double* r) {
+    r[0] = a[1] * b[2] - a[2] * b[1];
+    r[1] = a[2] * b[0] - a[0] * b[2];
+    r[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+}  // namespace
+
+NlSystem make_nl_system(const double* cell, double cutoff, int64_t atom_offset, int64_t n_atoms, int64_t cell_offset) {
+    NlSystem s;
+    std::memset(&s, 0, sizeof(s));
+    s.atom_offset = atom_offset;
+    s.cell_offset = cell_offset;
+    s.n_atoms = (int32_t)n_atoms;
+    s.cutoff2 = cutoff * cutoff;
+    bool zero = true;
+    for (int k = 0; k < 9; k++) {
+        s.H[k] = cell[k];
+        if (cell[k] != 0.0) zero = false;
+    }
+    s.infinite = zero ? 1 : 0;
+    double dbf[3] = {1.0, 1.0, 1.0};
+    if (!zero) {
+        double det = det3(cell);
+        if (!(std::fabs(det) > 1e-6)) throw invalid_parameter("the unit cell matrix is not invertible");
+        double id = 1.0 / det;
+        const double* m = cell;
+        s.inv[0] = (m[4] * m[8] - m[7] * m[5]) * id;
+        s.inv[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+        s.inv[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+        s.inv[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+        s.inv[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+        s.inv[5] = (m[3] * m[2] - m[0] * m[5]) * id;
+        s.inv[6] = (m[3] * m[7] - m[6] * m[4]) * id;
+        s.inv[7] = (m[6] * m[1] - m[0] * m[7]) * id;
+        s.inv[8] = (m[0] * m[4] - m[3] * m[1]) * id;
+        const double* a = &cell[0];
+        const double* b = &cell[3];
+        const double* c = &cell[6];
+        double na[3], nb[3], nc[3];
+        cross3(b, c, na);
+        cross3(c, a, nb);
+        cross3(a, b, nc);
+        double la = std::sqrt(dot3(na, na)), lb = std::sqrt(dot3(nb, nb)), lc = std::sqrt(dot3(nc, nc));
+        for (int k = 0; k < 3; k++) {
+            na[k] = na[k] / la;
+            nb[k] = nb[k] / lb;
+            nc[k] = nc[k] / lc;
+        }
+        dbf[0] = std::fabs(dot3(na, a));
+        dbf[1] = std::fabs(dot3(nb, b));
+        dbf[2] = std::fabs(dot3(nc, c));
+    }
+    double nf[3];
+    for (int k = 0; k < 3; k++) {
+        double v = std::trunc(dbf[k] / cutoff);
+        nf[k] = v < 1.0 ? 1.0 : v;
+    }
+    double total = nf[0] * nf[1] * nf[2];
+    if (total > 1e5) {
+        double rxy = nf[0] / nf[1];
+        double ryz = nf[1] / nf[2];
+        nf[2] = std::trunc(std::cbrt(1e5 / (rxy * ryz * ryz)));
+        nf[1] = std::trunc(ryz * nf[2]);
+        nf[0] = std::trunc(rxy * nf[1]);
+    }
+    for (int k = 0; k < 3; k++) {
+        s.n_search[k] = (int32_t)std::ceil(cutoff * nf[k] / dbf[k]);
+        s.n_cells[k] = (int32_t)nf[k];
+        if (s.n_search[k] < 1) s.n_search[k] = 1;
+        if (s.n_cells[k] == 1 && s.infinite) s.n_search[k] = 0;
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// pinned host memory for outputs, recycled across calls
+// ---------------------------------------------------------------------------
+namespace {
+
+struct PinnedPool {
+    std::mutex mutex;
+    std::vector<std::pair<void*, size_t>> free_list;
+    size_t cached = 0;
+
+    void* get(size_t bytes) {
+        {
+            std::lock_guard<std::mutex> lock(mutex);
+            size_t best = (size_t)-1;
+            for (size_t k = 0; k < free_list.size(); k++)
+                if (free_list[k].second >= bytes && (best == (size_t)-1 || free_list[k].second < free_list[best].second)) best = k;
+            if (best != (size_t)-1) {
+                void* p = free_list[best].first;
+                cached -= free_list[best].second;
+                free_list.erase(free_list.begin() + best);
+                return p;
+            }
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            p = std::malloc(bytes);
+            if (!p) throw internal_error("out of host memory");
+            return p;  // plain memory, freed with free()
+        }
+        return p;
+    }
+
+    void put(void* p, size_t bytes, bool pinned) {
+        if (!pinned) {
+            std::free(p);
+            return;
+        }
+        std::lock_guard<std::mutex> lock(mutex);
+        free_list.emplace_back(p, bytes);
+        cached += bytes;
+        // keep at most 4 buffers
+        while (free_list.size() > 4) {
+            cudaFreeHost(free_list.front().first);
+            cached -= free_list.front().second;
+            free_list.erase(free_list.begin());
+        }
+    }
+};
+
+PinnedPool& pinned_pool() {
+    static PinnedPool* pool = new PinnedPool();  // never destroyed: buffers may outlive static destruction
+    return *pool;
+}
+
+bool is_pinned(void* p) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeHost;
+}
+
+template <typename T>
+T* upload(DeviceArena& arena, const std::string& name, const std::vector<T>& host, cudaStream_t stream) {
+    T* d = arena.alloc<T>(name, (int64_t)host.size());
+    if (!host.empty()) CUDA_CHECK(cudaMemcpyAsync(d, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice, stream));
+    return d;
+}
+
+double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    return (double)ms;
+}
+
+Labels xyz_labels(const char* name) {
+    Labels l;
+    l.names = {name};
+    l.values = {0, 1, 2};
+    return l;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+Engine::Engine(const Hypers& h) : h_(h) {
+    radial_ = build_radial_tables(h);
+    ylm_ = build_ylm_tables(h.max_angular);
+}
+
+Engine::~Engine() {
+    for (void* p : table_buffers_) cudaFree(p);
+}
+
+void Engine::upload_tables() {
+    int dev = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    if (tables_ready_ && dev == device_) return;
+    if (tables_ready_) throw invalid_parameter("a calculator can only be used on the device it first ran on");
+    device_ = dev;
+    auto put = [&](const void* src, size_t bytes) -> void* {
+        void* d = nullptr;
+        CUDA_CHECK(cudaMalloc(&d, bytes > 0 ? bytes : 8));
+        if (bytes) CUDA_CHECK(cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice));
+        table_buffers_.push_back(d);
+        return d;
+    };
+    auto putv = [&](const std::vector<double>& v) { return (const double*)put(v.data(), v.size() * sizeof(double)); };
+    d_radial_.lmax = radial_.lmax;
+    d_radial_.nmax = radial_.nmax;
+    d_radial_.splined = radial_.splined ? 1 : 0;
+    d_radial_.knot_offset = (const int32_t*)put(radial_.knot_offset.data(), radial_.knot_offset.size() * 4);
+    d_radial_.knot_count = (const int32_t*)put(radial_.knot_count.data(), radial_.knot_count.size() * 4);
+    d_radial_.positions = putv(radial_.positions);
+    d_radial_.values = putv(radial_.values);
+    d_radial_.derivs = putv(radial_.derivs);
+    d_radial_.c = radial_.c;
+    d_radial_.width2 = radial_.width2;
+    d_radial_.bn = putv(radial_.bn);
+    d_radial_.ortho = putv(radial_.ortho);
+    d_ylm_.lmax = ylm_.lmax;
+    d_ylm_.A = putv(ylm_.A);
+    d_ylm_.B = putv(ylm_.B);
+    d_ylm_.sq_plus = putv(ylm_.sq_plus);
+    d_ylm_.sq_minus = putv(ylm_.sq_minus);
+    d_ylm_.sq_2l1 = putv(ylm_.sq_2l1);
+    d_ylm_.sq_half = putv(ylm_.sq_half);
+    d_ylm_.sq_ll1 = putv(ylm_.sq_ll1);
+    d_ylm_.inv_ll = putv(ylm_.inv_ll);
+    d_self_ = (double*)putv(radial_.self_contribution);
+    tables_ready_ = true;
+}
+
+std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& systems, const GradientOptions& g,
+                                           bool device_output, const double* d_positions_in, cudaStream_t stream) {
+    auto t_start = std::chrono::steady_clock::now();
+    upload_tables();
+    cudaEvent_t ev[12];
+    for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
+    struct EventGuard {
+        cudaEvent_t* e;
+        ~EventGuard() {
+            for (int k = 0; k < 12; k++) cudaEventDestroy(e[k]);
+        }
+    } guard{ev};
+    CUDA_CHECK(cudaEventRecord(ev[0], stream));
+
+    // ---- gather atoms -------------------------------------------------------
+    int64_t n_atoms = 0;
+    bool user_pairs = false, native_pairs = false;
+    for (auto& s : systems) {
+        n_atoms += s.n_atoms;
+        if (s.has_pairs) user_pairs = true;
+        else native_pairs = true;
+    }
+    if (user_pairs && native_pairs) throw internal_error("mixing systems with and without neighbour lists");
+    if (n_atoms >= (int64_t)INT32_MAX / 2) throw invalid_parameter("too many atoms");
+    std::vector<int32_t> atom_system;
+    atom_system.reserve(n_atoms);
+    for (size_t s = 0; s < systems.size(); s++)
+        for (int64_t i = 0; i < systems[s].n_atoms; i++) atom_system.push_back((int32_t)s);
+
+    const double* d_positions = d_positions_in;
+    if (!d_positions && !user_pairs) {
+        double* d = arena_.alloc<double>("positions", 3 * n_atoms);
+        int64_t off = 0;
+        for (auto& s : systems) {
+            if (s.n_atoms)
+                CUDA_CHECK(cudaMemcpyAsync(d + 3 * off, s.positions.data(), sizeof(double) * 3 * s.n_atoms,
+                                           cudaMemcpyHostToDevice, stream));
+            off += s.n_atoms;
+        }
+        d_positions = d;
+    }
+
+    // ---- kernel (a): neighbour list ------------------------------------------
+    DevicePairs pairs;
+    if (!user_pairs) {
+        std::vector<NlSystem> nls;
+        int64_t atom_off = 0, cell_off = 0;
+        for (auto& s : systems) {
+            NlSystem n = make_nl_system(s.cell, h_.cutoff, atom_off, s.n_atoms, cell_off);
+            cell_off += (int64_t)n.n_cells[0] * n.n_cells[1] * n.n_cells[2];
+            atom_off += s.n_atoms;
+            nls.push_back(n);
+        }
+        nl_.build(nls, atom_system, d_positions, n_atoms, arena_, stream);
+        pairs = nl_.pairs;
+    } else {
+        // neighbour list given by the caller's systems
+        std::vector<int32_t> f, sd, sh;
+        std::vector<double> dist, vec;
+        int64_t off = 0;
+        for (auto& s : systems) {
+            for (auto& p : s.pairs) {
+                if ((int64_t)p.first >= s.n_atoms || (int64_t)p.second >= s.n_atoms)
+                    throw Error(STATUS_SYSTEM_ERROR, "pair index out of bounds in the system's neighbour list");
+                f.push_back((int32_t)(p.first + off));
+                sd.push_back((int32_t)(p.second + off));
+                dist.push_back(p.distance);
+                vec.insert(vec.end(), p.vector, p.vector + 3);
+                sh.insert(sh.end(), p.shift, p.shift + 3);
+            }
+            off += s.n_atoms;
+        }
+        pairs.count = (int64_t)f.size();
+        pairs.first = upload(arena_, "pairs.first", f, stream);
+        pairs.second = upload(arena_, "pairs.second", sd, stream);
+        pairs.distance = upload(arena_, "pairs.distance", dist, stream);
+        pairs.vector = upload(arena_, "pairs.vector", vec, stream);
+        pairs.shift = upload(arena_, "pairs.shift", sh, stream);
+    }
+    CUDA_CHECK(cudaEventRecord(ev[1], stream));
+
+    // ---- pair indices to the host, then the per-pair features run on the GPU
+    // while the host builds the metadata ----------------------------------------
+    std::vector<int32_t> h_first(pairs.count), h_second(pairs.count);
+    if (pairs.count) {
+        CUDA_CHECK(cudaMemcpyAsync(h_first.data(), pairs.first, sizeof(int32_t) * pairs.count, cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaMemcpyAsync(h_second.data(), pairs.second, sizeof(int32_t) * pairs.count, cudaMemcpyDeviceToHost, stream));
+    }
+    CUDA_CHECK(cudaEventRecord(ev[6], stream));
+
+    FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), g.any());
+    double* features = arena_.alloc<double>("features", pairs.count * layout.stride);
+    int32_t* status = arena_.alloc<int32_t>("status", 1);
+    CUDA_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t), stream));
+    CutoffParams cut{h_.cutoff, h_.smoothing_width, h_.smoothing, h_.scaling ? 1 : 0,
+                     h_.scaling_scale, h_.scaling_rate, h_.scaling_exponent};
+    launch_pair_features(pairs, d_radial_, d_ylm_, cut, layout, features, status, stream);
+    CUDA_CHECK(cudaEventRecord(ev[2], stream));
+
+    CUDA_CHECK(cudaEventSynchronize(ev[6]));
+    auto t_meta0 = std::chrono::steady_clock::now();
+    Neighborhoods nh = build_neighborhoods(systems, pairs.count, h_first.data(), h_second.data());
+    OutputPlan plan = ps ? plan_power_spectrum(nh, h_, g) : plan_spherical_expansion(nh, h_, g);
+    auto t_meta1 = std::chrono::steady_clock::now();
+    const int S = nh.n_species;
+
+    auto tm = std::make_unique<TensorMap>();
+    tm->keys = plan.keys;
+    tm->on_device = device_output;
+    tm->device = device_;
+
+    int64_t total = plan.total_doubles;
+    double* d_out = nullptr;
+    if (device_output) {
+        void* p = nullptr;
+        CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(8, sizeof(double) * (size_t)total)));
+        tm->storage = std::shared_ptr<void>(p, [](void* q) { cudaFree(q); });
+        d_out = (double*)p;
+    } else {
+        d_out = arena_.alloc<double>("output", total);
+    }
+
+    if (nh.n_atoms > 0 && !plan.blocks.empty()) {
+        // ---- kernel (b): spherical expansion --------------------------------
+        int K = layout.L2 * layout.nmax;
+        SeArgs se{};
+        se.layout = layout;
+        se.n_centres = nh.n_atoms;
+        se.n_species = S;
+        se.centre_species = upload(arena_, "meta.atom_species", nh.atom_species, stream);
+        se.seg_offset = upload(arena_, "meta.seg_offset", nh.seg_offset, stream);
+        se.dir_code = upload(arena_, "meta.dir_code", nh.dir_code, stream);
+        se.features = features;
+        se.self_contribution = d_self_;
+        se.do_positions = g.positions;
+        se.do_strain = g.strain;
+        se.do_cell = g.cell;
+        se.coef = arena_.alloc<double>("se.coef", nh.n_atoms * S * K);
+        se.pair_grad = g.positions ? arena_.alloc<double>("se.pair_grad", pairs.count * 3 * K) : nullptr;
+        se.self_grad = g.positions ? arena_.alloc<double>("se.self_grad", nh.n_atoms * S * 3 * K) : nullptr;
+        se.strain = g.strain ? arena_.alloc<double>("se.strain", nh.n_atoms * S * 9 * K) : nullptr;
+        se.cellg = g.cell ? arena_.alloc<double>("se.cell", nh.n_atoms * S * 9 * K) : nullptr;
+        CUDA_CHECK(cudaEventRecord(ev[7], stream));
+        launch_se_accumulate(se, stream);
+        CUDA_CHECK(cudaEventRecord(ev[3], stream));
+
+        std::vector<int64_t> offv, offp, offs, offc;
+        for (auto& b : plan.blocks) {
+            offv.push_back(b.off_values);
+            offp.push_back(b.off_positions);
+            offs.push_back(b.off_strain);
+            offc.push_back(b.off_cell);
+        }
+        if (ps) {
+            // ---- kernel (c): power spectrum ------------------------------------
+            PsArgs pa{};
+            pa.lmax = h_.max_angular;
+            pa.nmax = h_.nmax();
+            pa.n_species = S;
+            pa.n_centres = nh.n_atoms;
+            pa.n_props = (int64_t)(h_.max_angular + 1) * h_.nmax() * h_.nmax();
+            pa.coef = se.coef;
+            pa.pair_grad = se.pair_grad;
+            pa.self_grad = se.self_grad;
+            pa.strain = se.strain;
+            pa.cellg = se.cellg;
+            pa.dir_code = se.dir_code;
+            pa.slot_offset = upload(arena_, "ps.slot_offset", plan.slot_offset, stream);
+            pa.slots = upload(arena_, "ps.slots", plan.slots, stream);
+            pa.entry_offset = upload(arena_, "ps.entry_offset", nh.entry_offset, stream);
+            pa.entries = upload(arena_, "ps.entries", nh.entries, stream);
+            pa.row_offset = upload(arena_, "ps.row_offset", plan.row_offset, stream);
+            pa.rows = upload(arena_, "ps.rows", plan.rows, stream);
+            pa.off_values = upload(arena_, "ps.offv", offv, stream);
+            pa.off_positions = upload(arena_, "ps.offp", offp, stream);
+            pa.off_strain = upload(arena_, "ps.offs", offs, stream);
+            pa.off_cell = upload(arena_, "ps.offc", offc, stream);
+            pa.out = d_out;
+            launch_ps_values(pa, stream);
+            CUDA_CHECK(cudaEventRecord(ev[8], stream));
+            if (g.positions) launch_ps_positions(pa, stream);
+            CUDA_CHECK(cudaEventRecord(ev[9], stream));
+            if (g.strain || g.cell) launch_ps_strain_cell(pa, g.strain, g.cell, stream);
+        } else {
+            SeOutArgs so{};
+            so.lmax = h_.max_angular;
+            so.nmax = h_.nmax();
+            so.n_species = S;
+            so.coef = se.coef;
+            so.pair_grad = se.pair_grad;
+            so.self_grad = se.self_grad;
+            so.strain = se.strain;
+            so.cellg = se.cellg;
+            so.dir_code = se.dir_code;
+            so.n_rows = (int64_t)plan.row_centre.size();
+            so.row_centre = upload(arena_, "so.row_centre", plan.row_centre, stream);
+            so.row_block = upload(arena_, "so.row_block", plan.row_block, stream);
+            so.row_sample = upload(arena_, "so.row_sample", plan.row_sample, stream);
+            so.n_grad_rows = (int64_t)plan.grad_block.size();
+            so.grad_block = upload(arena_, "so.grad_block", plan.grad_block, stream);
+            so.grad_row = upload(arena_, "so.grad_row", plan.grad_row, stream);
+            so.grad_centre = upload(arena_, "so.grad_centre", plan.grad_centre, stream);
+            so.grad_atom = upload(arena_, "so.grad_atom", plan.grad_atom, stream);
+            so.grad_d0 = upload(arena_, "so.grad_d0", plan.grad_d0, stream);
+            so.grad_d1 = upload(arena_, "so.grad_d1", plan.grad_d1, stream);
+            so.block_l = upload(arena_, "so.block_l", plan.block_l, stream);
+            so.block_species = upload(arena_, "so.block_species", plan.block_species, stream);
+            so.off_values = upload(arena_, "so.offv", offv, stream);
+            so.off_positions = upload(arena_, "so.offp", offp, stream);
+            so.off_strain = upload(arena_, "so.offs", offs, stream);
+            so.off_cell = upload(arena_, "so.offc", offc, stream);
+            so.out = d_out;
+            CUDA_CHECK(cudaEventRecord(ev[8], stream));
+            CUDA_CHECK(cudaEventRecord(ev[9], stream));
+            launch_se_output(so, g.positions, g.strain, g.cell, stream);
+        }
+        CUDA_CHECK(cudaEventRecord(ev[4], stream));
+        int32_t h_status = 0;
+        CUDA_CHECK(cudaMemcpyAsync(&h_status, status, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        if (h_status != 0) {
+            throw internal_error("Failed to compute radial integral with GTO basis. Try increasing decreasing the "
+                                 "`cutoff`, or increasing the Gaussian's `width`.");
+        }
+    } else {
+        for (int k : {7, 3, 8, 9, 4}) CUDA_CHECK(cudaEventRecord(ev[k], stream));
+    }
+
+    // ---- output TensorMap ------------------------------------------------------
+    double* base = d_out;
+    if (!device_output) {
+        size_t bytes = std::max<size_t>(8, sizeof(double) * (size_t)total);
+        void* host = pinned_pool().get(bytes);
+        bool pinned = is_pinned(host);
+        tm->storage = std::shared_ptr<void>(host, [bytes, pinned](void* q) { pinned_pool().put(q, bytes, pinned); });
+        if (total) CUDA_CHECK(cudaMemcpyAsync(host, d_out, sizeof(double) * total, cudaMemcpyDeviceToHost, stream));
+        base = (double*)host;
+    }
+    CUDA_CHECK(cudaEventRecord(ev[5], stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+
+    std::vector<Labels> components_base;
+    Labels properties = ps ? ps_properties(h_) : se_properties(h_);
+    for (size_t b = 0; b < plan.blocks.size(); b++) {
+        auto& bp = plan.blocks[b];
+        auto blk = std::make_unique<Block>();
+        blk->samples = bp.samples;
+        blk->properties = properties;
+        std::vector<Labels> comps;
+        std::vector<size_t> comp_shape;
+        if (!ps) {
+            Labels mu;
+            mu.names = {"o3_mu"};
+            for (int m = -bp.l; m <= bp.l; m++) mu.values.push_back(m);
+            comps.push_back(mu);
+            comp_shape.push_back(2 * bp.l + 1);
+        }
+        blk->components = comps;
+        blk->shape = {(size_t)bp.n_samples};
+        blk->shape.insert(blk->shape.end(), comp_shape.begin(), comp_shape.end());
+        blk->shape.push_back(properties.count());
+        blk->data = base + bp.off_values;
+        if (g.positions) {
+            auto gb = std::make_unique<Block>();
+            gb->samples = bp.gradient_samples;
+            gb->components = {xyz_labels("xyz")};
+            gb->components.insert(gb->components.end(), comps.begin(), comps.end());
+            gb->properties = properties;
+            gb->shape = {(size_t)bp.n_grad_rows, 3};
+            gb->shape.insert(gb->shape.end(), comp_shape.begin(), comp_shape.end());
+            gb->shape.push_back(properties.count());
+            gb->data = base + bp.off_positions;
+            blk->gradients.emplace_back("positions", std::move(gb));
+        }
+        // calculator.rs:448-490: cell components [xyz, abc, ...], strain [xyz_2, xyz_1, ...]
+        for (int which = 0; which < 2; which++) {
+            bool want = which == 0 ? g.cell : g.strain;
+            if (!want) continue;
+            auto gb = std::make_unique<Block>();
+            gb->samples.names = {"sample"};
+            for (int64_t s = 0; s < bp.n_samples; s++) gb->samples.values.push_back((int32_t)s);
+            if (which == 0) gb->components = {xyz_labels("xyz"), xyz_labels("abc")};
+            else gb->components = {xyz_labels("xyz_2"), xyz_labels("xyz_1")};
+            gb->components.insert(gb->components.end(), comps.begin(), comps.end());
+            gb->properties = properties;
+            gb->shape = {(size_t)bp.n_samples, 3, 3};
+            gb->shape.insert(gb->shape.end(), comp_shape.begin(), comp_shape.end());
+            gb->shape.push_back(properties.count());
+            gb->data = base + (which == 0 ? bp.off_cell : bp.off_strain);
+            blk->gradients.emplace_back(which == 0 ? "cell" : "strain", std::move(gb));
+        }
+        tm->blocks.push_back(std::move(blk));
+    }
+
+    times_.neighbors = elapsed_ms(ev[0], ev[1]);
+    times_.metadata = std::chrono::duration<double, std::milli>(t_meta1 - t_meta0).count();
+    times_.features = elapsed_ms(ev[6], ev[2]);
+    times_.expansion = elapsed_ms(ev[7], ev[3]);
+    times_.contraction = elapsed_ms(ev[3], ev[4]);
+    times_.ps_values = elapsed_ms(ev[3], ev[8]);
+    times_.ps_positions = elapsed_ms(ev[8], ev[9]);
+    times_.ps_strain_cell = elapsed_ms(ev[9], ev[4]);
+    times_.transfer = elapsed_ms(ev[4], ev[5]);
+    times_.total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    return tm;
+}
+
+}  // namespace fb200

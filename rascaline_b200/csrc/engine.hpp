@@ -1,0 +1,269 @@
+// Device-side data structures and launchers of the B200 SOAP engine.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "host.hpp"
+
+#define CUDA_CHECK(expr)                                                                         \
+    do {                                                                                         \
+        cudaError_t err__ = (expr);                                                              \
+        if (err__ != cudaSuccess) {                                                              \
+            throw ::fb200::internal_error(std::string("CUDA error: ") + cudaGetErrorString(err__) + \
+                                          " at " + __FILE__ + ":" + std::to_string(__LINE__));   \
+        }                                                                                        \
+    } while (0)
+
+namespace fb200 {
+
+// Named, growing device buffers reused across calls of one calculator.
+class DeviceArena {
+  public:
+    DeviceArena() = default;
+    DeviceArena(const DeviceArena&) = delete;
+    ~DeviceArena();
+
+    void* alloc_bytes(const std::string& name, size_t bytes);
+    template <typename T>
+    T* alloc(const std::string& name, int64_t count) {
+        return static_cast<T*>(alloc_bytes(name, sizeof(T) * (size_t)(count > 0 ? count : 1)));
+    }
+    // out[i] = sum_{k<i} in[k]
+    void exclusive_scan(const int32_t* in, int32_t* out, int64_t n, cudaStream_t stream);
+    void exclusive_scan(const int64_t* in, int64_t* out, int64_t n, cudaStream_t stream);
+    size_t bytes_reserved() const;
+    void release();
+
+  private:
+    struct Buffer {
+        void* ptr = nullptr;
+        size_t bytes = 0;
+    };
+    std::map<std::string, Buffer> buffers_;
+};
+
+// Cell-list parameters of one system
+struct NlSystem {
+    int64_t atom_offset;
+    int64_t cell_offset;
+    int32_t n_atoms;
+    int32_t infinite;
+    int32_t n_cells[3];
+    int32_t n_search[3];
+    double cutoff2;
+    double H[9];
+    double inv[9];
+};
+
+NlSystem make_nl_system(const double* cell, double cutoff, int64_t atom_offset, int64_t n_atoms, int64_t cell_offset);
+
+// Half neighbour list on the device (global atom indices), structure of arrays
+struct DevicePairs {
+    int32_t* first = nullptr;
+    int32_t* second = nullptr;
+    double* distance = nullptr;
+    double* vector = nullptr;  // [count][3]
+    int32_t* shift = nullptr;  // [count][3]
+    int64_t count = 0;
+};
+
+class NeighborBuilder {
+  public:
+    DevicePairs pairs;
+    int64_t build(const std::vector<NlSystem>& systems, const std::vector<int32_t>& atom_system,
+                  const double* d_positions, int64_t n_atoms, DeviceArena& arena, cudaStream_t stream);
+};
+
+// ---------------------------------------------------------------------------
+// Spherical expansion (kernel b)
+// ---------------------------------------------------------------------------
+struct DeviceRadial {
+    int lmax, nmax;
+    int splined;
+    const int32_t* knot_offset;
+    const int32_t* knot_count;
+    const double* positions;
+    const double* values;
+    const double* derivs;
+    double c, width2;
+    const double* bn;
+    const double* ortho;
+};
+
+struct DeviceYlm {
+    int lmax;
+    const double *A, *B, *sq_plus, *sq_minus, *sq_2l1, *sq_half, *sq_ll1, *inv_ll;
+};
+
+struct CutoffParams {
+    double rc, width;
+    int smoothing;
+    int scaling;
+    double scale, rate, exponent;
+};
+
+// layout of the per-pair feature record (doubles)
+struct FeatureLayout {
+    int lmax, nmax, L2, with_grad;
+    int off_y, off_dy, off_r, off_dr, stride;
+    static FeatureLayout make(int lmax, int nmax, bool grad) {
+        FeatureLayout f;
+        f.lmax = lmax;
+        f.nmax = nmax;
+        f.L2 = (lmax + 1) * (lmax + 1);
+        f.with_grad = grad ? 1 : 0;
+        f.off_y = 16;
+        f.off_dy = f.off_y + f.L2;
+        f.off_r = f.off_dy + (grad ? 3 * f.L2 : 0);
+        f.off_dr = f.off_r + (lmax + 1) * nmax;
+        int end = f.off_dr + (grad ? (lmax + 1) * nmax : 0);
+        f.stride = (end + 3) / 4 * 4;
+        return f;
+    }
+};
+
+struct SeArgs {
+    FeatureLayout layout;
+    int64_t n_centres;
+    int n_species;
+    const int32_t* centre_species;  // [n_centres]
+    const int64_t* seg_offset;      // [n_centres * S + 1]
+    const int32_t* dir_code;        // (pair << 1) | inverse
+    const double* features;         // [pairs][stride]
+    const double* self_contribution;
+    int do_positions, do_strain, do_cell;
+    // outputs
+    double* coef;       // [c][S][L2][nmax]
+    double* pair_grad;  // [pair][3][L2][nmax]
+    double* self_grad;  // [c][S][3][L2][nmax]
+    double* strain;     // [c][S][3][3][L2][nmax]
+    double* cellg;      // [c][S][3][3][L2][nmax]
+};
+
+void launch_pair_features(const DevicePairs& pairs, const DeviceRadial& radial, const DeviceYlm& ylm,
+                          const CutoffParams& cut, const FeatureLayout& layout, double* features, int32_t* status,
+                          cudaStream_t stream);
+void launch_se_accumulate(const SeArgs& args, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
+// Power spectrum (kernel c)
+// ---------------------------------------------------------------------------
+struct PsKeySlot {
+    int32_t block;
+    int32_t sample;
+    int32_t a;  // species index of neighbor_1_type
+    int32_t b;  // species index of neighbor_2_type
+};
+
+struct PsEntry {
+    int32_t atom;     // global atom index of the neighbour (or the centre)
+    int32_t species;
+    int32_t d0, d1;   // direction range in the (centre, species) segment
+};
+
+struct PsArgs {
+    int lmax, nmax, n_species;
+    int64_t n_centres;
+    int64_t n_props;
+    const double* coef;
+    const double* pair_grad;
+    const double* self_grad;
+    const double* strain;
+    const double* cellg;
+    const int32_t* dir_code;
+    const int64_t* slot_offset;     // [n_centres + 1]
+    const PsKeySlot* slots;
+    const int64_t* entry_offset;    // [n_centres + 1]
+    const PsEntry* entries;
+    const int64_t* row_offset;      // [n_centres + 1], into rows: entries x slots
+    const int64_t* rows;            // gradient row in the block, or -1
+    const int64_t* off_values;      // per block, offsets into `out` (doubles)
+    const int64_t* off_positions;
+    const int64_t* off_strain;
+    const int64_t* off_cell;
+    double* out;
+};
+
+void launch_ps_values(const PsArgs& args, cudaStream_t stream);
+void launch_ps_positions(const PsArgs& args, cudaStream_t stream);
+void launch_ps_strain_cell(const PsArgs& args, bool strain, bool cell, cudaStream_t stream);
+
+// Spherical expansion output scatter (spherical_expansion calculator)
+struct SeOutArgs {
+    int lmax, nmax, n_species;
+    const double* coef;
+    const double* pair_grad;
+    const double* self_grad;
+    const double* strain;
+    const double* cellg;
+    const int32_t* dir_code;
+    // one entry per (block, sample)
+    int64_t n_rows;
+    const int32_t* row_centre;   // global centre
+    const int32_t* row_block;    // block index
+    const int32_t* row_sample;   // sample index in the block
+    // one entry per gradient row
+    int64_t n_grad_rows;
+    const int32_t* grad_block;
+    const int64_t* grad_row;     // row index in the block
+    const int32_t* grad_centre;
+    const int32_t* grad_atom;    // neighbour (== centre for self rows)
+    const int32_t* grad_d0;      // direction range
+    const int32_t* grad_d1;
+    const int32_t* block_l;
+    const int32_t* block_species;
+    const int64_t* off_values;
+    const int64_t* off_positions;
+    const int64_t* off_strain;
+    const int64_t* off_cell;
+    double* out;
+};
+
+void launch_se_output(const SeOutArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream);
+
+}  // namespace fb200
+
+namespace fb200 {
+
+struct PhaseTimes {
+    double neighbors = 0, metadata = 0, features = 0, expansion = 0, contraction = 0, transfer = 0, total = 0;
+    // kernels of the contraction phase
+    double ps_values = 0, ps_positions = 0, ps_strain_cell = 0;
+};
+
+// One calculator's GPU state: constant tables on the device, the workspace
+// arena, and the compute pipeline.
+class Engine {
+  public:
+    explicit Engine(const Hypers& h);
+    ~Engine();
+
+    std::unique_ptr<TensorMap> compute(bool power_spectrum, std::vector<HostSystem>& systems, const GradientOptions& g,
+                                       bool device_output, const double* d_positions, cudaStream_t stream);
+
+    const RadialTables& radial() const { return radial_; }
+    const PhaseTimes& last_times() const { return times_; }
+    int device() const { return device_; }
+
+  private:
+    void upload_tables();
+    Hypers h_;
+    RadialTables radial_;
+    YlmTables ylm_;
+    DeviceArena arena_;
+    NeighborBuilder nl_;
+    int device_ = -1;
+    bool tables_ready_ = false;
+    DeviceRadial d_radial_{};
+    DeviceYlm d_ylm_{};
+    double* d_self_ = nullptr;
+    std::vector<void*> table_buffers_;
+    PhaseTimes times_;
+};
+
+}  // namespace fb200

@@ -1,0 +1,410 @@
+// Kernel (b): SOAP spherical expansion on the GPU, FP64.
+//
+// Two launches:
+//
+// * `pair_features` -- one thread per half pair: cutoff / radial scaling,
+//   real spherical harmonics Y_lm (and their Cartesian gradients) by the
+//   Legendre recursion of featomic/src/math/spherical_harmonics.rs:228-424,
+//   and the radial integral R_nl(r) (and dR/dr) from the Hermite spline
+//   tables (featomic/src/math/splines.rs:225-289) or, when the spline is
+//   disabled, analytically (radial_integral/gto.rs:115-205).  The result is a
+//   per-pair feature record in HBM.
+//
+// * `se_accumulate` -- one CTA per centre, one thread per coefficient
+//   (l, m, n).  Directions (pair, orientation) are sorted by
+//   (centre, neighbour species, pair), so every (centre, species) segment is a
+//   contiguous run reduced in registers: no atomics, deterministic order.  It
+//   reproduces accumulate_all_pairs (featomic/src/calculators/soap/
+//   spherical_expansion.rs:101-358): values, the per-pair gradient of the
+//   first->second orientation, the self (centre) gradient, and the strain and
+//   cell gradients, with the (-1)^l / -(-1)^l factors of the reversed pair
+//   (spherical_expansion_pair.rs:130-163).
+#include "engine.hpp"
+#include "soap_math.cuh"
+
+namespace fb200 {
+
+namespace {
+
+constexpr int LMAX_SMALL = 8;
+constexpr int LMAX_LARGE = 24;
+
+template <int LCAP>
+struct LegendreScratch {
+    static constexpr int N = (LCAP + 1) * (LCAP + 2) / 2;
+    double P[N], dP[N], Pot[N];
+};
+
+__device__ __forceinline__ int lidx(int l, int m) { return m + l * (l + 1) / 2; }
+
+// Real spherical harmonics without the Condon-Shortley phase, and their
+// gradients w.r.t. the unit direction (spherical_harmonics.rs:304-424).
+template <int LCAP>
+__device__ void ylm_compute(const DeviceYlm& T, double ux, double uy, double uz, double* __restrict__ Y,
+                            double* __restrict__ GX, double* __restrict__ GY, double* __restrict__ GZ) {
+    LegendreScratch<LCAP> s;
+    const int lmax = T.lmax;
+    const double SQRT_1_OVER_2PI = 0.3989422804014327;
+    const double SQRT_3 = 1.7320508075688772;
+    const double SQRT_3_OVER_2 = 1.224744871391589;
+    const double SQRT_2 = 1.4142135623730951;
+
+    double sxy = hypot(ux, uy);
+    double ct = uz, st = sxy;
+    double cp, sp;
+    if (sxy > soap::DBL_EPS) {
+        cp = ux / sxy;
+        sp = uy / sxy;
+    } else {
+        cp = 1.0;
+        sp = 0.0;
+    }
+    // associated Legendre polynomials (:228-251)
+    double value = SQRT_1_OVER_2PI;
+    s.P[0] = value;
+    if (lmax > 0) {
+        s.P[lidx(1, 0)] = ct * SQRT_3 * value;
+        value *= -SQRT_3_OVER_2 * st;
+        s.P[lidx(1, 1)] = value;
+        for (int l = 2; l <= lmax; l++) {
+            for (int m = 0; m < l - 1; m++)
+                s.P[lidx(l, m)] = T.A[lidx(l, m)] * (ct * s.P[lidx(l - 1, m)] + T.B[lidx(l, m)] * s.P[lidx(l - 2, m)]);
+            s.P[lidx(l, l - 1)] = ct * T.sq_2l1[l] * value;
+            value *= -T.sq_half[l] * st;
+            s.P[lidx(l, l)] = value;
+        }
+    }
+    bool grad = GX != nullptr;
+    if (grad) {
+        // derivative factors (:256-298)
+        s.dP[0] = 0.0;
+        for (int l = 1; l <= lmax; l++) {
+            double pm1 = T.inv_ll[l] * s.P[lidx(l, 1)];
+            double pp1 = s.P[lidx(l, 1)];
+            s.dP[lidx(l, 0)] = T.sq_plus[lidx(l, 0)] * pm1 - T.sq_minus[lidx(l, 0)] * pp1;
+            for (int m = 1; m < l; m++)
+                s.dP[lidx(l, m)] = T.sq_plus[lidx(l, m)] * s.P[lidx(l, m - 1)] - T.sq_minus[lidx(l, m)] * s.P[lidx(l, m + 1)];
+            s.dP[lidx(l, l)] = T.sq_plus[lidx(l, l)] * s.P[lidx(l, l - 1)] - T.sq_minus[lidx(l, l)] * 0.0;
+        }
+        if (st > 0.1) {
+            for (int l = 0; l <= lmax; l++)
+                for (int m = 0; m <= l; m++) s.Pot[lidx(l, m)] = (double)m / st * s.P[lidx(l, m)];
+        } else {
+            for (int l = 0; l <= lmax; l++)
+                for (int m = 0; m <= l; m++) s.Pot[lidx(l, m)] = -0.5 / ct * s.dP[lidx(l, m)];
+        }
+    }
+    for (int l = 0; l <= lmax; l++) Y[l * l + l] = s.P[lidx(l, 0)] / SQRT_2;
+    if (grad) {
+        GX[0] = 0.0;
+        GY[0] = 0.0;
+        GZ[0] = 0.0;
+        for (int l = 1; l <= lmax; l++) {
+            double lf = T.sq_ll1[l] * s.P[lidx(l, 1)];
+            GX[l * l + l] = cp * ct * lf;
+            GY[l * l + l] = sp * ct * lf;
+            GZ[l * l + l] = -st * lf;
+        }
+    }
+    double cos1 = 1.0, sin1 = 0.0, cos2 = -cp, sin2 = sp;
+    double m2c = -2.0 * cp;
+    for (int m = 1; m <= lmax; m++) {
+        double smp = m2c * sin1 - sin2;
+        double cmp = m2c * cos1 - cos2;
+        sin2 = sin1;
+        sin1 = smp;
+        cos2 = cos1;
+        cos1 = cmp;
+        for (int l = m; l <= lmax; l++) {
+            double p = s.P[lidx(l, m)];
+            Y[l * l + l + m] = p * cmp;
+            Y[l * l + l - m] = p * smp;
+        }
+        if (grad) {
+            for (int l = m; l <= lmax; l++) {
+                double dp = s.dP[lidx(l, m)];
+                double sdp = smp * dp, cdp = cmp * dp;
+                double pot = s.Pot[lidx(l, m)];
+                GX[l * l + l + m] = sp * pot * smp - 0.5 * ct * cp * cdp;
+                GX[l * l + l - m] = -sp * pot * cmp - 0.5 * ct * cp * sdp;
+                GY[l * l + l + m] = -cp * pot * smp - 0.5 * ct * sp * cdp;
+                GY[l * l + l - m] = cp * pot * cmp - 0.5 * ct * sp * sdp;
+                GZ[l * l + l + m] = 0.5 * st * cdp;
+                GZ[l * l + l - m] = 0.5 * st * sdp;
+            }
+        }
+    }
+}
+
+__device__ bool radial_compute(const DeviceRadial& R, int l, double r, double* __restrict__ val, double* __restrict__ grad) {
+    const int N = R.nmax;
+    if (R.splined) {
+        const double* pos = R.positions + R.knot_offset[l];
+        int count = R.knot_count[l];
+        int k = soap::spline_interval(pos, count, r);
+        soap::HermiteWeights w = soap::hermite_weights(pos[k], pos[k + 1], r);
+        const double* pv = R.values + ((size_t)R.knot_offset[l] + k) * N;
+        const double* pd = R.derivs + ((size_t)R.knot_offset[l] + k) * N;
+        for (int n = 0; n < N; n++) {
+            val[n] = soap::hermite_value(w, pv[n], pd[n], pv[N + n], pd[N + n]);
+            if (grad) grad[n] = soap::hermite_derivative(w, pv[n], pd[n], pv[N + n], pd[N + n]);
+        }
+        return true;
+    }
+    double raw[64], graw[64];
+    bool ok = soap::gto_radial_raw(l, N, r, R.c, R.width2, R.bn, raw, grad ? graw : nullptr);
+    for (int k = 0; k < N; k++) {
+        double s = 0.0, sg = 0.0;
+        for (int n = 0; n < N; n++) {
+            s += raw[n] * R.ortho[k * N + n];
+            if (grad) sg += graw[n] * R.ortho[k * N + n];
+        }
+        val[k] = s;
+        if (grad) grad[k] = sg;
+    }
+    return ok;
+}
+
+template <int LCAP>
+__global__ void pair_features_kernel(DevicePairs pairs, DeviceRadial radial, DeviceYlm ylm, CutoffParams cut,
+                                     FeatureLayout L, double* __restrict__ features, int32_t* __restrict__ status) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pairs.count) return;
+    double* f = features + p * L.stride;
+    double r = pairs.distance[p];
+    double v0 = pairs.vector[3 * p], v1 = pairs.vector[3 * p + 1], v2 = pairs.vector[3 * p + 2];
+    double u0 = v0 / r, u1 = v1 / r, u2 = v2 / r;
+    if (r < 1e-6) {
+        // coincident atoms: spherical_expansion_pair.rs:337-339
+        u0 = 0.0;
+        u1 = 0.0;
+        u2 = 1.0;
+    }
+    double fc, dfc;
+    soap::cutoff_function(cut.smoothing, cut.rc, cut.width, r, &fc, &dfc);
+    double sc = 1.0, dsc = 0.0;
+    if (cut.scaling) soap::willatt2018(cut.scale, cut.rate, cut.exponent, r, &sc, &dsc);
+    f[0] = sc * fc;
+    f[1] = dfc * sc + fc * dsc;
+    f[2] = r;
+    f[3] = u0;
+    f[4] = u1;
+    f[5] = u2;
+    f[6] = v0;
+    f[7] = v1;
+    f[8] = v2;
+    f[9] = pairs.first[p] == pairs.second[p] ? 1.0 : 0.0;
+    f[10] = (double)pairs.shift[3 * p];
+    f[11] = (double)pairs.shift[3 * p + 1];
+    f[12] = (double)pairs.shift[3 * p + 2];
+    if (L.with_grad) {
+        ylm_compute<LCAP>(ylm, u0, u1, u2, f + L.off_y, f + L.off_dy, f + L.off_dy + L.L2, f + L.off_dy + 2 * L.L2);
+    } else {
+        ylm_compute<LCAP>(ylm, u0, u1, u2, f + L.off_y, nullptr, nullptr, nullptr);
+    }
+    bool ok = true;
+    for (int l = 0; l <= L.lmax; l++) {
+        ok &= radial_compute(radial, l, r, f + L.off_r + l * L.nmax, L.with_grad ? f + L.off_dr + l * L.nmax : nullptr);
+    }
+    if (!ok) atomicExch(status, 1);
+}
+
+__global__ void se_accumulate_kernel(SeArgs a) {
+    const FeatureLayout L = a.layout;
+    const int64_t c = blockIdx.x;
+    const int S = a.n_species;
+    const int K = L.L2 * L.nmax;
+    const int tc = a.centre_species[c];
+    const bool grad = L.with_grad && (a.do_positions || a.do_strain || a.do_cell);
+
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int lm = k / L.nmax;
+        const int n = k - lm * L.nmax;
+        int l = (int)sqrt((double)lm);
+        while (l * l > lm) l--;
+        while ((l + 1) * (l + 1) <= lm) l++;
+        const double sign_l = (l & 1) ? -1.0 : 1.0;
+        const int ri = l * L.nmax + n;
+
+        for (int t = 0; t < S; t++) {
+            const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
+            double acc = 0.0;
+            double sg0 = 0.0, sg1 = 0.0, sg2 = 0.0;
+            double st[9], ce[9];
+#pragma unroll
+            for (int x = 0; x < 9; x++) {
+                st[x] = 0.0;
+                ce[x] = 0.0;
+            }
+            for (int64_t d = d0; d < d1; d++) {
+                const int32_t code = a.dir_code[d];
+                const int64_t p = code >> 1;
+                const bool inv = code & 1;
+                const double* __restrict__ F = a.features + p * L.stride;
+                const double fsc = __ldg(F + 0);
+                const double Yv = __ldg(F + L.off_y + lm);
+                const double Rv = __ldg(F + L.off_r + ri);
+                const double val = fsc * Yv * Rv;
+                acc += inv ? sign_l * val : val;
+                if (!grad) continue;
+                const double fg = __ldg(F + 1), r = __ldg(F + 2);
+                const double u[3] = {__ldg(F + 3), __ldg(F + 4), __ldg(F + 5)};
+                const double dR = __ldg(F + L.off_dr + ri);
+                double g[3];
+#pragma unroll
+                for (int x = 0; x < 3; x++) {
+                    const double dY = __ldg(F + L.off_dy + x * L.L2 + lm);
+                    g[x] = fg * u[x] * Rv * Yv + fsc * dR * u[x] * Yv + fsc * Rv * dY / r;
+                }
+                if (!inv && a.do_positions) {
+                    double* pg = a.pair_grad + p * 3 * K;
+                    pg[k] = g[0];
+                    pg[K + k] = g[1];
+                    pg[2 * K + k] = g[2];
+                }
+                const double gf = inv ? -sign_l : 1.0;
+                const double gi[3] = {gf * g[0], gf * g[1], gf * g[2]};
+                if (a.do_positions && __ldg(F + 9) == 0.0) {
+                    sg0 -= gi[0];
+                    sg1 -= gi[1];
+                    sg2 -= gi[2];
+                }
+                if (a.do_strain) {
+                    const double vec[3] = {__ldg(F + 6), __ldg(F + 7), __ldg(F + 8)};
+#pragma unroll
+                    for (int x = 0; x < 3; x++) {
+                        const double vx = inv ? -vec[x] : vec[x];
+#pragma unroll
+                        for (int y = 0; y < 3; y++) st[x * 3 + y] += vx * gi[y];
+                    }
+                }
+                if (a.do_cell) {
+                    const double sh[3] = {__ldg(F + 10), __ldg(F + 11), __ldg(F + 12)};
+#pragma unroll
+                    for (int x = 0; x < 3; x++) {
+                        const double sx = inv ? -sh[x] : sh[x];
+#pragma unroll
+                        for (int y = 0; y < 3; y++) ce[x * 3 + y] += sx * gi[y];
+                    }
+                }
+            }
+            const int64_t base = (c * S + t);
+            double self = (t == tc && l == 0) ? a.self_contribution[n] : 0.0;
+            a.coef[base * K + k] = self + acc;
+            if (a.do_positions) {
+                double* sgp = a.self_grad + base * 3 * K;
+                sgp[k] = sg0;
+                sgp[K + k] = sg1;
+                sgp[2 * K + k] = sg2;
+            }
+            if (a.do_strain) {
+                double* o = a.strain + base * 9 * K;
+#pragma unroll
+                for (int x = 0; x < 9; x++) o[x * K + k] = st[x];
+            }
+            if (a.do_cell) {
+                double* o = a.cellg + base * 9 * K;
+#pragma unroll
+                for (int x = 0; x < 9; x++) o[x * K + k] = ce[x];
+            }
+        }
+    }
+}
+
+// spherical_expansion calculator output: values / strain / cell of one
+// (block, sample) row per CTA
+__global__ void se_output_rows_kernel(SeOutArgs a, int do_strain, int do_cell) {
+    const int64_t row = blockIdx.x;
+    const int K = (a.lmax + 1) * (a.lmax + 1) * a.nmax;
+    const int c = a.row_centre[row];
+    const int blk = a.row_block[row];
+    const int s = a.row_sample[row];
+    const int l = a.block_l[blk];
+    const int t = a.block_species[blk];
+    const int width = (2 * l + 1) * a.nmax;
+    const int64_t src = ((int64_t)c * a.n_species + t);
+    const int start = l * l * a.nmax;
+    for (int q = threadIdx.x; q < width; q += blockDim.x)
+        a.out[a.off_values[blk] + (int64_t)s * width + q] = a.coef[src * K + start + q];
+    if (do_strain) {
+        for (int q = threadIdx.x; q < 9 * width; q += blockDim.x) {
+            int x = q / width, w = q - x * width;
+            a.out[a.off_strain[blk] + (int64_t)s * 9 * width + q] = a.strain[(src * 9 + x) * K + start + w];
+        }
+    }
+    if (do_cell) {
+        for (int q = threadIdx.x; q < 9 * width; q += blockDim.x) {
+            int x = q / width, w = q - x * width;
+            a.out[a.off_cell[blk] + (int64_t)s * 9 * width + q] = a.cellg[(src * 9 + x) * K + start + w];
+        }
+    }
+}
+
+// positions gradient rows: self gradient for the centre, sum over the pairs
+// between centre and neighbour otherwise (spherical_expansion.rs:468-521)
+__global__ void se_output_gradients_kernel(SeOutArgs a) {
+    const int64_t row = blockIdx.x;
+    const int K = (a.lmax + 1) * (a.lmax + 1) * a.nmax;
+    const int blk = a.grad_block[row];
+    const int l = a.block_l[blk];
+    const int t = a.block_species[blk];
+    const int c = a.grad_centre[row];
+    const int j = a.grad_atom[row];
+    const int width = (2 * l + 1) * a.nmax;
+    const int start = l * l * a.nmax;
+    const double sign_l = (l & 1) ? -1.0 : 1.0;
+    double* out = a.out + a.off_positions[blk] + a.grad_row[row] * 3 * width;
+    for (int q = threadIdx.x; q < 3 * width; q += blockDim.x) {
+        int x = q / width, w = q - x * width;
+        double v;
+        if (c == j) {
+            v = a.self_grad[(((int64_t)c * a.n_species + t) * 3 + x) * K + start + w];
+        } else {
+            v = 0.0;
+            for (int d = a.grad_d0[row]; d < a.grad_d1[row]; d++) {
+                int32_t code = a.dir_code[d];
+                int64_t p = code >> 1;
+                double factor = (code & 1) ? -sign_l : 1.0;
+                v += factor * a.pair_grad[(p * 3 + x) * K + start + w];
+            }
+        }
+        out[q] = v;
+    }
+}
+
+}  // namespace
+
+void launch_pair_features(const DevicePairs& pairs, const DeviceRadial& radial, const DeviceYlm& ylm,
+                          const CutoffParams& cut, const FeatureLayout& layout, double* features, int32_t* status,
+                          cudaStream_t stream) {
+    if (pairs.count == 0) return;
+    int threads = 64;
+    int blocks = (int)((pairs.count + threads - 1) / threads);
+    if (ylm.lmax <= LMAX_SMALL) {
+        pair_features_kernel<LMAX_SMALL><<<blocks, threads, 0, stream>>>(pairs, radial, ylm, cut, layout, features, status);
+    } else {
+        pair_features_kernel<LMAX_LARGE><<<blocks, threads, 0, stream>>>(pairs, radial, ylm, cut, layout, features, status);
+    }
+    CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_se_accumulate(const SeArgs& args, cudaStream_t stream) {
+    if (args.n_centres == 0) return;
+    int K = args.layout.L2 * args.layout.nmax;
+    int threads = std::min(1024, (K + 31) / 32 * 32);
+    se_accumulate_kernel<<<(unsigned)args.n_centres, threads, 0, stream>>>(args);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_se_output(const SeOutArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream) {
+    if (args.n_rows > 0) {
+        se_output_rows_kernel<<<(unsigned)args.n_rows, 128, 0, stream>>>(args, strain, cell);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    if (positions && args.n_grad_rows > 0) {
+        se_output_gradients_kernel<<<(unsigned)args.n_grad_rows, 128, 0, stream>>>(args);
+        CUDA_CHECK(cudaGetLastError());
+    }
+}
+
+}  // namespace fb200

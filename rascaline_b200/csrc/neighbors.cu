@@ -1,0 +1,305 @@
+// Kernel (a): periodic cell-list neighbour search on the GPU.
+//
+// Produces featomic's half neighbour list (featomic/src/systems/neighbors.rs:
+// CellList::new :101-163, add_atom :167-201, pairs :217-309,
+// NeighborsList::new :349-403) for a batch of systems in one pass:
+//
+//   1. bin atoms: fractional coordinates (vector x inverse cell), floor, Python
+//      divmod wrap (one thread per atom; atomics only on integer cell counts)
+//   2. count the candidate pairs of every atom i over the (2 n_search + 1)^3
+//      neighbouring cells (j >= i, the self-image half-space rules), keeping
+//      those with |r_ij|^2 < rc^2
+//   3. exclusive scan of the counts (CUB)
+//   4. write the pairs of every atom into its slot range and sort that range
+//      by (second, shift)
+//
+// The list is therefore ordered by (first, second, shift); featomic sorts by
+// (first, second) with an unstable sort, so only ties between periodic images
+// of the same two atoms can be ordered differently (tests compare those runs
+// as multisets).  Distances and vectors use explicit round-to-nearest
+// intrinsics so that no FMA is contracted and the bits match the CPU
+// evaluation order: vector = (r_j - r_i) + (H^T s), d^2 = x x + y y + z z.
+#include <cub/cub.cuh>
+
+#include "engine.hpp"
+
+namespace fb200 {
+
+namespace {
+
+__device__ __forceinline__ void divmod_i(int a, int b, int* q, int* r) {
+    int quotient = a / b;
+    int remainder = a % b;
+    if (remainder < 0) {
+        remainder += b;
+        quotient -= 1;
+    }
+    *q = quotient;
+    *r = remainder;
+}
+
+__global__ void nl_assign_cells(const NlSystem* __restrict__ systems, const int32_t* __restrict__ atom_system,
+                                const double* __restrict__ positions, int64_t n_atoms, int32_t* __restrict__ cell_of,
+                                int32_t* __restrict__ atom_shift, int32_t* __restrict__ cell_count) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_atoms) return;
+    const NlSystem& s = systems[atom_system[g]];
+    double p0 = positions[3 * g], p1 = positions[3 * g + 1], p2 = positions[3 * g + 2];
+    double f[3];
+    if (s.infinite) {
+        f[0] = p0;
+        f[1] = p1;
+        f[2] = p2;
+    } else {
+        // row vector times inverse matrix, matrix.rs:399-407
+        for (int k = 0; k < 3; k++) {
+            f[k] = __dadd_rn(__dadd_rn(__dmul_rn(p0, s.inv[0 * 3 + k]), __dmul_rn(p1, s.inv[1 * 3 + k])),
+                             __dmul_rn(p2, s.inv[2 * 3 + k]));
+        }
+    }
+    int idx[3], sh[3];
+    for (int k = 0; k < 3; k++) {
+        int ci = (int)floor(__dmul_rn(f[k], (double)s.n_cells[k]));
+        if (s.infinite) {
+            // `cell_index as usize` then usize::clamp(.., 0, n - 1): negative
+            // values wrap to huge numbers and land in the last cell
+            unsigned long long u = (unsigned long long)(long long)ci;
+            unsigned long long hi = (unsigned long long)(s.n_cells[k] - 1);
+            idx[k] = (int)(u > hi ? hi : u);
+            sh[k] = 0;
+        } else {
+            divmod_i(ci, s.n_cells[k], &sh[k], &idx[k]);
+        }
+    }
+    int32_t cell = (int32_t)(s.cell_offset + ((int64_t)idx[0] * s.n_cells[1] + idx[1]) * s.n_cells[2] + idx[2]);
+    cell_of[g] = cell;
+    atom_shift[3 * g] = sh[0];
+    atom_shift[3 * g + 1] = sh[1];
+    atom_shift[3 * g + 2] = sh[2];
+    atomicAdd(&cell_count[cell], 1);
+}
+
+__global__ void nl_fill_cells(const int32_t* __restrict__ cell_of, int64_t n_atoms, const int32_t* __restrict__ cell_start,
+                              int32_t* __restrict__ cell_fill, int32_t* __restrict__ cell_atoms) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_atoms) return;
+    int32_t c = cell_of[g];
+    int slot = atomicAdd(&cell_fill[c], 1);
+    cell_atoms[cell_start[c] + slot] = (int32_t)g;
+}
+
+// Enumerate the candidate pairs of atom g.  `emit(j, shift, v, d2)` is called
+// for every kept pair, in enumeration order.
+template <typename Emit>
+__device__ __forceinline__ void nl_enumerate(const NlSystem& s, int64_t g, const double* __restrict__ positions,
+                                             const int32_t* __restrict__ cell_of, const int32_t* __restrict__ atom_shift,
+                                             const int32_t* __restrict__ cell_start, const int32_t* __restrict__ cell_count,
+                                             const int32_t* __restrict__ cell_atoms, double cutoff2, Emit emit) {
+    int local = (int)(cell_of[g] - s.cell_offset);
+    int cz = local % s.n_cells[2];
+    int cy = (local / s.n_cells[2]) % s.n_cells[1];
+    int cx = local / (s.n_cells[2] * s.n_cells[1]);
+    int si[3] = {atom_shift[3 * g], atom_shift[3 * g + 1], atom_shift[3 * g + 2]};
+    double pi0 = positions[3 * g], pi1 = positions[3 * g + 1], pi2 = positions[3 * g + 2];
+    for (int dx = -s.n_search[0]; dx <= s.n_search[0]; dx++)
+    for (int dy = -s.n_search[1]; dy <= s.n_search[1]; dy++)
+    for (int dz = -s.n_search[2]; dz <= s.n_search[2]; dz++) {
+        int cs[3], ni[3];
+        divmod_i(cx + dx, s.n_cells[0], &cs[0], &ni[0]);
+        divmod_i(cy + dy, s.n_cells[1], &cs[1], &ni[1]);
+        divmod_i(cz + dz, s.n_cells[2], &cs[2], &ni[2]);
+        int32_t nc = (int32_t)(s.cell_offset + ((int64_t)ni[0] * s.n_cells[1] + ni[1]) * s.n_cells[2] + ni[2]);
+        int32_t start = cell_start[nc], count = cell_count[nc];
+        for (int32_t q = 0; q < count; q++) {
+            int64_t j = cell_atoms[start + q];
+            if (g > j) continue;
+            int sh[3];
+            for (int k = 0; k < 3; k++) sh[k] = cs[k] + si[k] - atom_shift[3 * j + k];
+            bool zero = sh[0] == 0 && sh[1] == 0 && sh[2] == 0;
+            if (g == j) {
+                if (zero) continue;
+                int sum = sh[0] + sh[1] + sh[2];
+                if (sum < 0) continue;
+                if (sum == 0 && (sh[2] < 0 || (sh[2] == 0 && sh[1] < 0))) continue;
+            }
+            if (s.infinite && !zero) continue;
+            double v[3];
+            double pj[3] = {positions[3 * j], positions[3 * j + 1], positions[3 * j + 2]};
+            double pi[3] = {pi0, pi1, pi2};
+            for (int k = 0; k < 3; k++) {
+                // CellShift::cartesian, neighbors.rs:52-57
+                double c = __dadd_rn(__dadd_rn(__dmul_rn(s.H[0 * 3 + k], (double)sh[0]), __dmul_rn(s.H[1 * 3 + k], (double)sh[1])),
+                                     __dmul_rn(s.H[2 * 3 + k], (double)sh[2]));
+                v[k] = __dadd_rn(__dsub_rn(pj[k], pi[k]), c);
+            }
+            double d2 = __dadd_rn(__dadd_rn(__dmul_rn(v[0], v[0]), __dmul_rn(v[1], v[1])), __dmul_rn(v[2], v[2]));
+            if (d2 < cutoff2) emit((int32_t)j, sh, v, d2);
+        }
+    }
+}
+
+__global__ void nl_count(const NlSystem* __restrict__ systems, const int32_t* __restrict__ atom_system,
+                         const double* __restrict__ positions, int64_t n_atoms, const int32_t* __restrict__ cell_of,
+                         const int32_t* __restrict__ atom_shift, const int32_t* __restrict__ cell_start,
+                         const int32_t* __restrict__ cell_count, const int32_t* __restrict__ cell_atoms,
+                         int64_t* __restrict__ pair_count) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_atoms) return;
+    const NlSystem& s = systems[atom_system[g]];
+    int64_t count = 0;
+    nl_enumerate(s, g, positions, cell_of, atom_shift, cell_start, cell_count, cell_atoms, s.cutoff2,
+                 [&](int32_t, const int*, const double*, double) { count++; });
+    pair_count[g] = count;
+}
+
+__device__ __forceinline__ bool pair_key_less(int32_t j1, const int32_t* s1, int32_t j2, const int32_t* s2) {
+    if (j1 != j2) return j1 < j2;
+    for (int k = 0; k < 3; k++)
+        if (s1[k] != s2[k]) return s1[k] < s2[k];
+    return false;
+}
+
+__global__ void nl_write(const NlSystem* __restrict__ systems, const int32_t* __restrict__ atom_system,
+                         const double* __restrict__ positions, int64_t n_atoms, const int32_t* __restrict__ cell_of,
+                         const int32_t* __restrict__ atom_shift, const int32_t* __restrict__ cell_start,
+                         const int32_t* __restrict__ cell_count, const int32_t* __restrict__ cell_atoms,
+                         const int64_t* __restrict__ pair_start, DevicePairs pairs) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_atoms) return;
+    const NlSystem& s = systems[atom_system[g]];
+    int64_t base = pair_start[g];
+    int64_t w = base;
+    nl_enumerate(s, g, positions, cell_of, atom_shift, cell_start, cell_count, cell_atoms, s.cutoff2,
+                 [&](int32_t j, const int* sh, const double* v, double d2) {
+                     pairs.first[w] = (int32_t)g;
+                     pairs.second[w] = j;
+                     pairs.distance[w] = __dsqrt_rn(d2);
+                     pairs.vector[3 * w] = v[0];
+                     pairs.vector[3 * w + 1] = v[1];
+                     pairs.vector[3 * w + 2] = v[2];
+                     pairs.shift[3 * w] = sh[0];
+                     pairs.shift[3 * w + 1] = sh[1];
+                     pairs.shift[3 * w + 2] = sh[2];
+                     w++;
+                 });
+    // insertion sort of this atom's pairs by (second, shift)
+    for (int64_t a = base + 1; a < w; a++) {
+        int32_t j = pairs.second[a];
+        int32_t sh[3] = {pairs.shift[3 * a], pairs.shift[3 * a + 1], pairs.shift[3 * a + 2]};
+        double d = pairs.distance[a];
+        double v[3] = {pairs.vector[3 * a], pairs.vector[3 * a + 1], pairs.vector[3 * a + 2]};
+        int64_t b = a - 1;
+        while (b >= base && pair_key_less(j, sh, pairs.second[b], &pairs.shift[3 * b])) {
+            pairs.second[b + 1] = pairs.second[b];
+            pairs.distance[b + 1] = pairs.distance[b];
+            for (int k = 0; k < 3; k++) {
+                pairs.vector[3 * (b + 1) + k] = pairs.vector[3 * b + k];
+                pairs.shift[3 * (b + 1) + k] = pairs.shift[3 * b + k];
+            }
+            b--;
+        }
+        pairs.second[b + 1] = j;
+        pairs.distance[b + 1] = d;
+        for (int k = 0; k < 3; k++) {
+            pairs.vector[3 * (b + 1) + k] = v[k];
+            pairs.shift[3 * (b + 1) + k] = sh[k];
+        }
+    }
+}
+
+}  // namespace
+
+// Host-side cell-list parameters, CellList::new (neighbors.rs:101-163) and
+// UnitCell (cell.rs:34-66, :154-169).  Compiled with FMA contraction off.
+NlSystem make_nl_system(const double* cell, double cutoff, int64_t atom_offset, int64_t n_atoms, int64_t cell_offset);
+
+int64_t NeighborBuilder::build(const std::vector<NlSystem>& systems, const std::vector<int32_t>& atom_system,
+                               const double* d_positions, int64_t n_atoms, DeviceArena& arena, cudaStream_t stream) {
+    int64_t n_systems = (int64_t)systems.size();
+    int64_t n_cells = 0;
+    for (auto& s : systems) n_cells = std::max<int64_t>(n_cells, s.cell_offset + (int64_t)s.n_cells[0] * s.n_cells[1] * s.n_cells[2]);
+    if (n_cells >= (int64_t)INT32_MAX || n_atoms >= (int64_t)INT32_MAX) throw internal_error("too many atoms or cells for the neighbour list");
+
+    NlSystem* d_sys = arena.alloc<NlSystem>("nl.systems", n_systems);
+    int32_t* d_atom_system = arena.alloc<int32_t>("nl.atom_system", n_atoms);
+    int32_t* d_cell_of = arena.alloc<int32_t>("nl.cell_of", n_atoms);
+    int32_t* d_atom_shift = arena.alloc<int32_t>("nl.atom_shift", 3 * n_atoms);
+    int32_t* d_cell_count = arena.alloc<int32_t>("nl.cell_count", n_cells + 1);
+    int32_t* d_cell_start = arena.alloc<int32_t>("nl.cell_start", n_cells + 1);
+    int32_t* d_cell_fill = arena.alloc<int32_t>("nl.cell_fill", n_cells + 1);
+    int32_t* d_cell_atoms = arena.alloc<int32_t>("nl.cell_atoms", n_atoms);
+    int64_t* d_pair_count = arena.alloc<int64_t>("nl.pair_count", n_atoms + 1);
+    int64_t* d_pair_start = arena.alloc<int64_t>("nl.pair_start", n_atoms + 1);
+
+    CUDA_CHECK(cudaMemcpyAsync(d_sys, systems.data(), sizeof(NlSystem) * n_systems, cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaMemcpyAsync(d_atom_system, atom_system.data(), sizeof(int32_t) * n_atoms, cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaMemsetAsync(d_cell_count, 0, sizeof(int32_t) * (n_cells + 1), stream));
+    CUDA_CHECK(cudaMemsetAsync(d_cell_fill, 0, sizeof(int32_t) * (n_cells + 1), stream));
+    CUDA_CHECK(cudaMemsetAsync(d_pair_count, 0, sizeof(int64_t) * (n_atoms + 1), stream));
+
+    int threads = 128;
+    int blocks = (int)((n_atoms + threads - 1) / threads);
+    if (n_atoms > 0) {
+        nl_assign_cells<<<blocks, threads, 0, stream>>>(d_sys, d_atom_system, d_positions, n_atoms, d_cell_of, d_atom_shift, d_cell_count);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    arena.exclusive_scan(d_cell_count, d_cell_start, n_cells + 1, stream);
+    if (n_atoms > 0) {
+        nl_fill_cells<<<blocks, threads, 0, stream>>>(d_cell_of, n_atoms, d_cell_start, d_cell_fill, d_cell_atoms);
+        CUDA_CHECK(cudaGetLastError());
+        nl_count<<<blocks, threads, 0, stream>>>(d_sys, d_atom_system, d_positions, n_atoms, d_cell_of, d_atom_shift,
+                                                 d_cell_start, d_cell_count, d_cell_atoms, d_pair_count);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    arena.exclusive_scan(d_pair_count, d_pair_start, n_atoms + 1, stream);
+    int64_t total = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&total, d_pair_start + n_atoms, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (total >= (int64_t)INT32_MAX) throw internal_error("too many pairs for the neighbour list");
+
+    pairs.first = arena.alloc<int32_t>("pairs.first", total);
+    pairs.second = arena.alloc<int32_t>("pairs.second", total);
+    pairs.distance = arena.alloc<double>("pairs.distance", total);
+    pairs.vector = arena.alloc<double>("pairs.vector", 3 * total);
+    pairs.shift = arena.alloc<int32_t>("pairs.shift", 3 * total);
+    pairs.count = total;
+    if (n_atoms > 0 && total > 0) {
+        nl_write<<<blocks, threads, 0, stream>>>(d_sys, d_atom_system, d_positions, n_atoms, d_cell_of, d_atom_shift,
+                                                 d_cell_start, d_cell_count, d_cell_atoms, d_pair_start, pairs);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    return total;
+}
+
+std::vector<Pair> neighbor_list(const double* positions, int64_t n_atoms, const double* cell, double cutoff) {
+    DeviceArena arena;
+    NeighborBuilder nb;
+    cudaStream_t stream = nullptr;
+    std::vector<NlSystem> systems = {make_nl_system(cell, cutoff, 0, n_atoms, 0)};
+    std::vector<int32_t> atom_system(n_atoms, 0);
+    double* d_pos = arena.alloc<double>("positions", 3 * n_atoms);
+    if (n_atoms) CUDA_CHECK(cudaMemcpy(d_pos, positions, sizeof(double) * 3 * n_atoms, cudaMemcpyHostToDevice));
+    int64_t n = nb.build(systems, atom_system, d_pos, n_atoms, arena, stream);
+    std::vector<int32_t> first(n), second(n), shift(3 * n);
+    std::vector<double> dist(n), vec(3 * n);
+    if (n) {
+        CUDA_CHECK(cudaMemcpy(first.data(), nb.pairs.first, 4 * n, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(second.data(), nb.pairs.second, 4 * n, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(shift.data(), nb.pairs.shift, 12 * n, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(dist.data(), nb.pairs.distance, 8 * n, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(vec.data(), nb.pairs.vector, 24 * n, cudaMemcpyDeviceToHost));
+    }
+    std::vector<Pair> out(n);
+    for (int64_t k = 0; k < n; k++) {
+        out[k].first = (uint64_t)first[k];
+        out[k].second = (uint64_t)second[k];
+        out[k].distance = dist[k];
+        for (int x = 0; x < 3; x++) {
+            out[k].vector[x] = vec[3 * k + x];
+            out[k].shift[x] = shift[3 * k + x];
+        }
+    }
+    return out;
+}
+
+}  // namespace fb200

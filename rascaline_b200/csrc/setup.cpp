@@ -1,0 +1,459 @@
+// Calculator set-up on the host: hyper-parameter parsing / validation, the GTO
+// radial basis orthonormalisation, the adaptive Hermite spline tables of the
+// radial integral, and the constant tables of the spherical harmonics.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+#include "host.hpp"
+#include "soap_math.cuh"
+
+namespace fb200 {
+
+using json::Value;
+
+// ---------------------------------------------------------------------------
+// JSON -> Hypers, with serde's accept / reject rules:
+// deny_unknown_fields on Cutoff, Smoothing, DensityScaling, the basis and the
+// radial basis (featomic/src/calculators/soap/cutoff.rs:4-29,
+// calculators/shared/density.rs:4-75, calculators/shared/basis/mod.rs:11-59,
+// calculators/shared/basis/radial/mod.rs:9-37).  Type errors are JSON errors
+// (FEATOMIC_JSON_ERROR), semantic errors are invalid parameters.
+// ---------------------------------------------------------------------------
+namespace {
+
+Error json_error(const std::string& m) { return Error(STATUS_JSON_ERROR, m); }
+
+const Value& field(const Value& obj, const char* name, const char* context) {
+    const Value* v = obj.get(name);
+    if (!v) throw json_error(std::string("missing field `") + name + "` in " + context);
+    return *v;
+}
+
+void deny_unknown(const Value& obj, std::initializer_list<const char*> allowed, const char* context) {
+    for (auto& kv : obj.object) {
+        bool ok = false;
+        for (auto a : allowed)
+            if (kv.first == a) ok = true;
+        if (!ok) {
+            std::string list;
+            for (auto a : allowed) list += std::string(list.empty() ? "" : ", ") + "`" + a + "`";
+            throw json_error("unknown field `" + kv.first + "` in " + context + ", expected one of " + list);
+        }
+    }
+}
+
+const Value& object(const Value& v, const char* context) {
+    if (v.kind != Value::Object)
+        throw json_error(std::string("invalid type: ") + v.kind_name() + ", expected " + context);
+    return v;
+}
+
+double as_f64(const Value& v, const char* name) {
+    if (v.kind != Value::Number) throw json_error(std::string("invalid type: ") + v.kind_name() + " for `" + name + "`, expected f64");
+    return v.number;
+}
+
+int64_t as_usize(const Value& v, const char* name) {
+    if (v.kind != Value::Number || !v.is_integer)
+        throw json_error(std::string("invalid type: ") + v.kind_name() + " for `" + name + "`, expected usize");
+    if (v.integer < 0) throw json_error(std::string("invalid value: integer `") + std::to_string(v.integer) + "` for `" + name + "`, expected usize");
+    return v.integer;
+}
+
+std::string tag(const Value& v, const char* context) {
+    const Value* t = v.get("type");
+    if (!t) throw json_error(std::string("missing field `type` in ") + context);
+    if (t->kind != Value::String) throw json_error(std::string("invalid type for `type` in ") + context);
+    return t->string;
+}
+
+}  // namespace
+
+Hypers parse_hypers(const std::string& text, bool deny_unknown_top) {
+    Value root;
+    try {
+        root = json::parse(text);
+    } catch (json::ParseError& e) {
+        throw json_error(e.what());
+    }
+    object(root, "struct parameters");
+    if (deny_unknown_top) deny_unknown(root, {"cutoff", "density", "basis"}, "parameters");
+    Hypers h;
+
+    // cutoff
+    const Value& cutoff = object(field(root, "cutoff", "parameters"), "struct Cutoff");
+    deny_unknown(cutoff, {"radius", "smoothing"}, "Cutoff");
+    h.cutoff = as_f64(field(cutoff, "radius", "Cutoff"), "radius");
+    const Value& smoothing = object(field(cutoff, "smoothing", "Cutoff"), "internally tagged enum Smoothing");
+    std::string st = tag(smoothing, "Smoothing");
+    if (st == "ShiftedCosine") {
+        deny_unknown(smoothing, {"type", "width"}, "ShiftedCosine");
+        h.smoothing = 0;
+        h.smoothing_width = as_f64(field(smoothing, "width", "ShiftedCosine"), "width");
+    } else if (st == "Step") {
+        deny_unknown(smoothing, {"type"}, "Step");
+        h.smoothing = 1;
+    } else {
+        throw json_error("unknown variant `" + st + "`, expected `ShiftedCosine` or `Step`");
+    }
+
+    // density: DensityKind is flattened, so unknown fields are not rejected
+    const Value& density = object(field(root, "density", "parameters"), "struct Density");
+    std::string dt = tag(density, "Density");
+    bool gaussian = false;
+    if (dt == "Gaussian") {
+        gaussian = true;
+        h.density_width = as_f64(field(density, "width", "Gaussian"), "width");
+    } else if (dt == "DiracDelta") {
+    } else if (dt == "SmearedPowerLaw") {
+        as_f64(field(density, "smearing", "SmearedPowerLaw"), "smearing");
+        as_usize(field(density, "exponent", "SmearedPowerLaw"), "exponent");
+    } else {
+        throw json_error("unknown variant `" + dt + "`, expected one of `DiracDelta`, `Gaussian`, `SmearedPowerLaw`");
+    }
+    if (const Value* cw = density.get("center_atom_weight")) h.center_atom_weight = as_f64(*cw, "center_atom_weight");
+    if (const Value* sc = density.get("scaling")) {
+        if (sc->kind != Value::Null) {
+            object(*sc, "internally tagged enum DensityScaling");
+            std::string t = tag(*sc, "DensityScaling");
+            if (t != "Willatt2018") throw json_error("unknown variant `" + t + "`, expected `Willatt2018`");
+            deny_unknown(*sc, {"type", "scale", "rate", "exponent"}, "Willatt2018");
+            h.scaling = true;
+            h.scaling_scale = as_f64(field(*sc, "scale", "Willatt2018"), "scale");
+            h.scaling_rate = as_f64(field(*sc, "rate", "Willatt2018"), "rate");
+            h.scaling_exponent = as_f64(field(*sc, "exponent", "Willatt2018"), "exponent");
+        }
+    }
+
+    // basis
+    const Value& basis = object(field(root, "basis", "parameters"), "internally tagged enum SphericalExpansionBasis");
+    std::string bt = tag(basis, "SphericalExpansionBasis");
+    if (bt == "Explicit") {
+        throw invalid_parameter("the 'Explicit' spherical expansion basis is not supported by featomic-b200 yet");
+    } else if (bt != "TensorProduct") {
+        throw json_error("unknown variant `" + bt + "`, expected `TensorProduct` or `Explicit`");
+    }
+    deny_unknown(basis, {"type", "max_angular", "radial", "spline_accuracy"}, "TensorProduct");
+    h.max_angular = (int)as_usize(field(basis, "max_angular", "TensorProduct"), "max_angular");
+    const Value& radial = object(field(basis, "radial", "TensorProduct"), "internally tagged enum SoapRadialBasis");
+    std::string rt = tag(radial, "SoapRadialBasis");
+    if (rt == "Tabulated") {
+        throw invalid_parameter("the 'Tabulated' radial basis is not supported by featomic-b200 yet");
+    } else if (rt != "Gto") {
+        throw json_error("unknown variant `" + rt + "`, expected `Gto` or `Tabulated`");
+    }
+    deny_unknown(radial, {"type", "max_radial", "radius"}, "Gto");
+    h.max_radial = (int)as_usize(field(radial, "max_radial", "Gto"), "max_radial");
+    if (const Value* rr = radial.get("radius")) {
+        if (rr->kind != Value::Null) {
+            double radius = as_f64(*rr, "radius");
+            if (radius != h.cutoff)
+                throw internal_error("GTO radius must be the same as the cutoff radius in SOAP, or should not provided");
+        }
+    }
+    if (const Value* sa = basis.get("spline_accuracy")) {
+        if (sa->kind == Value::Null) {
+            h.splined = false;
+        } else {
+            h.spline_accuracy = as_f64(*sa, "spline_accuracy");
+        }
+    }
+
+    // validation: cutoff.rs:32-45, density.rs:79-105, radial_integral/mod.rs:78-123
+    if (h.smoothing == 0 && (h.smoothing_width <= 0.0 || !std::isfinite(h.smoothing_width))) {
+        std::ostringstream m;
+        m << "expected positive width for shifted cosine cutoff function, got " << h.smoothing_width;
+        throw invalid_parameter(m.str());
+    }
+    if (h.scaling) {
+        if (h.scaling_scale <= 0.0) throw invalid_parameter("expected positive scale for Willatt2018 radial scaling function");
+        if (h.scaling_rate <= 0.0) throw invalid_parameter("expected positive rate for Willatt2018 radial scaling function");
+        if (h.scaling_exponent <= 0.0) throw invalid_parameter("expected positive exponent for Willatt2018 radial scaling function");
+    }
+    if (!gaussian) throw invalid_parameter("this combination of basis and density is not supported in SOAP");
+    if (!(h.density_width > 1e-16 && std::isfinite(h.density_width)))
+        throw invalid_parameter("expected positive and finite Gaussian width");
+    if (!(h.cutoff > 0.0 && std::isfinite(h.cutoff))) throw invalid_parameter("cutoff must be positive and finite");
+    if (h.splined && h.spline_accuracy < 0.0) {
+        std::ostringstream m;
+        m << "got invalid accuracy in spline (" << h.spline_accuracy << "), it must be positive";
+        throw invalid_parameter(m.str());
+    }
+    if (h.max_angular > 24) throw invalid_parameter("max_angular larger than 24 is not supported by featomic-b200");
+    if (h.max_radial > 63) throw invalid_parameter("max_radial larger than 63 is not supported by featomic-b200");
+    return h;
+}
+
+// ---------------------------------------------------------------------------
+// GTO radial basis: widths sigma_n = rc max(sqrt n, 1) / n_max and the
+// orthonormalisation S^{-1/2} diag(norm) of the analytic overlap
+// (featomic/src/calculators/shared/basis/radial/gto.rs:17-75).  The inverse
+// square root uses a cyclic Jacobi eigen-decomposition.
+// ---------------------------------------------------------------------------
+namespace {
+
+void jacobi_eigen(std::vector<double>& a, int n, std::vector<double>& evals, std::vector<double>& evecs) {
+    evecs.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) evecs[(size_t)i * n + i] = 1.0;
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++) off += a[(size_t)i * n + j] * a[(size_t)i * n + j];
+        if (off < 1e-300) break;
+        for (int p = 0; p < n; p++) {
+            for (int q = p + 1; q < n; q++) {
+                double apq = a[(size_t)p * n + q];
+                if (apq == 0.0) continue;
+                double app = a[(size_t)p * n + p], aqq = a[(size_t)q * n + q];
+                double theta = (aqq - app) / (2.0 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < n; k++) {
+                    double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
+                    a[(size_t)k * n + p] = c * akp - s * akq;
+                    a[(size_t)k * n + q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < n; k++) {
+                    double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
+                    a[(size_t)p * n + k] = c * apk - s * aqk;
+                    a[(size_t)q * n + k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < n; k++) {
+                    double vkp = evecs[(size_t)k * n + p], vkq = evecs[(size_t)k * n + q];
+                    evecs[(size_t)k * n + p] = c * vkp - s * vkq;
+                    evecs[(size_t)k * n + q] = s * vkp + c * vkq;
+                }
+            }
+        }
+    }
+    evals.resize(n);
+    for (int i = 0; i < n; i++) evals[i] = a[(size_t)i * n + i];
+}
+
+std::vector<double> gto_widths(int size, double radius) {
+    std::vector<double> w(size);
+    for (int n = 0; n < size; n++) w[n] = radius * std::max(std::sqrt((double)n), 1.0) / (double)size;
+    return w;
+}
+
+std::vector<double> gto_orthonormalization(int size, double radius) {
+    auto w = gto_widths(size, radius);
+    std::vector<double> S((size_t)size * size);
+    for (int n1 = 0; n1 < size; n1++) {
+        for (int n2 = n1; n2 < size; n2++) {
+            double s1 = w[n1], s2 = w[n2];
+            double e = 0.5 * (3.0 + n1 + n2);
+            double v = std::pow(0.5 / (s1 * s1) + 0.5 / (s2 * s2), -e) / (soap::powi(s1, n1) * soap::powi(s2, n2)) *
+                       std::tgamma(e) / (std::pow(s1 * s2, 1.5) * std::sqrt(std::tgamma(n1 + 1.5) * std::tgamma(n2 + 1.5)));
+            S[(size_t)n1 * size + n2] = v;
+            S[(size_t)n2 * size + n1] = v;
+        }
+    }
+    std::vector<double> evals, evecs;
+    jacobi_eigen(S, size, evals, evecs);
+    for (int n = 0; n < size; n++) {
+        if (evals[n] <= soap::DBL_EPS) {
+            throw internal_error("radial overlap matrix is singular, try with a lower max_radial (current value is " +
+                                 std::to_string(size - 1) + ")");
+        }
+    }
+    std::vector<double> M((size_t)size * size, 0.0);
+    for (int i = 0; i < size; i++) {
+        for (int j = 0; j < size; j++) {
+            double s = 0.0;
+            for (int k = 0; k < size; k++) s += evecs[(size_t)i * size + k] / std::sqrt(evals[k]) * evecs[(size_t)j * size + k];
+            double norm = std::sqrt(2.0 / (soap::powi(w[j], 2 * j + 3) * std::tgamma(j + 1.5)));
+            M[(size_t)i * size + j] = s * norm;
+        }
+    }
+    return M;
+}
+
+}  // namespace
+
+void radial_integral_host(const RadialTables& t, int l, double r, double* values, double* grads) {
+    int N = t.nmax;
+    if (t.splined) {
+        const double* pos = &t.positions[t.knot_offset[l]];
+        int count = t.knot_count[l];
+        int k = soap::spline_interval(pos, count, r);
+        auto w = soap::hermite_weights(pos[k], pos[k + 1], r);
+        const double* pv = &t.values[((size_t)t.knot_offset[l] + k) * N];
+        const double* pd = &t.derivs[((size_t)t.knot_offset[l] + k) * N];
+        for (int n = 0; n < N; n++) {
+            values[n] = soap::hermite_value(w, pv[n], pd[n], pv[N + n], pd[N + n]);
+            if (grads) grads[n] = soap::hermite_derivative(w, pv[n], pd[n], pv[N + n], pd[N + n]);
+        }
+        return;
+    }
+    std::vector<double> v(N), g(N);
+    if (!soap::gto_radial_raw(l, N, r, t.c, t.width2, t.bn.data(), v.data(), grads ? g.data() : nullptr)) {
+        throw internal_error("Failed to compute radial integral with GTO basis. Try increasing decreasing the `cutoff`, "
+                             "or increasing the Gaussian's `width`.");
+    }
+    for (int k = 0; k < N; k++) {
+        double s = 0.0, sg = 0.0;
+        for (int n = 0; n < N; n++) {
+            s += v[n] * t.ortho[(size_t)k * N + n];
+            if (grads) sg += g[n] * t.ortho[(size_t)k * N + n];
+        }
+        values[k] = s;
+        if (grads) grads[k] = sg;
+    }
+}
+
+// Adaptive knots: 11 uniform points on [0, rc], then every interval midpoint
+// is added until the mean absolute or the mean relative interpolation error
+// at the midpoints drops below the accuracy (featomic/src/math/splines.rs:79-193,
+// limit of 10 000 points).
+RadialTables build_radial_tables(const Hypers& h) {
+    RadialTables t;
+    t.lmax = h.max_angular;
+    t.nmax = h.nmax();
+    t.splined = false;  // evaluate analytically while building the knots
+    t.c = 1.0 / (2.0 * h.density_width * h.density_width);
+    t.width2 = h.density_width * h.density_width;
+    for (double s : gto_widths(t.nmax, h.cutoff)) t.bn.push_back(1.0 / (2.0 * s * s));
+    t.ortho = gto_orthonormalization(t.nmax, h.cutoff);
+    int N = t.nmax;
+
+    std::vector<double> all_pos, all_val, all_der;
+    std::vector<int32_t> offsets, counts;
+    if (h.splined) {
+        for (int l = 0; l <= h.max_angular; l++) {
+            std::vector<double> pos, val, der;
+            auto eval = [&](double x, std::vector<double>& v, std::vector<double>& d) {
+                v.assign(N, 0.0);
+                d.assign(N, 0.0);
+                radial_integral_host(t, l, x, v.data(), d.data());
+            };
+            const int initial = 11;
+            double step = (h.cutoff - 0.0) / (double)(initial - 1);
+            std::vector<double> v, d;
+            for (int k = 0; k < initial - 1; k++) {
+                double x = 0.0 + (double)k * step;
+                eval(x, v, d);
+                pos.push_back(x);
+                val.insert(val.end(), v.begin(), v.end());
+                der.insert(der.end(), d.begin(), d.end());
+            }
+            eval(h.cutoff, v, d);
+            pos.push_back(h.cutoff);
+            val.insert(val.end(), v.begin(), v.end());
+            der.insert(der.end(), d.begin(), d.end());
+
+            std::vector<double> interp(N);
+            while (true) {
+                double mean_abs = 0.0, mean_rel = 0.0;
+                size_t count = 0;
+                std::vector<double> mid_pos, mid_val, mid_der;
+                for (size_t k = 0; k + 1 < pos.size(); k++) {
+                    double x = (pos[k] + pos[k + 1]) / 2.0;
+                    eval(x, v, d);
+                    auto w = soap::hermite_weights(pos[k], pos[k + 1], x);
+                    for (int n = 0; n < N; n++) {
+                        double s = soap::hermite_value(w, val[k * N + n], der[k * N + n], val[(k + 1) * N + n], der[(k + 1) * N + n]);
+                        mean_abs += std::fabs(s - v[n]);
+                        mean_rel += std::fabs((s - v[n]) / v[n]);
+                        count++;
+                    }
+                    mid_pos.push_back(x);
+                    mid_val.insert(mid_val.end(), v.begin(), v.end());
+                    mid_der.insert(mid_der.end(), d.begin(), d.end());
+                }
+                mean_abs /= (double)count;
+                mean_rel /= (double)count;
+                if (mean_abs < h.spline_accuracy || mean_rel < h.spline_accuracy) break;
+                if (pos.size() + mid_pos.size() > 10000) {
+                    std::ostringstream m;
+                    m << "failed to reach requested accuracy (" << h.spline_accuracy
+                      << ") in spline interpolation, mean absolute error is " << mean_abs
+                      << " and mean relative error is " << mean_rel;
+                    throw internal_error(m.str());
+                }
+                std::vector<double> p2, v2, d2;
+                for (size_t k = 0; k < pos.size(); k++) {
+                    p2.push_back(pos[k]);
+                    v2.insert(v2.end(), val.begin() + k * N, val.begin() + (k + 1) * N);
+                    d2.insert(d2.end(), der.begin() + k * N, der.begin() + (k + 1) * N);
+                    if (k < mid_pos.size()) {
+                        p2.push_back(mid_pos[k]);
+                        v2.insert(v2.end(), mid_val.begin() + k * N, mid_val.begin() + (k + 1) * N);
+                        d2.insert(d2.end(), mid_der.begin() + k * N, mid_der.begin() + (k + 1) * N);
+                    }
+                }
+                pos.swap(p2);
+                val.swap(v2);
+                der.swap(d2);
+            }
+            offsets.push_back((int32_t)all_pos.size());
+            counts.push_back((int32_t)pos.size());
+            all_pos.insert(all_pos.end(), pos.begin(), pos.end());
+            all_val.insert(all_val.end(), val.begin(), val.end());
+            all_der.insert(all_der.end(), der.begin(), der.end());
+        }
+        t.knot_offset = offsets;
+        t.knot_count = counts;
+        t.positions = all_pos;
+        t.values = all_val;
+        t.derivs = all_der;
+        t.splined = true;
+    }
+
+    // self contribution: centre weight * f(0) * Y00(z) * I_n^{l=0}(0)
+    std::vector<double> r0(N);
+    radial_integral_host(t, 0, 0.0, r0.data(), nullptr);
+    double f0, df0;
+    soap::cutoff_function(h.smoothing, h.cutoff, h.smoothing_width, 0.0, &f0, &df0);
+    double scale = 1.0;
+    if (h.scaling) {
+        double ds;
+        soap::willatt2018(h.scaling_scale, h.scaling_rate, h.scaling_exponent, 0.0, &scale, &ds);
+    }
+    const double y00 = 0.3989422804014327 / 1.4142135623730951;  // P_0^0 / sqrt(2)
+    double factor = h.center_atom_weight * (scale * f0) * y00;
+    t.self_contribution.resize(N);
+    for (int n = 0; n < N; n++) t.self_contribution[n] = factor * r0[n];
+    return t;
+}
+
+// Constant factors of the Legendre recursion and of the derivative factors,
+// featomic/src/math/spherical_harmonics.rs:203-301 (same expressions, hoisted
+// out of the per-pair evaluation).
+YlmTables build_ylm_tables(int lmax) {
+    YlmTables t;
+    t.lmax = lmax;
+    size_t n = (size_t)(lmax + 1) * (lmax + 2) / 2;
+    t.A.assign(n, 0.0);
+    t.B.assign(n, 0.0);
+    t.sq_plus.assign(n, 0.0);
+    t.sq_minus.assign(n, 0.0);
+    t.sq_2l1.assign(lmax + 1, 0.0);
+    t.sq_half.assign(lmax + 1, 0.0);
+    t.sq_ll1.assign(lmax + 1, 0.0);
+    t.inv_ll.assign(lmax + 1, 0.0);
+    auto li = [](int l, int m) { return (size_t)(m + l * (l + 1) / 2); };
+    for (int l = 2; l <= lmax; l++) {
+        double ls = (double)(l * l), lm1s = (double)((l - 1) * (l - 1));
+        for (int m = 0; m < l - 1; m++) {
+            double ms = (double)(m * m);
+            t.A[li(l, m)] = std::sqrt((4.0 * ls - 1.0) / (ls - ms));
+            t.B[li(l, m)] = -std::sqrt((lm1s - ms) / (4.0 * lm1s - 1.0));
+        }
+    }
+    for (int l = 0; l <= lmax; l++) {
+        t.sq_2l1[l] = std::sqrt(2.0 * (double)l + 1.0);
+        t.sq_half[l] = l > 0 ? std::sqrt(1.0 + 0.5 / (double)l) : 0.0;
+        t.sq_ll1[l] = std::sqrt(0.5 * (double)(l * (l + 1)));
+        t.inv_ll[l] = l > 0 ? -1.0 / (double)(l * l + l) : 0.0;
+        for (int m = 0; m <= l; m++) {
+            t.sq_plus[li(l, m)] = std::sqrt((double)((l + m) * (l - m + 1)));
+            t.sq_minus[li(l, m)] = std::sqrt((double)((l - m) * (l + m + 1)));
+        }
+    }
+    return t;
+}
+
+}  // namespace fb200
