@@ -185,6 +185,16 @@ featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t
                                               double cutoff, featomic_pair_t* pairs, uintptr_t capacity,
                                               uintptr_t* count);
 
+/* Radial integral R_nl(r) and dR_nl/dr of this calculator, as the kernels see
+ * it (the Hermite spline of featomic/src/calculators/soap/radial_integral/
+ * spline.rs, or the analytic GTO integral of radial_integral/gto.rs when
+ * spline_accuracy is null), evaluated on the host for `n_r` distances:
+ * values / gradients are [n_r][max_angular + 1][max_radial + 1].
+ * `knots`, when not NULL, receives the number of spline knots of each angular
+ * channel ([max_angular + 1], 0 for the analytic integral). */
+featomic_status_t featomic_b200_radial_integral(const featomic_calculator_t* calculator, const double* r,
+                                                uintptr_t n_r, double* values, double* gradients, int32_t* knots);
+
 /* Per-phase device time (ms) of the last compute call of this calculator:
  * [neighbours, host metadata, pair features, expansion, contraction,
  *  device->host transfer, total wall, power-spectrum values kernel,

@@ -23,6 +23,10 @@ BUILD = os.path.join(HERE, "_build")
 LIBRARY = os.path.join(HERE, "libfeatomic_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# The FP64 drop-in kernels evaluate featomic's expressions in featomic's order
+# without contracting a*b+c into FMAs (rustc never contracts), so that sums
+# that cancel keep the reference's rounding.
+DEVICE = ["-fmad=false"]
 COMMON = [
     "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
     f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}", "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets",
@@ -54,7 +58,7 @@ def up_to_date():
 
 def _compile(src, verbose):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    cmd = [nvcc()] + ARCH + COMMON + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + ARCH + DEVICE + COMMON + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [nvcc(), "-x", "c++"] + COMMON + ["-c", src, "-o", obj]
     if verbose:

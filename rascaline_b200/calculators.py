@@ -349,6 +349,21 @@ class CalculatorBase:
                                                                 opts, ctypes.c_void_p(stream)))
         return TensorMap(out)
 
+    def radial_integral(self, r):
+        """(values, gradients, knots): the radial integral the kernels use,
+        evaluated on the host, shapes [len(r), max_angular + 1, max_radial + 1]."""
+        h = json.loads(self._parameters)
+        L = h["basis"]["max_angular"]
+        N = h["basis"]["radial"]["max_radial"] + 1
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        values = np.zeros((len(r), L + 1, N))
+        grads = np.zeros((len(r), L + 1, N))
+        knots = np.zeros(L + 1, dtype=np.int32)
+        dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+        C.check(C.lib().featomic_b200_radial_integral(self._handle, dp(r), len(r), dp(values), dp(grads),
+                                                      knots.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return values, grads, knots
+
     def timings(self):
         """Per-phase time (ms) of the last call."""
         out = (ctypes.c_double * 10)()

@@ -367,6 +367,28 @@ featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t
     });
 }
 
+featomic_status_t featomic_b200_radial_integral(const featomic_calculator_t* calculator, const double* r,
+                                                uintptr_t n_r, double* values, double* gradients, int32_t* knots) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        const RadialTables& t = calculator->impl->engine->radial();
+        if (n_r > 0) {
+            CHECK_POINTER(r);
+            CHECK_POINTER(values);
+        }
+        size_t per = (size_t)(t.lmax + 1) * t.nmax;
+        for (uintptr_t k = 0; k < n_r; k++) {
+            if (!(r[k] >= 0.0 && r[k] <= calculator->impl->hypers.cutoff))
+                throw invalid_parameter("distances must be in [0, cutoff]");
+            for (int l = 0; l <= t.lmax; l++)
+                radial_integral_host(t, l, r[k], values + k * per + (size_t)l * t.nmax,
+                                     gradients ? gradients + k * per + (size_t)l * t.nmax : nullptr);
+        }
+        if (knots)
+            for (int l = 0; l <= t.lmax; l++) knots[l] = t.splined ? t.knot_count[l] : 0;
+    });
+}
+
 featomic_status_t featomic_b200_calculator_timings(const featomic_calculator_t* calculator, double* times,
                                                    uintptr_t count) {
     return guarded([&] {

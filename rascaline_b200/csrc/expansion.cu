@@ -209,7 +209,7 @@ __global__ void pair_features_kernel(DevicePairs pairs, DeviceRadial radial, Dev
     if (!ok) atomicExch(status, 1);
 }
 
-__global__ void se_accumulate_kernel(SeArgs a) {
+__global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
     const FeatureLayout L = a.layout;
     const int64_t c = blockIdx.x;
     const int S = a.n_species;
@@ -391,7 +391,7 @@ void launch_pair_features(const DevicePairs& pairs, const DeviceRadial& radial, 
 void launch_se_accumulate(const SeArgs& args, cudaStream_t stream) {
     if (args.n_centres == 0) return;
     int K = args.layout.L2 * args.layout.nmax;
-    int threads = std::min(1024, (K + 31) / 32 * 32);
+    int threads = std::min(256, (K + 31) / 32 * 32);
     se_accumulate_kernel<<<(unsigned)args.n_centres, threads, 0, stream>>>(args);
     CUDA_CHECK(cudaGetLastError());
 }

@@ -189,47 +189,164 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top) {
 // ---------------------------------------------------------------------------
 // GTO radial basis: widths sigma_n = rc max(sqrt n, 1) / n_max and the
 // orthonormalisation S^{-1/2} diag(norm) of the analytic overlap
-// (featomic/src/calculators/shared/basis/radial/gto.rs:17-75).  The inverse
-// square root uses a cyclic Jacobi eigen-decomposition.
+// (featomic/src/calculators/shared/basis/radial/gto.rs:17-75).
 // ---------------------------------------------------------------------------
 namespace {
 
-void jacobi_eigen(std::vector<double>& a, int n, std::vector<double>& evals, std::vector<double>& evecs) {
-    evecs.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; i++) evecs[(size_t)i * n + i] = 1.0;
-    for (int sweep = 0; sweep < 100; sweep++) {
-        double off = 0.0;
-        for (int i = 0; i < n; i++)
-            for (int j = i + 1; j < n; j++) off += a[(size_t)i * n + j] * a[(size_t)i * n + j];
-        if (off < 1e-300) break;
-        for (int p = 0; p < n; p++) {
-            for (int q = p + 1; q < n; q++) {
-                double apq = a[(size_t)p * n + q];
-                if (apq == 0.0) continue;
-                double app = a[(size_t)p * n + p], aqq = a[(size_t)q * n + q];
-                double theta = (aqq - app) / (2.0 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-                for (int k = 0; k < n; k++) {
-                    double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
-                    a[(size_t)k * n + p] = c * akp - s * akq;
-                    a[(size_t)k * n + q] = s * akp + c * akq;
+// Eigen-decomposition of a real symmetric matrix: Householder reduction to
+// tridiagonal form followed by the implicit QL algorithm (EISPACK tred2 /
+// tql2, Bowdler, Martin, Reinsch and Wilkinson, Handbook for Automatic
+// Computation vol. II), eigenvalues sorted in increasing order.  featomic
+// uses this algorithm (featomic/src/math/eigen.rs:23-244); the overlap matrix
+// is ill-conditioned, so S^{-1/2} depends on the solver at 5e-11 (8 radial
+// functions) to 2e-8 (12) and the same solver is needed to agree with
+// featomic.  `v` is row-major n x n: the input matrix on entry, the
+// eigenvectors (columns) on exit.
+void symmetric_eigen(std::vector<double>& v, int n, std::vector<double>& d) {
+    auto V = [&](int i, int j) -> double& { return v[(size_t)i * n + j]; };
+    std::vector<double> e(n, 0.0);
+    d.assign(n, 0.0);
+    for (int j = 0; j < n; j++) d[j] = V(n - 1, j);
+    for (int i = n - 1; i > 0; i--) {
+        double scale = 0.0, h = 0.0;
+        for (int k = 0; k < i; k++) scale += std::fabs(d[k]);
+        if (scale == 0.0) {
+            e[i] = d[i - 1];
+            for (int j = 0; j < i; j++) {
+                d[j] = V(i - 1, j);
+                V(i, j) = 0.0;
+                V(j, i) = 0.0;
+            }
+        } else {
+            for (int k = 0; k < i; k++) {
+                d[k] /= scale;
+                h += d[k] * d[k];
+            }
+            double f = d[i - 1];
+            double g = std::sqrt(h);
+            if (f > 0) g = -g;
+            e[i] = scale * g;
+            h -= f * g;
+            d[i - 1] = f - g;
+            for (int j = 0; j < i; j++) e[j] = 0.0;
+            for (int j = 0; j < i; j++) {
+                f = d[j];
+                V(j, i) = f;
+                g = e[j] + V(j, j) * f;
+                for (int k = j + 1; k <= i - 1; k++) {
+                    g += V(k, j) * d[k];
+                    e[k] += V(k, j) * f;
                 }
-                for (int k = 0; k < n; k++) {
-                    double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
-                    a[(size_t)p * n + k] = c * apk - s * aqk;
-                    a[(size_t)q * n + k] = s * apk + c * aqk;
-                }
-                for (int k = 0; k < n; k++) {
-                    double vkp = evecs[(size_t)k * n + p], vkq = evecs[(size_t)k * n + q];
-                    evecs[(size_t)k * n + p] = c * vkp - s * vkq;
-                    evecs[(size_t)k * n + q] = s * vkp + c * vkq;
-                }
+                e[j] = g;
+            }
+            f = 0.0;
+            for (int j = 0; j < i; j++) {
+                e[j] /= h;
+                f += e[j] * d[j];
+            }
+            double hh = f / (h + h);
+            for (int j = 0; j < i; j++) e[j] -= hh * d[j];
+            for (int j = 0; j < i; j++) {
+                f = d[j];
+                g = e[j];
+                for (int k = j; k <= i - 1; k++) V(k, j) -= (f * e[k] + g * d[k]);
+                d[j] = V(i - 1, j);
+                V(i, j) = 0.0;
             }
         }
+        d[i] = h;
     }
-    evals.resize(n);
-    for (int i = 0; i < n; i++) evals[i] = a[(size_t)i * n + i];
+    for (int i = 0; i < n - 1; i++) {
+        V(n - 1, i) = V(i, i);
+        V(i, i) = 1.0;
+        double h = d[i + 1];
+        if (h != 0.0) {
+            for (int k = 0; k <= i; k++) d[k] = V(k, i + 1) / h;
+            for (int j = 0; j <= i; j++) {
+                double g = 0.0;
+                for (int k = 0; k <= i; k++) g += V(k, i + 1) * V(k, j);
+                for (int k = 0; k <= i; k++) V(k, j) -= g * d[k];
+            }
+        }
+        for (int k = 0; k <= i; k++) V(k, i + 1) = 0.0;
+    }
+    for (int j = 0; j < n; j++) {
+        d[j] = V(n - 1, j);
+        V(n - 1, j) = 0.0;
+    }
+    V(n - 1, n - 1) = 1.0;
+    e[0] = 0.0;
+
+    // implicit QL
+    for (int i = 1; i < n; i++) e[i - 1] = e[i];
+    e[n - 1] = 0.0;
+    double f = 0.0, tst1 = 0.0;
+    for (int l = 0; l < n; l++) {
+        tst1 = std::max(tst1, std::fabs(d[l]) + std::fabs(e[l]));
+        int m = l;
+        while (m < n) {
+            if (std::fabs(e[m]) <= soap::DBL_EPS * tst1) break;
+            m++;
+        }
+        if (m > l) {
+            for (int iter = 0; iter < 10000; iter++) {
+                double g = d[l];
+                double p = (d[l + 1] - g) / (2.0 * e[l]);
+                double r = std::hypot(p, 1.0);
+                if (p < 0) r = -r;
+                d[l] = e[l] / (p + r);
+                d[l + 1] = e[l] * (p + r);
+                double dl1 = d[l + 1];
+                double h = g - d[l];
+                for (int i = l + 2; i < n; i++) d[i] -= h;
+                f += h;
+                p = d[m];
+                double c = 1.0, c2 = c, c3 = c;
+                double el1 = e[l + 1];
+                double s = 0.0, s2 = 0.0;
+                for (int i = m - 1; i >= l; i--) {
+                    c3 = c2;
+                    c2 = c;
+                    s2 = s;
+                    g = c * e[i];
+                    h = c * p;
+                    r = std::hypot(p, e[i]);
+                    e[i + 1] = s * r;
+                    s = e[i] / r;
+                    c = p / r;
+                    p = c * d[i] - s * g;
+                    d[i + 1] = h + s * (c * g + s * d[i]);
+                    for (int k = 0; k < n; k++) {
+                        h = V(k, i + 1);
+                        V(k, i + 1) = s * V(k, i) + c * h;
+                        V(k, i) = c * V(k, i) - s * h;
+                    }
+                }
+                p = -s * s2 * c3 * el1 * e[l] / dl1;
+                e[l] = s * p;
+                d[l] = c * p;
+                if (std::fabs(e[l]) <= soap::DBL_EPS * tst1) break;
+            }
+        }
+        d[l] += f;
+        e[l] = 0.0;
+    }
+    // selection sort of the eigenvalues (and their vectors), increasing
+    for (int i = 0; i < n - 1; i++) {
+        int k = i;
+        double p = d[i];
+        for (int j = i + 1; j < n; j++) {
+            if (d[j] < p) {
+                k = j;
+                p = d[j];
+            }
+        }
+        if (k != i) {
+            d[k] = d[i];
+            d[i] = p;
+            for (int j = 0; j < n; j++) std::swap(V(j, i), V(j, k));
+        }
+    }
 }
 
 std::vector<double> gto_widths(int size, double radius) {
@@ -242,29 +359,34 @@ std::vector<double> gto_orthonormalization(int size, double radius) {
     auto w = gto_widths(size, radius);
     std::vector<double> S((size_t)size * size);
     for (int n1 = 0; n1 < size; n1++) {
+        double s1 = w[n1], s1sq = s1 * s1;
         for (int n2 = n1; n2 < size; n2++) {
-            double s1 = w[n1], s2 = w[n2];
-            double e = 0.5 * (3.0 + n1 + n2);
-            double v = std::pow(0.5 / (s1 * s1) + 0.5 / (s2 * s2), -e) / (soap::powi(s1, n1) * soap::powi(s2, n2)) *
-                       std::tgamma(e) / (std::pow(s1 * s2, 1.5) * std::sqrt(std::tgamma(n1 + 1.5) * std::tgamma(n2 + 1.5)));
-            S[(size_t)n1 * size + n2] = v;
+            double s2 = w[n2], s2sq = s2 * s2;
+            double e = 0.5 * (3.0 + (double)n1 + (double)n2);
+            double v = std::pow(0.5 / s1sq + 0.5 / s2sq, -e) / (soap::powi(s1, n1) * soap::powi(s2, n2)) * soap::gamma_fn(e) /
+                       (std::pow(s1 * s2, 1.5) * std::sqrt(soap::gamma_fn((double)n1 + 1.5) * soap::gamma_fn((double)n2 + 1.5)));
             S[(size_t)n2 * size + n1] = v;
+            S[(size_t)n1 * size + n2] = v;
         }
     }
-    std::vector<double> evals, evecs;
-    jacobi_eigen(S, size, evals, evecs);
+    std::vector<double> evals;
+    symmetric_eigen(S, size, evals);
     for (int n = 0; n < size; n++) {
         if (evals[n] <= soap::DBL_EPS) {
             throw internal_error("radial overlap matrix is singular, try with a lower max_radial (current value is " +
                                  std::to_string(size - 1) + ")");
         }
+        evals[n] = 1.0 / std::sqrt(evals[n]);
     }
-    std::vector<double> M((size_t)size * size, 0.0);
+    // (V diag(1/sqrt(lambda))) V^T diag(norm)
+    std::vector<double> vd((size_t)size * size), M((size_t)size * size, 0.0);
+    for (int i = 0; i < size; i++)
+        for (int j = 0; j < size; j++) vd[(size_t)i * size + j] = S[(size_t)i * size + j] * evals[j];
     for (int i = 0; i < size; i++) {
         for (int j = 0; j < size; j++) {
             double s = 0.0;
-            for (int k = 0; k < size; k++) s += evecs[(size_t)i * size + k] / std::sqrt(evals[k]) * evecs[(size_t)j * size + k];
-            double norm = std::sqrt(2.0 / (soap::powi(w[j], 2 * j + 3) * std::tgamma(j + 1.5)));
+            for (int k = 0; k < size; k++) s += vd[(size_t)i * size + k] * S[(size_t)j * size + k];
+            double norm = std::sqrt(2.0 / (soap::powi(w[j], 2 * j + 3) * soap::gamma_fn((double)j + 1.5)));
             M[(size_t)i * size + j] = s * norm;
         }
     }

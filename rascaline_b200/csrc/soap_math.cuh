@@ -11,7 +11,7 @@
 // * the Willatt2018 radial scaling follows
 //   featomic/src/calculators/shared/density.rs:108-128.
 //
-// Gamma functions use the C library's / CUDA's tgamma and lgamma.
+// Gamma functions use the Lanczos approximation below (host and device).
 #pragma once
 
 #include <cmath>
@@ -27,12 +27,54 @@ namespace soap {
 
 #ifndef __CUDA_ARCH__
 using std::isfinite;
-using std::lgamma;
-using std::tgamma;
 #endif
 
 constexpr double PI = 3.14159265358979323846;
 constexpr double DBL_EPS = 2.220446049250313e-16;
+
+// Gamma and log-Gamma by the Lanczos approximation with g = 10.900511 and the
+// 11-term coefficient table of G. R. Pugh, "An Analysis of the Lanczos Gamma
+// Approximation" (2004), p. 116 -- the approximation featomic uses
+// (featomic/src/math/gamma.rs:20-92).  The GTO overlap matrix is
+// ill-conditioned (condition number 3e4 at 8 radial functions, 4e7 at 12), so
+// its inverse square root, and every radial integral after it, moves by
+// cond * (relative change of the Gamma values): the same Gamma is needed to
+// agree with featomic to 1e-10.
+SOAP_HD double lanczos_series(double x, bool reflected) {
+    const double dk[11] = {
+        2.4857408913875355e-5, 1.0514237858172197, -3.4568709722201625, 4.512277094668948,
+        -2.9828522532357664, 1.056397115771267, -1.9542877319164587e-1, 1.709705434044412e-2,
+        -5.719261174043057e-4, 4.633994733599057e-6, -2.7199490848860772e-9,
+    };
+    double s = dk[0];
+    for (int t = 1; t < 11; t++) s = s + dk[t] / (reflected ? ((double)t - x) : (x + (double)t - 1.0));
+    return s;
+}
+
+SOAP_HD double gamma_fn(double x) {
+    const double two_sqrt_e_over_pi = 1.8603827342052657;
+    const double r = 10.900511;
+    const double e = 2.718281828459045;
+    if (x < 0.5) {
+        double s = lanczos_series(x, true);
+        return PI / (sin(PI * x) * s * two_sqrt_e_over_pi * pow((0.5 - x + r) / e, 0.5 - x));
+    }
+    double s = lanczos_series(x, false);
+    return s * two_sqrt_e_over_pi * pow((x - 0.5 + r) / e, x - 0.5);
+}
+
+SOAP_HD double ln_gamma_fn(double x) {
+    const double ln_pi = 1.1447298858494002;
+    const double ln_2_sqrt_e_over_pi = 0.6207822376352452;
+    const double r = 10.900511;
+    const double e = 2.718281828459045;
+    if (x < 0.5) {
+        double s = lanczos_series(x, true);
+        return ln_pi - log(sin(PI * x)) - log(s) - ln_2_sqrt_e_over_pi - (0.5 - x) * log((0.5 - x + r) / e);
+    }
+    double s = lanczos_series(x, false);
+    return log(s) + ln_2_sqrt_e_over_pi + (x - 0.5) * log((x - 0.5 + r) / e);
+}
 
 // b^n by repeated squaring (the lowering of f64::powi)
 SOAP_HD double powi(double a, int b) {
@@ -117,11 +159,11 @@ SOAP_HD double hyp1f1_chgm(double a, double b, double x) {
                     result += term;
                     if (result != 0.0 && fabs(term / result) < 1e-15) break;
                 }
-                result *= pow(x, a - b) * tgamma(b) / tgamma(a);
+                result *= pow(x, a - b) * gamma_fn(b) / gamma_fn(a);
                 if (x0 > 0.0) result *= exp(x);
             }
         } else {
-            double lga = lgamma(a), lgb = lgamma(b), lgba = lgamma(b - a);
+            double lga = ln_gamma_fn(a), lgb = ln_gamma_fn(b), lgba = ln_gamma_fn(b - a);
             double s1 = 1.0, s2 = 1.0, t1 = 1.0, t2 = 1.0;
             for (int i = 1; i <= 30; i++) {
                 double fi = (double)i;
@@ -177,7 +219,7 @@ SOAP_HD bool gto_radial_raw(int l, int nmax, double r, double c, double width2, 
     for (int n = 0; n < nmax; n++) {
         double z = c_rij * c_rij / (c + bn[n]);
         double a = 0.5 * (double)(n + l + 3), b = (double)l + 1.5;
-        double ratio = tgamma(a) / tgamma(b);
+        double ratio = gamma_fn(a) / gamma_fn(b);
         double v = ratio * hyp1f1(a, b, z);
         if (!isfinite(v)) ok = false;
         double c_dn = pow(c + bn[n], -(0.5 * (double)(n + l) + 1.5));
@@ -196,7 +238,7 @@ SOAP_HD bool gto_radial_raw(int l, int nmax, double r, double c, double width2, 
             if (l == 1) {
                 double a = 0.5 * (double)(n + l) + 1.5;
                 double c_dn = pow(c + bn[n], -a);
-                grad[n] = tgamma(a) / tgamma(2.5) * (global * c * c_dn);
+                grad[n] = gamma_fn(a) / gamma_fn(2.5) * (global * c * c_dn);
             } else {
                 grad[n] = 0.0;
             }
