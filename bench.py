@@ -227,7 +227,13 @@ def main():
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--atoms", type=int, default=1000,
+                        help="atoms in the box (1000 is the benchmark; smaller boxes are for profiling)")
     args = parser.parse_args()
+    global N_ATOMS, WORKLOAD
+    if args.atoms != N_ATOMS:
+        N_ATOMS = args.atoms
+        WORKLOAD = WORKLOAD.replace("random_box_1000", f"random_box_{N_ATOMS}")
     if args.impl == "reference":
         return run_reference(args)
 

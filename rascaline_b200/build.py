@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # that cancel keep the reference's rounding.
 DEVICE = ["-fmad=false"]
 COMMON = [
-    "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+    "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fopenmp",
     f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}", "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets",
 ]
 
@@ -82,7 +82,7 @@ def build(force=False, verbose=False, jobs=None):
                 sys.stderr.write(log)
     objects = [r[0] for r in results]
     tmp = LIBRARY + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objects
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objects + ["-lgomp"]
     out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{out.stdout}\n{out.stderr}")

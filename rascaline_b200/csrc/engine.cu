@@ -166,7 +166,8 @@ struct PinnedPool {
     std::vector<std::pair<void*, size_t>> free_list;
     size_t cached = 0;
 
-    void* get(size_t bytes) {
+    // returns the buffer and its real size (a recycled buffer can be larger)
+    void* get(size_t bytes, size_t* actual) {
         {
             std::lock_guard<std::mutex> lock(mutex);
             size_t best = (size_t)-1;
@@ -174,12 +175,14 @@ struct PinnedPool {
                 if (free_list[k].second >= bytes && (best == (size_t)-1 || free_list[k].second < free_list[best].second)) best = k;
             if (best != (size_t)-1) {
                 void* p = free_list[best].first;
+                *actual = free_list[best].second;
                 cached -= free_list[best].second;
                 free_list.erase(free_list.begin() + best);
                 return p;
             }
         }
         void* p = nullptr;
+        *actual = bytes;
         if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
             p = std::malloc(bytes);
@@ -260,6 +263,11 @@ void Engine::upload_tables() {
     if (tables_ready_ && dev == device_) return;
     if (tables_ready_) throw invalid_parameter("a calculator can only be used on the device it first ran on");
     device_ = dev;
+    // keep the memory of freed device TensorMaps in the default pool
+    cudaMemPool_t pool;
+    CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t threshold = UINT64_MAX;
+    CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
     auto put = [&](const void* src, size_t bytes) -> void* {
         void* d = nullptr;
         CUDA_CHECK(cudaMalloc(&d, bytes > 0 ? bytes : 8));
@@ -407,9 +415,11 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
     int64_t total = plan.total_doubles;
     double* d_out = nullptr;
     if (device_output) {
+        // stream-ordered allocation from the device's default pool, which keeps
+        // freed memory for reuse: no device-wide synchronisation per call
         void* p = nullptr;
-        CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(8, sizeof(double) * (size_t)total)));
-        tm->storage = std::shared_ptr<void>(p, [](void* q) { cudaFree(q); });
+        CUDA_CHECK(cudaMallocAsync(&p, std::max<size_t>(8, sizeof(double) * (size_t)total), stream));
+        tm->storage = std::shared_ptr<void>(p, [](void* q) { cudaFreeAsync(q, nullptr); });
         d_out = (double*)p;
     } else {
         d_out = arena_.alloc<double>("output", total);
@@ -464,18 +474,14 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
             pa.slots = upload(arena_, "ps.slots", plan.slots, stream);
             pa.entry_offset = upload(arena_, "ps.entry_offset", nh.entry_offset, stream);
             pa.entries = upload(arena_, "ps.entries", nh.entries, stream);
-            pa.row_offset = upload(arena_, "ps.row_offset", plan.row_offset, stream);
-            pa.rows = upload(arena_, "ps.rows", plan.rows, stream);
+            pa.entry_cum = upload(arena_, "ps.entry_cum", nh.entry_cum, stream);
+            pa.slot_row = upload(arena_, "ps.slot_row", plan.slot_row, stream);
             pa.off_values = upload(arena_, "ps.offv", offv, stream);
             pa.off_positions = upload(arena_, "ps.offp", offp, stream);
             pa.off_strain = upload(arena_, "ps.offs", offs, stream);
             pa.off_cell = upload(arena_, "ps.offc", offc, stream);
             pa.out = d_out;
-            launch_ps_values(pa, stream);
-            CUDA_CHECK(cudaEventRecord(ev[8], stream));
-            if (g.positions) launch_ps_positions(pa, stream);
-            CUDA_CHECK(cudaEventRecord(ev[9], stream));
-            if (g.strain || g.cell) launch_ps_strain_cell(pa, g.strain, g.cell, stream);
+            launch_power_spectrum(pa, g.positions, g.strain, g.cell, stream, ev[8], ev[9]);
         } else {
             SeOutArgs so{};
             so.lmax = h_.max_angular;
@@ -525,9 +531,10 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
     double* base = d_out;
     if (!device_output) {
         size_t bytes = std::max<size_t>(8, sizeof(double) * (size_t)total);
-        void* host = pinned_pool().get(bytes);
+        size_t actual = 0;
+        void* host = pinned_pool().get(bytes, &actual);
         bool pinned = is_pinned(host);
-        tm->storage = std::shared_ptr<void>(host, [bytes, pinned](void* q) { pinned_pool().put(q, bytes, pinned); });
+        tm->storage = std::shared_ptr<void>(host, [actual, pinned](void* q) { pinned_pool().put(q, actual, pinned); });
         if (total) CUDA_CHECK(cudaMemcpyAsync(host, d_out, sizeof(double) * total, cudaMemcpyDeviceToHost, stream));
         base = (double*)host;
     }
@@ -539,7 +546,7 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
     for (size_t b = 0; b < plan.blocks.size(); b++) {
         auto& bp = plan.blocks[b];
         auto blk = std::make_unique<Block>();
-        blk->samples = bp.samples;
+        blk->samples = std::move(bp.samples);
         blk->properties = properties;
         std::vector<Labels> comps;
         std::vector<size_t> comp_shape;
@@ -557,7 +564,7 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
         blk->data = base + bp.off_values;
         if (g.positions) {
             auto gb = std::make_unique<Block>();
-            gb->samples = bp.gradient_samples;
+            gb->samples = std::move(bp.gradient_samples);
             gb->components = {xyz_labels("xyz")};
             gb->components.insert(gb->components.end(), comps.begin(), comps.end());
             gb->properties = properties;

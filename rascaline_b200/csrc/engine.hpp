@@ -180,8 +180,10 @@ struct PsArgs {
     const PsKeySlot* slots;
     const int64_t* entry_offset;    // [n_centres + 1]
     const PsEntry* entries;
-    const int64_t* row_offset;      // [n_centres + 1], into rows: entries x slots
-    const int64_t* rows;            // gradient row in the block, or -1
+    // per entry: [S] number of earlier neighbours of each species in the
+    // centre's list, then [S] = 1 if the centre itself comes earlier
+    const int32_t* entry_cum;
+    const int64_t* slot_row;        // first positions-gradient row of each slot
     const int64_t* off_values;      // per block, offsets into `out` (doubles)
     const int64_t* off_positions;
     const int64_t* off_strain;
@@ -189,9 +191,10 @@ struct PsArgs {
     double* out;
 };
 
-void launch_ps_values(const PsArgs& args, cudaStream_t stream);
-void launch_ps_positions(const PsArgs& args, cudaStream_t stream);
-void launch_ps_strain_cell(const PsArgs& args, bool strain, bool cell, cudaStream_t stream);
+// values, then positions / strain / cell rows; events (may be null) are
+// recorded after the values and after the positions kernels
+void launch_power_spectrum(const PsArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream,
+                           cudaEvent_t after_values, cudaEvent_t after_positions);
 
 // Spherical expansion output scatter (spherical_expansion calculator)
 struct SeOutArgs {

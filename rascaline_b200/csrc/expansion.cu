@@ -209,17 +209,30 @@ __global__ void pair_features_kernel(DevicePairs pairs, DeviceRadial radial, Dev
     if (!ok) atomicExch(status, 1);
 }
 
+// Per-direction scalars staged in shared memory for a chunk of directions
+struct DirScalars {
+    double f, fg, r, u[3], v[3], sh[3];
+    int64_t feature;  // offset of the pair's feature record
+    int inv, self_image;
+};
+
+constexpr int SE_CHUNK = 32;
+
+template <bool POS, bool STRAIN, bool CELL>
 __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
+    constexpr bool GRAD = POS || STRAIN || CELL;
+    __shared__ DirScalars dirs[SE_CHUNK];
     const FeatureLayout L = a.layout;
     const int64_t c = blockIdx.x;
     const int S = a.n_species;
     const int K = L.L2 * L.nmax;
     const int tc = a.centre_species[c];
-    const bool grad = L.with_grad && (a.do_positions || a.do_strain || a.do_cell);
 
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        const int lm = k / L.nmax;
-        const int n = k - lm * L.nmax;
+    for (int k0 = 0; k0 < K; k0 += blockDim.x) {
+        const int k = k0 + threadIdx.x;
+        const bool active = k < K;
+        const int lm = active ? k / L.nmax : 0;
+        const int n = active ? k - lm * L.nmax : 0;
         int l = (int)sqrt((double)lm);
         while (l * l > lm) l--;
         while ((l + 1) * (l + 1) <= lm) l++;
@@ -229,80 +242,100 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
         for (int t = 0; t < S; t++) {
             const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
             double acc = 0.0;
-            double sg0 = 0.0, sg1 = 0.0, sg2 = 0.0;
+            double sg[3] = {0.0, 0.0, 0.0};
             double st[9], ce[9];
 #pragma unroll
             for (int x = 0; x < 9; x++) {
                 st[x] = 0.0;
                 ce[x] = 0.0;
             }
-            for (int64_t d = d0; d < d1; d++) {
-                const int32_t code = a.dir_code[d];
-                const int64_t p = code >> 1;
-                const bool inv = code & 1;
-                const double* __restrict__ F = a.features + p * L.stride;
-                const double fsc = __ldg(F + 0);
-                const double Yv = __ldg(F + L.off_y + lm);
-                const double Rv = __ldg(F + L.off_r + ri);
-                const double val = fsc * Yv * Rv;
-                acc += inv ? sign_l * val : val;
-                if (!grad) continue;
-                const double fg = __ldg(F + 1), r = __ldg(F + 2);
-                const double u[3] = {__ldg(F + 3), __ldg(F + 4), __ldg(F + 5)};
-                const double dR = __ldg(F + L.off_dr + ri);
-                double g[3];
-#pragma unroll
-                for (int x = 0; x < 3; x++) {
-                    const double dY = __ldg(F + L.off_dy + x * L.L2 + lm);
-                    g[x] = fg * u[x] * Rv * Yv + fsc * dR * u[x] * Yv + fsc * Rv * dY / r;
-                }
-                if (!inv && a.do_positions) {
-                    double* pg = a.pair_grad + p * 3 * K;
-                    pg[k] = g[0];
-                    pg[K + k] = g[1];
-                    pg[2 * K + k] = g[2];
-                }
-                const double gf = inv ? -sign_l : 1.0;
-                const double gi[3] = {gf * g[0], gf * g[1], gf * g[2]};
-                if (a.do_positions && __ldg(F + 9) == 0.0) {
-                    sg0 -= gi[0];
-                    sg1 -= gi[1];
-                    sg2 -= gi[2];
-                }
-                if (a.do_strain) {
-                    const double vec[3] = {__ldg(F + 6), __ldg(F + 7), __ldg(F + 8)};
-#pragma unroll
-                    for (int x = 0; x < 3; x++) {
-                        const double vx = inv ? -vec[x] : vec[x];
-#pragma unroll
-                        for (int y = 0; y < 3; y++) st[x * 3 + y] += vx * gi[y];
+            for (int64_t dc = d0; dc < d1; dc += SE_CHUNK) {
+                const int nd = (int)min((int64_t)SE_CHUNK, d1 - dc);
+                __syncthreads();
+                if (threadIdx.x < nd) {
+                    const int32_t code = a.dir_code[dc + threadIdx.x];
+                    const int64_t p = code >> 1;
+                    const double* F = a.features + p * L.stride;
+                    DirScalars& D = dirs[threadIdx.x];
+                    D.feature = p * L.stride;
+                    D.inv = code & 1;
+                    D.f = F[0];
+                    if (GRAD) {
+                        D.fg = F[1];
+                        D.r = F[2];
+                        for (int x = 0; x < 3; x++) {
+                            D.u[x] = F[3 + x];
+                            D.v[x] = F[6 + x];
+                            D.sh[x] = F[10 + x];
+                        }
+                        D.self_image = F[9] != 0.0;
                     }
                 }
-                if (a.do_cell) {
-                    const double sh[3] = {__ldg(F + 10), __ldg(F + 11), __ldg(F + 12)};
+                __syncthreads();
+                if (!active) continue;
+#pragma unroll 2
+                for (int q = 0; q < nd; q++) {
+                    const DirScalars& D = dirs[q];
+                    const double* __restrict__ F = a.features + D.feature;
+                    const double Yv = __ldg(F + L.off_y + lm);
+                    const double Rv = __ldg(F + L.off_r + ri);
+                    const double val = D.f * Yv * Rv;
+                    acc += D.inv ? sign_l * val : val;
+                    if (!GRAD) continue;
+                    const double dR = __ldg(F + L.off_dr + ri);
+                    double g[3];
 #pragma unroll
                     for (int x = 0; x < 3; x++) {
-                        const double sx = inv ? -sh[x] : sh[x];
+                        const double dY = __ldg(F + L.off_dy + x * L.L2 + lm);
+                        g[x] = D.fg * D.u[x] * Rv * Yv + D.f * dR * D.u[x] * Yv + D.f * Rv * dY / D.r;
+                    }
+                    if (POS && !D.inv) {
+                        double* pg = a.pair_grad + (D.feature / L.stride) * 3 * K;
+                        pg[k] = g[0];
+                        pg[K + k] = g[1];
+                        pg[2 * K + k] = g[2];
+                    }
+                    const double gf = D.inv ? -sign_l : 1.0;
+                    const double gi[3] = {gf * g[0], gf * g[1], gf * g[2]};
+                    if (POS && !D.self_image) {
+                        sg[0] -= gi[0];
+                        sg[1] -= gi[1];
+                        sg[2] -= gi[2];
+                    }
+                    if (STRAIN) {
 #pragma unroll
-                        for (int y = 0; y < 3; y++) ce[x * 3 + y] += sx * gi[y];
+                        for (int x = 0; x < 3; x++) {
+                            const double vx = D.inv ? -D.v[x] : D.v[x];
+#pragma unroll
+                            for (int y = 0; y < 3; y++) st[x * 3 + y] += vx * gi[y];
+                        }
+                    }
+                    if (CELL) {
+#pragma unroll
+                        for (int x = 0; x < 3; x++) {
+                            const double sx = D.inv ? -D.sh[x] : D.sh[x];
+#pragma unroll
+                            for (int y = 0; y < 3; y++) ce[x * 3 + y] += sx * gi[y];
+                        }
                     }
                 }
             }
+            if (!active) continue;
             const int64_t base = (c * S + t);
-            double self = (t == tc && l == 0) ? a.self_contribution[n] : 0.0;
+            const double self = (t == tc && l == 0) ? a.self_contribution[n] : 0.0;
             a.coef[base * K + k] = self + acc;
-            if (a.do_positions) {
+            if (POS) {
                 double* sgp = a.self_grad + base * 3 * K;
-                sgp[k] = sg0;
-                sgp[K + k] = sg1;
-                sgp[2 * K + k] = sg2;
+                sgp[k] = sg[0];
+                sgp[K + k] = sg[1];
+                sgp[2 * K + k] = sg[2];
             }
-            if (a.do_strain) {
+            if (STRAIN) {
                 double* o = a.strain + base * 9 * K;
 #pragma unroll
                 for (int x = 0; x < 9; x++) o[x * K + k] = st[x];
             }
-            if (a.do_cell) {
+            if (CELL) {
                 double* o = a.cellg + base * 9 * K;
 #pragma unroll
                 for (int x = 0; x < 9; x++) o[x * K + k] = ce[x];
@@ -391,8 +424,20 @@ void launch_pair_features(const DevicePairs& pairs, const DeviceRadial& radial, 
 void launch_se_accumulate(const SeArgs& args, cudaStream_t stream) {
     if (args.n_centres == 0) return;
     int K = args.layout.L2 * args.layout.nmax;
-    int threads = std::min(256, (K + 31) / 32 * 32);
-    se_accumulate_kernel<<<(unsigned)args.n_centres, threads, 0, stream>>>(args);
+    int threads = std::max(SE_CHUNK, std::min(256, (K + 31) / 32 * 32));
+    const bool grad = args.layout.with_grad;
+    const bool p = grad && args.do_positions, st = grad && args.do_strain, ce = grad && args.do_cell;
+    const unsigned blocks = (unsigned)args.n_centres;
+#define SE_LAUNCH(P, ST, CE) se_accumulate_kernel<P, ST, CE><<<blocks, threads, 0, stream>>>(args)
+    if (!p && !st && !ce) SE_LAUNCH(false, false, false);
+    else if (p && !st && !ce) SE_LAUNCH(true, false, false);
+    else if (p && st && !ce) SE_LAUNCH(true, true, false);
+    else if (p && st && ce) SE_LAUNCH(true, true, true);
+    else if (p && !st && ce) SE_LAUNCH(true, false, true);
+    else if (!p && st && !ce) SE_LAUNCH(false, true, false);
+    else if (!p && !st && ce) SE_LAUNCH(false, false, true);
+    else SE_LAUNCH(false, true, true);
+#undef SE_LAUNCH
     CUDA_CHECK(cudaGetLastError());
 }
 

@@ -8,10 +8,10 @@
 //      divmod wrap (one thread per atom; atomics only on integer cell counts)
 //   2. count the candidate pairs of every atom i over the (2 n_search + 1)^3
 //      neighbouring cells (j >= i, the self-image half-space rules), keeping
-//      those with |r_ij|^2 < rc^2
+//      those with |r_ij|^2 < rc^2 -- one warp per atom, lanes over candidates
 //   3. exclusive scan of the counts (CUB)
-//   4. write the pairs of every atom into its slot range and sort that range
-//      by (second, shift)
+//   4. the same warp compacts its kept pairs by ballot into a scratch list,
+//      then places every pair at its rank in (second, shift) order
 //
 // The list is therefore ordered by (first, second, shift); featomic sorts by
 // (first, second) with an unstable sort, so only ties between periodic images
@@ -88,19 +88,21 @@ __global__ void nl_fill_cells(const int32_t* __restrict__ cell_of, int64_t n_ato
     cell_atoms[cell_start[c] + slot] = (int32_t)g;
 }
 
-// Enumerate the candidate pairs of atom g.  `emit(j, shift, v, d2)` is called
-// for every kept pair, in enumeration order.
-template <typename Emit>
-__device__ __forceinline__ void nl_enumerate(const NlSystem& s, int64_t g, const double* __restrict__ positions,
-                                             const int32_t* __restrict__ cell_of, const int32_t* __restrict__ atom_shift,
-                                             const int32_t* __restrict__ cell_start, const int32_t* __restrict__ cell_count,
-                                             const int32_t* __restrict__ cell_atoms, double cutoff2, Emit emit) {
-    int local = (int)(cell_of[g] - s.cell_offset);
-    int cz = local % s.n_cells[2];
-    int cy = (local / s.n_cells[2]) % s.n_cells[1];
-    int cx = local / (s.n_cells[2] * s.n_cells[1]);
-    int si[3] = {atom_shift[3 * g], atom_shift[3 * g + 1], atom_shift[3 * g + 2]};
-    double pi0 = positions[3 * g], pi1 = positions[3 * g + 1], pi2 = positions[3 * g + 2];
+// Candidate pairs of atom g, enumerated by one warp: the lanes stride over
+// the atoms of every neighbouring cell.  `visit(keep, j, shift, v, d2)` is
+// called by every lane for every round (keep is false for lanes without a
+// kept pair), so that the caller can use warp-wide ballots.
+template <typename Visit>
+__device__ __forceinline__ void nl_warp_enumerate(const NlSystem& s, int64_t g, const double* __restrict__ positions,
+                                                  const int32_t* __restrict__ cell_of, const int32_t* __restrict__ atom_shift,
+                                                  const int32_t* __restrict__ cell_start, const int32_t* __restrict__ cell_count,
+                                                  const int32_t* __restrict__ cell_atoms, int lane, Visit visit) {
+    const int local = (int)(cell_of[g] - s.cell_offset);
+    const int cz = local % s.n_cells[2];
+    const int cy = (local / s.n_cells[2]) % s.n_cells[1];
+    const int cx = local / (s.n_cells[2] * s.n_cells[1]);
+    const int si[3] = {atom_shift[3 * g], atom_shift[3 * g + 1], atom_shift[3 * g + 2]};
+    const double pi[3] = {positions[3 * g], positions[3 * g + 1], positions[3 * g + 2]};
     for (int dx = -s.n_search[0]; dx <= s.n_search[0]; dx++)
     for (int dy = -s.n_search[1]; dy <= s.n_search[1]; dy++)
     for (int dz = -s.n_search[2]; dz <= s.n_search[2]; dz++) {
@@ -108,32 +110,39 @@ __device__ __forceinline__ void nl_enumerate(const NlSystem& s, int64_t g, const
         divmod_i(cx + dx, s.n_cells[0], &cs[0], &ni[0]);
         divmod_i(cy + dy, s.n_cells[1], &cs[1], &ni[1]);
         divmod_i(cz + dz, s.n_cells[2], &cs[2], &ni[2]);
-        int32_t nc = (int32_t)(s.cell_offset + ((int64_t)ni[0] * s.n_cells[1] + ni[1]) * s.n_cells[2] + ni[2]);
-        int32_t start = cell_start[nc], count = cell_count[nc];
-        for (int32_t q = 0; q < count; q++) {
-            int64_t j = cell_atoms[start + q];
-            if (g > j) continue;
-            int sh[3];
-            for (int k = 0; k < 3; k++) sh[k] = cs[k] + si[k] - atom_shift[3 * j + k];
-            bool zero = sh[0] == 0 && sh[1] == 0 && sh[2] == 0;
-            if (g == j) {
-                if (zero) continue;
-                int sum = sh[0] + sh[1] + sh[2];
-                if (sum < 0) continue;
-                if (sum == 0 && (sh[2] < 0 || (sh[2] == 0 && sh[1] < 0))) continue;
+        const int32_t nc = (int32_t)(s.cell_offset + ((int64_t)ni[0] * s.n_cells[1] + ni[1]) * s.n_cells[2] + ni[2]);
+        const int32_t start = cell_start[nc], count = cell_count[nc];
+        for (int32_t q0 = 0; q0 < count; q0 += 32) {
+            const int32_t q = q0 + lane;
+            bool keep = false;
+            int32_t j = -1;
+            int sh[3] = {0, 0, 0};
+            double v[3] = {0.0, 0.0, 0.0};
+            double d2 = 0.0;
+            if (q < count) {
+                j = cell_atoms[start + q];
+                keep = g <= j;
+                for (int k = 0; k < 3; k++) sh[k] = cs[k] + si[k] - atom_shift[3 * (int64_t)j + k];
+                const bool zero = sh[0] == 0 && sh[1] == 0 && sh[2] == 0;
+                if (keep && g == j) {
+                    // self images: one of each +/- shift pair (neighbors.rs:253-286)
+                    const int sum = sh[0] + sh[1] + sh[2];
+                    if (zero || sum < 0 || (sum == 0 && (sh[2] < 0 || (sh[2] == 0 && sh[1] < 0)))) keep = false;
+                }
+                if (s.infinite && !zero) keep = false;
+                if (keep) {
+                    for (int k = 0; k < 3; k++) {
+                        // CellShift::cartesian, neighbors.rs:52-57
+                        const double c = __dadd_rn(__dadd_rn(__dmul_rn(s.H[0 * 3 + k], (double)sh[0]),
+                                                             __dmul_rn(s.H[1 * 3 + k], (double)sh[1])),
+                                                   __dmul_rn(s.H[2 * 3 + k], (double)sh[2]));
+                        v[k] = __dadd_rn(__dsub_rn(positions[3 * (int64_t)j + k], pi[k]), c);
+                    }
+                    d2 = __dadd_rn(__dadd_rn(__dmul_rn(v[0], v[0]), __dmul_rn(v[1], v[1])), __dmul_rn(v[2], v[2]));
+                    keep = d2 < s.cutoff2;
+                }
             }
-            if (s.infinite && !zero) continue;
-            double v[3];
-            double pj[3] = {positions[3 * j], positions[3 * j + 1], positions[3 * j + 2]};
-            double pi[3] = {pi0, pi1, pi2};
-            for (int k = 0; k < 3; k++) {
-                // CellShift::cartesian, neighbors.rs:52-57
-                double c = __dadd_rn(__dadd_rn(__dmul_rn(s.H[0 * 3 + k], (double)sh[0]), __dmul_rn(s.H[1 * 3 + k], (double)sh[1])),
-                                     __dmul_rn(s.H[2 * 3 + k], (double)sh[2]));
-                v[k] = __dadd_rn(__dsub_rn(pj[k], pi[k]), c);
-            }
-            double d2 = __dadd_rn(__dadd_rn(__dmul_rn(v[0], v[0]), __dmul_rn(v[1], v[1])), __dmul_rn(v[2], v[2]));
-            if (d2 < cutoff2) emit((int32_t)j, sh, v, d2);
+            visit(keep, j, sh, v, d2);
         }
     }
 }
@@ -143,13 +152,16 @@ __global__ void nl_count(const NlSystem* __restrict__ systems, const int32_t* __
                          const int32_t* __restrict__ atom_shift, const int32_t* __restrict__ cell_start,
                          const int32_t* __restrict__ cell_count, const int32_t* __restrict__ cell_atoms,
                          int64_t* __restrict__ pair_count) {
-    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (g >= n_atoms) return;
     const NlSystem& s = systems[atom_system[g]];
     int64_t count = 0;
-    nl_enumerate(s, g, positions, cell_of, atom_shift, cell_start, cell_count, cell_atoms, s.cutoff2,
-                 [&](int32_t, const int*, const double*, double) { count++; });
-    pair_count[g] = count;
+    nl_warp_enumerate(s, g, positions, cell_of, atom_shift, cell_start, cell_count, cell_atoms, lane,
+                      [&](bool keep, int32_t, const int*, const double*, double) {
+                          count += __popc(__ballot_sync(0xffffffffu, keep));
+                      });
+    if (lane == 0) pair_count[g] = count;
 }
 
 __device__ __forceinline__ bool pair_key_less(int32_t j1, const int32_t* s1, int32_t j2, const int32_t* s2) {
@@ -159,50 +171,47 @@ __device__ __forceinline__ bool pair_key_less(int32_t j1, const int32_t* s1, int
     return false;
 }
 
+// kept pairs of atom g in enumeration order into `scratch`, then every lane
+// places its pairs at their rank in (second, shift) order
 __global__ void nl_write(const NlSystem* __restrict__ systems, const int32_t* __restrict__ atom_system,
                          const double* __restrict__ positions, int64_t n_atoms, const int32_t* __restrict__ cell_of,
                          const int32_t* __restrict__ atom_shift, const int32_t* __restrict__ cell_start,
                          const int32_t* __restrict__ cell_count, const int32_t* __restrict__ cell_atoms,
-                         const int64_t* __restrict__ pair_start, DevicePairs pairs) {
-    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                         const int64_t* __restrict__ pair_start, DevicePairs scratch, DevicePairs pairs) {
+    const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (g >= n_atoms) return;
     const NlSystem& s = systems[atom_system[g]];
-    int64_t base = pair_start[g];
-    int64_t w = base;
-    nl_enumerate(s, g, positions, cell_of, atom_shift, cell_start, cell_count, cell_atoms, s.cutoff2,
-                 [&](int32_t j, const int* sh, const double* v, double d2) {
-                     pairs.first[w] = (int32_t)g;
-                     pairs.second[w] = j;
-                     pairs.distance[w] = __dsqrt_rn(d2);
-                     pairs.vector[3 * w] = v[0];
-                     pairs.vector[3 * w + 1] = v[1];
-                     pairs.vector[3 * w + 2] = v[2];
-                     pairs.shift[3 * w] = sh[0];
-                     pairs.shift[3 * w + 1] = sh[1];
-                     pairs.shift[3 * w + 2] = sh[2];
-                     w++;
-                 });
-    // insertion sort of this atom's pairs by (second, shift)
-    for (int64_t a = base + 1; a < w; a++) {
-        int32_t j = pairs.second[a];
-        int32_t sh[3] = {pairs.shift[3 * a], pairs.shift[3 * a + 1], pairs.shift[3 * a + 2]};
-        double d = pairs.distance[a];
-        double v[3] = {pairs.vector[3 * a], pairs.vector[3 * a + 1], pairs.vector[3 * a + 2]};
-        int64_t b = a - 1;
-        while (b >= base && pair_key_less(j, sh, pairs.second[b], &pairs.shift[3 * b])) {
-            pairs.second[b + 1] = pairs.second[b];
-            pairs.distance[b + 1] = pairs.distance[b];
-            for (int k = 0; k < 3; k++) {
-                pairs.vector[3 * (b + 1) + k] = pairs.vector[3 * b + k];
-                pairs.shift[3 * (b + 1) + k] = pairs.shift[3 * b + k];
-            }
-            b--;
-        }
-        pairs.second[b + 1] = j;
-        pairs.distance[b + 1] = d;
+    const int64_t base = pair_start[g];
+    int64_t written = 0;
+    nl_warp_enumerate(s, g, positions, cell_of, atom_shift, cell_start, cell_count, cell_atoms, lane,
+                      [&](bool keep, int32_t j, const int* sh, const double* v, double d2) {
+                          const unsigned mask = __ballot_sync(0xffffffffu, keep);
+                          if (keep) {
+                              const int64_t w = base + written + __popc(mask & ((1u << lane) - 1u));
+                              scratch.second[w] = j;
+                              scratch.distance[w] = __dsqrt_rn(d2);
+                              for (int k = 0; k < 3; k++) {
+                                  scratch.vector[3 * w + k] = v[k];
+                                  scratch.shift[3 * w + k] = sh[k];
+                              }
+                          }
+                          written += __popc(mask);
+                      });
+    __syncwarp();
+    for (int64_t a = lane; a < written; a += 32) {
+        const int32_t j = scratch.second[base + a];
+        const int32_t* sh = &scratch.shift[3 * (base + a)];
+        int64_t rank = 0;
+        for (int64_t b = 0; b < written; b++)
+            if (pair_key_less(scratch.second[base + b], &scratch.shift[3 * (base + b)], j, sh)) rank++;
+        const int64_t w = base + rank;
+        pairs.first[w] = (int32_t)g;
+        pairs.second[w] = j;
+        pairs.distance[w] = scratch.distance[base + a];
         for (int k = 0; k < 3; k++) {
-            pairs.vector[3 * (b + 1) + k] = v[k];
-            pairs.shift[3 * (b + 1) + k] = sh[k];
+            pairs.vector[3 * w + k] = scratch.vector[3 * (base + a) + k];
+            pairs.shift[3 * w + k] = sh[k];
         }
     }
 }
@@ -239,6 +248,8 @@ int64_t NeighborBuilder::build(const std::vector<NlSystem>& systems, const std::
 
     int threads = 128;
     int blocks = (int)((n_atoms + threads - 1) / threads);
+    // one warp per atom for the pair search
+    int warp_blocks = (int)((n_atoms * 32 + threads - 1) / threads);
     if (n_atoms > 0) {
         nl_assign_cells<<<blocks, threads, 0, stream>>>(d_sys, d_atom_system, d_positions, n_atoms, d_cell_of, d_atom_shift, d_cell_count);
         CUDA_CHECK(cudaGetLastError());
@@ -247,8 +258,8 @@ int64_t NeighborBuilder::build(const std::vector<NlSystem>& systems, const std::
     if (n_atoms > 0) {
         nl_fill_cells<<<blocks, threads, 0, stream>>>(d_cell_of, n_atoms, d_cell_start, d_cell_fill, d_cell_atoms);
         CUDA_CHECK(cudaGetLastError());
-        nl_count<<<blocks, threads, 0, stream>>>(d_sys, d_atom_system, d_positions, n_atoms, d_cell_of, d_atom_shift,
-                                                 d_cell_start, d_cell_count, d_cell_atoms, d_pair_count);
+        nl_count<<<warp_blocks, threads, 0, stream>>>(d_sys, d_atom_system, d_positions, n_atoms, d_cell_of,
+                                                      d_atom_shift, d_cell_start, d_cell_count, d_cell_atoms, d_pair_count);
         CUDA_CHECK(cudaGetLastError());
     }
     arena.exclusive_scan(d_pair_count, d_pair_start, n_atoms + 1, stream);
@@ -263,9 +274,16 @@ int64_t NeighborBuilder::build(const std::vector<NlSystem>& systems, const std::
     pairs.vector = arena.alloc<double>("pairs.vector", 3 * total);
     pairs.shift = arena.alloc<int32_t>("pairs.shift", 3 * total);
     pairs.count = total;
+    DevicePairs scratch;
+    scratch.second = arena.alloc<int32_t>("nl.scratch.second", total);
+    scratch.distance = arena.alloc<double>("nl.scratch.distance", total);
+    scratch.vector = arena.alloc<double>("nl.scratch.vector", 3 * total);
+    scratch.shift = arena.alloc<int32_t>("nl.scratch.shift", 3 * total);
+    scratch.count = total;
     if (n_atoms > 0 && total > 0) {
-        nl_write<<<blocks, threads, 0, stream>>>(d_sys, d_atom_system, d_positions, n_atoms, d_cell_of, d_atom_shift,
-                                                 d_cell_start, d_cell_count, d_cell_atoms, d_pair_start, pairs);
+        nl_write<<<warp_blocks, threads, 0, stream>>>(d_sys, d_atom_system, d_positions, n_atoms, d_cell_of,
+                                                      d_atom_shift, d_cell_start, d_cell_count, d_cell_atoms,
+                                                      d_pair_start, scratch, pairs);
         CUDA_CHECK(cudaGetLastError());
     }
     return total;

@@ -6,95 +6,139 @@
 //   blocks     featomic/src/calculator.rs:414-495
 //   power spectrum keys / samples: featomic/src/calculators/soap/power_spectrum.rs:423-481
 //   spherical expansion keys / samples: spherical_expansion.rs:662-742
+//
+// Every table is built in O(pairs + rows) with exact pre-sizing; the
+// gradient sample labels are the only per-row work.
 #include "plan.hpp"
 
 #include <algorithm>
-#include <map>
-#include <tuple>
 
 namespace fb200 {
 
 Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_t n_pairs, const int32_t* first,
                                   const int32_t* second) {
     Neighborhoods nh;
-    nh.atom_offset.push_back(0);
-    std::vector<int32_t> types;
-    for (size_t s = 0; s < systems.size(); s++) {
-        for (int64_t i = 0; i < systems[s].n_atoms; i++) {
-            types.push_back(systems[s].types[i]);
-            nh.atom_system.push_back((int32_t)s);
-            nh.atom_local.push_back((int32_t)i);
+    int64_t n_atoms = 0;
+    for (auto& s : systems) n_atoms += s.n_atoms;
+    nh.n_atoms = n_atoms;
+    nh.atom_offset.resize(systems.size() + 1);
+    nh.atom_system.resize(n_atoms);
+    nh.atom_local.resize(n_atoms);
+    std::vector<int32_t> types(n_atoms);
+    {
+        int64_t a = 0;
+        nh.atom_offset[0] = 0;
+        for (size_t s = 0; s < systems.size(); s++) {
+            for (int64_t i = 0; i < systems[s].n_atoms; i++, a++) {
+                types[a] = systems[s].types[i];
+                nh.atom_system[a] = (int32_t)s;
+                nh.atom_local[a] = (int32_t)i;
+            }
+            nh.atom_offset[s + 1] = a;
         }
-        nh.atom_offset.push_back(nh.atom_offset.back() + systems[s].n_atoms);
     }
-    nh.n_atoms = (int64_t)types.size();
     nh.species_types = types;
     std::sort(nh.species_types.begin(), nh.species_types.end());
     nh.species_types.erase(std::unique(nh.species_types.begin(), nh.species_types.end()), nh.species_types.end());
-    nh.n_species = (int)nh.species_types.size();
-    const int S = nh.n_species;
-    nh.atom_species.resize(nh.n_atoms);
-    for (int64_t a = 0; a < nh.n_atoms; a++)
+    const int S = nh.n_species = (int)nh.species_types.size();
+    nh.atom_species.resize(n_atoms);
+    for (int64_t a = 0; a < n_atoms; a++)
         nh.atom_species[a] = (int32_t)(std::lower_bound(nh.species_types.begin(), nh.species_types.end(), types[a]) -
                                        nh.species_types.begin());
+    const int32_t* sp = nh.atom_species.data();
 
-    // directions, counting sort on (centre, species of the other atom), stable in pair order
-    std::vector<int64_t> count((size_t)nh.n_atoms * S + 1, 0);
+    // directions: counting sort on (centre, species of the other atom), stable in pair order
+    nh.seg_offset.assign((size_t)n_atoms * S + 1, 0);
+    int64_t* seg = nh.seg_offset.data();
     for (int64_t p = 0; p < n_pairs; p++) {
-        count[(size_t)first[p] * S + nh.atom_species[second[p]]]++;
-        count[(size_t)second[p] * S + nh.atom_species[first[p]]]++;
+        seg[(size_t)first[p] * S + sp[second[p]] + 1]++;
+        seg[(size_t)second[p] * S + sp[first[p]] + 1]++;
     }
-    nh.seg_offset.assign((size_t)nh.n_atoms * S + 1, 0);
-    for (size_t k = 0; k + 1 < nh.seg_offset.size(); k++) nh.seg_offset[k + 1] = nh.seg_offset[k] + count[k];
+    for (size_t k = 1; k < nh.seg_offset.size(); k++) seg[k] += seg[k - 1];
     std::vector<int64_t> fill(nh.seg_offset.begin(), nh.seg_offset.end() - 1);
     nh.dir_code.resize(2 * (size_t)n_pairs);
+    int32_t* dir = nh.dir_code.data();
     for (int64_t p = 0; p < n_pairs; p++) {
-        nh.dir_code[fill[(size_t)first[p] * S + nh.atom_species[second[p]]]++] = (int32_t)(p << 1);
-        nh.dir_code[fill[(size_t)second[p] * S + nh.atom_species[first[p]]]++] = (int32_t)((p << 1) | 1);
+        dir[fill[(size_t)first[p] * S + sp[second[p]]]++] = (int32_t)(p << 1);
+        dir[fill[(size_t)second[p] * S + sp[first[p]]]++] = (int32_t)((p << 1) | 1);
     }
+    auto other_of = [&](int32_t code) { return (code & 1) ? first[code >> 1] : second[code >> 1]; };
 
     // unique neighbours.  Inside a segment the other atoms are sorted (pairs
     // with the centre second come first, ordered by first; then the centre's
-    // own pairs, ordered by second), so equal atoms are contiguous.
-    nh.species_mask.assign((size_t)nh.n_atoms * S, 0);
-    nh.entry_offset.assign(nh.n_atoms + 1, 0);
-    std::vector<PsEntry> tmp;
-    for (int64_t c = 0; c < nh.n_atoms; c++) {
-        tmp.clear();
-        nh.species_mask[(size_t)c * S + nh.atom_species[c]] = 1;
+    // own pairs, ordered by second), so an S-way merge of the segments lists
+    // every centre's neighbours by atom index.  Centres are independent: a
+    // counting pass sizes every centre's list, a second pass fills it.
+    nh.species_mask.assign((size_t)n_atoms * S, 0);
+    nh.species_count.assign((size_t)n_atoms * S, 0);
+    nh.entry_offset.assign(n_atoms + 1, 0);
+    auto merge = [&](int64_t c, PsEntry* out, int32_t* cum_out, int32_t* count_out) -> int64_t {
+        int64_t pos[64], end[64];
+        int32_t cum[65];
+        const int sc = sp[c];
         for (int t = 0; t < S; t++) {
-            int64_t d0 = nh.seg_offset[(size_t)c * S + t], d1 = nh.seg_offset[(size_t)c * S + t + 1];
-            if (d1 > d0) nh.species_mask[(size_t)c * S + t] = 1;
-            int64_t d = d0;
-            while (d < d1) {
-                int32_t code = nh.dir_code[d];
-                int32_t p = code >> 1;
-                int32_t other = (code & 1) ? first[p] : second[p];
-                int64_t e = d + 1;
-                while (e < d1) {
-                    int32_t c2 = nh.dir_code[e];
-                    int32_t p2 = c2 >> 1;
-                    int32_t o2 = (c2 & 1) ? first[p2] : second[p2];
-                    if (o2 != other) break;
-                    e++;
-                }
-                if (other != (int32_t)c) tmp.push_back(PsEntry{other, t, (int32_t)d, (int32_t)e});
-                d = e;
-            }
+            pos[t] = seg[(size_t)c * S + t];
+            end[t] = seg[(size_t)c * S + t + 1];
         }
-        tmp.push_back(PsEntry{(int32_t)c, nh.atom_species[c], -1, -1});
-        std::sort(tmp.begin(), tmp.end(), [](const PsEntry& x, const PsEntry& y) { return x.atom < y.atom; });
-        nh.entries.insert(nh.entries.end(), tmp.begin(), tmp.end());
-        nh.entry_offset[c + 1] = (int64_t)nh.entries.size();
+        for (int t = 0; t <= S; t++) cum[t] = 0;
+        bool self_done = false;
+        int64_t n = 0;
+        auto emit = [&](const PsEntry& e) {
+            if (out) {
+                out[n] = e;
+                for (int t = 0; t <= S; t++) cum_out[n * (S + 1) + t] = cum[t];
+            }
+            n++;
+        };
+        while (true) {
+            int best = -1;
+            int32_t best_atom = 0;
+            for (int t = 0; t < S; t++) {
+                if (pos[t] < end[t]) {
+                    int32_t o = other_of(dir[pos[t]]);
+                    if (best < 0 || o < best_atom) {
+                        best = t;
+                        best_atom = o;
+                    }
+                }
+            }
+            if (!self_done && (best < 0 || best_atom >= (int32_t)c)) {
+                emit(PsEntry{(int32_t)c, sc, -1, -1});
+                cum[S] = 1;
+                self_done = true;
+            }
+            if (best < 0) break;
+            int64_t d0 = pos[best], d = d0 + 1;
+            while (d < end[best] && other_of(dir[d]) == best_atom) d++;
+            pos[best] = d;
+            if (best_atom == (int32_t)c) continue;  // periodic images of the centre itself
+            emit(PsEntry{best_atom, best, (int32_t)d0, (int32_t)d});
+            cum[best]++;
+        }
+        if (count_out)
+            for (int t = 0; t < S; t++) count_out[t] = cum[t];
+        return n;
+    };
+    if (S > 64) throw invalid_parameter("more than 64 atomic types are not supported");
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < n_atoms; c++) {
+        nh.entry_offset[c + 1] = merge(c, nullptr, nullptr, &nh.species_count[(size_t)c * S]);
+        for (int t = 0; t < S; t++)
+            nh.species_mask[(size_t)c * S + t] = (seg[(size_t)c * S + t + 1] > seg[(size_t)c * S + t] || t == sp[c]) ? 1 : 0;
     }
+    for (int64_t c = 0; c < n_atoms; c++) nh.entry_offset[c + 1] += nh.entry_offset[c];
+    nh.entries.resize(nh.entry_offset[n_atoms]);
+    nh.entry_cum.resize((size_t)nh.entry_offset[n_atoms] * (S + 1));
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < n_atoms; c++)
+        merge(c, nh.entries.data() + nh.entry_offset[c], nh.entry_cum.data() + nh.entry_offset[c] * (S + 1), nullptr);
     return nh;
 }
-
-std::vector<Labels> ps_components() { return {}; }
 
 Labels ps_properties(const Hypers& h) {
     Labels p;
     p.names = {"l", "n_1", "n_2"};
+    p.values.reserve((size_t)(h.max_angular + 1) * h.nmax() * h.nmax() * 3);
     for (int l = 0; l <= h.max_angular; l++)
         for (int n1 = 0; n1 < h.nmax(); n1++)
             for (int n2 = 0; n2 < h.nmax(); n2++) p.values.insert(p.values.end(), {l, n1, n2});
@@ -110,12 +154,11 @@ Labels se_properties(const Hypers& h) {
 
 namespace {
 
-void assign_offsets(OutputPlan& plan, int64_t per_value_row, const GradientOptions& g,
-                    const std::vector<int64_t>& per_block_width) {
+void assign_offsets(OutputPlan& plan, const GradientOptions& g, const std::vector<int64_t>& width) {
     int64_t off = 0;
     for (size_t b = 0; b < plan.blocks.size(); b++) {
         auto& bp = plan.blocks[b];
-        int64_t w = per_block_width.empty() ? per_value_row : per_block_width[b];
+        int64_t w = width[b];
         bp.off_values = off;
         off += bp.n_samples * w;
         if (g.positions) {
@@ -139,71 +182,82 @@ void assign_offsets(OutputPlan& plan, int64_t per_value_row, const GradientOptio
 OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g) {
     OutputPlan plan;
     const int S = nh.n_species;
+    const int64_t N = nh.n_atoms;
     // keys: (center, a, b) with a <= b among the species around every centre
-    std::vector<uint8_t> present((size_t)S * S * S, 0);
-    for (int64_t c = 0; c < nh.n_atoms; c++) {
+    std::vector<int32_t> key_index((size_t)S * S * S, -1);
+    for (int64_t c = 0; c < N; c++) {
         const uint8_t* mask = &nh.species_mask[(size_t)c * S];
         for (int a = 0; a < S; a++) {
             if (!mask[a]) continue;
             for (int b = a; b < S; b++)
-                if (mask[b]) present[((size_t)nh.atom_species[c] * S + a) * S + b] = 1;
+                if (mask[b]) key_index[((size_t)nh.atom_species[c] * S + a) * S + b] = 0;
         }
     }
-    std::vector<int32_t> key_index((size_t)S * S * S, -1);
     plan.keys.names = {"center_type", "neighbor_1_type", "neighbor_2_type"};
-    for (int ct = 0; ct < S; ct++)
-        for (int a = 0; a < S; a++)
-            for (int b = a; b < S; b++) {
-                if (!present[((size_t)ct * S + a) * S + b]) continue;
-                key_index[((size_t)ct * S + a) * S + b] = (int32_t)plan.blocks.size();
-                plan.keys.values.insert(plan.keys.values.end(), {nh.species_types[ct], nh.species_types[a], nh.species_types[b]});
-                plan.blocks.emplace_back();
-            }
-    for (auto& bp : plan.blocks) {
-        bp.samples.names = {"system", "atom"};
-        bp.gradient_samples.names = {"sample", "system", "atom"};
+    int32_t nb = 0;
+    for (size_t k = 0; k < key_index.size(); k++) {
+        if (key_index[k] < 0) continue;
+        key_index[k] = nb++;
+        int ct = (int)(k / ((size_t)S * S)), a = (int)((k / S) % S), b = (int)(k % S);
+        plan.keys.values.insert(plan.keys.values.end(), {nh.species_types[ct], nh.species_types[a], nh.species_types[b]});
     }
+    plan.blocks.resize(nb);
 
-    // samples (AllOf{a, b}) and gradient samples (OneOf[a, b]), centre by centre
-    plan.slot_offset.assign(nh.n_atoms + 1, 0);
-    plan.row_offset.assign(nh.n_atoms + 1, 0);
-    for (int64_t c = 0; c < nh.n_atoms; c++) {
+    // slots, sample rows and the first gradient row of every slot
+    plan.slot_offset.assign(N + 1, 0);
+    for (int64_t c = 0; c < N; c++) {
         const uint8_t* mask = &nh.species_mask[(size_t)c * S];
-        int64_t e0 = nh.entry_offset[c], e1 = nh.entry_offset[c + 1];
-        int64_t first_slot = (int64_t)plan.slots.size();
+        const int32_t* count = &nh.species_count[(size_t)c * S];
         for (int a = 0; a < S; a++) {
             if (!mask[a]) continue;
             for (int b = a; b < S; b++) {
                 if (!mask[b]) continue;
                 int32_t k = key_index[((size_t)nh.atom_species[c] * S + a) * S + b];
                 auto& bp = plan.blocks[k];
-                int32_t sample = (int32_t)bp.n_samples++;
-                bp.samples.values.insert(bp.samples.values.end(), {nh.atom_system[c], nh.atom_local[c]});
-                plan.slots.push_back(PsKeySlot{k, sample, a, b});
+                plan.slots.push_back(PsKeySlot{k, (int32_t)bp.n_samples++, a, b});
+                plan.slot_row.push_back(bp.n_grad_rows);
+                bp.n_grad_rows += count[a] + (a != b ? count[b] : 0) + 1;
             }
         }
-        int64_t ns = (int64_t)plan.slots.size() - first_slot;
         plan.slot_offset[c + 1] = (int64_t)plan.slots.size();
+    }
+
+    // labels, written in place: every slot knows its sample row and its first
+    // gradient row, so centres fill their rows independently
+    std::vector<int32_t*> sample_w(nb), grad_w(nb);
+    for (int32_t k = 0; k < nb; k++) {
+        auto& bp = plan.blocks[k];
+        bp.samples.names = {"system", "atom"};
+        bp.samples.values.resize((size_t)bp.n_samples * 2);
+        sample_w[k] = bp.samples.values.data();
+        bp.gradient_samples.names = {"sample", "system", "atom"};
         if (g.positions) {
-            int64_t base = (int64_t)plan.rows.size();
-            plan.rows.resize(base + (e1 - e0) * ns, -1);
-            // rows of one sample are contiguous and sorted by neighbour atom
-            for (int64_t s = 0; s < ns; s++) {
-                const PsKeySlot& slot = plan.slots[first_slot + s];
-                auto& bp = plan.blocks[slot.block];
-                for (int64_t e = e0; e < e1; e++) {
-                    const PsEntry& en = nh.entries[e];
-                    if (en.atom != (int32_t)c && en.species != slot.a && en.species != slot.b) continue;
-                    plan.rows[base + (e - e0) * ns + s] = bp.n_grad_rows++;
-                    bp.gradient_samples.values.insert(bp.gradient_samples.values.end(),
-                                                      {slot.sample, nh.atom_system[c], nh.atom_local[en.atom]});
-                }
+            bp.gradient_samples.values.resize((size_t)bp.n_grad_rows * 3);
+            grad_w[k] = bp.gradient_samples.values.data();
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < N; c++) {
+        const int32_t sys = nh.atom_system[c];
+        for (int64_t s = plan.slot_offset[c]; s < plan.slot_offset[c + 1]; s++) {
+            const PsKeySlot& slot = plan.slots[s];
+            int32_t* w = sample_w[slot.block] + 2 * (size_t)slot.sample;
+            w[0] = sys;
+            w[1] = nh.atom_local[c];
+            if (!g.positions) continue;
+            int32_t* gw = grad_w[slot.block] + 3 * (size_t)plan.slot_row[s];
+            for (int64_t e = nh.entry_offset[c]; e < nh.entry_offset[c + 1]; e++) {
+                const PsEntry& en = nh.entries[e];
+                if (en.atom != (int32_t)c && en.species != slot.a && en.species != slot.b) continue;
+                gw[0] = slot.sample;
+                gw[1] = sys;
+                gw[2] = nh.atom_local[en.atom];
+                gw += 3;
             }
         }
-        plan.row_offset[c + 1] = (int64_t)plan.rows.size();
     }
     int64_t n_props = (int64_t)(h.max_angular + 1) * h.nmax() * h.nmax();
-    assign_offsets(plan, n_props, g, {});
+    assign_offsets(plan, g, std::vector<int64_t>(nb, n_props));
     return plan;
 }
 
@@ -262,7 +316,7 @@ OutputPlan plan_spherical_expansion(const Neighborhoods& nh, const Hypers& h, co
     }
     std::vector<int64_t> widths;
     for (auto& bp : plan.blocks) widths.push_back((int64_t)(2 * bp.l + 1) * h.nmax());
-    assign_offsets(plan, 0, g, widths);
+    assign_offsets(plan, g, widths);
     return plan;
 }
 

@@ -27,6 +27,11 @@ struct Neighborhoods {
     // unique neighbours of every centre plus the centre itself, by atom index
     std::vector<int64_t> entry_offset;   // [n_atoms + 1]
     std::vector<PsEntry> entries;
+    // per entry: S prefix counts of earlier neighbours by species, then 1 if
+    // the centre itself comes earlier in the list
+    std::vector<int32_t> entry_cum;      // [entries][S + 1]
+    // per centre: number of unique neighbours of each species
+    std::vector<int32_t> species_count;  // [n_atoms * S]
     // species present around each centre (own species included)
     std::vector<uint8_t> species_mask;   // [n_atoms * S]
 };
@@ -52,8 +57,7 @@ struct OutputPlan {
     // power spectrum tables
     std::vector<int64_t> slot_offset;  // [n_atoms + 1]
     std::vector<PsKeySlot> slots;
-    std::vector<int64_t> row_offset;   // [n_atoms + 1]
-    std::vector<int64_t> rows;
+    std::vector<int64_t> slot_row;     // first gradient row of every slot
     // spherical expansion tables
     std::vector<int32_t> row_centre, row_block, row_sample;
     std::vector<int32_t> grad_block, grad_centre, grad_atom, grad_d0, grad_d1;
@@ -64,8 +68,7 @@ struct OutputPlan {
 OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g);
 OutputPlan plan_spherical_expansion(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g);
 
-// Labels of the components / properties of each calculator
-std::vector<Labels> ps_components();
+// Labels of the properties of each calculator
 Labels ps_properties(const Hypers& h);
 Labels se_properties(const Hypers& h);
 

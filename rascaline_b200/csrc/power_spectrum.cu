@@ -3,35 +3,41 @@
 //   P[l, n1, n2] = sum_m c_a[l m n1] c_b[l m n2] * (sqrt 2 if a != b) / ((-1)^l sqrt(2l+1))
 //
 // featomic/src/calculators/soap/power_spectrum.rs:571-764.  One CTA per
-// centre: the centre's key slots (block, sample row, neighbour species a, b)
-// and its unique-neighbour entries are precomputed on the host, so every
-// output row is written exactly once, contiguously, straight into the final
-// TensorMap block layout ([sample][property], [gradient row][xyz][property],
-// [sample][3][3][property]).
+// centre keeps the centre's expansion coefficients (all neighbour species) in
+// shared memory.  Every output row is a set of per-l products
+//
+//   G[x][n1][n2] = sum_m v[l m n2] g[x][l m n1]  (+ sum_m v'[l m n1] g'[x][l m n2])
+//
+// evaluated one l at a time by a warp: all lanes share l (so the m-loops do
+// not diverge) and each lane accumulates two consecutive (n1, n2) outputs for
+// every component.  Sums run over m in featomic's order, without fused
+// multiply-adds, and each row is written exactly once, with 512-byte
+// contiguous stores, into the final TensorMap block layout ([sample][property], [gradient row][xyz]
+// [property], [sample][3][3][property]).
 //
 // positions gradient of row (centre i, atom j):
 //   j == i : sum_m c_b dself_a + c_a dself_b
 //   j != i : sum_m c_b dc_a(i<-j) [type(j) == a] + c_a dc_b(i<-j) [type(j) == b]
 // with dc(i<-j) = sum over the pairs between i and j of g_pair (i first) or
-// -(-1)^l g_pair (i second), in pair order.
+// -(-1)^l g_pair (i second), in pair order, read in place.  The row index
+// inside a block is
+// the slot's first row plus the rank of the neighbour among the rows of that
+// sample (prefix counts per species).
+#include <cuda_pipeline.h>
+
 #include "engine.hpp"
 
 namespace fb200 {
 
 namespace {
 
-struct PropIndex {
-    int l, n1, n2;
-};
+constexpr double SQRT_2 = 1.4142135623730951;
 
-__device__ __forceinline__ PropIndex decode_prop(int64_t p, int nmax) {
-    PropIndex r;
-    int nn = nmax * nmax;
-    r.l = (int)(p / nn);
-    int rem = (int)(p - (int64_t)r.l * nn);
-    r.n1 = rem / nmax;
-    r.n2 = rem - r.n1 * nmax;
-    return r;
+__device__ __forceinline__ int isqrt_lm(int lm) {
+    int l = (int)sqrt((double)lm);
+    while (l * l > lm) l--;
+    while ((l + 1) * (l + 1) <= lm) l++;
+    return l;
 }
 
 __device__ __forceinline__ double ps_norm(int l) {
@@ -39,139 +45,398 @@ __device__ __forceinline__ double ps_norm(int l) {
     return (l % 2 == 0) ? s : -s;
 }
 
-__global__ void ps_values_kernel(PsArgs a) {
-    const int64_t c = blockIdx.x;
-    const int K = (a.lmax + 1) * (a.lmax + 1) * a.nmax;
-    const int S = a.n_species;
-    for (int64_t s = a.slot_offset[c]; s < a.slot_offset[c + 1]; s++) {
-        const PsKeySlot slot = a.slots[s];
-        const double* ca = a.coef + ((int64_t)c * S + slot.a) * K;
-        const double* cb = a.coef + ((int64_t)c * S + slot.b) * K;
-        double* out = a.out + a.off_values[slot.block] + (int64_t)slot.sample * a.n_props;
-        const double scale = slot.a != slot.b ? 1.4142135623730951 : 1.0;
-        for (int64_t p = threadIdx.x; p < a.n_props; p += blockDim.x) {
-            PropIndex q = decode_prop(p, a.nmax);
-            double sum = 0.0;
-            const int base = q.l * q.l * a.nmax;
-            for (int m = 0; m < 2 * q.l + 1; m++)
-                sum += __ldg(ca + base + m * a.nmax + q.n1) * __ldg(cb + base + m * a.nmax + q.n2);
-            if (slot.a != slot.b) sum *= scale;
-            out[p] = sum / ps_norm(q.l);
-        }
-    }
-}
+// Sources of the "gradient" operand of a tile.  Multiplying by
+// -(-1)^l (the reversed orientation of a pair) is exact, so reading a pair
+// gradient in place equals staging its flipped copy; several periodic images
+// are summed element by element in pair order, like featomic's
+// positions-gradient block.
+struct DirectSource {
+    const double* p;
+    bool flip;
+    __device__ __forceinline__ double load(int idx, double sl) const { return flip ? sl * p[idx] : p[idx]; }
+};
 
-__global__ void ps_positions_kernel(PsArgs a) {
-    const int64_t c = blockIdx.x;
-    const int K = (a.lmax + 1) * (a.lmax + 1) * a.nmax;
-    const int S = a.n_species;
-    const int64_t s0 = a.slot_offset[c], ns = a.slot_offset[c + 1] - s0;
-    const int64_t e0 = a.entry_offset[c], ne = a.entry_offset[c + 1] - e0;
-    const int64_t rbase = a.row_offset[c];
-    for (int64_t e = 0; e < ne; e++) {
-        const PsEntry entry = a.entries[e0 + e];
-        const bool self = entry.atom == (int32_t)c;
-        for (int64_t s = 0; s < ns; s++) {
-            const int64_t row = a.rows[rbase + e * ns + s];
-            if (row < 0) continue;
-            const PsKeySlot slot = a.slots[s0 + s];
-            const double* ca = a.coef + ((int64_t)c * S + slot.a) * K;
-            const double* cb = a.coef + ((int64_t)c * S + slot.b) * K;
-            const bool has1 = self || entry.species == slot.a;
-            const bool has2 = self || entry.species == slot.b;
-            double* out = a.out + a.off_positions[slot.block] + row * 3 * a.n_props;
-            for (int64_t qi = threadIdx.x; qi < 3 * a.n_props; qi += blockDim.x) {
-                const int x = (int)(qi / a.n_props);
-                const int64_t p = qi - x * a.n_props;
-                PropIndex q = decode_prop(p, a.nmax);
-                const int base = q.l * q.l * a.nmax;
-                const double sign_l = (q.l & 1) ? -1.0 : 1.0;
-                double sum = 0.0;
-                for (int pass = 0; pass < 2; pass++) {
-                    if (pass == 0 && !has1) continue;
-                    if (pass == 1 && !has2) continue;
-                    // pass 0: value of b, gradient of a (column n1); pass 1: value of a, gradient of b (column n2)
-                    const double* cv = pass == 0 ? cb : ca;
-                    const int nv = pass == 0 ? q.n2 : q.n1;
-                    const int ng = pass == 0 ? q.n1 : q.n2;
-                    const int tg = pass == 0 ? slot.a : slot.b;
-                    for (int m = 0; m < 2 * q.l + 1; m++) {
-                        const int idx = base + m * a.nmax + ng;
-                        double g;
-                        if (self) {
-                            g = __ldg(a.self_grad + (((int64_t)c * S + tg) * 3 + x) * K + idx);
-                        } else {
-                            g = 0.0;
-                            for (int d = entry.d0; d < entry.d1; d++) {
-                                const int32_t code = a.dir_code[d];
-                                const int64_t pr = code >> 1;
-                                const double factor = (code & 1) ? -sign_l : 1.0;
-                                g += factor * __ldg(a.pair_grad + (pr * 3 + x) * K + idx);
-                            }
-                        }
-                        sum += __ldg(cv + base + m * a.nmax + nv) * g;
-                    }
-                }
-                if (slot.a != slot.b) sum *= 1.4142135623730951;
-                out[qi] = sum / ps_norm(q.l);
+struct ImagesSource {
+    const int32_t* codes;
+    int n;
+    const double* pair_grad;
+    int64_t stride;  // 3 K
+    __device__ __forceinline__ double load(int idx, double sl) const {
+        double v = 0.0;
+        for (int d = 0; d < n; d++) {
+            const int32_t code = codes[d];
+            const double g = pair_grad[(int64_t)(code >> 1) * stride + idx];
+            v += (code & 1) ? sl * g : g;
+        }
+        return v;
+    }
+};
+
+// m-sum of one (l, lane) tile from raw pointers (already offset to the
+// lane's n1 / n2 and to the first m of l).  NEG subtracts the products, which
+// equals adding the products with the operand negated (negation is exact).
+template <int NC, bool NEG, bool PAIRED>
+__device__ __forceinline__ void sum_term1(int nm, int nmax, int stride, const double* __restrict__ g,
+                                          const double* __restrict__ v, double (&acc)[NC][2]) {
+    // acc[x][j] += v[m][n2_j] * g[x][m][n1]   (PAIRED: both outputs share n1)
+    for (int m = 0; m < nm; m++, g += nmax, v += nmax) {
+        const double va = v[0], vb = v[1];
+#pragma unroll
+        for (int x = 0; x < NC; x++) {
+            const double gx = g[x * stride];
+            if (NEG) {
+                acc[x][0] -= va * gx;
+                acc[x][1] -= vb * gx;
+            } else {
+                acc[x][0] += va * gx;
+                acc[x][1] += vb * gx;
             }
         }
     }
 }
 
-__global__ void ps_strain_cell_kernel(PsArgs a, int which) {
+template <int NC, bool NEG>
+__device__ __forceinline__ void sum_term2(int nm, int nmax, int stride, const double* __restrict__ g,
+                                          const double* __restrict__ v, double (&acc)[NC][2]) {
+    // acc[x][j] += v[m][n1] * g[x][m][n2_j]
+    for (int m = 0; m < nm; m++, g += nmax, v += nmax) {
+        const double u = v[0];
+#pragma unroll
+        for (int x = 0; x < NC; x++) {
+            const double ga = g[x * stride], gb = g[x * stride + 1];
+            if (NEG) {
+                acc[x][0] -= u * ga;
+                acc[x][1] -= u * gb;
+            } else {
+                acc[x][0] += u * ga;
+                acc[x][1] += u * gb;
+            }
+        }
+    }
+}
+
+// Tile rows of one output row, even nmax: every lane of the warp shares l
+// (uniform m-loop trip counts) and owns the two consecutive outputs
+// q = 2 lane, 2 lane + 1 (+ 64 k) of q = n1 nmax + n2, for all NC components:
+//   acc[x][j] = sum_m v2[l m n2] * g1[x][l m n1]   (if g1)
+//             + sum_m v1[l m n1] * g2[x][l m n2]   (if g2)
+// with g1 / g2 negated on even l when flip1 / flip2 (the -(-1)^l factor of a
+// reversed pair).  Each element is summed over m in featomic's order; the
+// scaling (sqrt 2 if a != b) / ((-1)^l sqrt(2l+1)) is applied at the end.
+template <int NC>
+__device__ __forceinline__ void rows_even(int lane, int lmax, int nmax, int stride, const double* g1, bool flip1,
+                                          const double* v2, const double* v1, const double* g2, bool flip2,
+                                          double* __restrict__ out, int64_t xstride, const double* scale_l) {
+    const int nn = nmax * nmax;
+    for (int qa = 2 * lane; qa < nn; qa += 64) {
+        const int n1 = qa / nmax, n2 = qa - n1 * nmax;
+        for (int l = 0; l <= lmax; l++) {
+            const int base = l * l * nmax;
+            const int nm = 2 * l + 1;
+            const bool even = (l & 1) == 0;
+            double acc[NC][2];
+#pragma unroll
+            for (int x = 0; x < NC; x++) acc[x][0] = acc[x][1] = 0.0;
+            if (g1) {
+                if (flip1 && even) sum_term1<NC, true, true>(nm, nmax, stride, g1 + base + n1, v2 + base + n2, acc);
+                else sum_term1<NC, false, true>(nm, nmax, stride, g1 + base + n1, v2 + base + n2, acc);
+            }
+            if (g2) {
+                if (flip2 && even) sum_term2<NC, true>(nm, nmax, stride, g2 + base + n2, v1 + base + n1, acc);
+                else sum_term2<NC, false>(nm, nmax, stride, g2 + base + n2, v1 + base + n1, acc);
+            }
+            const double scale = scale_l[l];
+            double* o = out + (int64_t)l * nn + qa;
+#pragma unroll
+            for (int x = 0; x < NC; x++) {
+                double2 w;
+                w.x = acc[x][0] * scale;
+                w.y = acc[x][1] * scale;
+                *reinterpret_cast<double2*>(o + x * xstride) = w;
+            }
+        }
+    }
+}
+
+// Generic tile of one l (odd nmax, or several periodic images summed on the
+// fly): the lane owns outputs q = 2 lane, 2 lane + 1 (+ 64 k).
+template <int NC, typename G1, typename G2>
+__device__ __forceinline__ void l_tile(int lane, int l, int nmax, int stride, bool use1, const G1& g1,
+                                       const double* __restrict__ v2, const double* __restrict__ v1, bool use2,
+                                       const G2& g2, double* __restrict__ out, int64_t xstride, double scale) {
+    const int nn = nmax * nmax;
+    const int base = l * l * nmax;
+    const int nm = 2 * l + 1;
+    const double sl = (l & 1) ? 1.0 : -1.0;
+    double* o = out + (int64_t)l * nn;
+    for (int qa = 2 * lane; qa < nn; qa += 64) {
+        const int qb = qa + 1;
+        const bool hasb = qb < nn;
+        const int n1a = qa / nmax, n2a = qa - n1a * nmax;
+        const int n1b = hasb ? qb / nmax : n1a, n2b = hasb ? qb - n1b * nmax : n2a;
+        double acc[NC][2];
+#pragma unroll
+        for (int x = 0; x < NC; x++) acc[x][0] = acc[x][1] = 0.0;
+        if (use1) {
+            for (int m = 0; m < nm; m++) {
+                const int row = base + m * nmax;
+                const double va = v2[row + n2a], vb = v2[row + n2b];
+#pragma unroll
+                for (int x = 0; x < NC; x++) {
+                    const double ga = g1.load(x * stride + row + n1a, sl);
+                    const double gb = (n1b == n1a) ? ga : g1.load(x * stride + row + n1b, sl);
+                    acc[x][0] += va * ga;
+                    acc[x][1] += vb * gb;
+                }
+            }
+        }
+        if (use2) {
+            for (int m = 0; m < nm; m++) {
+                const int row = base + m * nmax;
+                const double ua = v1[row + n1a], ub = v1[row + n1b];
+#pragma unroll
+                for (int x = 0; x < NC; x++) {
+                    acc[x][0] += ua * g2.load(x * stride + row + n2a, sl);
+                    acc[x][1] += ub * g2.load(x * stride + row + n2b, sl);
+                }
+            }
+        }
+#pragma unroll
+        for (int x = 0; x < NC; x++) {
+            o[x * xstride + qa] = acc[x][0] * scale;
+            if (hasb) o[x * xstride + qb] = acc[x][1] * scale;
+        }
+    }
+}
+
+// one output row (all l): the fast even-nmax path for in-place operands,
+// the generic path otherwise
+template <int NC, typename G1, typename G2>
+__device__ __forceinline__ void rows(int lane, int lmax, int nmax, int stride, bool use1, const G1& g1,
+                                     const double* v2, const double* v1, bool use2, const G2& g2, double* out,
+                                     int64_t xstride, const double* scale_l) {
+    for (int l = 0; l <= lmax; l++)
+        l_tile<NC>(lane, l, nmax, stride, use1, g1, v2, v1, use2, g2, out, xstride, scale_l[l]);
+}
+
+template <int NC>
+__device__ __forceinline__ void rows(int lane, int lmax, int nmax, int stride, bool use1, const DirectSource& g1,
+                                     const double* v2, const double* v1, bool use2, const DirectSource& g2, double* out,
+                                     int64_t xstride, const double* scale_l) {
+    if ((nmax & 1) == 0 && ((xstride & 1) == 0) && ((((uintptr_t)out) & 15) == 0)) {
+        rows_even<NC>(lane, lmax, nmax, stride, use1 ? g1.p : nullptr, g1.flip, v2, v1, use2 ? g2.p : nullptr, g2.flip,
+                      out, xstride, scale_l);
+    } else {
+        for (int l = 0; l <= lmax; l++)
+            l_tile<NC>(lane, l, nmax, stride, use1, g1, v2, v1, use2, g2, out, xstride, scale_l[l]);
+    }
+}
+
+// (sqrt 2 if mixed) / ((-1)^l sqrt(2l+1)) for l = 0..lmax, in shared memory:
+// entries [0, L] unmixed, [L + 1, 2L + 1] mixed
+__device__ __forceinline__ void load_scales(int lmax, double* scale_s) {
+    for (int i = threadIdx.x; i < 2 * (lmax + 1); i += blockDim.x) {
+        const int l = i % (lmax + 1);
+        const double s = sqrt((double)(2 * l + 1));
+        const double norm = (l % 2 == 0) ? s : -s;
+        scale_s[i] = (i > lmax ? SQRT_2 : 1.0) * (1.0 / norm);
+    }
+}
+
+__device__ __forceinline__ void load_coefficients(const PsArgs& a, int64_t c, double* coef_s, int SK) {
+    const double* src = a.coef + c * SK;
+    for (int i = threadIdx.x; i < SK; i += blockDim.x) coef_s[i] = src[i];
+}
+
+template <int MAXN>
+__global__ void __launch_bounds__(256) ps_values_kernel(PsArgs a) {
+    extern __shared__ double smem[];
     const int64_t c = blockIdx.x;
     const int K = (a.lmax + 1) * (a.lmax + 1) * a.nmax;
+    double* coef_s = smem;
+    double* scale_s = smem + a.n_species * K;
+    load_coefficients(a, c, coef_s, a.n_species * K);
+    load_scales(a.lmax, scale_s);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int64_t s0 = a.slot_offset[c], ns = a.slot_offset[c + 1] - s0;
+    for (int64_t s = warp; s < ns; s += nwarps) {
+        const PsKeySlot slot = a.slots[s0 + s];
+        double* out = a.out + a.off_values[slot.block] + (int64_t)slot.sample * a.n_props;
+        DirectSource ca{coef_s + slot.a * K, false};
+        rows<1>(lane, a.lmax, a.nmax, K, true, ca, coef_s + slot.b * K, nullptr, false, ca, out, a.n_props,
+                scale_s + (slot.a != slot.b ? a.lmax + 1 : 0));
+    }
+}
+
+// one positions-gradient row (both kinds of source)
+template <typename G>
+__device__ __forceinline__ void positions_row(const PsArgs& a, int lane, int K, const double* coef_s,
+                                              const double* scale_s, const PsKeySlot& slot, bool self, int species,
+                                              const G& g, const double* self_a, const double* self_b, double* out) {
+    const double* scales = scale_s + (slot.a != slot.b ? a.lmax + 1 : 0);
+    const double* ca = coef_s + slot.a * K;
+    const double* cb = coef_s + slot.b * K;
+    if (self) {
+        DirectSource s1{self_a, false}, s2{self_b, false};
+        rows<3>(lane, a.lmax, a.nmax, K, true, s1, cb, ca, true, s2, out, a.n_props, scales);
+    } else {
+        rows<3>(lane, a.lmax, a.nmax, K, species == slot.a, g, cb, ca, species == slot.b, g, out, a.n_props, scales);
+    }
+}
+
+// The gradient record of a neighbour that shares one pair with the centre
+// (3 K doubles, the common case) is copied to shared memory asynchronously:
+// each warp prefetches its next neighbour while it contracts the current one.
+__device__ __forceinline__ void stage_record(double* dst, const double* src, int n, int lane) {
+    if ((n & 1) == 0) {
+        for (int i = 2 * lane; i < n; i += 64) __pipeline_memcpy_async(dst + i, src + i, 16);
+    } else {
+        for (int i = lane; i < n; i += 32) __pipeline_memcpy_async(dst + i, src + i, 8);
+    }
+}
+
+__device__ __forceinline__ const double* staged_source(const PsArgs& a, int64_t c, int64_t entry_index, int K) {
+    const PsEntry entry = a.entries[entry_index];
+    if (entry.atom == (int32_t)c || entry.d1 - entry.d0 != 1) return nullptr;
+    return a.pair_grad + (int64_t)(a.dir_code[entry.d0] >> 1) * 3 * K;
+}
+
+constexpr int POS_WARPS = 4;
+
+template <int MAXN>
+__global__ void __launch_bounds__(POS_WARPS * 32) ps_positions_kernel(PsArgs a) {
+    extern __shared__ double smem[];
+    const int64_t c = blockIdx.x;
     const int S = a.n_species;
+    const int K = (a.lmax + 1) * (a.lmax + 1) * a.nmax;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    double* coef_s = smem;
+    double* scale_s = smem + S * K;
+    double* stage = smem + ((S * K + 2 * (a.lmax + 1) + 1) & ~1) + (int64_t)warp * 6 * K;
+    load_coefficients(a, c, coef_s, S * K);
+    load_scales(a.lmax, scale_s);
+    __syncthreads();
+    const int64_t s0 = a.slot_offset[c], ns = a.slot_offset[c + 1] - s0;
+    const int64_t e0 = a.entry_offset[c], ne = a.entry_offset[c + 1] - e0;
+    if (warp < ne) {
+        const double* src = staged_source(a, c, e0 + warp, K);
+        if (src) stage_record(stage, src, 3 * K, lane);
+    }
+    __pipeline_commit();
+    int it = 0;
+    for (int64_t e = warp; e < ne; e += nwarps, it ^= 1) {
+        double* cur = stage + it * 3 * K;
+        const int64_t next = e + nwarps;
+        if (next < ne) {
+            const double* src = staged_source(a, c, e0 + next, K);
+            if (src) stage_record(stage + (it ^ 1) * 3 * K, src, 3 * K, lane);
+        }
+        __pipeline_commit();
+        __pipeline_wait_prior(1);
+        __syncwarp();
+
+        const PsEntry entry = a.entries[e0 + e];
+        const bool self = entry.atom == (int32_t)c;
+        const int32_t* cum = a.entry_cum + (e0 + e) * (S + 1);
+        const bool single = entry.d1 - entry.d0 <= 1;
+        DirectSource direct{nullptr, false};
+        ImagesSource images{a.dir_code + entry.d0, entry.d1 - entry.d0, a.pair_grad, 3 * (int64_t)K};
+        if (!self && single) {
+            direct.p = cur;
+            direct.flip = a.dir_code[entry.d0] & 1;
+        }
+        for (int64_t s = 0; s < ns; s++) {
+            const PsKeySlot slot = a.slots[s0 + s];
+            if (!self && entry.species != slot.a && entry.species != slot.b) continue;
+            const int64_t rank = cum[slot.a] + (slot.a != slot.b ? cum[slot.b] : 0) + cum[S];
+            const int64_t row = a.slot_row[s0 + s] + rank;
+            double* out = a.out + a.off_positions[slot.block] + row * 3 * a.n_props;
+            const double* self_a = a.self_grad + ((int64_t)c * S + slot.a) * 3 * K;
+            const double* self_b = a.self_grad + ((int64_t)c * S + slot.b) * 3 * K;
+            if (self || single) {
+                positions_row(a, lane, K, coef_s, scale_s, slot, self, entry.species, direct, self_a, self_b, out);
+            } else {
+                positions_row(a, lane, K, coef_s, scale_s, slot, self, entry.species, images, self_a, self_b, out);
+            }
+        }
+        __syncwarp();
+    }
+    __pipeline_wait_prior(0);
+}
+
+// strain (which = 0) or cell (which = 1) rows: 9 components, done as three
+// passes of 3 to bound the register tile
+template <int MAXN>
+__global__ void __launch_bounds__(256) ps_strain_cell_kernel(PsArgs a, int which) {
+    extern __shared__ double smem[];
+    const int64_t c = blockIdx.x;
+    const int S = a.n_species;
+    const int K = (a.lmax + 1) * (a.lmax + 1) * a.nmax;
+    double* coef_s = smem;
+    double* scale_s = smem + S * K;
+    load_coefficients(a, c, coef_s, S * K);
+    load_scales(a.lmax, scale_s);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const double* src = which == 0 ? a.strain : a.cellg;
     const int64_t* offs = which == 0 ? a.off_strain : a.off_cell;
-    for (int64_t s = a.slot_offset[c]; s < a.slot_offset[c + 1]; s++) {
-        const PsKeySlot slot = a.slots[s];
-        const double* ca = a.coef + ((int64_t)c * S + slot.a) * K;
-        const double* cb = a.coef + ((int64_t)c * S + slot.b) * K;
-        const double* ga = src + ((int64_t)c * S + slot.a) * 9 * K;
-        const double* gb = src + ((int64_t)c * S + slot.b) * 9 * K;
-        double* out = a.out + offs[slot.block] + (int64_t)slot.sample * 9 * a.n_props;
-        for (int64_t qi = threadIdx.x; qi < 9 * a.n_props; qi += blockDim.x) {
-            const int x = (int)(qi / a.n_props);
-            const int64_t p = qi - x * a.n_props;
-            PropIndex q = decode_prop(p, a.nmax);
-            const int base = q.l * q.l * a.nmax;
-            double sum = 0.0;
-            for (int m = 0; m < 2 * q.l + 1; m++)
-                sum += __ldg(cb + base + m * a.nmax + q.n2) * __ldg(ga + (int64_t)x * K + base + m * a.nmax + q.n1);
-            for (int m = 0; m < 2 * q.l + 1; m++)
-                sum += __ldg(ca + base + m * a.nmax + q.n1) * __ldg(gb + (int64_t)x * K + base + m * a.nmax + q.n2);
-            if (slot.a != slot.b) sum *= 1.4142135623730951;
-            out[qi] = sum / ps_norm(q.l);
-        }
+    const int64_t s0 = a.slot_offset[c], ns = a.slot_offset[c + 1] - s0;
+    for (int64_t task = warp; task < 3 * ns; task += nwarps) {
+        const int64_t s = task / 3;
+        const int xr = (int)(task - s * 3);
+        const PsKeySlot slot = a.slots[s0 + s];
+        DirectSource ga{src + (((int64_t)c * S + slot.a) * 9 + 3 * xr) * K, false};
+        DirectSource gb{src + (((int64_t)c * S + slot.b) * 9 + 3 * xr) * K, false};
+        double* out = a.out + offs[slot.block] + ((int64_t)slot.sample * 9 + 3 * xr) * a.n_props;
+        rows<3>(lane, a.lmax, a.nmax, K, true, ga, coef_s + slot.b * K, coef_s + slot.a * K, true, gb, out, a.n_props,
+                scale_s + (slot.a != slot.b ? a.lmax + 1 : 0));
+    }
+}
+
+template <int MAXN>
+void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bool cell, cudaStream_t stream,
+                cudaEvent_t after_values, cudaEvent_t after_positions) {
+    const int K = (args.lmax + 1) * (args.lmax + 1) * args.nmax;
+    const size_t coef_bytes = sizeof(double) * ((size_t)args.n_species * K + 2 * (args.lmax + 1));
+    const int threads = 256;
+    static bool configured = false;
+    if (!configured) {
+        CUDA_CHECK(cudaFuncSetAttribute(ps_values_kernel<MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(ps_positions_kernel<MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(ps_strain_cell_kernel<MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        configured = true;
+    }
+    if (coef_bytes > 200 * 1024) throw invalid_parameter("too many species / radial / angular functions for the power spectrum kernels");
+    if (values) {
+        ps_values_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, stream>>>(args);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    if (after_values) CUDA_CHECK(cudaEventRecord(after_values, stream));
+    if (positions) {
+        const size_t pos_bytes = sizeof(double) * (((size_t)args.n_species * K + 2 * (args.lmax + 1) + 1) / 2 * 2 +
+                                                   (size_t)POS_WARPS * 6 * K);
+        if (pos_bytes > 200 * 1024) throw invalid_parameter("too many radial / angular functions for the positions gradient kernel");
+        ps_positions_kernel<MAXN><<<(unsigned)args.n_centres, POS_WARPS * 32, pos_bytes, stream>>>(args);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    if (after_positions) CUDA_CHECK(cudaEventRecord(after_positions, stream));
+    if (strain) {
+        ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, stream>>>(args, 0);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    if (cell) {
+        ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, stream>>>(args, 1);
+        CUDA_CHECK(cudaGetLastError());
     }
 }
 
 }  // namespace
 
-void launch_ps_values(const PsArgs& args, cudaStream_t stream) {
+void launch_power_spectrum(const PsArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream,
+                           cudaEvent_t after_values, cudaEvent_t after_positions) {
     if (args.n_centres == 0) return;
-    ps_values_kernel<<<(unsigned)args.n_centres, 128, 0, stream>>>(args);
-    CUDA_CHECK(cudaGetLastError());
-}
-
-void launch_ps_positions(const PsArgs& args, cudaStream_t stream) {
-    if (args.n_centres == 0) return;
-    ps_positions_kernel<<<(unsigned)args.n_centres, 256, 0, stream>>>(args);
-    CUDA_CHECK(cudaGetLastError());
-}
-
-void launch_ps_strain_cell(const PsArgs& args, bool strain, bool cell, cudaStream_t stream) {
-    if (args.n_centres == 0) return;
-    if (strain) {
-        ps_strain_cell_kernel<<<(unsigned)args.n_centres, 256, 0, stream>>>(args, 0);
-        CUDA_CHECK(cudaGetLastError());
-    }
-    if (cell) {
-        ps_strain_cell_kernel<<<(unsigned)args.n_centres, 256, 0, stream>>>(args, 1);
-        CUDA_CHECK(cudaGetLastError());
-    }
+    launch_all<0>(args, true, positions, strain, cell, stream, after_values, after_positions);
 }
 
 }  // namespace fb200
