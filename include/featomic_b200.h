@@ -185,6 +185,42 @@ featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t
                                               double cutoff, featomic_pair_t* pairs, uintptr_t capacity,
                                               uintptr_t* count);
 
+/* The same half neighbour list (same pairs, same order, same bits as
+ * featomic_b200_neighbor_list) computed without allocating any device memory.
+ * No counterpart in featomic.
+ *
+ * For callers that cannot allocate device memory while they run: an
+ * application whose own allocator owns the whole device memory budget (a
+ * molecular-dynamics engine with a fixed pool, or torch's caching allocator
+ * holding the free memory), where a cudaMalloc would fail or fragment the
+ * pool, and time steps that must not pay for cudaMalloc / cudaFree, whose
+ * cudaFree waits for the whole device.  All working tables live in one fixed
+ * array of about 3.7 MB in this library's device memory, one copy per device.
+ *
+ * `positions` ([n_atoms][3] float64) and `pairs` (`capacity` entries) are
+ * device memory of the current CUDA device, owned by the caller; `cell` [9] is
+ * a host array.  Work is enqueued on `stream` (a cudaStream_t, NULL for the
+ * legacy default stream); the call waits for `stream` once, to learn the
+ * number of pairs, which it stores in `*count`.  The pairs are written
+ * asynchronously and are ready when `stream` reaches the end of the call.
+ *
+ * Limits: at most 65536 atoms, 100000 cells (featomic's own cap) and 2048
+ * pairs per atom in the half list; beyond them the call returns
+ * FEATOMIC_INVALID_PARAMETER_ERROR with a message naming the limit and writes
+ * nothing.  When `capacity` < `*count` it returns FEATOMIC_BUFFER_SIZE_ERROR
+ * and writes no pair (query the size with capacity 0).  Nothing has to be
+ * zeroed by the caller: the call clears its own counters.
+ *
+ * The first call on each device does a one-time set-up (it looks up the
+ * address of that device's scratch array with the device current); make that
+ * first call before any stream capture begins.  Calls on the same device share
+ * the scratch array, so calls that overlap race: make them one after another
+ * (one host thread at a time) on the same stream, or synchronize the stream of
+ * the previous call before starting a call on another stream. */
+featomic_status_t featomic_b200_neighbor_list_noalloc(const double* positions, uintptr_t n_atoms, const double* cell,
+                                                      double cutoff, featomic_pair_t* pairs, uintptr_t capacity,
+                                                      uintptr_t* count, void* stream);
+
 /* Radial integral R_nl(r) and dR_nl/dr of this calculator, as the kernels see
  * it (the Hermite spline of featomic/src/calculators/soap/radial_integral/
  * spline.rs, or the analytic GTO integral of radial_integral/gto.rs when

@@ -111,7 +111,11 @@ SIGNATURES = {
                                                         ctypes.POINTER(ctypes.c_double), ctypes.c_double,
                                                         ctypes.POINTER(featomic_pair_t), ctypes.c_size_t,
                                                         ctypes.POINTER(ctypes.c_size_t)]),
-    "featomic_b200_radial_integral": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+    "featomic_b200_neighbor_list_noalloc": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t,
+                                                                ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                                                ctypes.c_void_p, ctypes.c_size_t,
+                                                                ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p]),
+    "featomic_b200_radial_integral":(featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                           ctypes.c_size_t, ctypes.POINTER(ctypes.c_double),
                                                           ctypes.POINTER(ctypes.c_double),
                                                           ctypes.POINTER(ctypes.c_int32)]),

@@ -5,6 +5,7 @@
 // featomic_last_error(), and returns the status code of the error kind.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -364,6 +365,20 @@ featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t
                 pairs[k].cell_shift_indices[x] = out[k].shift[x];
             }
         }
+    });
+}
+
+featomic_status_t featomic_b200_neighbor_list_noalloc(const double* positions, uintptr_t n_atoms, const double* cell,
+                                                      double cutoff, featomic_pair_t* pairs, uintptr_t capacity,
+                                                      uintptr_t* count, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(cell);
+        CHECK_POINTER(count);
+        if (n_atoms > 0) CHECK_POINTER(positions);
+        if (!(cutoff > 0.0 && std::isfinite(cutoff))) throw invalid_parameter("cutoff must be positive and finite");
+        const int64_t cap = capacity > (uintptr_t)INT64_MAX ? INT64_MAX : (int64_t)capacity;
+        neighbor_list_noalloc(positions, (int64_t)std::min<uintptr_t>(n_atoms, (uintptr_t)INT64_MAX), cell, cutoff,
+                              pairs, cap, count, stream);
     });
 }
 

@@ -11,6 +11,8 @@
 
 #include "json.hpp"
 
+struct featomic_pair_t;
+
 namespace fb200 {
 
 // featomic status codes, featomic/include/featomic.h
@@ -176,6 +178,11 @@ std::unique_ptr<TensorMap> compute(CalculatorImpl& calc, std::vector<HostSystem>
 
 // run kernel (a) on one system given on the host, return the pairs
 std::vector<Pair> neighbor_list(const double* positions, int64_t n_atoms, const double* cell, double cutoff);
+
+// kernel (a) on one system whose positions are on the current device, pairs
+// written to the caller's device buffer, with no device allocation
+void neighbor_list_noalloc(const double* positions, int64_t n_atoms, const double* cell, double cutoff,
+                           featomic_pair_t* pairs, int64_t capacity, uintptr_t* count, void* stream);
 
 // last-call timings (ms) for the profiling API
 std::string profiling_report(const std::string& format);

@@ -21,7 +21,10 @@
 // evaluation order: vector = (r_j - r_i) + (H^T s), d^2 = x x + y y + z z.
 #include <cub/cub.cuh>
 
+#include <mutex>
+
 #include "engine.hpp"
+#include "featomic_b200.h"
 
 namespace fb200 {
 
@@ -318,6 +321,263 @@ std::vector<Pair> neighbor_list(const double* positions, int64_t n_atoms, const 
         }
     }
     return out;
+}
+
+// ---------------------------------------------------------------------------
+// The same neighbour list without any device allocation
+// ---------------------------------------------------------------------------
+//
+// Every table of the cell list lives in one fixed array in device memory
+// (defined below, about 3.7 MB per device), so the call never asks the CUDA
+// runtime or any allocator for memory.  The caller owns the positions and the
+// output pairs.  The atom and cell kernels are the ones above; the scans are a
+// single-block kernel instead of CUB (which needs allocated temporary storage)
+// and the pairs are sorted per atom in shared memory and written straight into
+// the caller's featomic_pair_t array.
+
+namespace {
+
+constexpr int64_t NOALLOC_MAX_ATOMS = 65536;
+// featomic caps the number of cells of one cell list at 1e5
+// (CellList::new, neighbors.rs:128-139); make_nl_system does the same
+constexpr int64_t NOALLOC_MAX_CELLS = 100000;
+// pairs of one atom in the half list (j >= i), sorted in shared memory
+constexpr int NOALLOC_MAX_PAIRS_PER_ATOM = 2048;
+
+constexpr size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// byte offsets of the tables inside the scratch array
+constexpr size_t NOALLOC_SYSTEM = 0;
+constexpr size_t NOALLOC_ATOM_SYSTEM = align256(NOALLOC_SYSTEM + sizeof(NlSystem));
+constexpr size_t NOALLOC_CELL_OF = align256(NOALLOC_ATOM_SYSTEM + 4 * NOALLOC_MAX_ATOMS);
+constexpr size_t NOALLOC_ATOM_SHIFT = align256(NOALLOC_CELL_OF + 4 * NOALLOC_MAX_ATOMS);
+constexpr size_t NOALLOC_CELL_ATOMS = align256(NOALLOC_ATOM_SHIFT + 12 * NOALLOC_MAX_ATOMS);
+constexpr size_t NOALLOC_CELL_COUNT = align256(NOALLOC_CELL_ATOMS + 4 * NOALLOC_MAX_ATOMS);
+constexpr size_t NOALLOC_CELL_START = align256(NOALLOC_CELL_COUNT + 4 * (NOALLOC_MAX_CELLS + 1));
+constexpr size_t NOALLOC_CELL_FILL = align256(NOALLOC_CELL_START + 4 * (NOALLOC_MAX_CELLS + 1));
+constexpr size_t NOALLOC_PAIR_COUNT = align256(NOALLOC_CELL_FILL + 4 * (NOALLOC_MAX_CELLS + 1));
+constexpr size_t NOALLOC_PAIR_START = align256(NOALLOC_PAIR_COUNT + 8 * (NOALLOC_MAX_ATOMS + 1));
+constexpr size_t NOALLOC_OVERFLOW = align256(NOALLOC_PAIR_START + 8 * (NOALLOC_MAX_ATOMS + 1));
+constexpr size_t NOALLOC_BYTES = align256(NOALLOC_OVERFLOW + 8);
+
+}  // namespace
+
+// One copy per device, shared by every call on that device
+static __device__ __align__(256) unsigned char nl_noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+
+__global__ void nl_noalloc_store_system(NlSystem system, NlSystem* __restrict__ out) { *out = system; }
+
+// Exclusive scan of `n` counts into out[0..n] (out[n] = total) by one block of
+// 1024 threads, each over a contiguous chunk.  Counts above `limit` (when
+// limit >= 0) set *over.
+template <typename T>
+__global__ void __launch_bounds__(1024) nl_noalloc_scan(const T* __restrict__ in, T* __restrict__ out, int64_t n,
+                                                        int64_t limit, int32_t* __restrict__ over) {
+    __shared__ T warp_total[32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int64_t chunk = (n + blockDim.x - 1) / blockDim.x;
+    const int64_t lo = (int64_t)t * chunk < n ? (int64_t)t * chunk : n;
+    const int64_t hi = lo + chunk < n ? lo + chunk : n;
+    T local = 0;
+    for (int64_t i = lo; i < hi; i++) {
+        const T c = in[i];
+        if (limit >= 0 && (int64_t)c > limit) atomicOr(over, 1);
+        local += c;
+    }
+    T incl = local;
+    for (int off = 1; off < 32; off <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+    }
+    if (lane == 31) warp_total[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < (int)(blockDim.x >> 5) ? warp_total[lane] : T(0);
+        for (int off = 1; off < 32; off <<= 1) {
+            const T y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        warp_total[lane] = w;
+    }
+    __syncthreads();
+    T prefix = incl - local + (warp > 0 ? warp_total[warp - 1] : T(0));
+    for (int64_t i = lo; i < hi; i++) {
+        out[i] = prefix;
+        prefix += in[i];
+    }
+    if (t == (int)blockDim.x - 1) out[n] = prefix;
+}
+
+// One warp (one block) per atom.  First pass: the keys (second, shift) of the
+// atom's kept pairs go to shared memory in enumeration order.  Second pass:
+// the same enumeration again, every kept pair written at base + its rank among
+// the keys, which is featomic's (first, second, shift) order.
+__global__ void __launch_bounds__(32) nl_noalloc_write(
+    const NlSystem* __restrict__ systems, const int32_t* __restrict__ atom_system, const double* __restrict__ positions,
+    int64_t n_atoms, const int32_t* __restrict__ cell_of, const int32_t* __restrict__ atom_shift,
+    const int32_t* __restrict__ cell_start, const int32_t* __restrict__ cell_count,
+    const int32_t* __restrict__ cell_atoms, const int64_t* __restrict__ pair_start, featomic_pair_t* __restrict__ out,
+    int64_t capacity) {
+    __shared__ int32_t key_second[NOALLOC_MAX_PAIRS_PER_ATOM];
+    __shared__ int32_t key_shift[3 * NOALLOC_MAX_PAIRS_PER_ATOM];
+    const int64_t g = blockIdx.x;
+    const int lane = threadIdx.x & 31;
+    if (g >= n_atoms) return;
+    const int64_t base = pair_start[g];
+    const int64_t n = pair_start[g + 1] - base;
+    // both are rejected on the host before this kernel is launched
+    if (n > NOALLOC_MAX_PAIRS_PER_ATOM || base + n > capacity) return;
+    const NlSystem& s = systems[atom_system[g]];
+    int64_t written = 0;
+    nl_warp_enumerate(s, g, positions, cell_of, atom_shift, cell_start, cell_count, cell_atoms, lane,
+                      [&](bool keep, int32_t j, const int* sh, const double*, double) {
+                          const unsigned mask = __ballot_sync(0xffffffffu, keep);
+                          if (keep) {
+                              const int64_t w = written + __popc(mask & ((1u << lane) - 1u));
+                              if (w < n) {
+                                  key_second[w] = j;
+                                  for (int k = 0; k < 3; k++) key_shift[3 * w + k] = sh[k];
+                              }
+                          }
+                          written += __popc(mask);
+                      });
+    __syncwarp();
+    nl_warp_enumerate(s, g, positions, cell_of, atom_shift, cell_start, cell_count, cell_atoms, lane,
+                      [&](bool keep, int32_t j, const int* sh, const double* v, double d2) {
+                          if (!keep) return;
+                          int64_t rank = 0;
+                          for (int64_t b = 0; b < n; b++)
+                              if (pair_key_less(key_second[b], &key_shift[3 * b], j, sh)) rank++;
+                          if (rank >= n) return;
+                          featomic_pair_t* p = out + base + rank;
+                          p->first = (uintptr_t)g;
+                          p->second = (uintptr_t)j;
+                          p->distance = __dsqrt_rn(d2);
+                          for (int k = 0; k < 3; k++) {
+                              p->vector[k] = v[k];
+                              p->cell_shift_indices[k] = sh[k];
+                          }
+                      });
+}
+
+std::mutex noalloc_setup_mutex;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+unsigned char* noalloc_scratch_address[NOALLOC_MAX_DEVICES] = {};
+
+// Set-up, once per device: the address of this device's copy of the scratch
+// array, looked up with that device current.
+unsigned char* noalloc_scratch_for_current_device() {
+    int device = -1;
+    CUDA_CHECK(cudaGetDevice(&device));
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) throw internal_error("unsupported CUDA device index");
+    std::lock_guard<std::mutex> lock(noalloc_setup_mutex);
+    if (noalloc_scratch_address[device] == nullptr) {
+        void* address = nullptr;
+        cudaError_t status = cudaGetSymbolAddress(&address, nl_noalloc_scratch);
+        if (status != cudaSuccess || address == nullptr) {
+            throw internal_error(std::string("could not find the neighbour-list scratch array on device ") +
+                                 std::to_string(device) + ": " + cudaGetErrorString(status));
+        }
+        noalloc_scratch_address[device] = static_cast<unsigned char*>(address);
+    }
+    return noalloc_scratch_address[device];
+}
+
+void check_device_buffer(const void* ptr, size_t alignment, const char* what) {
+    cudaPointerAttributes attributes;
+    CUDA_CHECK(cudaPointerGetAttributes(&attributes, ptr));
+    int device = -1;
+    CUDA_CHECK(cudaGetDevice(&device));
+    const bool on_device = attributes.type == cudaMemoryTypeDevice || attributes.type == cudaMemoryTypeManaged;
+    if (!on_device || (attributes.type == cudaMemoryTypeDevice && attributes.device != device)) {
+        throw invalid_parameter(std::string(what) + " must be device memory of the current CUDA device");
+    }
+    if (reinterpret_cast<uintptr_t>(ptr) % alignment != 0) {
+        throw invalid_parameter(std::string(what) + " must be aligned to " + std::to_string(alignment) + " bytes");
+    }
+}
+
+}  // namespace
+
+void neighbor_list_noalloc(const double* positions, int64_t n_atoms, const double* cell, double cutoff,
+                           featomic_pair_t* pairs, int64_t capacity, uintptr_t* count, void* stream_ptr) {
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    if (n_atoms > NOALLOC_MAX_ATOMS) {
+        throw invalid_parameter("featomic_b200_neighbor_list_noalloc handles at most " +
+                                std::to_string(NOALLOC_MAX_ATOMS) + " atoms, got " + std::to_string(n_atoms));
+    }
+    const NlSystem system = make_nl_system(cell, cutoff, 0, n_atoms, 0);
+    const int64_t n_cells = (int64_t)system.n_cells[0] * system.n_cells[1] * system.n_cells[2];
+    if (n_cells < 1 || n_cells > NOALLOC_MAX_CELLS) {
+        throw invalid_parameter("featomic_b200_neighbor_list_noalloc handles at most " +
+                                std::to_string(NOALLOC_MAX_CELLS) + " cells, got " + std::to_string(n_cells));
+    }
+    unsigned char* scratch = noalloc_scratch_for_current_device();
+    *count = 0;
+    if (n_atoms == 0) return;
+    check_device_buffer(positions, alignof(double), "positions");
+
+    NlSystem* d_system = reinterpret_cast<NlSystem*>(scratch + NOALLOC_SYSTEM);
+    int32_t* d_atom_system = reinterpret_cast<int32_t*>(scratch + NOALLOC_ATOM_SYSTEM);
+    int32_t* d_cell_of = reinterpret_cast<int32_t*>(scratch + NOALLOC_CELL_OF);
+    int32_t* d_atom_shift = reinterpret_cast<int32_t*>(scratch + NOALLOC_ATOM_SHIFT);
+    int32_t* d_cell_atoms = reinterpret_cast<int32_t*>(scratch + NOALLOC_CELL_ATOMS);
+    int32_t* d_cell_count = reinterpret_cast<int32_t*>(scratch + NOALLOC_CELL_COUNT);
+    int32_t* d_cell_start = reinterpret_cast<int32_t*>(scratch + NOALLOC_CELL_START);
+    int32_t* d_cell_fill = reinterpret_cast<int32_t*>(scratch + NOALLOC_CELL_FILL);
+    int64_t* d_pair_count = reinterpret_cast<int64_t*>(scratch + NOALLOC_PAIR_COUNT);
+    int64_t* d_pair_start = reinterpret_cast<int64_t*>(scratch + NOALLOC_PAIR_START);
+    int32_t* d_overflow = reinterpret_cast<int32_t*>(scratch + NOALLOC_OVERFLOW);
+
+    // must start at zero: the system index of every atom (one system), the two
+    // per-cell atomic counters and the per-atom overflow flag
+    CUDA_CHECK(cudaMemsetAsync(d_atom_system, 0, sizeof(int32_t) * n_atoms, stream));
+    CUDA_CHECK(cudaMemsetAsync(d_cell_count, 0, sizeof(int32_t) * (n_cells + 1), stream));
+    CUDA_CHECK(cudaMemsetAsync(d_cell_fill, 0, sizeof(int32_t) * (n_cells + 1), stream));
+    CUDA_CHECK(cudaMemsetAsync(d_overflow, 0, sizeof(int32_t), stream));
+
+    const int threads = 128;
+    const int blocks = (int)((n_atoms + threads - 1) / threads);
+    const int warp_blocks = (int)((n_atoms * 32 + threads - 1) / threads);
+    nl_noalloc_store_system<<<1, 1, 0, stream>>>(system, d_system);
+    CUDA_CHECK(cudaGetLastError());
+    nl_assign_cells<<<blocks, threads, 0, stream>>>(d_system, d_atom_system, positions, n_atoms, d_cell_of,
+                                                    d_atom_shift, d_cell_count);
+    CUDA_CHECK(cudaGetLastError());
+    nl_noalloc_scan<int32_t><<<1, 1024, 0, stream>>>(d_cell_count, d_cell_start, n_cells, -1, nullptr);
+    CUDA_CHECK(cudaGetLastError());
+    nl_fill_cells<<<blocks, threads, 0, stream>>>(d_cell_of, n_atoms, d_cell_start, d_cell_fill, d_cell_atoms);
+    CUDA_CHECK(cudaGetLastError());
+    nl_count<<<warp_blocks, threads, 0, stream>>>(d_system, d_atom_system, positions, n_atoms, d_cell_of, d_atom_shift,
+                                                  d_cell_start, d_cell_count, d_cell_atoms, d_pair_count);
+    CUDA_CHECK(cudaGetLastError());
+    nl_noalloc_scan<int64_t><<<1, 1024, 0, stream>>>(d_pair_count, d_pair_start, n_atoms, NOALLOC_MAX_PAIRS_PER_ATOM,
+                                                     d_overflow);
+    CUDA_CHECK(cudaGetLastError());
+
+    int64_t total = 0;
+    int32_t overflow = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&total, d_pair_start + n_atoms, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaMemcpyAsync(&overflow, d_overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (overflow != 0) {
+        throw invalid_parameter("featomic_b200_neighbor_list_noalloc handles at most " +
+                                std::to_string(NOALLOC_MAX_PAIRS_PER_ATOM) +
+                                " pairs per atom in the half list; use a smaller cutoff or featomic_b200_neighbor_list");
+    }
+    *count = (uintptr_t)total;
+    if (total > capacity) {
+        throw Error(STATUS_BUFFER_SIZE_ERROR, "pair buffer is too small: got space for " + std::to_string(capacity) +
+                                                  " pairs, need " + std::to_string(total));
+    }
+    if (total == 0) return;
+    check_device_buffer(pairs, alignof(featomic_pair_t), "pairs");
+    nl_noalloc_write<<<(unsigned)n_atoms, 32, 0, stream>>>(d_system, d_atom_system, positions, n_atoms, d_cell_of,
+                                                          d_atom_shift, d_cell_start, d_cell_count, d_cell_atoms,
+                                                          d_pair_start, pairs, capacity);
+    CUDA_CHECK(cudaGetLastError());
 }
 
 }  // namespace fb200
