@@ -221,6 +221,59 @@ featomic_status_t featomic_b200_neighbor_list_noalloc(const double* positions, u
                                                       double cutoff, featomic_pair_t* pairs, uintptr_t capacity,
                                                       uintptr_t* count, void* stream);
 
+/* ---- dense power spectrum with an adjoint backward pass ---------------------
+ *
+ * The power spectrum of every atom as one dense row, computed in FP64
+ * (precision 64, same values as featomic_calculator_compute) or with FP32
+ * arithmetic (precision 32), plus a backward pass that turns dL/dvalues into
+ * dL/dpositions, dL/dcell and dL/dstrain without materialising the gradient
+ * blocks.  This replaces the explicit-gradient autograd of featomic-torch
+ * (featomic-torch/src/autograd.cpp:237-317 PositionsGrad, :429-503 CellGrad).
+ *
+ * Layout of `values` (device memory, float64 or float32):
+ *   [atom][species pair (a, b), a <= b][l, n1, n2]
+ * with the species pairs of the sorted species list in row-major upper
+ * triangle order, n_keys = S (S + 1) / 2, and the properties in featomic's
+ * (l, n_1, n_2) order, n_properties = (max_angular + 1) (max_radial + 1)^2.
+ * Rows of species pairs absent around an atom are zero; featomic's block
+ * (center_type, neighbor_1_type, neighbor_2_type) holds the rows of the atoms of
+ * center_type that have both neighbour types (the atom itself counts). */
+typedef struct featomic_b200_dense_t featomic_b200_dense_t;
+
+/* Forward pass.  `species` (n_species sorted or not, NULL for the types of the
+ * systems) fixes the species list; every atom's type must be in it.
+ * `values_count` must be n_atoms x n_keys x n_properties.  The returned state
+ * keeps what the backward pass needs; free it with featomic_b200_dense_free,
+ * before the calculator.  Work is enqueued on `stream` (the neighbour list
+ * waits for it once). */
+featomic_status_t featomic_b200_power_spectrum_dense(featomic_calculator_t* calculator,
+                                                     const featomic_b200_device_systems_t* systems,
+                                                     const int32_t* species, uintptr_t n_species, int32_t precision,
+                                                     void* values, uintptr_t values_count,
+                                                     featomic_b200_dense_t** state, void* stream);
+
+/* Sizes of a forward pass: atoms, species, species pairs, properties, pairs */
+featomic_status_t featomic_b200_dense_shape(const featomic_b200_dense_t* state, uintptr_t* n_atoms,
+                                            uintptr_t* n_species, uintptr_t* n_keys, uintptr_t* n_properties,
+                                            uintptr_t* n_pairs);
+
+/* Host copies of the species list ([n_species]) and of the number of
+ * neighbour directions of each species around every atom
+ * ([n_atoms][n_species], may be NULL); waits for the forward pass. */
+featomic_status_t featomic_b200_dense_species(const featomic_b200_dense_t* state, int32_t* species,
+                                              int32_t* neighbor_counts);
+
+/* Backward pass: `grad_values` has the layout of `values`; writes
+ * dL/dpositions [n_atoms][3] and, when not NULL, dL/dstrain and dL/dcell
+ * [n_systems][3][3] (strain: sum over pairs of r_ij[x] dL/dr_ij[y]; cell:
+ * dL/dH[abc][xyz] with the cell vectors as rows), all device memory of the
+ * forward precision.  May be called more than once per state. */
+featomic_status_t featomic_b200_power_spectrum_dense_backward(featomic_b200_dense_t* state, const void* grad_values,
+                                                              void* grad_positions, void* grad_strain,
+                                                              void* grad_cell, void* stream);
+
+featomic_status_t featomic_b200_dense_free(featomic_b200_dense_t* state);
+
 /* Radial integral R_nl(r) and dR_nl/dr of this calculator, as the kernels see
  * it (the Hermite spline of featomic/src/calculators/soap/radial_integral/
  * spline.rs, or the analytic GTO integral of radial_integral/gto.rs when

@@ -142,7 +142,10 @@ class TensorMap:
 
     def __del__(self):
         if getattr(self, "_handle", None):
-            C.lib().mts_tensormap_free(self._handle)
+            try:
+                C.lib().mts_tensormap_free(self._handle)
+            except (AttributeError, TypeError):  # interpreter shutdown
+                pass
             self._handle = None
 
     @property
@@ -291,7 +294,10 @@ class CalculatorBase:
 
     def __del__(self):
         if getattr(self, "_handle", None):
-            C.lib().featomic_calculator_free(self._handle)
+            try:
+                C.lib().featomic_calculator_free(self._handle)
+            except (AttributeError, TypeError):  # interpreter shutdown
+                pass
             self._handle = None
 
     @property

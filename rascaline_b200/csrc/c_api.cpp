@@ -15,6 +15,7 @@
 #include <sstream>
 
 #include "../../include/featomic_b200.h"
+#include "dense.hpp"
 #include "engine.hpp"
 #include "host.hpp"
 
@@ -339,6 +340,107 @@ featomic_status_t featomic_b200_calculator_compute_device(featomic_calculator_t*
         record_profile(calculator->impl->engine->last_times());
         *descriptor = wrap(std::move(tm));
     });
+}
+
+struct featomic_b200_dense_t {
+    std::unique_ptr<fb200::DenseState> state;
+};
+
+namespace {
+
+std::vector<HostSystem> device_systems(const featomic_b200_device_systems_t* systems) {
+    std::vector<HostSystem> host(systems->n_systems);
+    if (systems->n_systems == 0) return host;
+    CHECK_POINTER(systems->system_sizes);
+    CHECK_POINTER(systems->cells);
+    int64_t off = 0;
+    for (uintptr_t s = 0; s < systems->n_systems; s++) {
+        host[s].n_atoms = (int64_t)systems->system_sizes[s];
+        if (host[s].n_atoms > 0) CHECK_POINTER(systems->types);
+        host[s].types.assign(systems->types + off, systems->types + off + host[s].n_atoms);
+        std::memcpy(host[s].cell, systems->cells + 9 * s, 9 * sizeof(double));
+        off += host[s].n_atoms;
+    }
+    if (off > 0) {
+        CHECK_POINTER(systems->positions);
+        cudaPointerAttributes attr;
+        if (cudaPointerGetAttributes(&attr, systems->positions) != cudaSuccess || attr.type != cudaMemoryTypeDevice) {
+            cudaGetLastError();
+            throw invalid_parameter("expected device positions");
+        }
+    }
+    return host;
+}
+
+}  // namespace
+
+featomic_status_t featomic_b200_power_spectrum_dense(featomic_calculator_t* calculator,
+                                                     const featomic_b200_device_systems_t* systems,
+                                                     const int32_t* species, uintptr_t n_species, int32_t precision,
+                                                     void* values, uintptr_t values_count,
+                                                     featomic_b200_dense_t** state, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(systems);
+        CHECK_POINTER(state);
+        *state = nullptr;
+        if (!calculator->impl->power_spectrum)
+            throw invalid_parameter("featomic_b200_power_spectrum_dense needs a soap_power_spectrum calculator");
+        std::vector<HostSystem> host = device_systems(systems);
+        std::vector<int32_t> sp;
+        if (n_species > 0) {
+            CHECK_POINTER(species);
+            sp.assign(species, species + n_species);
+        }
+        auto result = std::make_unique<featomic_b200_dense_t>();
+        result->state = calculator->impl->engine->forward_dense(precision, host, systems->positions, sp, values,
+                                                                (int64_t)values_count, (cudaStream_t)stream);
+        *state = result.release();
+    });
+}
+
+featomic_status_t featomic_b200_dense_shape(const featomic_b200_dense_t* state, uintptr_t* n_atoms,
+                                            uintptr_t* n_species, uintptr_t* n_keys, uintptr_t* n_properties,
+                                            uintptr_t* n_pairs) {
+    return guarded([&] {
+        CHECK_POINTER(state);
+        const DenseState& st = *state->state;
+        if (n_atoms) *n_atoms = (uintptr_t)st.n_atoms;
+        if (n_species) *n_species = (uintptr_t)st.n_species;
+        if (n_keys) *n_keys = (uintptr_t)st.n_keys;
+        if (n_properties) *n_properties = (uintptr_t)st.n_props;
+        if (n_pairs) *n_pairs = (uintptr_t)st.n_pairs;
+    });
+}
+
+featomic_status_t featomic_b200_dense_species(const featomic_b200_dense_t* state, int32_t* species,
+                                              int32_t* neighbor_counts) {
+    return guarded([&] {
+        CHECK_POINTER(state);
+        const DenseState& st = *state->state;
+        if (species) std::copy(st.species_types.begin(), st.species_types.end(), species);
+        if (neighbor_counts && st.n_atoms > 0) {
+            const int64_t n = st.n_atoms * st.n_species + 1;
+            std::vector<int64_t> seg(n);
+            CUDA_CHECK(cudaMemcpyAsync(seg.data(), st.seg_offset, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, st.stream));
+            CUDA_CHECK(cudaStreamSynchronize(st.stream));
+            for (int64_t k = 0; k + 1 < n; k++) neighbor_counts[k] = (int32_t)(seg[k + 1] - seg[k]);
+        }
+    });
+}
+
+featomic_status_t featomic_b200_power_spectrum_dense_backward(featomic_b200_dense_t* state, const void* grad_values,
+                                                              void* grad_positions, void* grad_strain,
+                                                              void* grad_cell, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(state);
+        DenseState& st = *state->state;
+        st.engine->backward_dense(st, grad_values, grad_positions, grad_strain, grad_cell, (cudaStream_t)stream);
+    });
+}
+
+featomic_status_t featomic_b200_dense_free(featomic_b200_dense_t* state) {
+    return guarded([&] { delete state; });
 }
 
 featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t n_atoms, const double* cell,

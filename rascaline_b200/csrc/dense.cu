@@ -1,0 +1,448 @@
+// Dense power spectrum (FP64 or FP32) and its adjoint backward pass.
+//
+// Forward, per call:
+//   directions   every half pair gives two directions (pair << 1 | reversed);
+//                a stable radix sort on (centre, species of the other atom)
+//                keeps pair order inside each segment, the order of
+//                featomic's accumulate_all_pairs (spherical_expansion.rs:
+//                101-358); segment starts by binary search
+//   features     thread per pair: cutoff, Y_lm, R_nl in T
+//   expansion    CTA per centre, thread per (l, m, n), segments reduced in
+//                registers (no atomics), inverse pairs with (-1)^l
+//                (spherical_expansion_pair.rs:130-163), self term on l = 0
+//   contraction  warp per (centre, species pair a <= b):
+//                P[l n1 n2] = sum_m c_a[l m n1] c_b[l m n2] / ((-1)^l sqrt(2l+1)),
+//                times sqrt(2) when a != b (power_spectrum.rs:529-780)
+//
+// Backward (adjoint of the above for a loss L with dL/dP given):
+//   dL/dc        CTA per centre: dL/dc_a[l m n] = sum over the species pairs
+//                containing a of scale * sum_n' G[n n'] c_b[l m n']
+//   dL/dr_ij     warp per pair, Y_lm, dY_lm, R_nl, dR_nl recomputed:
+//                D = dL/dc_i[s_j] + (-1)^l dL/dc_j[s_i],
+//                dL/dr_ij = sum_lm Y A u + f/r dY B, A = sum_n D (f' R + f R'),
+//                B = sum_n D R  (the pair gradient of spherical_expansion_pair.rs:323-422)
+//   atoms        thread per atom: dL/dr_a = sum over its directions of
+//                -+dL/dr_ij (self images cancel and are skipped), plus the
+//                strain (r_ij x dL/dr_ij) and cell (shift x dL/dr_ij) sums of
+//                its own pairs
+//   systems      CTA per system: strain and cell derivatives summed over atoms
+// Every reduction has a fixed order: results are deterministic.
+#include <cub/cub.cuh>
+
+#include "dense.hpp"
+#include "pair_math.cuh"
+
+namespace fb200 {
+
+namespace {
+
+constexpr int DENSE_LMAX_SMALL = 8;
+constexpr int DENSE_LMAX_LARGE = 24;
+constexpr int DENSE_CHUNK = 32;
+
+__device__ __forceinline__ int isqrt_lm(int lm) {
+    int l = (int)sqrtf((float)lm);
+    while (l * l > lm) l--;
+    while ((l + 1) * (l + 1) <= lm) l++;
+    return l;
+}
+
+// power spectrum normalisation 1 / ((-1)^l sqrt(2l + 1)), times sqrt(2) for
+// two different neighbour species
+__device__ __forceinline__ double ps_scale(int l, bool mixed) {
+    const double s = sqrt((double)(2 * l + 1));
+    const double norm = (l % 2 == 0) ? s : -s;
+    return (mixed ? 1.4142135623730951 : 1.0) * (1.0 / norm);
+}
+
+__device__ __forceinline__ void key_species(int key, int S, int* a, int* b) {
+    int x = 0;
+    while (key >= S - x) {
+        key -= S - x;
+        x++;
+    }
+    *a = x;
+    *b = x + key;
+}
+
+__device__ __forceinline__ int key_index(int a, int b, int S) { return a * S - a * (a - 1) / 2 + (b - a); }
+
+__global__ void dense_direction_keys(const int32_t* __restrict__ first, const int32_t* __restrict__ second,
+                                     const int32_t* __restrict__ species, int64_t n_pairs, int S,
+                                     int32_t* __restrict__ keys, int32_t* __restrict__ codes) {
+    const int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= 2 * n_pairs) return;
+    const int64_t p = d >> 1;
+    const bool reversed = d & 1;
+    const int32_t centre = reversed ? second[p] : first[p];
+    const int32_t other = reversed ? first[p] : second[p];
+    keys[d] = centre * S + species[other];
+    codes[d] = (int32_t)d;
+}
+
+__global__ void dense_segments(const int32_t* __restrict__ sorted, int64_t n_dirs, int64_t n_segments,
+                               int64_t* __restrict__ seg_offset) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > n_segments) return;
+    int64_t lo = 0, hi = n_dirs;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)sorted[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    seg_offset[k] = lo;
+}
+
+template <typename T, int LCAP, bool GRAD>
+__global__ void dense_pair_features(DevicePairs pairs, DeviceRadial exact, DenseTables<T> tab, CutoffParams cut,
+                                    FeatureLayout L, T* __restrict__ features, int32_t* __restrict__ status) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pairs.count) return;
+    T* f = features + p * L.stride;
+    const double r = pairs.distance[p];
+    const double v0 = pairs.vector[3 * p], v1 = pairs.vector[3 * p + 1], v2 = pairs.vector[3 * p + 2];
+    double u0 = v0 / r, u1 = v1 / r, u2 = v2 / r;
+    if (r < 1e-6) {
+        u0 = 0.0;
+        u1 = 0.0;
+        u2 = 1.0;
+    }
+    double fc, dfc;
+    soap::cutoff_function(cut.smoothing, cut.rc, cut.width, r, &fc, &dfc);
+    double sc = 1.0, dsc = 0.0;
+    if (cut.scaling) soap::willatt2018(cut.scale, cut.rate, cut.exponent, r, &sc, &dsc);
+    f[0] = (T)(sc * fc);
+    f[1] = (T)(dfc * sc + fc * dsc);
+    f[2] = (T)r;
+    f[3] = (T)u0;
+    f[4] = (T)u1;
+    f[5] = (T)u2;
+    if (GRAD) {
+        ylm_compute<T, LCAP>(tab.ylm, (T)u0, (T)u1, (T)u2, f + L.off_y, f + L.off_dy, f + L.off_dy + L.L2,
+                             f + L.off_dy + 2 * L.L2);
+    } else {
+        ylm_compute<T, LCAP>(tab.ylm, (T)u0, (T)u1, (T)u2, f + L.off_y, nullptr, nullptr, nullptr);
+    }
+    bool ok = true;
+    for (int l = 0; l <= L.lmax; l++)
+        ok &= radial_eval<T>(exact, tab.spline, l, r, f + L.off_r + l * L.nmax, GRAD ? f + L.off_dr + l * L.nmax : nullptr);
+    if (!ok) atomicExch(status, 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) dense_expansion(DenseArgs<T> a) {
+    __shared__ int64_t dir_feature[DENSE_CHUNK];
+    __shared__ T dir_f[DENSE_CHUNK];
+    __shared__ int dir_inv[DENSE_CHUNK];
+    const FeatureLayout L = a.layout;
+    const int64_t c = blockIdx.x;
+    const int S = a.n_species;
+    const int K = a.K;
+    const int tc = a.atom_species[c];
+    for (int k0 = 0; k0 < K; k0 += blockDim.x) {
+        const int k = k0 + threadIdx.x;
+        const bool active = k < K;
+        const int lm = active ? k / L.nmax : 0;
+        const int n = active ? k - lm * L.nmax : 0;
+        const int l = isqrt_lm(lm);
+        const T sign_l = (l & 1) ? T(-1) : T(1);
+        const int ri = l * L.nmax + n;
+        for (int t = 0; t < S; t++) {
+            const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
+            T acc = T(0);
+            for (int64_t dc = d0; dc < d1; dc += DENSE_CHUNK) {
+                const int nd = (int)min((int64_t)DENSE_CHUNK, d1 - dc);
+                __syncthreads();
+                if (threadIdx.x < nd) {
+                    const int32_t code = a.dir_code[dc + threadIdx.x];
+                    const int64_t p = code >> 1;
+                    dir_feature[threadIdx.x] = p * L.stride;
+                    dir_inv[threadIdx.x] = code & 1;
+                    dir_f[threadIdx.x] = a.features[p * L.stride];
+                }
+                __syncthreads();
+                if (!active) continue;
+                for (int q = 0; q < nd; q++) {
+                    const T* __restrict__ F = a.features + dir_feature[q];
+                    const T val = dir_f[q] * F[L.off_y + lm] * F[L.off_r + ri];
+                    acc += dir_inv[q] ? sign_l * val : val;
+                }
+            }
+            if (!active) continue;
+            const T self = (t == tc && l == 0) ? a.tab.self_contribution[n] : T(0);
+            a.coef[(c * S + t) * K + k] = self + acc;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) dense_contraction(DenseArgs<T> a) {
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t item = (int64_t)blockIdx.x * warps + warp;
+    if (item >= a.n_atoms * a.n_keys) return;
+    const int64_t c = item / a.n_keys;
+    const int key = (int)(item - c * a.n_keys);
+    int sa, sb;
+    key_species(key, a.n_species, &sa, &sb);
+    const int N = a.nmax, NN = N * N;
+    const T* ca = a.coef + (c * a.n_species + sa) * a.K;
+    const T* cb = a.coef + (c * a.n_species + sb) * a.K;
+    T* out = a.values + item * a.n_props;
+    for (int o = lane; o < a.n_props; o += 32) {
+        const int l = o / NN;
+        const int rem = o - l * NN;
+        const int n1 = rem / N, n2 = rem - n1 * N;
+        const int base = l * l * N;
+        T s = T(0);
+        for (int m = 0; m < 2 * l + 1; m++) s += ca[base + m * N + n1] * cb[base + m * N + n2];
+        out[o] = s * (T)ps_scale(l, sa != sb);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) dense_grad_coef(DenseArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char dense_smem[];
+    T* cs = reinterpret_cast<T*>(dense_smem);
+    const int64_t c = blockIdx.x;
+    const int S = a.n_species, K = a.K, N = a.nmax, NN = N * N;
+    for (int i = threadIdx.x; i < S * K; i += blockDim.x) cs[i] = a.coef[c * S * K + i];
+    __syncthreads();
+    const T* G = a.grad_values + c * a.n_keys * a.n_props;
+    for (int o = threadIdx.x; o < S * K; o += blockDim.x) {
+        const int sa = o / K;
+        const int k = o - sa * K;
+        const int lm = k / N;
+        const int n = k - lm * N;
+        const int l = isqrt_lm(lm);
+        T acc = T(0);
+        for (int b = 0; b < S; b++) {
+            const T* cb = cs + b * K + lm * N;
+            T s = T(0);
+            if (sa < b) {
+                const T* g = G + (int64_t)key_index(sa, b, S) * a.n_props + l * NN + n * N;
+                for (int q = 0; q < N; q++) s += g[q] * cb[q];
+                acc += (T)ps_scale(l, true) * s;
+            } else if (sa > b) {
+                const T* g = G + (int64_t)key_index(b, sa, S) * a.n_props + l * NN + n;
+                for (int q = 0; q < N; q++) s += g[q * N] * cb[q];
+                acc += (T)ps_scale(l, true) * s;
+            } else {
+                const T* g = G + (int64_t)key_index(sa, sa, S) * a.n_props + l * NN;
+                for (int q = 0; q < N; q++) s += (g[n * N + q] + g[q * N + n]) * cb[q];
+                acc += (T)ps_scale(l, false) * s;
+            }
+        }
+        a.grad_coef[c * S * K + o] = acc;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) dense_pair_adjoint(DenseArgs<T> a, int64_t n_pairs) {
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t p = (int64_t)blockIdx.x * warps + warp;
+    if (p >= n_pairs) return;
+    const FeatureLayout L = a.layout;
+    const T* __restrict__ F = a.features + p * L.stride;
+    const T f = F[0], fg = F[1], r = F[2];
+    const T u0 = F[3], u1 = F[4], u2 = F[5];
+    const T f_over_r = f / r;
+    const int i = a.pairs.first[p], j = a.pairs.second[p];
+    const int S = a.n_species, N = a.nmax;
+    const T* Di = a.grad_coef + ((int64_t)i * S + a.atom_species[j]) * a.K;
+    const T* Dj = a.grad_coef + ((int64_t)j * S + a.atom_species[i]) * a.K;
+    T g0 = T(0), g1 = T(0), g2 = T(0);
+    for (int lm = lane; lm < L.L2; lm += 32) {
+        const int l = isqrt_lm(lm);
+        const T sign = (l & 1) ? T(-1) : T(1);
+        T A = T(0), B = T(0);
+        for (int n = 0; n < N; n++) {
+            const T D = Di[lm * N + n] + sign * Dj[lm * N + n];
+            const T R = F[L.off_r + l * N + n];
+            const T dR = F[L.off_dr + l * N + n];
+            A += D * (fg * R + f * dR);
+            B += D * R;
+        }
+        const T AY = A * F[L.off_y + lm];
+        const T Bf = B * f_over_r;
+        g0 += AY * u0 + Bf * F[L.off_dy + lm];
+        g1 += AY * u1 + Bf * F[L.off_dy + L.L2 + lm];
+        g2 += AY * u2 + Bf * F[L.off_dy + 2 * L.L2 + lm];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        g0 += __shfl_down_sync(0xffffffffu, g0, off);
+        g1 += __shfl_down_sync(0xffffffffu, g1, off);
+        g2 += __shfl_down_sync(0xffffffffu, g2, off);
+    }
+    if (lane == 0) {
+        a.pair_grad[3 * p] = g0;
+        a.pair_grad[3 * p + 1] = g1;
+        a.pair_grad[3 * p + 2] = g2;
+    }
+}
+
+template <typename T>
+__global__ void dense_atom_reduce(DenseArgs<T> a, int with_partials) {
+    const int64_t atom = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (atom >= a.n_atoms) return;
+    const int S = a.n_species;
+    const int64_t d0 = a.seg_offset[atom * S], d1 = a.seg_offset[(atom + 1) * S];
+    T g[3] = {T(0), T(0), T(0)};
+    for (int64_t d = d0; d < d1; d++) {
+        const int32_t code = a.dir_code[d];
+        const int64_t p = code >> 1;
+        if (a.pairs.first[p] == a.pairs.second[p]) continue;
+        const T* pg = a.pair_grad + 3 * p;
+        if (code & 1) {
+            g[0] += pg[0];
+            g[1] += pg[1];
+            g[2] += pg[2];
+        } else {
+            g[0] -= pg[0];
+            g[1] -= pg[1];
+            g[2] -= pg[2];
+        }
+    }
+    a.grad_positions[3 * atom] = g[0];
+    a.grad_positions[3 * atom + 1] = g[1];
+    a.grad_positions[3 * atom + 2] = g[2];
+    if (!with_partials) return;
+    T w[18];
+#pragma unroll
+    for (int x = 0; x < 18; x++) w[x] = T(0);
+    for (int64_t p = a.pair_start[atom]; p < a.pair_start[atom + 1]; p++) {
+        const T* pg = a.pair_grad + 3 * p;
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            const T v = (T)a.pairs.vector[3 * p + x];
+            const T sh = (T)a.pairs.shift[3 * p + x];
+#pragma unroll
+            for (int y = 0; y < 3; y++) {
+                w[x * 3 + y] += v * pg[y];
+                w[9 + x * 3 + y] += sh * pg[y];
+            }
+        }
+    }
+    T* out = a.atom_partial + 18 * atom;
+#pragma unroll
+    for (int x = 0; x < 18; x++) out[x] = w[x];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) dense_system_reduce(DenseArgs<T> a) {
+    __shared__ T red[256];
+    const int64_t s = blockIdx.x;
+    const int64_t a0 = a.atom_offset[s], a1 = a.atom_offset[s + 1];
+    for (int x = 0; x < 18; x++) {
+        T acc = T(0);
+        for (int64_t atom = a0 + threadIdx.x; atom < a1; atom += blockDim.x) acc += a.atom_partial[18 * atom + x];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int width = blockDim.x / 2; width > 0; width >>= 1) {
+            if ((int)threadIdx.x < width) red[threadIdx.x] += red[threadIdx.x + width];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            if (x < 9 && a.grad_strain) a.grad_strain[9 * s + x] = red[0];
+            if (x >= 9 && a.grad_cell) a.grad_cell[9 * s + x - 9] = red[0];
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, bool GRAD>
+void launch_features(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream) {
+    if (n_pairs == 0) return;
+    DevicePairs pairs = a.pairs;
+    pairs.count = n_pairs;
+    const int threads = 64;
+    const unsigned blocks = (unsigned)((n_pairs + threads - 1) / threads);
+    if (a.lmax <= DENSE_LMAX_SMALL) {
+        dense_pair_features<T, DENSE_LMAX_SMALL, GRAD>
+            <<<blocks, threads, 0, stream>>>(pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status);
+    } else {
+        dense_pair_features<T, DENSE_LMAX_LARGE, GRAD>
+            <<<blocks, threads, 0, stream>>>(pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status);
+    }
+    CUDA_CHECK(cudaGetLastError());
+}
+
+int coefficient_threads(int K) { return std::max(DENSE_CHUNK, std::min(256, (K + 31) / 32 * 32)); }
+
+}  // namespace
+
+void launch_dense_directions(const DevicePairs& pairs, const int32_t* atom_species, int n_species, int64_t n_atoms,
+                             int32_t* dir_code, int64_t* seg_offset, DeviceArena& arena, cudaStream_t stream) {
+    const int64_t n_dirs = 2 * pairs.count;
+    const int64_t n_segments = n_atoms * n_species;
+    if (n_segments >= (int64_t)INT32_MAX) throw invalid_parameter("too many atoms x species for the dense layout");
+    if (n_dirs > 0) {
+        int32_t* keys = arena.alloc<int32_t>("dense.keys", n_dirs);
+        int32_t* sorted = arena.alloc<int32_t>("dense.sorted_keys", n_dirs);
+        int32_t* codes = arena.alloc<int32_t>("dense.codes", n_dirs);
+        const int threads = 256;
+        dense_direction_keys<<<(unsigned)((n_dirs + threads - 1) / threads), threads, 0, stream>>>(
+            pairs.first, pairs.second, atom_species, pairs.count, n_species, keys, codes);
+        CUDA_CHECK(cudaGetLastError());
+        int end_bit = 1;
+        while (end_bit < 31 && ((int64_t)1 << end_bit) <= n_segments) end_bit++;
+        size_t temp = 0;
+        CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, temp, keys, sorted, codes, dir_code, (int)n_dirs, 0, end_bit,
+                                                   stream));
+        void* t = arena.alloc_bytes("dense.sort_temp", temp);
+        CUDA_CHECK(cub::DeviceRadixSort::SortPairs(t, temp, keys, sorted, codes, dir_code, (int)n_dirs, 0, end_bit,
+                                                   stream));
+        dense_segments<<<(unsigned)((n_segments + 1 + threads - 1) / threads), threads, 0, stream>>>(
+            sorted, n_dirs, n_segments, seg_offset);
+        CUDA_CHECK(cudaGetLastError());
+    } else {
+        CUDA_CHECK(cudaMemsetAsync(seg_offset, 0, sizeof(int64_t) * (n_segments + 1), stream));
+    }
+}
+
+template <typename T>
+void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream) {
+    launch_features<T, false>(a, n_pairs, stream);
+    if (a.n_atoms == 0) return;
+    dense_expansion<T><<<(unsigned)a.n_atoms, coefficient_threads(a.K), 0, stream>>>(a);
+    CUDA_CHECK(cudaGetLastError());
+    const int64_t items = a.n_atoms * a.n_keys;
+    const int warps = 8;
+    dense_contraction<T><<<(unsigned)((items + warps - 1) / warps), 32 * warps, 0, stream>>>(a);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream) {
+    if (a.n_atoms == 0) return;
+    const size_t smem = sizeof(T) * (size_t)a.n_species * a.K;
+    if (smem > 200 * 1024) throw invalid_parameter("too many species x coefficients for the adjoint kernel");
+    static bool configured[2] = {false, false};
+    const int which = sizeof(T) == 8 ? 1 : 0;
+    if (!configured[which]) {
+        CUDA_CHECK(cudaFuncSetAttribute(dense_grad_coef<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        configured[which] = true;
+    }
+    dense_grad_coef<T><<<(unsigned)a.n_atoms, 256, smem, stream>>>(a);
+    CUDA_CHECK(cudaGetLastError());
+    if (n_pairs > 0) {
+        launch_features<T, true>(a, n_pairs, stream);
+        const int warps = 8;
+        dense_pair_adjoint<T><<<(unsigned)((n_pairs + warps - 1) / warps), 32 * warps, 0, stream>>>(a, n_pairs);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    const bool partials = a.grad_strain || a.grad_cell;
+    const int threads = 128;
+    dense_atom_reduce<T><<<(unsigned)((a.n_atoms + threads - 1) / threads), threads, 0, stream>>>(a, partials ? 1 : 0);
+    CUDA_CHECK(cudaGetLastError());
+    if (partials && a.n_systems > 0) {
+        dense_system_reduce<T><<<(unsigned)a.n_systems, 256, 0, stream>>>(a);
+        CUDA_CHECK(cudaGetLastError());
+    }
+}
+
+template void launch_dense_forward<float>(const DenseArgs<float>&, int64_t, cudaStream_t);
+template void launch_dense_forward<double>(const DenseArgs<double>&, int64_t, cudaStream_t);
+template void launch_dense_backward<float>(const DenseArgs<float>&, int64_t, cudaStream_t);
+template void launch_dense_backward<double>(const DenseArgs<double>&, int64_t, cudaStream_t);
+
+}  // namespace fb200

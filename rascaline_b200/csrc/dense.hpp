@@ -1,0 +1,80 @@
+// Dense power spectrum with an adjoint backward pass.
+//
+// The forward pass writes the power spectrum of every atom as one dense row
+// [species pair (a <= b)][l, n1, n2] (zero for species pairs absent around the
+// atom) in FP64 or FP32, and keeps what the backward pass needs: the pairs,
+// the direction segments and the spherical expansion coefficients.  The
+// backward pass contracts dL/dP into dL/dpositions, dL/dcell and the strain
+// derivative without materialising any per-pair gradient block; the
+// per-pair Y_lm, R_nl and their derivatives are recomputed.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace fb200 {
+
+template <typename T>
+struct DenseArgs {
+    int lmax, nmax, n_species, n_keys, K;
+    int64_t n_atoms, n_props, n_systems;
+    FeatureLayout layout;
+    DevicePairs pairs;
+    const int32_t* atom_species;  // [n_atoms]
+    const int64_t* seg_offset;    // [n_atoms * S + 1]
+    const int32_t* dir_code;      // [2 n_pairs]
+    const int64_t* pair_start;    // [n_atoms + 1] pairs of each first atom
+    const int64_t* atom_offset;   // [n_systems + 1]
+    DeviceRadial exact;
+    DenseTables<T> tab;
+    CutoffParams cut;
+    T* features;          // [n_pairs][layout.stride]
+    T* coef;              // [n_atoms][S][K]
+    T* values;            // [n_atoms][n_keys][n_props]
+    const T* grad_values; // same layout
+    T* grad_coef;         // [n_atoms][S][K]
+    T* pair_grad;         // [n_pairs][3] dL/dr_ij
+    T* grad_positions;    // [n_atoms][3]
+    T* atom_partial;      // [n_atoms][18] strain then cell sums over the atom's own pairs
+    T* grad_strain;       // [n_systems][9] or null
+    T* grad_cell;         // [n_systems][9] or null
+    int32_t* status;
+};
+
+// State of one forward pass, owned by the caller until the backward pass
+struct DenseState {
+    Engine* engine = nullptr;
+    int device = -1;
+    int precision = 64;
+    cudaStream_t stream = nullptr;
+    int64_t n_atoms = 0, n_pairs = 0, n_systems = 0, n_props = 0;
+    int n_species = 0, n_keys = 0, K = 0;
+    std::vector<int32_t> species_types;
+    std::vector<int64_t> atom_offset;
+    DevicePairs pairs;
+    int64_t* pair_start = nullptr;
+    int32_t* atom_species = nullptr;
+    int64_t* seg_offset = nullptr;
+    int32_t* dir_code = nullptr;
+    int64_t* d_atom_offset = nullptr;
+    void* coef = nullptr;
+
+    DenseState() = default;
+    DenseState(const DenseState&) = delete;
+    ~DenseState();
+    void* alloc(size_t bytes);
+
+  private:
+    std::vector<void*> allocations_;
+};
+
+template <typename T>
+void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream);
+template <typename T>
+void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream);
+void launch_dense_directions(const DevicePairs& pairs, const int32_t* atom_species, int n_species, int64_t n_atoms,
+                             int32_t* dir_code, int64_t* seg_offset, DeviceArena& arena, cudaStream_t stream);
+
+}  // namespace fb200

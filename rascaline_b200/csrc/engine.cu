@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "dense.hpp"
 #include "engine.hpp"
 #include "plan.hpp"
 
@@ -298,6 +299,21 @@ void Engine::upload_tables() {
     d_ylm_.sq_ll1 = putv(ylm_.sq_ll1);
     d_ylm_.inv_ll = putv(ylm_.inv_ll);
     d_self_ = (double*)putv(radial_.self_contribution);
+
+    // the same tables for the dense kernels, in FP64 and rounded to FP32
+    auto putf = [&](const std::vector<double>& v) {
+        std::vector<float> f(v.begin(), v.end());
+        return (const float*)put(f.data(), f.size() * sizeof(float));
+    };
+    dense_d_.ylm = d_ylm_;
+    dense_d_.spline = {d_radial_.lmax, d_radial_.nmax, d_radial_.splined, d_radial_.knot_offset,
+                       d_radial_.knot_count, d_radial_.positions, d_radial_.values, d_radial_.derivs};
+    dense_d_.self_contribution = d_self_;
+    dense_f_.ylm = {ylm_.lmax,          putf(ylm_.A),      putf(ylm_.B),       putf(ylm_.sq_plus), putf(ylm_.sq_minus),
+                    putf(ylm_.sq_2l1), putf(ylm_.sq_half), putf(ylm_.sq_ll1), putf(ylm_.inv_ll)};
+    dense_f_.spline = {d_radial_.lmax,        d_radial_.nmax,       d_radial_.splined,    d_radial_.knot_offset,
+                       d_radial_.knot_count,  d_radial_.positions, putf(radial_.values), putf(radial_.derivs)};
+    dense_f_.self_contribution = putf(radial_.self_contribution);
     tables_ready_ = true;
 }
 
@@ -605,6 +621,203 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
     times_.transfer = elapsed_ms(ev[4], ev[5]);
     times_.total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     return tm;
+}
+
+// ---------------------------------------------------------------------------
+// Dense power spectrum and its adjoint
+// ---------------------------------------------------------------------------
+DenseState::~DenseState() {
+    for (void* p : allocations_) cudaFreeAsync(p, stream);
+}
+
+void* DenseState::alloc(size_t bytes) {
+    void* p = nullptr;
+    CUDA_CHECK(cudaMallocAsync(&p, std::max<size_t>(bytes, 8), stream));
+    allocations_.push_back(p);
+    return p;
+}
+
+template <typename T>
+void Engine::dense_args(const DenseState& st, bool grad, DenseArgs<T>& a) {
+    a = DenseArgs<T>{};
+    a.lmax = h_.max_angular;
+    a.nmax = h_.nmax();
+    a.n_species = st.n_species;
+    a.n_keys = st.n_keys;
+    a.K = st.K;
+    a.n_atoms = st.n_atoms;
+    a.n_props = st.n_props;
+    a.n_systems = st.n_systems;
+    a.layout = FeatureLayout::make(h_.max_angular, h_.nmax(), grad);
+    a.pairs = st.pairs;
+    a.atom_species = st.atom_species;
+    a.seg_offset = st.seg_offset;
+    a.dir_code = st.dir_code;
+    a.pair_start = st.pair_start;
+    a.atom_offset = st.d_atom_offset;
+    a.exact = d_radial_;
+    if constexpr (sizeof(T) == 8) a.tab = dense_d_;
+    else a.tab = dense_f_;
+    a.cut = CutoffParams{h_.cutoff, h_.smoothing_width, h_.smoothing, h_.scaling ? 1 : 0,
+                         h_.scaling_scale, h_.scaling_rate, h_.scaling_exponent};
+    a.coef = static_cast<T*>(st.coef);
+}
+
+std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<HostSystem>& systems,
+                                                  const double* d_positions, const std::vector<int32_t>& species,
+                                                  void* values, int64_t values_count, cudaStream_t stream) {
+    if (precision != 32 && precision != 64) throw invalid_parameter("precision must be 32 or 64");
+    upload_tables();
+    auto st = std::make_unique<DenseState>();
+    st->engine = this;
+    st->device = device_;
+    st->precision = precision;
+    st->stream = stream;
+    st->n_systems = (int64_t)systems.size();
+
+    std::vector<int32_t> types, atom_system;
+    st->atom_offset.assign(1, 0);
+    for (size_t s = 0; s < systems.size(); s++) {
+        types.insert(types.end(), systems[s].types.begin(), systems[s].types.end());
+        atom_system.insert(atom_system.end(), (size_t)systems[s].n_atoms, (int32_t)s);
+        st->atom_offset.push_back(st->atom_offset.back() + systems[s].n_atoms);
+    }
+    const int64_t n_atoms = st->n_atoms = (int64_t)types.size();
+    if (n_atoms >= (int64_t)INT32_MAX / 2) throw invalid_parameter("too many atoms");
+    std::vector<int32_t> sp = species.empty() ? types : species;
+    std::sort(sp.begin(), sp.end());
+    sp.erase(std::unique(sp.begin(), sp.end()), sp.end());
+    std::vector<int32_t> atom_species(n_atoms);
+    for (int64_t i = 0; i < n_atoms; i++) {
+        auto it = std::lower_bound(sp.begin(), sp.end(), types[i]);
+        if (it == sp.end() || *it != types[i])
+            throw invalid_parameter("atomic type " + std::to_string(types[i]) + " is not in the list of species");
+        atom_species[i] = (int32_t)(it - sp.begin());
+    }
+    st->species_types = sp;
+    const int S = st->n_species = (int)sp.size();
+    st->n_keys = S * (S + 1) / 2;
+    st->n_props = (int64_t)(h_.max_angular + 1) * h_.nmax() * h_.nmax();
+    st->K = (h_.max_angular + 1) * (h_.max_angular + 1) * h_.nmax();
+    const int64_t expected = n_atoms * st->n_keys * st->n_props;
+    if (values_count != expected) {
+        throw invalid_parameter("the values buffer must hold n_atoms x n_keys x n_properties = " +
+                                std::to_string(expected) + " elements, got " + std::to_string(values_count));
+    }
+    if (n_atoms > 0 && !values) throw invalid_parameter("values must not be NULL");
+    const size_t T_size = precision == 64 ? 8 : 4;
+
+    st->d_atom_offset = (int64_t*)st->alloc(sizeof(int64_t) * st->atom_offset.size());
+    CUDA_CHECK(cudaMemcpyAsync(st->d_atom_offset, st->atom_offset.data(), sizeof(int64_t) * st->atom_offset.size(),
+                               cudaMemcpyHostToDevice, stream));
+    if (n_atoms == 0) return st;
+    st->atom_species = (int32_t*)st->alloc(sizeof(int32_t) * n_atoms);
+    CUDA_CHECK(cudaMemcpyAsync(st->atom_species, atom_species.data(), sizeof(int32_t) * n_atoms,
+                               cudaMemcpyHostToDevice, stream));
+
+    // neighbour list (kernel a), then a private copy for the backward pass
+    std::vector<NlSystem> nls;
+    int64_t atom_off = 0, cell_off = 0;
+    for (auto& s : systems) {
+        NlSystem n = make_nl_system(s.cell, h_.cutoff, atom_off, s.n_atoms, cell_off);
+        cell_off += (int64_t)n.n_cells[0] * n.n_cells[1] * n.n_cells[2];
+        atom_off += s.n_atoms;
+        nls.push_back(n);
+    }
+    const int64_t P = nl_.build(nls, atom_system, d_positions, n_atoms, arena_, stream);
+    st->n_pairs = P;
+    st->pairs.count = P;
+    st->pairs.first = (int32_t*)st->alloc(sizeof(int32_t) * P);
+    st->pairs.second = (int32_t*)st->alloc(sizeof(int32_t) * P);
+    st->pairs.distance = (double*)st->alloc(sizeof(double) * P);
+    st->pairs.vector = (double*)st->alloc(sizeof(double) * 3 * P);
+    st->pairs.shift = (int32_t*)st->alloc(sizeof(int32_t) * 3 * P);
+    st->pair_start = (int64_t*)st->alloc(sizeof(int64_t) * (n_atoms + 1));
+    if (P > 0) {
+        CUDA_CHECK(cudaMemcpyAsync(st->pairs.first, nl_.pairs.first, 4 * P, cudaMemcpyDeviceToDevice, stream));
+        CUDA_CHECK(cudaMemcpyAsync(st->pairs.second, nl_.pairs.second, 4 * P, cudaMemcpyDeviceToDevice, stream));
+        CUDA_CHECK(cudaMemcpyAsync(st->pairs.distance, nl_.pairs.distance, 8 * P, cudaMemcpyDeviceToDevice, stream));
+        CUDA_CHECK(cudaMemcpyAsync(st->pairs.vector, nl_.pairs.vector, 24 * P, cudaMemcpyDeviceToDevice, stream));
+        CUDA_CHECK(cudaMemcpyAsync(st->pairs.shift, nl_.pairs.shift, 12 * P, cudaMemcpyDeviceToDevice, stream));
+    }
+    CUDA_CHECK(cudaMemcpyAsync(st->pair_start, nl_.pair_start, sizeof(int64_t) * (n_atoms + 1),
+                               cudaMemcpyDeviceToDevice, stream));
+
+    // direction segments, coefficients, power spectrum
+    st->dir_code = (int32_t*)st->alloc(sizeof(int32_t) * 2 * P);
+    st->seg_offset = (int64_t*)st->alloc(sizeof(int64_t) * (n_atoms * S + 1));
+    launch_dense_directions(st->pairs, st->atom_species, S, n_atoms, st->dir_code, st->seg_offset, arena_, stream);
+    st->coef = st->alloc(T_size * (size_t)n_atoms * S * st->K);
+    int32_t* status = arena_.alloc<int32_t>("dense.status", 1);
+    CUDA_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t), stream));
+    const FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), false);
+    void* features = arena_.alloc_bytes("dense.features", T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride);
+    if (precision == 64) {
+        DenseArgs<double> a;
+        dense_args(*st, false, a);
+        a.features = (double*)features;
+        a.values = (double*)values;
+        a.status = status;
+        launch_dense_forward<double>(a, P, stream);
+    } else {
+        DenseArgs<float> a;
+        dense_args(*st, false, a);
+        a.features = (float*)features;
+        a.values = (float*)values;
+        a.status = status;
+        launch_dense_forward<float>(a, P, stream);
+    }
+    if (!radial_.splined) {
+        int32_t h_status = 0;
+        CUDA_CHECK(cudaMemcpyAsync(&h_status, status, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        if (h_status) throw internal_error("the analytic radial integral did not converge");
+    }
+    return st;
+}
+
+void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_positions, void* grad_strain,
+                            void* grad_cell, cudaStream_t stream) {
+    int dev = -1;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev != st.device) throw invalid_parameter("the backward pass must run on the device of the forward pass");
+    if (st.n_atoms == 0) return;
+    if (!grad_values || !grad_positions) throw invalid_parameter("grad_values and grad_positions must not be NULL");
+    const size_t T_size = st.precision == 64 ? 8 : 4;
+    const int64_t P = st.n_pairs;
+    const FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), true);
+    void* features = arena_.alloc_bytes("dense.features_grad", T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride);
+    void* grad_coef = arena_.alloc_bytes("dense.grad_coef", T_size * (size_t)st.n_atoms * st.n_species * st.K);
+    void* pair_grad = arena_.alloc_bytes("dense.pair_grad", T_size * 3 * (size_t)std::max<int64_t>(P, 1));
+    void* partial = arena_.alloc_bytes("dense.atom_partial", T_size * 18 * (size_t)st.n_atoms);
+    int32_t* status = arena_.alloc<int32_t>("dense.status", 1);
+    if (st.precision == 64) {
+        DenseArgs<double> a;
+        dense_args(st, true, a);
+        a.features = (double*)features;
+        a.grad_values = (const double*)grad_values;
+        a.grad_coef = (double*)grad_coef;
+        a.pair_grad = (double*)pair_grad;
+        a.atom_partial = (double*)partial;
+        a.grad_positions = (double*)grad_positions;
+        a.grad_strain = (double*)grad_strain;
+        a.grad_cell = (double*)grad_cell;
+        a.status = status;
+        launch_dense_backward<double>(a, P, stream);
+    } else {
+        DenseArgs<float> a;
+        dense_args(st, true, a);
+        a.features = (float*)features;
+        a.grad_values = (const float*)grad_values;
+        a.grad_coef = (float*)grad_coef;
+        a.pair_grad = (float*)pair_grad;
+        a.atom_partial = (float*)partial;
+        a.grad_positions = (float*)grad_positions;
+        a.grad_strain = (float*)grad_strain;
+        a.grad_cell = (float*)grad_cell;
+        a.status = status;
+        launch_dense_backward<float>(a, P, stream);
+    }
 }
 
 }  // namespace fb200

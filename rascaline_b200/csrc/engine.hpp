@@ -75,6 +75,8 @@ struct DevicePairs {
 class NeighborBuilder {
   public:
     DevicePairs pairs;
+    // [n_atoms + 1] first pair of every atom (pairs are sorted by first atom)
+    const int64_t* pair_start = nullptr;
     int64_t build(const std::vector<NlSystem>& systems, const std::vector<int32_t>& atom_system,
                   const double* d_positions, int64_t n_atoms, DeviceArena& arena, cudaStream_t stream);
 };
@@ -95,9 +97,31 @@ struct DeviceRadial {
     const double* ortho;
 };
 
-struct DeviceYlm {
+// recursion coefficients of the spherical harmonics, in the arithmetic type T
+template <typename T>
+struct DeviceYlmT {
     int lmax;
-    const double *A, *B, *sq_plus, *sq_minus, *sq_2l1, *sq_half, *sq_ll1, *inv_ll;
+    const T *A, *B, *sq_plus, *sq_minus, *sq_2l1, *sq_half, *sq_ll1, *inv_ll;
+};
+using DeviceYlm = DeviceYlmT<double>;
+
+// spline tables with values / derivatives in T (knot positions in FP64)
+template <typename T>
+struct DeviceSplineT {
+    int lmax, nmax, splined;
+    const int32_t* knot_offset;
+    const int32_t* knot_count;
+    const double* positions;
+    const T* values;
+    const T* derivs;
+};
+
+// device tables of the dense kernels in one arithmetic type
+template <typename T>
+struct DenseTables {
+    DeviceYlmT<T> ylm;
+    DeviceSplineT<T> spline;
+    const T* self_contribution = nullptr;
 };
 
 struct CutoffParams {
@@ -233,6 +257,10 @@ void launch_se_output(const SeOutArgs& args, bool positions, bool strain, bool c
 
 namespace fb200 {
 
+struct DenseState;
+template <typename T>
+struct DenseArgs;
+
 struct PhaseTimes {
     double neighbors = 0, metadata = 0, features = 0, expansion = 0, contraction = 0, transfer = 0, total = 0;
     // kernels of the contraction phase
@@ -253,8 +281,23 @@ class Engine {
     const PhaseTimes& last_times() const { return times_; }
     int device() const { return device_; }
 
+    // dense power spectrum with its adjoint (dense.hpp); `species` empty means
+    // the sorted atomic types of the systems; `values` is a device buffer of
+    // n_atoms x n_keys x n_properties elements of the precision (32 / 64)
+    std::unique_ptr<DenseState> forward_dense(int precision, std::vector<HostSystem>& systems,
+                                              const double* d_positions, const std::vector<int32_t>& species,
+                                              void* values, int64_t values_count, cudaStream_t stream);
+    // dL/dpositions [n_atoms][3], and when not null dL/dstrain and dL/dcell
+    // [n_systems][3][3], all device buffers of the forward precision
+    void backward_dense(DenseState& state, const void* grad_values, void* grad_positions, void* grad_strain,
+                        void* grad_cell, cudaStream_t stream);
+
   private:
     void upload_tables();
+    template <typename T>
+    void dense_args(const DenseState& st, bool grad, DenseArgs<T>& a);
+    DenseTables<double> dense_d_{};
+    DenseTables<float> dense_f_{};
     Hypers h_;
     RadialTables radial_;
     YlmTables ylm_;

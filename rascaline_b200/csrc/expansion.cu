@@ -20,6 +20,7 @@
 //   cell gradients, with the (-1)^l / -(-1)^l factors of the reversed pair
 //   (spherical_expansion_pair.rs:130-163).
 #include "engine.hpp"
+#include "pair_math.cuh"
 #include "soap_math.cuh"
 
 namespace fb200 {
@@ -28,142 +29,6 @@ namespace {
 
 constexpr int LMAX_SMALL = 8;
 constexpr int LMAX_LARGE = 24;
-
-template <int LCAP>
-struct LegendreScratch {
-    static constexpr int N = (LCAP + 1) * (LCAP + 2) / 2;
-    double P[N], dP[N], Pot[N];
-};
-
-__device__ __forceinline__ int lidx(int l, int m) { return m + l * (l + 1) / 2; }
-
-// Real spherical harmonics without the Condon-Shortley phase, and their
-// gradients w.r.t. the unit direction (spherical_harmonics.rs:304-424).
-template <int LCAP>
-__device__ void ylm_compute(const DeviceYlm& T, double ux, double uy, double uz, double* __restrict__ Y,
-                            double* __restrict__ GX, double* __restrict__ GY, double* __restrict__ GZ) {
-    LegendreScratch<LCAP> s;
-    const int lmax = T.lmax;
-    const double SQRT_1_OVER_2PI = 0.3989422804014327;
-    const double SQRT_3 = 1.7320508075688772;
-    const double SQRT_3_OVER_2 = 1.224744871391589;
-    const double SQRT_2 = 1.4142135623730951;
-
-    double sxy = hypot(ux, uy);
-    double ct = uz, st = sxy;
-    double cp, sp;
-    if (sxy > soap::DBL_EPS) {
-        cp = ux / sxy;
-        sp = uy / sxy;
-    } else {
-        cp = 1.0;
-        sp = 0.0;
-    }
-    // associated Legendre polynomials (:228-251)
-    double value = SQRT_1_OVER_2PI;
-    s.P[0] = value;
-    if (lmax > 0) {
-        s.P[lidx(1, 0)] = ct * SQRT_3 * value;
-        value *= -SQRT_3_OVER_2 * st;
-        s.P[lidx(1, 1)] = value;
-        for (int l = 2; l <= lmax; l++) {
-            for (int m = 0; m < l - 1; m++)
-                s.P[lidx(l, m)] = T.A[lidx(l, m)] * (ct * s.P[lidx(l - 1, m)] + T.B[lidx(l, m)] * s.P[lidx(l - 2, m)]);
-            s.P[lidx(l, l - 1)] = ct * T.sq_2l1[l] * value;
-            value *= -T.sq_half[l] * st;
-            s.P[lidx(l, l)] = value;
-        }
-    }
-    bool grad = GX != nullptr;
-    if (grad) {
-        // derivative factors (:256-298)
-        s.dP[0] = 0.0;
-        for (int l = 1; l <= lmax; l++) {
-            double pm1 = T.inv_ll[l] * s.P[lidx(l, 1)];
-            double pp1 = s.P[lidx(l, 1)];
-            s.dP[lidx(l, 0)] = T.sq_plus[lidx(l, 0)] * pm1 - T.sq_minus[lidx(l, 0)] * pp1;
-            for (int m = 1; m < l; m++)
-                s.dP[lidx(l, m)] = T.sq_plus[lidx(l, m)] * s.P[lidx(l, m - 1)] - T.sq_minus[lidx(l, m)] * s.P[lidx(l, m + 1)];
-            s.dP[lidx(l, l)] = T.sq_plus[lidx(l, l)] * s.P[lidx(l, l - 1)] - T.sq_minus[lidx(l, l)] * 0.0;
-        }
-        if (st > 0.1) {
-            for (int l = 0; l <= lmax; l++)
-                for (int m = 0; m <= l; m++) s.Pot[lidx(l, m)] = (double)m / st * s.P[lidx(l, m)];
-        } else {
-            for (int l = 0; l <= lmax; l++)
-                for (int m = 0; m <= l; m++) s.Pot[lidx(l, m)] = -0.5 / ct * s.dP[lidx(l, m)];
-        }
-    }
-    for (int l = 0; l <= lmax; l++) Y[l * l + l] = s.P[lidx(l, 0)] / SQRT_2;
-    if (grad) {
-        GX[0] = 0.0;
-        GY[0] = 0.0;
-        GZ[0] = 0.0;
-        for (int l = 1; l <= lmax; l++) {
-            double lf = T.sq_ll1[l] * s.P[lidx(l, 1)];
-            GX[l * l + l] = cp * ct * lf;
-            GY[l * l + l] = sp * ct * lf;
-            GZ[l * l + l] = -st * lf;
-        }
-    }
-    double cos1 = 1.0, sin1 = 0.0, cos2 = -cp, sin2 = sp;
-    double m2c = -2.0 * cp;
-    for (int m = 1; m <= lmax; m++) {
-        double smp = m2c * sin1 - sin2;
-        double cmp = m2c * cos1 - cos2;
-        sin2 = sin1;
-        sin1 = smp;
-        cos2 = cos1;
-        cos1 = cmp;
-        for (int l = m; l <= lmax; l++) {
-            double p = s.P[lidx(l, m)];
-            Y[l * l + l + m] = p * cmp;
-            Y[l * l + l - m] = p * smp;
-        }
-        if (grad) {
-            for (int l = m; l <= lmax; l++) {
-                double dp = s.dP[lidx(l, m)];
-                double sdp = smp * dp, cdp = cmp * dp;
-                double pot = s.Pot[lidx(l, m)];
-                GX[l * l + l + m] = sp * pot * smp - 0.5 * ct * cp * cdp;
-                GX[l * l + l - m] = -sp * pot * cmp - 0.5 * ct * cp * sdp;
-                GY[l * l + l + m] = -cp * pot * smp - 0.5 * ct * sp * cdp;
-                GY[l * l + l - m] = cp * pot * cmp - 0.5 * ct * sp * sdp;
-                GZ[l * l + l + m] = 0.5 * st * cdp;
-                GZ[l * l + l - m] = 0.5 * st * sdp;
-            }
-        }
-    }
-}
-
-__device__ bool radial_compute(const DeviceRadial& R, int l, double r, double* __restrict__ val, double* __restrict__ grad) {
-    const int N = R.nmax;
-    if (R.splined) {
-        const double* pos = R.positions + R.knot_offset[l];
-        int count = R.knot_count[l];
-        int k = soap::spline_interval(pos, count, r);
-        soap::HermiteWeights w = soap::hermite_weights(pos[k], pos[k + 1], r);
-        const double* pv = R.values + ((size_t)R.knot_offset[l] + k) * N;
-        const double* pd = R.derivs + ((size_t)R.knot_offset[l] + k) * N;
-        for (int n = 0; n < N; n++) {
-            val[n] = soap::hermite_value(w, pv[n], pd[n], pv[N + n], pd[N + n]);
-            if (grad) grad[n] = soap::hermite_derivative(w, pv[n], pd[n], pv[N + n], pd[N + n]);
-        }
-        return true;
-    }
-    double raw[64], graw[64];
-    bool ok = soap::gto_radial_raw(l, N, r, R.c, R.width2, R.bn, raw, grad ? graw : nullptr);
-    for (int k = 0; k < N; k++) {
-        double s = 0.0, sg = 0.0;
-        for (int n = 0; n < N; n++) {
-            s += raw[n] * R.ortho[k * N + n];
-            if (grad) sg += graw[n] * R.ortho[k * N + n];
-        }
-        val[k] = s;
-        if (grad) grad[k] = sg;
-    }
-    return ok;
-}
 
 template <int LCAP>
 __global__ void pair_features_kernel(DevicePairs pairs, DeviceRadial radial, DeviceYlm ylm, CutoffParams cut,
@@ -198,9 +63,10 @@ __global__ void pair_features_kernel(DevicePairs pairs, DeviceRadial radial, Dev
     f[11] = (double)pairs.shift[3 * p + 1];
     f[12] = (double)pairs.shift[3 * p + 2];
     if (L.with_grad) {
-        ylm_compute<LCAP>(ylm, u0, u1, u2, f + L.off_y, f + L.off_dy, f + L.off_dy + L.L2, f + L.off_dy + 2 * L.L2);
+        ylm_compute<double, LCAP>(ylm, u0, u1, u2, f + L.off_y, f + L.off_dy, f + L.off_dy + L.L2,
+                                  f + L.off_dy + 2 * L.L2);
     } else {
-        ylm_compute<LCAP>(ylm, u0, u1, u2, f + L.off_y, nullptr, nullptr, nullptr);
+        ylm_compute<double, LCAP>(ylm, u0, u1, u2, f + L.off_y, nullptr, nullptr, nullptr);
     }
     bool ok = true;
     for (int l = 0; l <= L.lmax; l++) {

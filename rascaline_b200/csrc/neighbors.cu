@@ -266,6 +266,7 @@ int64_t NeighborBuilder::build(const std::vector<NlSystem>& systems, const std::
         CUDA_CHECK(cudaGetLastError());
     }
     arena.exclusive_scan(d_pair_count, d_pair_start, n_atoms + 1, stream);
+    pair_start = d_pair_start;
     int64_t total = 0;
     CUDA_CHECK(cudaMemcpyAsync(&total, d_pair_start + n_atoms, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
     CUDA_CHECK(cudaStreamSynchronize(stream));

@@ -1,0 +1,259 @@
+"""featomic-torch style interface with an adjoint backward pass.
+
+Mirrors featomic-torch (``featomic-torch/include/featomic/torch/calculator.hpp``,
+``featomic-torch/src/calculator.cpp:190-383``): a calculator built from
+``(name, hypers)`` whose ``compute(systems)`` returns the SOAP power spectrum
+as a TensorMap of torch blocks connected to the systems' positions and cells
+in torch's autograd graph.
+
+featomic-torch's backward (``featomic-torch/src/autograd.cpp:237-317`` for
+positions, ``:429-503`` for the cell) contracts dL/dX with materialised
+explicit gradient blocks.  Here the backward pass is
+``featomic_b200_power_spectrum_dense_backward``: a CUDA adjoint that recomputes
+the per-pair terms and never builds the gradient blocks.  The forward runs in
+FP64 (``precision=64``, the drop-in values) or in FP32 (``precision=32``).
+The backward pass is not itself differentiable (no double backward).
+"""
+import ctypes
+import json
+
+import numpy as np
+import torch
+
+from . import _c_api as C
+from .calculators import CalculatorBase, Labels
+
+__all__ = ["System", "Calculator", "SoapPowerSpectrum", "TorchTensorMap", "TorchBlock", "dense_power_spectrum"]
+
+
+class System:
+    """Atomic types, positions [n, 3] and cell [3, 3] (rows are the cell
+    vectors; all zero for a non-periodic system) as torch tensors."""
+
+    def __init__(self, types, positions, cell=None):
+        self.types = torch.as_tensor(types, dtype=torch.int32).reshape(-1)
+        self.positions = positions
+        if cell is None:
+            cell = torch.zeros((3, 3), dtype=positions.dtype, device=positions.device)
+        self.cell = cell
+
+    def __len__(self):
+        return len(self.types)
+
+
+class DenseState:
+    """A forward pass kept for its backward pass (featomic_b200_dense_t)."""
+
+    def __init__(self, handle):
+        self._handle = handle
+        n = [ctypes.c_size_t() for _ in range(5)]
+        C.check(C.lib().featomic_b200_dense_shape(handle, *[ctypes.byref(x) for x in n]))
+        self.n_atoms, self.n_species, self.n_keys, self.n_properties, self.n_pairs = [x.value for x in n]
+
+    def species(self, with_counts=False):
+        species = np.zeros(max(1, self.n_species), dtype=np.int32)
+        counts = np.zeros((max(1, self.n_atoms), max(1, self.n_species)), dtype=np.int32)
+        ptr = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))  # noqa: E731
+        C.check(C.lib().featomic_b200_dense_species(self._handle, ptr(species),
+                                                     ptr(counts) if with_counts else None))
+        species = species[:self.n_species]
+        if with_counts:
+            return species, counts[:self.n_atoms, :self.n_species]
+        return species
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            try:
+                C.lib().featomic_b200_dense_free(self._handle)
+            except (AttributeError, TypeError):  # interpreter shutdown
+                pass
+            self._handle = None
+
+
+def _device_systems(positions, types, cells, sizes):
+    dev = C.featomic_b200_device_systems_t()
+    dev.n_systems = len(sizes)
+    dev.system_sizes = sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_size_t))
+    dev.types = types.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    dev.cells = cells.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    dev.positions = positions.data_ptr()
+    return dev
+
+
+def dense_power_spectrum(calculator, positions, types, cells, sizes, precision=64, species=None):
+    """Forward pass without autograd: (values [n_atoms, n_keys, n_properties]
+    torch tensor on the GPU, DenseState).  ``positions``: CUDA float64 tensor
+    [atoms, 3] of all systems; ``types`` [atoms]; ``cells`` [systems, 9] and
+    ``sizes`` [systems] on the host."""
+    if not (positions.is_cuda and positions.dtype == torch.float64 and positions.is_contiguous()):
+        raise ValueError("positions must be a contiguous CUDA float64 tensor")
+    types = np.ascontiguousarray(types, dtype=np.int32)
+    cells = np.ascontiguousarray(cells, dtype=np.float64).reshape(-1, 9)
+    sizes = np.ascontiguousarray(sizes, dtype=np.uintp)
+    if species is None:
+        sp = np.unique(types).astype(np.int32)
+    else:
+        sp = np.unique(np.asarray(species, dtype=np.int32)).astype(np.int32)
+    S = len(sp)
+    params = json.loads(calculator._parameters)
+    L = params["basis"]["max_angular"]
+    N = params["basis"]["radial"]["max_radial"] + 1
+    n_keys, n_props = S * (S + 1) // 2, (L + 1) * N * N
+    dtype = torch.float64 if precision == 64 else torch.float32
+    values = torch.empty((len(types), n_keys, n_props), dtype=dtype, device=positions.device)
+    dev = _device_systems(positions, types, cells, sizes)
+    handle = ctypes.c_void_p()
+    stream = torch.cuda.current_stream(positions.device).cuda_stream
+    C.check(C.lib().featomic_b200_power_spectrum_dense(
+        calculator._handle, ctypes.byref(dev), sp.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), S, precision,
+        values.data_ptr(), values.numel(), ctypes.byref(handle), ctypes.c_void_p(stream)))
+    return values, DenseState(handle)
+
+
+def dense_backward(state, grad_values, n_systems, strain=False, cell=True):
+    """(dL/dpositions [atoms, 3], dL/dstrain [systems, 3, 3] or None,
+    dL/dcell [systems, 3, 3] or None) for dL/dvalues ``grad_values``."""
+    grad_values = grad_values.contiguous()
+    device, dtype = grad_values.device, grad_values.dtype
+    gpos = torch.empty((state.n_atoms, 3), dtype=dtype, device=device)
+    gstrain = torch.empty((n_systems, 3, 3), dtype=dtype, device=device) if strain else None
+    gcell = torch.empty((n_systems, 3, 3), dtype=dtype, device=device) if cell else None
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else None)  # noqa: E731
+    stream = torch.cuda.current_stream(device).cuda_stream
+    C.check(C.lib().featomic_b200_power_spectrum_dense_backward(
+        state._handle, ptr(grad_values), ptr(gpos), ptr(gstrain), ptr(gcell), ctypes.c_void_p(stream)))
+    return gpos, gstrain, gcell
+
+
+class _DensePowerSpectrum(torch.autograd.Function):
+    """positions [atoms, 3], cells [systems, 3, 3] -> dense power spectrum;
+    the backward pass is the CUDA adjoint."""
+
+    @staticmethod
+    def forward(ctx, positions, cells, calculator, types, sizes, precision, species, holder):
+        pos = positions.detach().to(torch.float64).contiguous()
+        cell_host = cells.detach().to(torch.float64).cpu().numpy().reshape(-1, 9)
+        values, state = dense_power_spectrum(calculator, pos, types, cell_host, sizes, precision, species)
+        holder.append(state)
+        ctx.state = state
+        ctx.n_systems = len(sizes)
+        ctx.dtypes = (positions.dtype, cells.dtype)
+        return values
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx, grad_values):
+        need_pos, need_cell = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        gpos, _, gcell = dense_backward(ctx.state, grad_values, ctx.n_systems, strain=False, cell=need_cell)
+        gpos = gpos.to(ctx.dtypes[0]) if need_pos else None
+        gcell = gcell.to(ctx.dtypes[1]) if need_cell else None
+        return gpos, gcell, None, None, None, None, None, None
+
+
+class TorchBlock:
+    def __init__(self, values, samples, properties):
+        self.values = values
+        self.samples = samples
+        self.properties = properties
+        self.components = []
+
+
+class TorchTensorMap:
+    def __init__(self, keys, blocks):
+        self.keys = keys
+        self._blocks = blocks
+
+    def __len__(self):
+        return len(self._blocks)
+
+    def block(self, index):
+        return self._blocks[index]
+
+    def blocks(self):
+        return list(self._blocks)
+
+
+class Calculator:
+    """featomic-torch's CalculatorHolder for the SOAP power spectrum."""
+
+    def __init__(self, name, parameters, precision=64, species=None):
+        if name != "soap_power_spectrum":
+            raise ValueError(f"the torch interface of featomic-b200 supports soap_power_spectrum, not {name}")
+        if precision not in (32, 64):
+            raise ValueError("precision must be 32 or 64")
+        self._calculator = CalculatorBase(name, parameters)
+        self.hypers = parameters if isinstance(parameters, dict) else json.loads(parameters)
+        self.precision = precision
+        self.species = None if species is None else sorted(set(int(s) for s in species))
+
+    @property
+    def name(self):
+        return self._calculator.name
+
+    @property
+    def parameters(self):
+        return self._calculator.parameters
+
+    def _gather(self, systems):
+        if isinstance(systems, System):
+            systems = [systems]
+        positions = torch.cat([s.positions.reshape(-1, 3) for s in systems])
+        cells = torch.stack([s.cell.reshape(3, 3) for s in systems])
+        types = np.concatenate([s.types.cpu().numpy() for s in systems]).astype(np.int32)
+        sizes = np.array([len(s) for s in systems], dtype=np.uintp)
+        return systems, positions, cells, types, sizes
+
+    def dense(self, systems):
+        """Dense power spectrum [atoms, n_keys, n_properties] of all systems
+        (see featomic_b200_power_spectrum_dense for the layout), differentiable
+        w.r.t. the positions and cells."""
+        systems, positions, cells, types, sizes = self._gather(systems)
+        return _DensePowerSpectrum.apply(positions, cells, self._calculator, types, sizes, self.precision,
+                                         self.species, [])
+
+    def compute(self, systems):
+        """The power spectrum in featomic's TensorMap layout: keys
+        (center_type, neighbor_1_type, neighbor_2_type), samples (system, atom)
+        of the centres that have both neighbour types, properties (l, n_1, n_2)."""
+        systems, positions, cells, types, sizes = self._gather(systems)
+        holder = []
+        values = _DensePowerSpectrum.apply(positions, cells, self._calculator, types, sizes, self.precision,
+                                           self.species, holder)
+        # which neighbour species every atom has, from the forward pass
+        species, counts = holder[0].species(with_counts=True)
+        S = len(species)
+        present = counts > 0
+        own = np.searchsorted(species, types)
+        present[np.arange(len(types)), own] = True
+        system_of = np.repeat(np.arange(len(sizes)), sizes.astype(np.int64))
+        atom_of = np.concatenate([np.arange(n) for n in sizes.astype(np.int64)]) if len(types) else np.zeros(0, int)
+        L = self.hypers["basis"]["max_angular"]
+        N = self.hypers["basis"]["radial"]["max_radial"] + 1
+        properties = Labels(["l", "n_1", "n_2"],
+                            [[l, n1, n2] for l in range(L + 1) for n1 in range(N) for n2 in range(N)])
+        keys, blocks = [], []
+        key = 0
+        key_of = {}
+        for a in range(S):
+            for b in range(a, S):
+                key_of[(a, b)] = key
+                key += 1
+        for c in range(S):
+            centres = own == c
+            for a in range(S):
+                for b in range(a, S):
+                    rows = np.nonzero(centres & present[:, a] & present[:, b])[0]
+                    if len(rows) == 0:
+                        continue
+                    index = torch.as_tensor(rows, device=values.device)
+                    block_values = values[index, key_of[(a, b)], :]
+                    samples = Labels(["system", "atom"], np.stack([system_of[rows], atom_of[rows]], axis=1))
+                    keys.append([species[c], species[a], species[b]])
+                    blocks.append(TorchBlock(block_values, samples, properties))
+        return TorchTensorMap(Labels(["center_type", "neighbor_1_type", "neighbor_2_type"], keys), blocks)
+
+
+class SoapPowerSpectrum(Calculator):
+    def __init__(self, cutoff, density, basis, precision=64, species=None):
+        super().__init__("soap_power_spectrum", {"cutoff": cutoff, "density": density, "basis": basis},
+                         precision=precision, species=species)

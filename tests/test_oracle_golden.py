@@ -72,6 +72,34 @@ def test_spherical_harmonics(oracle):
             assert_relative_eq(values[l * l:(l + 1) ** 2], expected[i, l, :2 * l + 1], 1e-11, epsilon=1e-11)
 
 
+def test_spherical_harmonics_gradient_pole_branch(oracle):
+    """featomic's Y_lm gradient (spherical_harmonics.rs:285-297) replaces
+    m P_l^m / sin(theta) by -delta P_l^m / (2 cos(theta)) when sin(theta) <= 0.1.
+    Away from the pole the gradient is the exact derivative of Y_lm(r / |r|);
+    inside the pole region it is this approximation, which the oracle and the
+    CUDA kernels reproduce: finite differences of featomic's own Y_lm do not
+    match its gradient there."""
+    lmax = 6
+
+    def fd_error(theta):
+        d = np.array([np.sin(theta) * np.cos(0.7), np.sin(theta) * np.sin(0.7), np.cos(theta)])
+        _, grad = oracle.spherical_harmonics(lmax, d, gradients=True)
+        fd = np.zeros_like(grad)
+        h = 1e-6
+        for x in range(3):
+            e = np.zeros(3)
+            e[x] = h
+            plus = oracle.spherical_harmonics(lmax, (d + e) / np.linalg.norm(d + e))
+            minus = oracle.spherical_harmonics(lmax, (d - e) / np.linalg.norm(d - e))
+            fd[x] = (plus - minus) / (2 * h)
+        return np.max(np.abs(fd - grad)) / np.max(np.abs(grad))
+
+    for theta in (1.2, 0.5, 0.2, 0.11):
+        assert fd_error(theta) < 1e-8, theta
+    for theta in (0.09, 0.05):
+        assert fd_error(theta) > 1e-3, theta
+
+
 def test_hyp1f1_table(oracle):
     table = known()["hyp1f1"]
     for entry in table["table"]:
