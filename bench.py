@@ -14,6 +14,9 @@ contraction, every row materialised in featomic's TensorMap layout.
 * ``e2e``    the same through featomic's C API (featomic_calculator_compute)
   with host systems: host->device positions and device->host TensorMap
   inside the timed region.
+* ``adjoint_form`` the adjoint form beside it: dense power spectrum with
+  FP32 arithmetic plus forces and virial of a linear energy through the CUDA
+  adjoint, on a 20 000-atom strained box, with its error against FP64.
 * ``cpu_baseline`` / ``--impl reference``: featomic itself is Rust and cannot
   be built here (no cargo / crates), so the CPU side is the FP64 C++
   restatement in oracle/ (OpenMP, featomic's decomposition: spherical
@@ -220,6 +223,88 @@ def run_reference(args):
     barrier(world)
 
 
+def adjoint_form(steps, warmup):
+    """The adjoint form on the 20 000-atom strained box: dense power spectrum
+    in FP32 arithmetic, then forces and virial of a linear energy model through
+    the CUDA adjoint (no gradient blocks materialised).  One step = forward +
+    backward; errors are measured once against the same calculation in FP64."""
+    import torch
+    import rascaline_b200 as rb
+    from rascaline_b200 import workloads
+    from rascaline_b200.torch_api import dense_backward, dense_power_spectrum
+
+    n = 20000
+    system = workloads.random_box(n, density=0.1, min_distance=0.9, seed=5, strain=0.02)
+    calc = rb.SoapPowerSpectrum(**workloads.hypers(5.0, 7, 6))
+    positions = torch.tensor(system["positions"], device="cuda")
+    types = system["types"].astype(np.int32)
+    cells = np.asarray(system["cell"]).reshape(1, 9)
+    sizes = np.array([n])
+    species = np.unique(types)
+    S = len(species)
+    n_keys, n_props = S * (S + 1) // 2, 7 * 8 * 8
+    rng = np.random.default_rng(11)
+    d = n_keys * n_props
+    weights = rng.normal(0.0, 1.0 / np.sqrt(d), size=(S, n_keys, n_props))  # per centre species
+    grad = torch.as_tensor(weights[np.searchsorted(species, types)], device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def run(precision, g):
+        values, state = dense_power_spectrum(calc, positions, types, cells, sizes, precision)
+        forces, virial, _ = dense_backward(state, g, 1, strain=True, cell=False)
+        return values, forces, virial
+
+    results = {}
+    for precision in (32, 64):
+        g = grad.float() if precision == 32 else grad
+        for _ in range(max(3, warmup)):
+            run(precision, g)
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        mids = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        stream = torch.cuda.current_stream()
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            values, state = dense_power_spectrum(calc, positions, types, cells, sizes, precision)
+            mids[k].record(stream)
+            forces, virial, _ = dense_backward(state, g, 1, strain=True, cell=False)
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        fwd = float(np.mean([s.elapsed_time(m) for s, m in zip(starts, mids)]))
+        bwd = float(np.mean([m.elapsed_time(e) for m, e in zip(mids, ends)]))
+        values, forces, virial = run(precision, g)
+        energy = float((values.double() * grad).sum())
+        results[precision] = dict(ms=fwd + bwd, forward_ms=fwd, backward_ms=bwd, energy=energy,
+                                  values=values.double(), forces=forces.double(), virial=virial.double())
+    r32, r64 = results[32], results[64]
+
+    def rel(a, b):
+        return float((a - b).abs().max() / b.abs().max())
+
+    return {
+        "workload": "random_box_20000_rho0.1_strain0.02_rc5_nmax7_lmax6_ps+forces+virial_adjoint",
+        "metric": "atom-envs/s (power spectrum + forces + virial)",
+        "value": n / (r32["ms"] / 1000.0),
+        "ms_per_step": r32["ms"],
+        "forward_ms": r32["forward_ms"],
+        "backward_ms": r32["backward_ms"],
+        "dtype": "f32",
+        "fp64_value": n / (r64["ms"] / 1000.0),
+        "fp64_ms_per_step": r64["ms"],
+        "error_vs_fp64": {
+            "values_max_abs_over_max": rel(r32["values"], r64["values"]),
+            "forces_max_abs_over_max": rel(r32["forces"], r64["forces"]),
+            "virial_max_abs_over_max": rel(r32["virial"], r64["virial"]),
+            "energy_rel": abs(r32["energy"] - r64["energy"]) / abs(r64["energy"]),
+        },
+        "steps": steps,
+        "l2": "flushed between steps (256 MiB write); the 358 MB FP32 output also exceeds L2",
+        "energy_model": "E = sum over atoms of w[centre species] . P, w ~ N(0, 1/sqrt(d)) seeded",
+    }
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -227,6 +312,8 @@ def main():
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-chosen-forms", action="store_true",
+                        help="skip the FP32 adjoint form measured beside the drop-in")
     parser.add_argument("--atoms", type=int, default=1000,
                         help="atoms in the box (1000 is the benchmark; smaller boxes are for profiling)")
     args = parser.parse_args()
@@ -345,6 +432,9 @@ def main():
         "clocks": clocks,
         "gpu_launches": 11 * args.steps,
     }
+    if not args.no_chosen_forms:
+        line["adjoint_form"] = adjoint_form(args.steps, args.warmup)
+        line["adjoint_form"]["gpu_launches_per_step"] = 14
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(system, hypers)
     print(json.dumps(line), flush=True)
