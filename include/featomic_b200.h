@@ -274,6 +274,62 @@ featomic_status_t featomic_b200_power_spectrum_dense_backward(featomic_b200_dens
 
 featomic_status_t featomic_b200_dense_free(featomic_b200_dense_t* state);
 
+/* ---- batched form: many molecules in one persistent launch ------------------
+ *
+ * Non-periodic systems (molecules) of up to 4096 atoms each, computed with
+ * FP32 arithmetic by one persistent, cooperative kernel launch replayed from a
+ * captured CUDA graph.  Per atom it produces the dense power spectrum row (the
+ * layout of featomic_b200_power_spectrum_dense), and for a loss L the
+ * gradient dL/dpositions through the adjoint, without gradient blocks.  L is
+ * either a linear model E = sum_atoms weights[species] . P (`weights`, float32
+ * [n_species][n_keys][n_properties]) or any loss with dL/dP given per atom
+ * (`grad_values`, float32 [n_atoms][n_keys][n_properties]).  Limits:
+ * max_angular <= 8, max_radial <= 15, at most 8 species.  No counterpart in
+ * featomic. */
+typedef struct featomic_b200_batch_t featomic_b200_batch_t;
+
+/* Plan a batch: system sizes and atomic types (host); `species` (NULL for
+ * the types present) fixes the species list.  The plan keeps its own device
+ * tables and the captured graphs. */
+featomic_status_t featomic_b200_batch_create(featomic_calculator_t* calculator, uintptr_t n_systems,
+                                             const uintptr_t* system_sizes, const int32_t* types,
+                                             const int32_t* species, uintptr_t n_species,
+                                             featomic_b200_batch_t** batch);
+
+featomic_status_t featomic_b200_batch_shape(const featomic_b200_batch_t* batch, uintptr_t* n_atoms,
+                                            uintptr_t* n_systems, uintptr_t* n_species, uintptr_t* n_keys,
+                                            uintptr_t* n_properties);
+
+/* One replay on `stream`.  `positions` is device float64 [n_atoms][3]; every
+ * output is a device float32 buffer or NULL: `values` [n_atoms][n_keys]
+ * [n_properties], `grad_positions` dL/dr [n_atoms][3], `energies` (linear
+ * model) [n_systems], `grad_strain` dL/dstrain [n_systems][3][3].  Give at
+ * most one of `weights` and `grad_values`; with neither only the values are
+ * computed.  The first run with a new set of buffers captures a graph. */
+featomic_status_t featomic_b200_batch_run(featomic_b200_batch_t* batch, const double* positions,
+                                          const float* weights, const float* grad_values, float* values,
+                                          float* grad_positions, float* energies, float* grad_strain,
+                                          void* stream);
+
+/* Time every launch configuration on these buffers and keep the fastest;
+ * `best_ms` receives its time per run. */
+featomic_status_t featomic_b200_batch_tune(featomic_b200_batch_t* batch, const double* positions,
+                                           const float* weights, const float* grad_values, float* values,
+                                           float* grad_positions, float* energies, float* grad_strain,
+                                           void* stream, double* best_ms);
+
+/* The launch configuration: [warps per CTA, directions staged per warp,
+ * coefficient layout (0: lane per (l, m, n), 1: lane per (l, m)), CTAs per
+ * SM]. */
+featomic_status_t featomic_b200_batch_config(const featomic_b200_batch_t* batch, int32_t* config);
+featomic_status_t featomic_b200_batch_set_config(featomic_b200_batch_t* batch, const int32_t* config);
+
+/* Error bits of the last run (waits for `stream`): 1 the radial integral
+ * failed, 2 the grid barrier timed out. */
+featomic_status_t featomic_b200_batch_status(featomic_b200_batch_t* batch, void* stream, int32_t* status);
+
+featomic_status_t featomic_b200_batch_free(featomic_b200_batch_t* batch);
+
 /* Radial integral R_nl(r) and dR_nl/dr of this calculator, as the kernels see
  * it (the Hermite spline of featomic/src/calculators/soap/radial_integral/
  * spline.rs, or the analytic GTO integral of radial_integral/gto.rs when

@@ -125,6 +125,18 @@ SIGNATURES = {
                                                         ctypes.POINTER(ctypes.c_int32)]),
     "featomic_b200_power_spectrum_dense_backward": (featomic_status_t, [ctypes.c_void_p] + [ctypes.c_void_p] * 5),
     "featomic_b200_dense_free": (featomic_status_t, [ctypes.c_void_p]),
+    "featomic_b200_batch_create": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t,
+                                                       ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int32),
+                                                       ctypes.POINTER(ctypes.c_int32), ctypes.c_size_t,
+                                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "featomic_b200_batch_shape": (featomic_status_t, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_size_t)] * 5),
+    "featomic_b200_batch_run": (featomic_status_t, [ctypes.c_void_p] * 9),
+    "featomic_b200_batch_tune": (featomic_status_t, [ctypes.c_void_p] * 9 + [ctypes.POINTER(ctypes.c_double)]),
+    "featomic_b200_batch_config": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
+    "featomic_b200_batch_set_config": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
+    "featomic_b200_batch_status": (featomic_status_t, [ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.POINTER(ctypes.c_int32)]),
+    "featomic_b200_batch_free": (featomic_status_t, [ctypes.c_void_p]),
     "featomic_b200_radial_integral": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                           ctypes.c_size_t, ctypes.POINTER(ctypes.c_double),
                                                           ctypes.POINTER(ctypes.c_double),

@@ -15,6 +15,7 @@
 #include <sstream>
 
 #include "../../include/featomic_b200.h"
+#include "batched.hpp"
 #include "dense.hpp"
 #include "engine.hpp"
 #include "host.hpp"
@@ -441,6 +442,108 @@ featomic_status_t featomic_b200_power_spectrum_dense_backward(featomic_b200_dens
 
 featomic_status_t featomic_b200_dense_free(featomic_b200_dense_t* state) {
     return guarded([&] { delete state; });
+}
+
+struct featomic_b200_batch_t {
+    std::unique_ptr<fb200::BatchPlan> plan;
+};
+
+featomic_status_t featomic_b200_batch_create(featomic_calculator_t* calculator, uintptr_t n_systems,
+                                             const uintptr_t* system_sizes, const int32_t* types,
+                                             const int32_t* species, uintptr_t n_species,
+                                             featomic_b200_batch_t** batch) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(batch);
+        *batch = nullptr;
+        if (!calculator->impl->power_spectrum)
+            throw invalid_parameter("featomic_b200_batch_create needs a soap_power_spectrum calculator");
+        if (n_systems > 0) CHECK_POINTER(system_sizes);
+        std::vector<int64_t> sizes(n_systems);
+        int64_t total = 0;
+        for (uintptr_t s = 0; s < n_systems; s++) total += (int64_t)(sizes[s] = (int64_t)system_sizes[s]);
+        if (total > 0) CHECK_POINTER(types);
+        std::vector<int32_t> t(types, types + total), sp;
+        if (n_species > 0) {
+            CHECK_POINTER(species);
+            sp.assign(species, species + n_species);
+        }
+        auto result = std::make_unique<featomic_b200_batch_t>();
+        result->plan = std::make_unique<BatchPlan>(*calculator->impl->engine, sizes, t, sp);
+        *batch = result.release();
+    });
+}
+
+featomic_status_t featomic_b200_batch_shape(const featomic_b200_batch_t* batch, uintptr_t* n_atoms,
+                                            uintptr_t* n_systems, uintptr_t* n_species, uintptr_t* n_keys,
+                                            uintptr_t* n_properties) {
+    return guarded([&] {
+        CHECK_POINTER(batch);
+        const BatchPlan& p = *batch->plan;
+        if (n_atoms) *n_atoms = (uintptr_t)p.n_atoms();
+        if (n_systems) *n_systems = (uintptr_t)p.n_systems();
+        if (n_species) *n_species = (uintptr_t)p.n_species();
+        if (n_keys) *n_keys = (uintptr_t)p.n_keys();
+        if (n_properties) *n_properties = (uintptr_t)p.n_props();
+    });
+}
+
+featomic_status_t featomic_b200_batch_run(featomic_b200_batch_t* batch, const double* positions,
+                                          const float* weights, const float* grad_values, float* values,
+                                          float* grad_positions, float* energies, float* grad_strain,
+                                          void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(batch);
+        batch->plan->run(positions, weights, grad_values, values, grad_positions, energies, grad_strain,
+                         (cudaStream_t)stream);
+    });
+}
+
+featomic_status_t featomic_b200_batch_tune(featomic_b200_batch_t* batch, const double* positions,
+                                           const float* weights, const float* grad_values, float* values,
+                                           float* grad_positions, float* energies, float* grad_strain,
+                                           void* stream, double* best_ms) {
+    return guarded([&] {
+        CHECK_POINTER(batch);
+        const double ms = batch->plan->tune(positions, weights, grad_values, values, grad_positions, energies,
+                                            grad_strain, (cudaStream_t)stream);
+        if (best_ms) *best_ms = ms;
+    });
+}
+
+featomic_status_t featomic_b200_batch_config(const featomic_b200_batch_t* batch, int32_t* config) {
+    return guarded([&] {
+        CHECK_POINTER(batch);
+        CHECK_POINTER(config);
+        const BatchConfig& c = batch->plan->config;
+        config[0] = c.warps;
+        config[1] = c.chunk;
+        config[2] = c.layout;
+        config[3] = c.ctas_per_sm;
+    });
+}
+
+featomic_status_t featomic_b200_batch_set_config(featomic_b200_batch_t* batch, const int32_t* config) {
+    return guarded([&] {
+        CHECK_POINTER(batch);
+        CHECK_POINTER(config);
+        if ((config[0] != 4 && config[0] != 8) || (config[1] != 16 && config[1] != 32) ||
+            (config[2] != 0 && config[2] != 1) || config[3] < 1 || config[3] > 8)
+            throw invalid_parameter("invalid batch configuration");
+        batch->plan->config = BatchConfig{config[0], config[1], config[2], config[3]};
+    });
+}
+
+featomic_status_t featomic_b200_batch_status(featomic_b200_batch_t* batch, void* stream, int32_t* status) {
+    return guarded([&] {
+        CHECK_POINTER(batch);
+        CHECK_POINTER(status);
+        *status = batch->plan->status((cudaStream_t)stream);
+    });
+}
+
+featomic_status_t featomic_b200_batch_free(featomic_b200_batch_t* batch) {
+    return guarded([&] { delete batch; });
 }
 
 featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t n_atoms, const double* cell,

@@ -292,6 +292,17 @@ class Engine {
     void backward_dense(DenseState& state, const void* grad_values, void* grad_positions, void* grad_strain,
                         void* grad_cell, cudaStream_t stream);
 
+    // device tables for the kernels of the batched form (uploaded on first use)
+    const DenseTables<float>& dense_tables_f() {
+        upload_tables();
+        return dense_f_;
+    }
+    const DeviceRadial& device_radial() {
+        upload_tables();
+        return d_radial_;
+    }
+    const Hypers& hypers() const { return h_; }
+
   private:
     void upload_tables();
     template <typename T>

@@ -23,7 +23,7 @@ import torch
 from . import _c_api as C
 from .calculators import CalculatorBase, Labels
 
-__all__ = ["System", "Calculator", "SoapPowerSpectrum", "TorchTensorMap", "TorchBlock", "dense_power_spectrum"]
+__all__ = ["System", "Calculator", "SoapPowerSpectrum", "TorchTensorMap", "TorchBlock", "Batch", "dense_power_spectrum"]
 
 
 class System:
@@ -257,3 +257,91 @@ class SoapPowerSpectrum(Calculator):
     def __init__(self, cutoff, density, basis, precision=64, species=None):
         super().__init__("soap_power_spectrum", {"cutoff": cutoff, "density": density, "basis": basis},
                          precision=precision, species=species)
+
+
+class Batch:
+    """Many non-periodic systems (molecules) through one persistent launch
+    replayed from a captured CUDA graph, FP32 arithmetic
+    (``featomic_b200_batch_*``).  ``sizes`` and ``types`` describe the
+    systems; the positions can change between runs."""
+
+    def __init__(self, calculator, sizes, types, species=None):
+        calc = calculator._calculator if isinstance(calculator, Calculator) else calculator
+        self._calculator = calc
+        sizes = np.ascontiguousarray(sizes, dtype=np.uintp)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        sp = None if species is None else np.ascontiguousarray(sorted(set(int(s) for s in species)), dtype=np.int32)
+        handle = ctypes.c_void_p()
+        C.check(C.lib().featomic_b200_batch_create(
+            calc._handle, len(sizes), sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_size_t)),
+            types.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            sp.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if sp is not None else None,
+            0 if sp is None else len(sp), ctypes.byref(handle)))
+        self._handle = handle
+        n = [ctypes.c_size_t() for _ in range(5)]
+        C.check(C.lib().featomic_b200_batch_shape(handle, *[ctypes.byref(x) for x in n]))
+        self.n_atoms, self.n_systems, self.n_species, self.n_keys, self.n_properties = [x.value for x in n]
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            try:
+                C.lib().featomic_b200_batch_free(self._handle)
+            except (AttributeError, TypeError):  # interpreter shutdown
+                pass
+            self._handle = None
+
+    def outputs(self, device="cuda", values=True, gradients=True, energies=True, strain=False):
+        """Output buffers for run(): a dict of float32 CUDA tensors."""
+        out = {}
+        if values:
+            out["values"] = torch.empty((self.n_atoms, self.n_keys, self.n_properties), dtype=torch.float32,
+                                        device=device)
+        if gradients:
+            out["gradients"] = torch.empty((self.n_atoms, 3), dtype=torch.float32, device=device)
+        if energies:
+            out["energies"] = torch.empty(self.n_systems, dtype=torch.float32, device=device)
+        if strain:
+            out["strain"] = torch.empty((self.n_systems, 3, 3), dtype=torch.float32, device=device)
+        return out
+
+    def _pointers(self, positions, weights, grad_values, out):
+        if not (positions.is_cuda and positions.dtype == torch.float64 and positions.is_contiguous()):
+            raise ValueError("positions must be a contiguous CUDA float64 tensor")
+        for t in (weights, grad_values):
+            if t is not None and not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+                raise ValueError("weights / grad_values must be contiguous CUDA float32 tensors")
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else None)  # noqa: E731
+        return [ptr(positions), ptr(weights), ptr(grad_values), ptr(out.get("values")), ptr(out.get("gradients")),
+                ptr(out.get("energies")), ptr(out.get("strain"))]
+
+    def run(self, positions, out, weights=None, grad_values=None):
+        """One graph replay on the current stream, filling the tensors of ``out``."""
+        stream = ctypes.c_void_p(torch.cuda.current_stream(positions.device).cuda_stream)
+        C.check(C.lib().featomic_b200_batch_run(self._handle, *self._pointers(positions, weights, grad_values, out),
+                                                 stream))
+        return out
+
+    def tune(self, positions, out, weights=None, grad_values=None):
+        """Time every launch configuration and keep the fastest; returns ms per run."""
+        stream = ctypes.c_void_p(torch.cuda.current_stream(positions.device).cuda_stream)
+        best = ctypes.c_double()
+        C.check(C.lib().featomic_b200_batch_tune(self._handle, *self._pointers(positions, weights, grad_values, out),
+                                                  stream, ctypes.byref(best)))
+        return best.value
+
+    @property
+    def config(self):
+        c = (ctypes.c_int32 * 4)()
+        C.check(C.lib().featomic_b200_batch_config(self._handle, c))
+        return {"warps": c[0], "chunk": c[1], "layout": c[2], "ctas_per_sm": c[3]}
+
+    @config.setter
+    def config(self, value):
+        c = (ctypes.c_int32 * 4)(value["warps"], value["chunk"], value["layout"], value["ctas_per_sm"])
+        C.check(C.lib().featomic_b200_batch_set_config(self._handle, c))
+
+    def status(self):
+        s = ctypes.c_int32()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        C.check(C.lib().featomic_b200_batch_status(self._handle, stream, ctypes.byref(s)))
+        return s.value
