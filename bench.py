@@ -17,6 +17,8 @@ contraction, every row materialised in featomic's TensorMap layout.
 * ``adjoint_form`` the adjoint form beside it: dense power spectrum with
   FP32 arithmetic plus forces and virial of a linear energy through the CUDA
   adjoint, on a 20 000-atom strained box, with its error against FP64.
+* ``batched_form`` 4096 molecules through one persistent launch replayed from
+  a CUDA graph (FP32, autotuned), power spectrum + forces + energies.
 * ``cpu_baseline`` / ``--impl reference``: featomic itself is Rust and cannot
   be built here (no cargo / crates), so the CPU side is the FP64 C++
   restatement in oracle/ (OpenMP, featomic's decomposition: spherical
@@ -305,6 +307,103 @@ def adjoint_form(steps, warmup):
     }
 
 
+def batched_form(steps, warmup):
+    """The batched form on 4096 seeded molecules (5 to 60 atoms, species 1/6/7/8
+    with p = .5/.3/.1/.1, uniform in a sphere of radius 1.2 N^(1/3) A, minimum
+    distance 1.0 A): power spectrum rows, dE/dpositions and energies of a
+    linear model, FP32, one persistent launch replayed from a CUDA graph with
+    the configuration picked by the autotuner.  Errors against the dense FP64
+    path on the same molecules."""
+    import torch
+    import rascaline_b200 as rb
+    from rascaline_b200 import workloads
+    from rascaline_b200.torch_api import Batch, dense_backward, dense_power_spectrum
+
+    mols = workloads.molecules(4096, seed=3)
+    positions = np.concatenate([m["positions"] for m in mols])
+    types = np.concatenate([m["types"] for m in mols]).astype(np.int32)
+    sizes = np.array([len(m["types"]) for m in mols])
+    species = [1, 6, 7, 8]
+    calc = rb.SoapPowerSpectrum(**workloads.hypers(5.0, 7, 6))
+    batch = Batch(calc, sizes, types, species)
+    rng = np.random.default_rng(17)
+    W = rng.normal(0.0, 1.0 / np.sqrt(batch.n_keys * batch.n_properties),
+                   size=(len(species), batch.n_keys, batch.n_properties))
+    weights = torch.as_tensor(W, dtype=torch.float32, device="cuda").contiguous()
+    pos = torch.as_tensor(positions, device="cuda")
+    out = batch.outputs()
+    tuned_ms = batch.tune(pos, out, weights=weights)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(max(3, warmup)):
+        batch.run(pos, out, weights=weights)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        starts[k].record(stream)
+        batch.run(pos, out, weights=weights)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    ms = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)]))
+    if batch.status() != 0:
+        raise RuntimeError("the batched form reported an error")
+
+    # end to end: positions from pinned host memory, gradients and energies back
+    host_pos = torch.as_tensor(positions).pin_memory()
+    host_grad = torch.empty((batch.n_atoms, 3), dtype=torch.float32).pin_memory()
+    host_energy = torch.empty(batch.n_systems, dtype=torch.float32).pin_memory()
+    e2e = []
+    for k in range(max(3, steps // 2) + 2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pos.copy_(host_pos, non_blocking=True)
+        batch.run(pos, out, weights=weights)
+        host_grad.copy_(out["gradients"], non_blocking=True)
+        host_energy.copy_(out["energies"], non_blocking=True)
+        torch.cuda.synchronize()
+        if k >= 2:
+            e2e.append(time.perf_counter() - t0)
+    e2e_ms = 1000.0 * float(np.mean(e2e))
+
+    # error against FP64
+    values64, state = dense_power_spectrum(calc, pos, types, np.zeros((len(mols), 9)), sizes, 64, species)
+    G = torch.as_tensor(W[np.searchsorted(species, types)], device="cuda")
+    grad64, _, _ = dense_backward(state, G, len(mols), strain=False, cell=False)
+    atom_energy = (values64 * G).sum(dim=(1, 2))
+    system = torch.as_tensor(np.repeat(np.arange(len(mols)), sizes), device="cuda")
+    energy64 = torch.zeros(len(mols), dtype=torch.float64, device="cuda").index_add_(0, system, atom_energy)
+
+    def rel(a, b):
+        return float((a.double() - b).abs().max() / b.abs().max())
+
+    errors = {
+        "values_max_abs_over_max": rel(out["values"], values64),
+        "gradients_max_abs_over_max": rel(out["gradients"], grad64),
+        "energies_max_abs_over_max": rel(out["energies"], energy64),
+    }
+    del values64, state, G
+    n = batch.n_atoms
+    return {
+        "workload": "molecules_4096_sizes5-60_rc5_nmax7_lmax6_ps+gradients+energies_persistent_graph",
+        "metric": "atom-envs/s (power spectrum + forces)",
+        "value": n / (ms / 1000.0),
+        "ms_per_step": ms,
+        "n_atoms": n,
+        "dtype": "f32",
+        "config": batch.config,
+        "tuned_ms": tuned_ms,
+        "e2e": {"value": n / (e2e_ms / 1000.0), "unit": "atom-envs/s", "h2d_bytes_per_step": n * 24,
+                "d2h_bytes_per_step": n * 12 + batch.n_systems * 4},
+        "error_vs_fp64": errors,
+        "gpu_launches_per_step": 1,
+        "steps": steps,
+        "l2": "flushed between steps (256 MiB write); the 2.4 GB FP32 output also exceeds L2",
+        "energy_model": "E = sum over atoms of w[centre species] . P, w ~ N(0, 1/sqrt(d)) seeded",
+    }
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -435,6 +534,7 @@ def main():
     if not args.no_chosen_forms:
         line["adjoint_form"] = adjoint_form(args.steps, args.warmup)
         line["adjoint_form"]["gpu_launches_per_step"] = 14
+        line["batched_form"] = batched_form(args.steps, args.warmup)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(system, hypers)
     print(json.dumps(line), flush=True)
