@@ -330,6 +330,58 @@ featomic_status_t featomic_b200_batch_status(featomic_b200_batch_t* batch, void*
 
 featomic_status_t featomic_b200_batch_free(featomic_b200_batch_t* batch);
 
+/* ---- learned radial surrogate -------------------------------------------------
+ *
+ * A small MLP r -> R_nl(r), 1 -> 64 -> 64 -> (max_angular + 1) (max_radial + 1)
+ * with SiLU activations, trained on the GPU by this library's own kernels on
+ * exact (analytic GTO) radial integrals of the calculator, evaluated with
+ * BF16 weights and FP32 accumulation on the tensor cores.  Attached to a
+ * calculator it replaces the spline in the FP32 dense power spectrum and its
+ * adjoint.  featomic's radial basis does not depend on the atomic species, so
+ * one network serves every species pair.  No counterpart in featomic. */
+typedef struct featomic_b200_surrogate_t featomic_b200_surrogate_t;
+
+featomic_status_t featomic_b200_surrogate_create(featomic_calculator_t* calculator, int32_t hidden, uint64_t seed,
+                                                 featomic_b200_surrogate_t** surrogate);
+/* number of outputs, of parameters and of training samples */
+featomic_status_t featomic_b200_surrogate_shape(const featomic_b200_surrogate_t* surrogate, uintptr_t* n_outputs,
+                                                uintptr_t* n_parameters, uintptr_t* n_samples);
+/* training set: `n_samples` distances uniform in [0, cutoff] and their exact
+ * radial integrals, computed on the GPU */
+featomic_status_t featomic_b200_surrogate_dataset(featomic_b200_surrogate_t* surrogate, uintptr_t n_samples,
+                                                  uint64_t seed, void* stream);
+/* `steps` Adam steps on random minibatches (one captured CUDA graph per step);
+ * `loss` receives the mean squared error of the normalised outputs of the last
+ * minibatch */
+featomic_status_t featomic_b200_surrogate_train(featomic_b200_surrogate_t* surrogate, uintptr_t steps,
+                                                uintptr_t batch, double learning_rate, double* loss, void* stream);
+/* loss and gradient (host, n_parameters) on the first `n` training samples */
+featomic_status_t featomic_b200_surrogate_gradient(featomic_b200_surrogate_t* surrogate, uintptr_t n,
+                                                   float* gradient, double* loss, void* stream);
+/* host copy of the FP32 parameters (w1, b1, W2, b2, W3, b3), of the output
+ * scales and of the training distances; `set` != 0 writes the parameters */
+featomic_status_t featomic_b200_surrogate_parameters(featomic_b200_surrogate_t* surrogate, float* parameters,
+                                                     uintptr_t count, int32_t set, void* stream);
+featomic_status_t featomic_b200_surrogate_scales(const featomic_b200_surrogate_t* surrogate, float* scales,
+                                                 uintptr_t count);
+featomic_status_t featomic_b200_surrogate_samples(const featomic_b200_surrogate_t* surrogate, float* r,
+                                                  uintptr_t count, void* stream);
+/* R_o(r) and dR_o/dr (o = l (max_radial + 1) + n) for `n` device distances,
+ * written to device float32 rows of stride `ld`; `method` 0: tensor cores,
+ * 1: CUDA cores (same network), 2: the calculator's FP64 spline, 3: the exact
+ * analytic integral */
+featomic_status_t featomic_b200_surrogate_evaluate(featomic_b200_surrogate_t* surrogate, const double* r,
+                                                   uintptr_t n, float* values, float* derivs, uintptr_t ld,
+                                                   int32_t method, void* stream);
+/* use `surrogate` (NULL: the spline) for the radial integral of this
+ * calculator's FP32 dense power spectrum and adjoint; the calculator only
+ * holds it weakly and falls back to the spline once it is freed */
+featomic_status_t featomic_b200_calculator_set_surrogate(featomic_calculator_t* calculator,
+                                                         featomic_b200_surrogate_t* surrogate);
+/* a surrogate can be freed before or after its calculator, but not used
+ * after its calculator is freed */
+featomic_status_t featomic_b200_surrogate_free(featomic_b200_surrogate_t* surrogate);
+
 /* Radial integral R_nl(r) and dR_nl/dr of this calculator, as the kernels see
  * it (the Hermite spline of featomic/src/calculators/soap/radial_integral/
  * spline.rs, or the analytic GTO integral of radial_integral/gto.rs when

@@ -137,6 +137,28 @@ SIGNATURES = {
     "featomic_b200_batch_status": (featomic_status_t, [ctypes.c_void_p, ctypes.c_void_p,
                                                        ctypes.POINTER(ctypes.c_int32)]),
     "featomic_b200_batch_free": (featomic_status_t, [ctypes.c_void_p]),
+    "featomic_b200_surrogate_create": (featomic_status_t, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint64,
+                                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "featomic_b200_surrogate_shape": (featomic_status_t, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_size_t)] * 3),
+    "featomic_b200_surrogate_dataset": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64,
+                                                            ctypes.c_void_p]),
+    "featomic_b200_surrogate_train": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
+                                                          ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                                          ctypes.c_void_p]),
+    "featomic_b200_surrogate_gradient": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t,
+                                                             ctypes.POINTER(ctypes.c_float),
+                                                             ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "featomic_b200_surrogate_parameters": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
+                                                               ctypes.c_size_t, ctypes.c_int32, ctypes.c_void_p]),
+    "featomic_b200_surrogate_scales": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
+                                                           ctypes.c_size_t]),
+    "featomic_b200_surrogate_samples": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
+                                                            ctypes.c_size_t, ctypes.c_void_p]),
+    "featomic_b200_surrogate_evaluate": (featomic_status_t, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                                             ctypes.c_int32, ctypes.c_void_p]),
+    "featomic_b200_calculator_set_surrogate": (featomic_status_t, [ctypes.c_void_p, ctypes.c_void_p]),
+    "featomic_b200_surrogate_free": (featomic_status_t, [ctypes.c_void_p]),
     "featomic_b200_radial_integral": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                           ctypes.c_size_t, ctypes.POINTER(ctypes.c_double),
                                                           ctypes.POINTER(ctypes.c_double),

@@ -19,6 +19,7 @@
 #include "dense.hpp"
 #include "engine.hpp"
 #include "host.hpp"
+#include "surrogate.hpp"
 
 using namespace fb200;
 
@@ -544,6 +545,134 @@ featomic_status_t featomic_b200_batch_status(featomic_b200_batch_t* batch, void*
 
 featomic_status_t featomic_b200_batch_free(featomic_b200_batch_t* batch) {
     return guarded([&] { delete batch; });
+}
+
+struct featomic_b200_surrogate_t {
+    std::shared_ptr<fb200::RadialSurrogate> impl;
+};
+
+featomic_status_t featomic_b200_surrogate_create(featomic_calculator_t* calculator, int32_t hidden, uint64_t seed,
+                                                 featomic_b200_surrogate_t** surrogate) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(surrogate);
+        *surrogate = nullptr;
+        auto result = std::make_unique<featomic_b200_surrogate_t>();
+        result->impl = std::make_shared<RadialSurrogate>(*calculator->impl->engine, hidden, seed);
+        *surrogate = result.release();
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_shape(const featomic_b200_surrogate_t* surrogate, uintptr_t* n_outputs,
+                                                uintptr_t* n_parameters, uintptr_t* n_samples) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        if (n_outputs) *n_outputs = (uintptr_t)surrogate->impl->n_outputs();
+        if (n_parameters) *n_parameters = (uintptr_t)surrogate->impl->n_params();
+        if (n_samples) *n_samples = (uintptr_t)surrogate->impl->n_samples();
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_dataset(featomic_b200_surrogate_t* surrogate, uintptr_t n_samples,
+                                                  uint64_t seed, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        surrogate->impl->make_dataset((int64_t)n_samples, seed, (cudaStream_t)stream);
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_train(featomic_b200_surrogate_t* surrogate, uintptr_t steps,
+                                                uintptr_t batch, double learning_rate, double* loss, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        if (!(learning_rate > 0.0 && std::isfinite(learning_rate)))
+            throw invalid_parameter("the learning rate must be positive");
+        const double l = surrogate->impl->train((int64_t)steps, (int64_t)batch, learning_rate, (cudaStream_t)stream);
+        if (loss) *loss = l;
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_gradient(featomic_b200_surrogate_t* surrogate, uintptr_t n,
+                                                   float* gradient, double* loss, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        CHECK_POINTER(gradient);
+        std::vector<float> g;
+        const double l = surrogate->impl->loss_and_gradient((int64_t)n, g, (cudaStream_t)stream);
+        std::copy(g.begin(), g.end(), gradient);
+        if (loss) *loss = l;
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_parameters(featomic_b200_surrogate_t* surrogate, float* parameters,
+                                                     uintptr_t count, int32_t set, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        CHECK_POINTER(parameters);
+        if ((int64_t)count != surrogate->impl->n_params())
+            throw invalid_parameter("expected " + std::to_string(surrogate->impl->n_params()) + " parameters");
+        if (set) {
+            surrogate->impl->set_parameters(std::vector<float>(parameters, parameters + count), (cudaStream_t)stream);
+        } else {
+            const std::vector<float> p = surrogate->impl->parameters((cudaStream_t)stream);
+            std::copy(p.begin(), p.end(), parameters);
+        }
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_scales(const featomic_b200_surrogate_t* surrogate, float* scales,
+                                                 uintptr_t count) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        CHECK_POINTER(scales);
+        const std::vector<float> s = surrogate->impl->scales();
+        if (count != s.size()) throw invalid_parameter("expected " + std::to_string(s.size()) + " scales");
+        std::copy(s.begin(), s.end(), scales);
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_samples(const featomic_b200_surrogate_t* surrogate, float* r,
+                                                  uintptr_t count, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        CHECK_POINTER(r);
+        const std::vector<float> s = surrogate->impl->dataset_r((cudaStream_t)stream);
+        if (count != s.size()) throw invalid_parameter("expected " + std::to_string(s.size()) + " samples");
+        std::copy(s.begin(), s.end(), r);
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_evaluate(featomic_b200_surrogate_t* surrogate, const double* r,
+                                                   uintptr_t n, float* values, float* derivs, uintptr_t ld,
+                                                   int32_t method, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        if (n == 0) return;
+        CHECK_POINTER(r);
+        CHECK_POINTER(values);
+        cudaStream_t s = (cudaStream_t)stream;
+        switch (method) {
+            case 0: surrogate->impl->evaluate(r, (int64_t)n, values, derivs, (int64_t)ld, true, s); break;
+            case 1: surrogate->impl->evaluate(r, (int64_t)n, values, derivs, (int64_t)ld, false, s); break;
+            case 2: surrogate->impl->evaluate_reference(r, (int64_t)n, values, derivs, (int64_t)ld, false, s); break;
+            case 3: surrogate->impl->evaluate_reference(r, (int64_t)n, values, derivs, (int64_t)ld, true, s); break;
+            default: throw invalid_parameter("method must be 0, 1, 2 or 3");
+        }
+    });
+}
+
+featomic_status_t featomic_b200_calculator_set_surrogate(featomic_calculator_t* calculator,
+                                                         featomic_b200_surrogate_t* surrogate) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        if (surrogate && surrogate->impl->engine() != calculator->impl->engine.get())
+            throw invalid_parameter("the surrogate was trained for another calculator");
+        calculator->impl->engine->set_surrogate(surrogate ? surrogate->impl : nullptr);
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_free(featomic_b200_surrogate_t* surrogate) {
+    return guarded([&] { delete surrogate; });
 }
 
 featomic_status_t featomic_b200_neighbor_list(const double* positions, uintptr_t n_atoms, const double* cell,

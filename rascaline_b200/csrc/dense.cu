@@ -95,7 +95,8 @@ __global__ void dense_segments(const int32_t* __restrict__ sorted, int64_t n_dir
 
 template <typename T, int LCAP, bool GRAD>
 __global__ void dense_pair_features(DevicePairs pairs, DeviceRadial exact, DenseTables<T> tab, CutoffParams cut,
-                                    FeatureLayout L, T* __restrict__ features, int32_t* __restrict__ status) {
+                                    FeatureLayout L, T* __restrict__ features, int32_t* __restrict__ status,
+                                    int radial_external) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= pairs.count) return;
     T* f = features + p * L.stride;
@@ -123,6 +124,7 @@ __global__ void dense_pair_features(DevicePairs pairs, DeviceRadial exact, Dense
     } else {
         ylm_compute<T, LCAP>(tab.ylm, (T)u0, (T)u1, (T)u2, f + L.off_y, nullptr, nullptr, nullptr);
     }
+    if (radial_external) return;
     bool ok = true;
     for (int l = 0; l <= L.lmax; l++)
         ok &= radial_eval<T>(exact, tab.spline, l, r, f + L.off_r + l * L.nmax, GRAD ? f + L.off_dr + l * L.nmax : nullptr);
@@ -356,14 +358,22 @@ void launch_features(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream
     pairs.count = n_pairs;
     const int threads = 64;
     const unsigned blocks = (unsigned)((n_pairs + threads - 1) / threads);
+    const int external = a.surrogate != nullptr ? 1 : 0;
     if (a.lmax <= DENSE_LMAX_SMALL) {
         dense_pair_features<T, DENSE_LMAX_SMALL, GRAD>
-            <<<blocks, threads, 0, stream>>>(pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status);
+            <<<blocks, threads, 0, stream>>>(pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status, external);
     } else {
         dense_pair_features<T, DENSE_LMAX_LARGE, GRAD>
-            <<<blocks, threads, 0, stream>>>(pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status);
+            <<<blocks, threads, 0, stream>>>(pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status, external);
     }
     CUDA_CHECK(cudaGetLastError());
+    if constexpr (sizeof(T) == 4) {
+        if (a.surrogate) {
+            float* f = reinterpret_cast<float*>(a.features);
+            surrogate_fill(a.surrogate, a.pairs.distance, n_pairs, f + a.layout.off_r,
+                           GRAD ? f + a.layout.off_dr : nullptr, a.layout.stride, stream);
+        }
+    }
 }
 
 int coefficient_threads(int K) { return std::max(DENSE_CHUNK, std::min(256, (K + 31) / 32 * 32)); }

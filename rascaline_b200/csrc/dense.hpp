@@ -16,6 +16,8 @@
 
 namespace fb200 {
 
+class RadialSurrogate;
+
 template <typename T>
 struct DenseArgs {
     int lmax, nmax, n_species, n_keys, K;
@@ -41,7 +43,15 @@ struct DenseArgs {
     T* grad_strain;       // [n_systems][9] or null
     T* grad_cell;         // [n_systems][9] or null
     int32_t* status;
+    // FP32 only: R_nl and dR_nl/dr from the learned radial surrogate instead
+    // of the spline
+    RadialSurrogate* surrogate = nullptr;
 };
+
+// write the surrogate's R_nl(r) (and dR/dr when `derivs`) of every pair into
+// the feature records
+void surrogate_fill(RadialSurrogate* surrogate, const double* distance, int64_t n, float* values, float* derivs,
+                    int64_t ld, cudaStream_t stream);
 
 // State of one forward pass, owned by the caller until the backward pass
 struct DenseState {

@@ -656,8 +656,12 @@ void Engine::dense_args(const DenseState& st, bool grad, DenseArgs<T>& a) {
     a.pair_start = st.pair_start;
     a.atom_offset = st.d_atom_offset;
     a.exact = d_radial_;
-    if constexpr (sizeof(T) == 8) a.tab = dense_d_;
-    else a.tab = dense_f_;
+    if constexpr (sizeof(T) == 8) {
+        a.tab = dense_d_;
+    } else {
+        a.tab = dense_f_;
+        a.surrogate = active_surrogate_;
+    }
     a.cut = CutoffParams{h_.cutoff, h_.smoothing_width, h_.smoothing, h_.scaling ? 1 : 0,
                          h_.scaling_scale, h_.scaling_rate, h_.scaling_exponent};
     a.coef = static_cast<T*>(st.coef);
@@ -668,6 +672,12 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
                                                   void* values, int64_t values_count, cudaStream_t stream) {
     if (precision != 32 && precision != 64) throw invalid_parameter("precision must be 32 or 64");
     upload_tables();
+    const std::shared_ptr<RadialSurrogate> hold = surrogate_.lock();
+    active_surrogate_ = hold.get();
+    struct Release {
+        RadialSurrogate** p;
+        ~Release() { *p = nullptr; }
+    } release{&active_surrogate_};
     auto st = std::make_unique<DenseState>();
     st->engine = this;
     st->device = device_;
@@ -781,6 +791,12 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
     int dev = -1;
     CUDA_CHECK(cudaGetDevice(&dev));
     if (dev != st.device) throw invalid_parameter("the backward pass must run on the device of the forward pass");
+    const std::shared_ptr<RadialSurrogate> hold = surrogate_.lock();
+    active_surrogate_ = hold.get();
+    struct Release {
+        RadialSurrogate** p;
+        ~Release() { *p = nullptr; }
+    } release{&active_surrogate_};
     if (st.n_atoms == 0) return;
     if (!grad_values || !grad_positions) throw invalid_parameter("grad_values and grad_positions must not be NULL");
     const size_t T_size = st.precision == 64 ? 8 : 4;

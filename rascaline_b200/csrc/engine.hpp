@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -260,6 +261,7 @@ namespace fb200 {
 struct DenseState;
 template <typename T>
 struct DenseArgs;
+class RadialSurrogate;
 
 struct PhaseTimes {
     double neighbors = 0, metadata = 0, features = 0, expansion = 0, contraction = 0, transfer = 0, total = 0;
@@ -302,6 +304,10 @@ class Engine {
         return d_radial_;
     }
     const Hypers& hypers() const { return h_; }
+    // radial integral of the FP32 dense forms from a learned surrogate (empty:
+    // the spline); held weakly, so that a freed surrogate falls back to the
+    // spline
+    void set_surrogate(const std::shared_ptr<RadialSurrogate>& s) { surrogate_ = s; }
 
   private:
     void upload_tables();
@@ -309,6 +315,8 @@ class Engine {
     void dense_args(const DenseState& st, bool grad, DenseArgs<T>& a);
     DenseTables<double> dense_d_{};
     DenseTables<float> dense_f_{};
+    std::weak_ptr<RadialSurrogate> surrogate_;
+    RadialSurrogate* active_surrogate_ = nullptr;  // held during one forward / backward pass
     Hypers h_;
     RadialTables radial_;
     YlmTables ylm_;

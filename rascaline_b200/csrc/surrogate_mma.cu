@@ -1,0 +1,349 @@
+// Tensor-core inference of the radial surrogate (surrogate.hpp) on sm_100a:
+// tcgen05.mma with BF16 operands in shared memory and FP32 accumulators in
+// tensor memory, 128 distances per tile, persistent CTAs of 4 warps.
+//
+// Per tile:
+//   layer 1 (CUDA cores)  h1 = silu(w1 x + b1) and its r-derivative, each split
+//                         into BF16 hi + lo parts (hi + lo holds ~16 bits), written
+//                         as the A operands [128 x 64] of the next layer
+//   layer 2 (tcgen05)     D = (h1_hi + h1_lo) W2^T and (dh1_hi + dh1_lo) W2^T,
+//                         4 K-steps of 16, M = 128, N = 64, two TMEM regions
+//   epilogue              tcgen05.ld, h2 = silu(D + b2), dh2 = silu'(.) dD, split
+//   layer 3 (tcgen05)     Y = h2 W3^T, dY = dh2 W3^T, N = outputs rounded up to 16
+//   epilogue              R = s (Y + b3), dR/dr = s dY, stored per distance
+// One elected thread issues the MMAs and commits them to an mbarrier; every
+// wait is bounded and sets an error flag instead of hanging.
+//
+// Shared-memory operands use the canonical K-major layout without swizzle:
+// 8 x 8 BF16 core matrices of 128 contiguous bytes (row r at 16 r bytes),
+// K-adjacent core matrices 128 bytes apart (leading byte offset), 8-row
+// groups K/8 x 128 bytes apart (stride byte offset).
+#include <cuda_bf16.h>
+
+#include "engine.hpp"
+
+namespace fb200 {
+
+namespace {
+
+constexpr int SH = 64;          // hidden units
+constexpr int TILE = 128;       // distances per tile (MMA M)
+constexpr int TMEM_COLS = 256;  // [0, N) values, [128, 128 + N) derivatives
+constexpr long long MMA_SPINS = 1ll << 24;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// byte offset of element (row, k) in a K-major [rows x 64] BF16 operand
+__host__ __device__ __forceinline__ uint32_t core_offset(int row, int k) {
+    return (uint32_t)((row >> 3) * (SH / 8) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t operand_desc(uint32_t addr) {
+    const uint32_t lbo = 128, sbo = (SH / 8) * 128;
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    return d;                // base offset 0, no swizzle
+}
+
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+// K-major, M = 128, N = n
+__device__ __forceinline__ uint32_t mma_idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    for (long long spin = 0; spin < MMA_SPINS; spin++) {
+        uint32_t done = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (done) return true;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_load16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
+}
+
+__device__ __forceinline__ float sigmoid(float z) { return 1.0f / (1.0f + __expf(-z)); }
+
+__device__ __forceinline__ void store_split(unsigned char* base, int row, int k, float v) {
+    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+    *reinterpret_cast<__nv_bfloat16*>(base + core_offset(row, k)) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(base + TILE * SH * 2 + core_offset(row, k)) = lo;
+}
+
+struct MmaArgs {
+    int O, out_pad;
+    double rc;
+    const float* master;  // w1 [64], b1 [64], W2, b2 [64], W3, b3 [O]
+    const float* scale;
+    const uint4* w2;      // packed BF16 B operand [64 x 64]
+    const uint4* w3;      // packed BF16 B operand [out_pad x 64]
+    const double* r;
+    int64_t n;
+    float* values;
+    float* derivs;
+    int64_t ld;
+    int32_t* status;
+};
+
+__global__ void __launch_bounds__(TILE, 1) surrogate_mma_kernel(MmaArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned regions
+    unsigned char* base = smem_raw + ((1024 - (smem_addr(smem_raw) & 1023)) & 1023);
+    unsigned char* A_h = base;                           // hi, lo: 2 x 16 KB
+    unsigned char* A_t = A_h + 2 * TILE * SH * 2;        // hi, lo: 2 x 16 KB
+    unsigned char* B2 = A_t + 2 * TILE * SH * 2;         // 8 KB
+    unsigned char* B3 = B2 + SH * SH * 2;                // out_pad x 128 bytes
+    float* prm = reinterpret_cast<float*>(B3 + a.out_pad * SH * 2);  // w1, b1, b2, b3, scale
+    float* w1 = prm;
+    float* b1 = w1 + SH;
+    float* b2 = b1 + SH;
+    float* b3 = b2 + SH;
+    float* sc = b3 + a.out_pad;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sc + a.out_pad + 2);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    __shared__ int abort_flag;
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int O = a.O;
+    const int offW2 = 2 * SH, offB2 = offW2 + SH * SH, offW3 = offB2 + SH, offB3 = offW3 + O * SH;
+    for (int q = tid; q < SH * SH * 2 / 16; q += TILE) reinterpret_cast<uint4*>(B2)[q] = a.w2[q];
+    for (int q = tid; q < a.out_pad * SH * 2 / 16; q += TILE) reinterpret_cast<uint4*>(B3)[q] = a.w3[q];
+    for (int q = tid; q < SH; q += TILE) {
+        w1[q] = a.master[q];
+        b1[q] = a.master[SH + q];
+        b2[q] = a.master[offB2 + q];
+    }
+    for (int q = tid; q < a.out_pad; q += TILE) {
+        b3[q] = q < O ? a.master[offB3 + q] : 0.0f;
+        sc[q] = q < O ? a.scale[q] : 0.0f;
+    }
+    if (tid == 0) {
+        abort_flag = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const uint32_t bar_addr = smem_addr(bar);
+    const float dxdr = (float)(2.0 / a.rc);
+    uint32_t phase = 0;
+    const int64_t tiles = (a.n + TILE - 1) / TILE;
+
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t i = tile * TILE + tid;
+        const bool valid = i < a.n;
+        const float x = valid ? (float)(2.0 * a.r[i] / a.rc - 1.0) : 0.0f;
+        for (int k = 0; k < SH; k++) {
+            const float z = w1[k] * x + b1[k];
+            const float sg = sigmoid(z);
+            store_split(A_h, tid, k, z * sg);
+            store_split(A_t, tid, k, sg * (1.0f + z * (1.0f - sg)) * w1[k] * dxdr);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after();
+            const uint32_t id = mma_idesc(SH);
+            const uint32_t aH = smem_addr(A_h), aT = smem_addr(A_t), b = smem_addr(B2);
+            for (int s = 0; s < SH / 16; s++) {
+                mma_bf16(tmem, operand_desc(aH + 256 * s), operand_desc(b + 256 * s), id, s > 0);
+                mma_bf16(tmem, operand_desc(aH + TILE * SH * 2 + 256 * s), operand_desc(b + 256 * s), id, 1);
+                mma_bf16(tmem + 128, operand_desc(aT + 256 * s), operand_desc(b + 256 * s), id, s > 0);
+                mma_bf16(tmem + 128, operand_desc(aT + TILE * SH * 2 + 256 * s), operand_desc(b + 256 * s), id, 1);
+            }
+            mma_commit(bar_addr);
+        }
+        if (mbar_wait(bar_addr, phase)) {
+            phase ^= 1;
+        } else {
+            atomicOr(a.status, 1);
+            abort_flag = 1;
+        }
+        __syncthreads();
+        if (abort_flag) break;
+        fence_after();
+        for (int c = 0; c < SH; c += 16) {
+            float d[16], t[16];
+            tmem_load16(tmem + lane_base + c, d);
+            tmem_load16(tmem + lane_base + 128 + c, t);
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const float z = d[q] + b2[c + q];
+                const float sg = sigmoid(z);
+                store_split(A_h, tid, c + q, z * sg);
+                store_split(A_t, tid, c + q, sg * (1.0f + z * (1.0f - sg)) * t[q]);
+            }
+        }
+        fence_before();
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after();
+            const uint32_t id = mma_idesc(a.out_pad);
+            const uint32_t aH = smem_addr(A_h), aT = smem_addr(A_t), b = smem_addr(B3);
+            for (int s = 0; s < SH / 16; s++) {
+                mma_bf16(tmem, operand_desc(aH + 256 * s), operand_desc(b + 256 * s), id, s > 0);
+                mma_bf16(tmem, operand_desc(aH + TILE * SH * 2 + 256 * s), operand_desc(b + 256 * s), id, 1);
+                mma_bf16(tmem + 128, operand_desc(aT + 256 * s), operand_desc(b + 256 * s), id, s > 0);
+                mma_bf16(tmem + 128, operand_desc(aT + TILE * SH * 2 + 256 * s), operand_desc(b + 256 * s), id, 1);
+            }
+            mma_commit(bar_addr);
+        }
+        if (mbar_wait(bar_addr, phase)) {
+            phase ^= 1;
+        } else {
+            atomicOr(a.status, 1);
+            abort_flag = 1;
+        }
+        __syncthreads();
+        if (abort_flag) break;
+        fence_after();
+        for (int c = 0; c < a.out_pad; c += 16) {
+            float y[16], t[16];
+            tmem_load16(tmem + lane_base + c, y);
+            tmem_load16(tmem + lane_base + 128 + c, t);
+            if (valid) {
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const int o = c + q;
+                    if (o < O) {
+                        a.values[i * a.ld + o] = sc[o] * (y[q] + b3[o]);
+                        if (a.derivs) a.derivs[i * a.ld + o] = sc[o] * t[q];
+                    }
+                }
+            }
+        }
+        fence_before();
+        __syncthreads();
+    }
+    if (abort_flag) {
+        // let the MMAs in flight finish (bounded) before freeing tensor memory
+        mbar_wait(bar_addr, phase);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+__global__ void pack_weights_kernel(const float* __restrict__ master, int O, int out_pad, unsigned char* w2,
+                                    unsigned char* w3) {
+    const int offW2 = 2 * SH, offW3 = offW2 + SH * SH + SH;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < SH * SH) {
+        const int row = t / SH, k = t % SH;
+        *reinterpret_cast<__nv_bfloat16*>(w2 + core_offset(row, k)) = __float2bfloat16_rn(master[offW2 + t]);
+    }
+    if (t < out_pad * SH) {
+        const int row = t / SH, k = t % SH;
+        const float v = row < O ? master[offW3 + row * SH + k] : 0.0f;
+        *reinterpret_cast<__nv_bfloat16*>(w3 + core_offset(row, k)) = __float2bfloat16_rn(v);
+    }
+}
+
+size_t mma_shared_bytes(int out_pad) {
+    return 1024 + 4 * (size_t)TILE * SH * 2 + (size_t)SH * SH * 2 + (size_t)out_pad * SH * 2 +
+           4 * (size_t)(3 * SH + 2 * out_pad + 2) + 16 + 64;
+}
+
+}  // namespace
+
+void pack_surrogate_weights(const float* master, int hidden, int O, int out_pad, void* w2_bf16, void* w3_bf16,
+                            cudaStream_t stream) {
+    if (hidden != SH) throw invalid_parameter("the tensor-core surrogate kernel needs 64 hidden units");
+    const int total = std::max(SH * SH, out_pad * SH);
+    pack_weights_kernel<<<(total + 255) / 256, 256, 0, stream>>>(master, O, out_pad, (unsigned char*)w2_bf16,
+                                                                 (unsigned char*)w3_bf16);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_surrogate_mma(const float* master, int hidden, int O, int out_pad, double rc, const float* scale,
+                          const void* w2_bf16, const void* w3_bf16, const double* r, int64_t n, float* values,
+                          float* derivs, int64_t ld, int32_t* status, cudaStream_t stream) {
+    if (hidden != SH) throw invalid_parameter("the tensor-core surrogate kernel needs 64 hidden units");
+    if (out_pad > 128 || out_pad % 16 != 0)
+        throw invalid_parameter("the tensor-core surrogate kernel supports at most 128 outputs");
+    MmaArgs a{};
+    a.O = O;
+    a.out_pad = out_pad;
+    a.rc = rc;
+    a.master = master;
+    a.scale = scale;
+    a.w2 = (const uint4*)w2_bf16;
+    a.w3 = (const uint4*)w3_bf16;
+    a.r = r;
+    a.n = n;
+    a.values = values;
+    a.derivs = derivs;
+    a.ld = ld;
+    a.status = status;
+    const size_t smem = mma_shared_bytes(out_pad);
+    // every CTA holds 256 of the SM's 512 tensor-memory columns for its whole
+    // life: at most two CTAs may be resident on one SM, or a third would wait
+    // in tcgen05.alloc for memory that is never freed
+    const size_t smem_request = std::max<size_t>(smem, 228 * 1024 / 3 + 1024);
+    CUDA_CHECK(cudaFuncSetAttribute(surrogate_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_request));
+    int per_sm = 0;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, surrogate_mma_kernel, TILE, smem_request));
+    if (per_sm < 1 || per_sm > 2) throw internal_error("unexpected residency of the tensor-core surrogate kernel");
+    int device = 0, sms = 0;
+    CUDA_CHECK(cudaGetDevice(&device));
+    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int64_t tiles = (n + TILE - 1) / TILE;
+    const int blocks = (int)std::min<int64_t>(tiles, (int64_t)sms * per_sm);
+    surrogate_mma_kernel<<<blocks, TILE, smem_request, stream>>>(a);
+    CUDA_CHECK(cudaGetLastError());
+}
+
+}  // namespace fb200
