@@ -19,6 +19,9 @@ contraction, every row materialised in featomic's TensorMap layout.
   adjoint, on a 20 000-atom strained box, with its error against FP64.
 * ``batched_form`` 4096 molecules through one persistent launch replayed from
   a CUDA graph (FP32, autotuned), power spectrum + forces + energies.
+* ``surrogate_form`` the learned radial surrogate (MLP trained on the GPU,
+  tcgen05 inference) against the spline, on a 100 000-atom box, with errors
+  against FP64.
 * ``cpu_baseline`` / ``--impl reference``: featomic itself is Rust and cannot
   be built here (no cargo / crates), so the CPU side is the FP64 C++
   restatement in oracle/ (OpenMP, featomic's decomposition: spherical
@@ -404,6 +407,110 @@ def batched_form(steps, warmup):
     }
 
 
+def surrogate_form(steps, warmup):
+    """The learned radial surrogate on a 100 000-atom box (density 0.1 A^-3,
+    minimum distance 0.9 A, 4 species; rc 6 A, max_radial 11, max_angular 8):
+    the MLP 1 -> 64 -> 64 -> 108 (SiLU, BF16 weights, FP32 accumulation) is
+    trained on 2^20 exact radial integrals with r uniform in [0, 6] A, then the
+    FP32 dense power spectrum is computed with the spline and with the MLP;
+    both are compared with the FP64 power spectrum (spline accuracy 1e-8)."""
+    import torch
+    import rascaline_b200 as rb
+    from rascaline_b200 import workloads
+    from rascaline_b200.surrogate import RadialSurrogate
+    from rascaline_b200.torch_api import dense_power_spectrum
+
+    n = 100000
+    system = workloads.random_box(n, density=0.1, min_distance=0.9, seed=6)
+    calc = rb.SoapPowerSpectrum(**workloads.hypers(6.0, 11, 8))
+    pos = torch.tensor(system["positions"], device="cuda")
+    types = system["types"].astype(np.int32)
+    cells = np.asarray(system["cell"]).reshape(1, 9)
+
+    s = RadialSurrogate(calc, seed=3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.make_dataset(1 << 20, seed=7)
+    loss = s.train(20000, 8192, 3e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    r = torch.linspace(0.9, 6.0, 20001, dtype=torch.float64, device="cuda")
+    exact, dexact = s.evaluate(r, "analytic")
+    mlp, dmlp = s.evaluate(r, "tensor_cores")
+    spl, dspl = s.evaluate(r, "spline")
+    scale, dscale = exact.abs().amax(dim=0), dexact.abs().amax(dim=0)
+
+    def rms(a, b, sc):
+        return float((((a - b) / sc) ** 2).mean().sqrt())
+
+    def mx(a, b, sc):
+        return float(((a - b).abs() / sc).max())
+
+    radial = {
+        "mlp_values_rms": rms(mlp, exact, scale), "mlp_values_max": mx(mlp, exact, scale),
+        "mlp_derivatives_rms": rms(dmlp, dexact, dscale), "mlp_derivatives_max": mx(dmlp, dexact, dscale),
+        "spline_values_max": mx(spl, exact, scale), "spline_derivatives_max": mx(dspl, dexact, dscale),
+        "normalisation": "each output divided by its largest magnitude over r in [0.9, 6] A",
+    }
+    rates = {}
+    rr = torch.rand(1 << 22, dtype=torch.float64, device="cuda") * 6.0
+    for method in ("tensor_cores", "spline", "analytic"):
+        s.evaluate(rr[:4096], method)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.evaluate(rr, method)
+        e1.record()
+        torch.cuda.synchronize()
+        rates[method] = rr.numel() / (e0.elapsed_time(e1) / 1000.0)
+
+    def timed(precision):
+        for _ in range(max(3, warmup)):
+            dense_power_spectrum(calc, pos, types, cells, [n], precision)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            values, _ = dense_power_spectrum(calc, pos, types, cells, [n], precision)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            del values
+        values, _ = dense_power_spectrum(calc, pos, types, cells, [n], precision)
+        return float(np.mean(times)), values
+
+    ms64, v64 = timed(64)
+    v64_max = float(v64.abs().max())
+    ms_spline, v32 = timed(32)
+    spline_err = float((v32.double() - v64).abs().max()) / v64_max
+    del v32
+    s.attach()
+    try:
+        ms_mlp, vm = timed(32)
+    finally:
+        s.attach(False)
+    mlp_err = float((vm.double() - v64).abs().max()) / v64_max
+    mlp_rms = float(((vm.double() - v64) ** 2).mean().sqrt()) / float((v64 ** 2).mean().sqrt())
+    del vm, v64
+    return {
+        "workload": "random_box_100000_rho0.1_rc6_nmax11_lmax8_ps_values_fp32_spline_vs_mlp",
+        "training": {"samples": 1 << 20, "steps": 20000, "batch": 8192, "seconds": train_s, "final_loss": loss},
+        "radial_error_vs_exact": radial,
+        "radial_evaluations_per_s": rates,
+        "power_spectrum_error_vs_fp64": {
+            "spline_fp32_max_abs_over_max": spline_err,
+            "mlp_fp32_max_abs_over_max": mlp_err,
+            "mlp_fp32_rms_over_rms": mlp_rms,
+        },
+        "ms_per_step": {"fp64_spline": ms64, "fp32_spline": ms_spline, "fp32_mlp": ms_mlp},
+        "atom_envs_per_s": {"fp64_spline": n / ms64 * 1e3, "fp32_spline": n / ms_spline * 1e3,
+                            "fp32_mlp": n / ms_mlp * 1e3},
+        "steps": steps,
+        "note": "power spectrum values only (no gradients); the MLP replaces the spline in the FP32 pair features",
+    }
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -535,6 +642,7 @@ def main():
         line["adjoint_form"] = adjoint_form(args.steps, args.warmup)
         line["adjoint_form"]["gpu_launches_per_step"] = 14
         line["batched_form"] = batched_form(args.steps, args.warmup)
+        line["surrogate_form"] = surrogate_form(min(args.steps, 5), args.warmup)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(system, hypers)
     print(json.dumps(line), flush=True)
