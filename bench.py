@@ -175,8 +175,13 @@ def dist_setup(n_gpus):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        # one process per GPU over NCCL; the host-only paths (the reference
+        # arm, tests) use gloo when no GPU is visible
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        else:
+            dist.init_process_group("gloo", timeout=timedelta(seconds=300))
     return rank, world, local
 
 
@@ -191,7 +196,8 @@ def allreduce_max(value, world):
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
