@@ -12,7 +12,10 @@
  *
  * Supported calculators: "spherical_expansion", "soap_power_spectrum"
  * (Gaussian density, GTO radial basis, TensorProduct basis, ShiftedCosine or
- * Step smoothing, optional Willatt2018 radial scaling).
+ * Step smoothing, optional Willatt2018 radial scaling) and
+ * "soap_radial_spectrum" (featomic/src/calculators/soap/radial_spectrum.rs:
+ * the same density and GTO radial basis, l = 0 only, keys
+ * (center_type, neighbor_type), no components).
  */
 #ifndef FEATOMIC_B200_H
 #define FEATOMIC_B200_H

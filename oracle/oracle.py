@@ -130,8 +130,13 @@ def hypers_from_json(h):
         out.scaling_rate = float(scaling["rate"])
         out.scaling_exponent = float(scaling["exponent"])
     basis = h["basis"]
-    assert basis["type"] == "TensorProduct" and basis["radial"]["type"] == "Gto"
-    out.max_angular = int(basis["max_angular"])
+    if "type" in basis:
+        assert basis["type"] == "TensorProduct" and basis["radial"]["type"] == "Gto"
+        out.max_angular = int(basis["max_angular"])
+    else:
+        # RadialSpectrumBasis (featomic/src/calculators/soap/radial_spectrum.rs:44-57)
+        assert basis["radial"]["type"] == "Gto"
+        out.max_angular = 0
     out.max_radial = int(basis["radial"]["max_radial"])
     acc = basis.get("spline_accuracy", 1e-8)
     out.spline_accuracy = -1.0 if acc is None else float(acc)
@@ -241,6 +246,8 @@ def compute(calculator, hypers, systems, gradients=(), threads=1, se_over_centre
 
     Returns ``{"keys": int32[k, w], "blocks": [{"samples", "properties",
     "values", "gradients": {name: {"samples", "values"}}}]}``."""
+    if calculator == "soap_radial_spectrum":
+        return _radial_spectrum(compute("spherical_expansion", hypers, systems, gradients, threads, se_over_centres))
     kind = {"spherical_expansion": 0, "soap_power_spectrum": 1}[calculator]
     h = hypers_from_json(hypers)
     keep = []
@@ -282,3 +289,22 @@ def compute(calculator, hypers, systems, gradients=(), threads=1, se_over_centre
     finally:
         lib().oracle_result_free(res)
     return {"keys": keys, "blocks": blocks}
+
+
+def _radial_spectrum(se):
+    """featomic's SoapRadialSpectrum::compute (featomic/src/calculators/soap/
+    radial_spectrum.rs:237-323): the spherical expansion restricted to the
+    l = 0 radial basis, keys (center_type, neighbor_type) and the o3_mu axis
+    (size 1) dropped from values and gradients."""
+    assert (se["keys"][:, 0] == 0).all()
+    out = {"keys": np.ascontiguousarray(se["keys"][:, 2:4]), "blocks": []}
+    for block in se["blocks"]:
+        values = block["values"]
+        new = {"samples": block["samples"], "properties": block["properties"],
+               "values": values.reshape(values.shape[0], values.shape[2]), "gradients": {}}
+        for name, g in block["gradients"].items():
+            v = g["values"]
+            assert v.shape[-2] == 1
+            new["gradients"][name] = {"samples": g["samples"], "values": v.reshape(v.shape[:-2] + v.shape[-1:])}
+        out["blocks"].append(new)
+    return out

@@ -1,4 +1,4 @@
-"""featomic-b200: B200-native SOAP spherical expansion and power spectrum.
+"""featomic-b200: B200-native SOAP spherical expansion, power spectrum and radial spectrum.
 
 The numerical work runs in hand-written sm_100a CUDA kernels inside
 ``libfeatomic_b200.so`` (built in-tree by ``python -m rascaline_b200.build``),
@@ -9,6 +9,7 @@ from .calculators import (  # noqa: F401
     CalculatorBase,
     Labels,
     SoapPowerSpectrum,
+    SoapRadialSpectrum,
     SphericalExpansion,
     System,
     TensorBlock,

@@ -359,7 +359,7 @@ class CalculatorBase:
         """(values, gradients, knots): the radial integral the kernels use,
         evaluated on the host, shapes [len(r), max_angular + 1, max_radial + 1]."""
         h = json.loads(self._parameters)
-        L = h["basis"]["max_angular"]
+        L = h["basis"].get("max_angular", 0)
         N = h["basis"]["radial"]["max_radial"] + 1
         r = np.ascontiguousarray(r, dtype=np.float64)
         values = np.zeros((len(r), L + 1, N))
@@ -387,6 +387,16 @@ class SphericalExpansion(CalculatorBase):
 class SoapPowerSpectrum(CalculatorBase):
     def __init__(self, cutoff, density, basis):
         super().__init__("soap_power_spectrum", {"cutoff": cutoff, "density": density, "basis": basis})
+
+
+class SoapRadialSpectrum(CalculatorBase):
+    """featomic's ``soap_radial_spectrum``: the l = 0 spherical expansion, keys
+    (center_type, neighbor_type), properties n, no components
+    (featomic/src/calculators/soap/radial_spectrum.rs).  ``basis`` is
+    ``{"radial": {"type": "Gto", "max_radial": n}, "spline_accuracy": ...}``."""
+
+    def __init__(self, cutoff, density, basis):
+        super().__init__("soap_radial_spectrum", {"cutoff": cutoff, "density": density, "basis": basis})
 
 
 def neighbor_list(positions, cell, cutoff):

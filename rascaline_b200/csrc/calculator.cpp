@@ -1,5 +1,6 @@
 // Calculator facade: registry, construction from JSON and dispatch to the
-// engine (featomic/src/calculator.rs:243-526, registry :574-588).
+// engine (featomic/src/calculator.rs:243-526, registry :574-588): spherical
+// expansion, SOAP power spectrum and SOAP radial spectrum.
 #include "engine.hpp"
 #include "host.hpp"
 
@@ -19,7 +20,12 @@ std::unique_ptr<CalculatorImpl> create_calculator(const std::string& name, const
         c->pretty_name = "SOAP power spectrum";
         c->hypers = parse_hypers(json, /*deny_unknown_top=*/false);
         c->power_spectrum = true;
-    } else if (name == "spherical_expansion_by_pair" || name == "soap_radial_spectrum" ||
+    } else if (name == "soap_radial_spectrum") {
+        c->pretty_name = "radial spectrum";
+        c->hypers = parse_hypers(json, /*deny_unknown_top=*/false, /*radial_spectrum_basis=*/true);
+        c->power_spectrum = false;
+        c->radial_spectrum = true;
+    } else if (name == "spherical_expansion_by_pair" ||
                name == "lode_spherical_expansion" || name == "atomic_composition" || name == "dummy_calculator" ||
                name == "neighbor_list" || name == "sorted_distances") {
         throw invalid_parameter("calculator '" + name + "' is not implemented by featomic-b200");
@@ -31,10 +37,45 @@ std::unique_ptr<CalculatorImpl> create_calculator(const std::string& name, const
     return c;
 }
 
+namespace {
+
+// The radial spectrum is the l = 0 spherical expansion with its keys
+// (o3_lambda = 0, o3_sigma = 1, center_type, neighbor_type) reduced to
+// (center_type, neighbor_type) and the single o3_mu component dropped
+// (radial_spectrum.rs:102-130, :237-323).  The data layout is the same, so
+// only the metadata changes: values [samples, n], positions gradients
+// [rows, xyz, n], strain [samples, xyz_2, xyz_1, n], cell [samples, xyz, abc, n].
+void drop_mu_component(Block& b) {
+    if (b.components.empty() || b.components.back().names != std::vector<std::string>{"o3_mu"})
+        throw internal_error("radial spectrum: expected an o3_mu component");
+    b.components.pop_back();
+    b.shape.erase(b.shape.end() - 2);
+}
+
+void to_radial_spectrum(TensorMap& tm) {
+    Labels keys;
+    keys.names = {"center_type", "neighbor_type"};
+    const size_t width = tm.keys.names.size();
+    for (size_t k = 0; k < tm.keys.count(); k++) {
+        if (tm.keys.values[k * width] != 0) throw internal_error("radial spectrum: expected o3_lambda = 0 only");
+        keys.values.push_back(tm.keys.values[k * width + 2]);
+        keys.values.push_back(tm.keys.values[k * width + 3]);
+    }
+    tm.keys = std::move(keys);
+    for (auto& b : tm.blocks) {
+        drop_mu_component(*b);
+        for (auto& g : b->gradients) drop_mu_component(*g.second);
+    }
+}
+
+}  // namespace
+
 std::unique_ptr<TensorMap> compute(CalculatorImpl& calc, std::vector<HostSystem>& systems, const GradientOptions& grads,
                                    bool device_output, const double* positions_device, void* stream) {
-    return calc.engine->compute(calc.power_spectrum, systems, grads, device_output, positions_device,
-                                (cudaStream_t)stream);
+    auto tm = calc.engine->compute(calc.power_spectrum, systems, grads, device_output, positions_device,
+                                   (cudaStream_t)stream);
+    if (calc.radial_spectrum && tm) to_radial_spectrum(*tm);
+    return tm;
 }
 
 }  // namespace fb200

@@ -55,8 +55,11 @@ struct Hypers {
 };
 
 // parse + validate; `deny_unknown_top` mirrors serde's deny_unknown_fields on
-// the top-level struct (spherical expansion: yes, power spectrum: no)
-Hypers parse_hypers(const std::string& json, bool deny_unknown_top);
+// the top-level struct (spherical expansion: yes, power spectrum and radial
+// spectrum: no).  `radial_spectrum_basis` reads featomic's
+// RadialSpectrumBasis {radial, spline_accuracy} (radial_spectrum.rs:44-57)
+// instead of a SphericalExpansionBasis, with max_angular = 0.
+Hypers parse_hypers(const std::string& json, bool deny_unknown_top, bool radial_spectrum_basis = false);
 
 // ---------------------------------------------------------------------------
 // Radial integral tables (one Hermite spline per angular channel, knots chosen
@@ -163,6 +166,7 @@ struct CalculatorImpl {
     std::vector<double> cutoffs;
     std::unique_ptr<Engine> engine;
     bool power_spectrum = false;
+    bool radial_spectrum = false;  // spherical expansion l = 0, keys (center_type, neighbor_type)
     ~CalculatorImpl();
 };
 

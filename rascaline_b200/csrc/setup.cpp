@@ -71,7 +71,7 @@ std::string tag(const Value& v, const char* context) {
 
 }  // namespace
 
-Hypers parse_hypers(const std::string& text, bool deny_unknown_top) {
+Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_spectrum_basis) {
     Value root;
     try {
         root = json::parse(text);
@@ -128,16 +128,26 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top) {
     }
 
     // basis
-    const Value& basis = object(field(root, "basis", "parameters"), "internally tagged enum SphericalExpansionBasis");
-    std::string bt = tag(basis, "SphericalExpansionBasis");
-    if (bt == "Explicit") {
-        throw invalid_parameter("the 'Explicit' spherical expansion basis is not supported by featomic-b200 yet");
-    } else if (bt != "TensorProduct") {
-        throw json_error("unknown variant `" + bt + "`, expected `TensorProduct` or `Explicit`");
+    const char* basis_name = radial_spectrum_basis ? "RadialSpectrumBasis" : "TensorProduct";
+    const Value* basis_ptr = nullptr;
+    if (radial_spectrum_basis) {
+        // one radial basis, l = 0 only (radial_spectrum.rs:44-57, :79-91)
+        basis_ptr = &object(field(root, "basis", "parameters"), "struct RadialSpectrumBasis");
+        deny_unknown(*basis_ptr, {"radial", "spline_accuracy"}, "RadialSpectrumBasis");
+        h.max_angular = 0;
+    } else {
+        basis_ptr = &object(field(root, "basis", "parameters"), "internally tagged enum SphericalExpansionBasis");
+        std::string bt = tag(*basis_ptr, "SphericalExpansionBasis");
+        if (bt == "Explicit") {
+            throw invalid_parameter("the 'Explicit' spherical expansion basis is not supported by featomic-b200 yet");
+        } else if (bt != "TensorProduct") {
+            throw json_error("unknown variant `" + bt + "`, expected `TensorProduct` or `Explicit`");
+        }
+        deny_unknown(*basis_ptr, {"type", "max_angular", "radial", "spline_accuracy"}, "TensorProduct");
+        h.max_angular = (int)as_usize(field(*basis_ptr, "max_angular", "TensorProduct"), "max_angular");
     }
-    deny_unknown(basis, {"type", "max_angular", "radial", "spline_accuracy"}, "TensorProduct");
-    h.max_angular = (int)as_usize(field(basis, "max_angular", "TensorProduct"), "max_angular");
-    const Value& radial = object(field(basis, "radial", "TensorProduct"), "internally tagged enum SoapRadialBasis");
+    const Value& basis = *basis_ptr;
+    const Value& radial = object(field(basis, "radial", basis_name), "internally tagged enum SoapRadialBasis");
     std::string rt = tag(radial, "SoapRadialBasis");
     if (rt == "Tabulated") {
         throw invalid_parameter("the 'Tabulated' radial basis is not supported by featomic-b200 yet");

@@ -56,7 +56,8 @@ def compare_tensormaps(product, oracle_tm, gradients):
 
 
 def run_product(calculator, hypers, systems, gradients=(), use_native_system=True):
-    cls = {"spherical_expansion": rb.SphericalExpansion, "soap_power_spectrum": rb.SoapPowerSpectrum}[calculator]
+    cls = {"spherical_expansion": rb.SphericalExpansion, "soap_power_spectrum": rb.SoapPowerSpectrum,
+           "soap_radial_spectrum": rb.SoapRadialSpectrum}[calculator]
     calc = cls(**hypers)
     tm = calc.compute([rb.System.from_dict(s) for s in systems], gradients=list(gradients),
                       use_native_system=use_native_system)
