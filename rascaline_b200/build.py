@@ -56,8 +56,19 @@ def up_to_date():
     return all(os.path.getmtime(f) <= t for f in sources() + headers() + [__file__])
 
 
-def _compile(src, verbose):
+def _object_current(src, obj):
+    """An object is reused when it is newer than its source, every header and
+    this script (a header change rebuilds every object)."""
+    if not os.path.exists(obj):
+        return False
+    t = os.path.getmtime(obj)
+    return all(os.path.getmtime(f) <= t for f in [src, __file__] + headers())
+
+
+def _compile(src, verbose, force=True):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    if not force and not verbose and _object_current(src, obj):
+        return obj, ""
     cmd = [nvcc()] + ARCH + DEVICE + COMMON + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [nvcc(), "-x", "c++"] + COMMON + ["-c", src, "-o", obj]
@@ -75,7 +86,7 @@ def build(force=False, verbose=False, jobs=None):
     os.makedirs(BUILD, exist_ok=True)
     jobs = jobs or min(8, os.cpu_count() or 1)
     with concurrent.futures.ThreadPoolExecutor(jobs) as pool:
-        results = list(pool.map(lambda s: _compile(s, verbose), sources()))
+        results = list(pool.map(lambda s: _compile(s, verbose, force), sources()))
     if verbose:
         for _, log in results:
             if log:

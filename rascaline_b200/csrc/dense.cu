@@ -118,7 +118,25 @@ __global__ void dense_pair_features(DevicePairs pairs, DeviceRadial exact, Dense
     f[3] = (T)u0;
     f[4] = (T)u1;
     f[5] = (T)u2;
-    if (GRAD) {
+    if constexpr (LCAP <= 8) {
+        // row by row in registers, stored straight into the pair record
+        T* __restrict__ Y = f + L.off_y;
+        T* __restrict__ G = f + L.off_dy;
+        const int L2 = L.L2;
+        ylm_rows<T, LCAP, GRAD>(tab.ylm, (T)u0, (T)u1, (T)u2, [](int) {},
+                                [&](int l, int m, T yp, T ym, const T* gp, const T* gm) {
+                                    const int ip = l * l + l + m, im = l * l + l - m;
+                                    Y[ip] = yp;
+                                    if (m > 0) Y[im] = ym;
+                                    if (GRAD) {
+#pragma unroll
+                                        for (int x = 0; x < 3; x++) {
+                                            G[x * L2 + ip] = gp[x];
+                                            if (m > 0) G[x * L2 + im] = gm[x];
+                                        }
+                                    }
+                                });
+    } else if (GRAD) {
         ylm_compute<T, LCAP>(tab.ylm, (T)u0, (T)u1, (T)u2, f + L.off_y, f + L.off_dy, f + L.off_dy + L.L2,
                              f + L.off_dy + 2 * L.L2);
     } else {
@@ -282,6 +300,104 @@ __global__ void __launch_bounds__(256) dense_pair_adjoint(DenseArgs<T> a, int64_
     }
 }
 
+// Spline R_nl(r) and dR_nl/dr of one angular channel into registers: the
+// arithmetic of radial_eval (featomic/src/math/splines.rs:225-289), unrolled
+// over at most NCAP radial functions.
+template <typename T, int NCAP>
+__device__ __forceinline__ void spline_row(const DeviceSplineT<T>& S, int l, double r, T (&R)[NCAP], T (&dR)[NCAP]) {
+    const int N = S.nmax;
+    const double* pos = S.positions + S.knot_offset[l];
+    const int k = soap::spline_interval(pos, S.knot_count[l], r);
+    const soap::HermiteWeights w = soap::hermite_weights(pos[k], pos[k + 1], r);
+    const T* pv = S.values + ((size_t)S.knot_offset[l] + k) * N;
+    const T* pd = S.derivs + ((size_t)S.knot_offset[l] + k) * N;
+    const T h00 = (T)w.h00, h10 = (T)(w.h10 * w.delta), h01 = (T)w.h01, h11 = (T)(w.h11 * w.delta);
+    const T d00 = (T)(w.d00 * w.dxdt), d10 = (T)w.d10, d01 = (T)(w.d01 * w.dxdt), d11 = (T)w.d11;
+#pragma unroll
+    for (int n = 0; n < NCAP; n++) {
+        if (n < N) {
+            const T p0 = pv[n], m0 = pd[n], p1 = pv[N + n], m1 = pd[N + n];
+            R[n] = h00 * p0 + h10 * m0 + h01 * p1 + h11 * m1;
+            dR[n] = d00 * p0 + d10 * m0 + d01 * p1 + d11 * m1;
+        } else {
+            R[n] = T(0);
+            dR[n] = T(0);
+        }
+    }
+}
+
+// dense_pair_features<GRAD> + dense_pair_adjoint in one pass, one pair per
+// thread, nothing written but dL/dr_ij: the cutoff, Y_lm and dY_lm (row by
+// row in registers) and the spline R_nl, dR_nl (one channel at a time in
+// registers) are contracted at once with
+//   D_lmn = dL/dc_i[s_j][lmn] + (-1)^l dL/dc_j[s_i][lmn]
+// (the pair term of both centres, spherical_expansion_pair.rs:130-163, 323-422):
+//   dL/dr_ij = sum_lm [A_lm Y_lm u + B_lm f / r dY_lm/du],
+//   A_lm = sum_n D_lmn (f' R_ln + f dR_ln),  B_lm = sum_n D_lmn R_ln.
+// Pairs are ordered by first atom, so the Di rows of a warp are mostly the
+// same (broadcast loads).  Used when lmax <= 8, nmax <= NCAP, the radial
+// integral is splined and no learned surrogate replaces it.
+template <typename T, int NCAP>
+__global__ void __launch_bounds__(128) dense_pair_adjoint_fused(DenseArgs<T> a, int64_t n_pairs) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_pairs) return;
+    const double r = a.pairs.distance[p];
+    const double v0 = a.pairs.vector[3 * p], v1 = a.pairs.vector[3 * p + 1], v2 = a.pairs.vector[3 * p + 2];
+    double ud0 = v0 / r, ud1 = v1 / r, ud2 = v2 / r;
+    if (r < 1e-6) {
+        ud0 = 0.0;
+        ud1 = 0.0;
+        ud2 = 1.0;
+    }
+    double fc, dfc;
+    soap::cutoff_function(a.cut.smoothing, a.cut.rc, a.cut.width, r, &fc, &dfc);
+    double sc = 1.0, dsc = 0.0;
+    if (a.cut.scaling) soap::willatt2018(a.cut.scale, a.cut.rate, a.cut.exponent, r, &sc, &dsc);
+    const T f = (T)(sc * fc), fg = (T)(dfc * sc + fc * dsc);
+    const T u0 = (T)ud0, u1 = (T)ud1, u2 = (T)ud2;
+    const T f_over_r = f / (T)r;
+    const int i = a.pairs.first[p], j = a.pairs.second[p];
+    const int S = a.n_species, N = a.nmax;
+    const T* __restrict__ Di = a.grad_coef + ((int64_t)i * S + a.atom_species[j]) * a.K;
+    const T* __restrict__ Dj = a.grad_coef + ((int64_t)j * S + a.atom_species[i]) * a.K;
+    T R[NCAP], dR[NCAP], P[NCAP];
+    T sign = T(1);
+    T g0 = T(0), g1 = T(0), g2 = T(0);
+    auto term = [&](int lm, T y, const T* gy) {
+        T A = T(0), B = T(0);
+        const T* di = Di + lm * N;
+        const T* dj = Dj + lm * N;
+#pragma unroll
+        for (int n = 0; n < NCAP; n++) {
+            if (n < N) {
+                const T D = di[n] + sign * dj[n];
+                A += D * P[n];
+                B += D * R[n];
+            }
+        }
+        const T AY = A * y;
+        const T Bf = B * f_over_r;
+        g0 += AY * u0 + Bf * gy[0];
+        g1 += AY * u1 + Bf * gy[1];
+        g2 += AY * u2 + Bf * gy[2];
+    };
+    ylm_rows<T, 8, true>(
+        a.tab.ylm, u0, u1, u2,
+        [&](int l) {
+            spline_row<T, NCAP>(a.tab.spline, l, r, R, dR);
+#pragma unroll
+            for (int n = 0; n < NCAP; n++) P[n] = fg * R[n] + f * dR[n];
+            sign = (l & 1) ? T(-1) : T(1);
+        },
+        [&](int l, int m, T yp, T ym, const T* gp, const T* gm) {
+            term(l * l + l + m, yp, gp);
+            if (m > 0) term(l * l + l - m, ym, gm);
+        });
+    a.pair_grad[3 * p] = g0;
+    a.pair_grad[3 * p + 1] = g1;
+    a.pair_grad[3 * p + 2] = g2;
+}
+
 template <typename T>
 __global__ void dense_atom_reduce(DenseArgs<T> a, int with_partials) {
     const int64_t atom = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -434,7 +550,15 @@ void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t 
     }
     dense_grad_coef<T><<<(unsigned)a.n_atoms, 256, smem, stream>>>(a);
     CUDA_CHECK(cudaGetLastError());
-    if (n_pairs > 0) {
+    bool fused = a.lmax <= DENSE_LMAX_SMALL && a.nmax <= 16 && a.tab.spline.splined;
+    if constexpr (sizeof(T) == 4) fused = fused && a.surrogate == nullptr;
+    if (n_pairs > 0 && fused) {
+        const int threads = 128;
+        const unsigned blocks = (unsigned)((n_pairs + threads - 1) / threads);
+        if (a.nmax <= 8) dense_pair_adjoint_fused<T, 8><<<blocks, threads, 0, stream>>>(a, n_pairs);
+        else dense_pair_adjoint_fused<T, 16><<<blocks, threads, 0, stream>>>(a, n_pairs);
+        CUDA_CHECK(cudaGetLastError());
+    } else if (n_pairs > 0) {
         launch_features<T, true>(a, n_pairs, stream);
         const int warps = 8;
         dense_pair_adjoint<T><<<(unsigned)((n_pairs + warps - 1) / warps), 32 * warps, 0, stream>>>(a, n_pairs);

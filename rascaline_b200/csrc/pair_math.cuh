@@ -119,6 +119,118 @@ __device__ void ylm_compute(const DeviceYlmT<T>& tab, T ux, T uy, T uz, T* __res
     }
 }
 
+// The same harmonics row by row: begin(l) is called before row l and
+// visit(l, m, y+, y-, g+, g-) for m = 0..l with Y_l^{+m}, Y_l^{-m} (y- unused
+// for m = 0) and their gradients w.r.t. the unit direction (g+/g- all zero
+// when GRAD is false).  Same operations in the same order as ylm_compute, so
+// the results are identical, but in l-outer order: three rows of Legendre
+// polynomials live in registers instead of a local-memory table.  For
+// LCAP <= 8 (the register arrays are unrolled).
+template <typename T, int LCAP, bool GRAD, typename Begin, typename Visit>
+__device__ __forceinline__ void ylm_rows(const DeviceYlmT<T>& tab, T ux, T uy, T uz, Begin begin, Visit visit) {
+    static_assert(LCAP <= 8, "ylm_rows keeps (LCAP + 1) x 4 Legendre values in registers");
+    const int lmax = tab.lmax;
+    const T SQRT_1_OVER_2PI = T(0.3989422804014327);
+    const T SQRT_3 = T(1.7320508075688772);
+    const T SQRT_3_OVER_2 = T(1.224744871391589);
+    const T SQRT_2 = T(1.4142135623730951);
+    const T sxy = hypot(ux, uy);
+    const T ct = uz, st = sxy;
+    T cp, sp;
+    if (sxy > T(soap::DBL_EPS)) {
+        cp = ux / sxy;
+        sp = uy / sxy;
+    } else {
+        cp = T(1);
+        sp = T(0);
+    }
+    // cos(m phi), sin(m phi) by the recursion of :300-306
+    T cm[LCAP + 1], sm[LCAP + 1];
+    {
+        T cos1 = T(1), sin1 = T(0), cos2 = -cp, sin2 = sp;
+        const T m2c = T(-2) * cp;
+        cm[0] = T(1);
+        sm[0] = T(0);
+#pragma unroll
+        for (int m = 1; m <= LCAP; m++) {
+            const T smp = m2c * sin1 - sin2;
+            const T cmp = m2c * cos1 - cos2;
+            sin2 = sin1;
+            sin1 = smp;
+            cos2 = cos1;
+            cos1 = cmp;
+            cm[m] = cmp;
+            sm[m] = smp;
+        }
+    }
+    T p2[LCAP + 1], p1[LCAP + 1], p0[LCAP + 1], dp[LCAP + 1];
+    T value = SQRT_1_OVER_2PI;
+#pragma unroll
+    for (int l = 0; l <= LCAP; l++) {
+        if (l > lmax) break;
+        // associated Legendre row l (:228-251)
+        if (l == 0) {
+            p0[0] = value;
+        } else if (l == 1) {
+            p0[0] = ct * SQRT_3 * value;
+            value *= -SQRT_3_OVER_2 * st;
+            p0[1] = value;
+        } else {
+#pragma unroll
+            for (int m = 0; m < l - 1; m++) p0[m] = tab.A[lidx(l, m)] * (ct * p1[m] + tab.B[lidx(l, m)] * p2[m]);
+            p0[l - 1] = ct * tab.sq_2l1[l] * value;
+            value *= -tab.sq_half[l] * st;
+            p0[l] = value;
+        }
+        // derivative factors (:256-298)
+        if (GRAD) {
+            if (l == 0) {
+                dp[0] = T(0);
+            } else {
+                const T pm1 = tab.inv_ll[l] * p0[1];
+                dp[0] = tab.sq_plus[lidx(l, 0)] * pm1 - tab.sq_minus[lidx(l, 0)] * p0[1];
+#pragma unroll
+                for (int m = 1; m < l; m++)
+                    dp[m] = tab.sq_plus[lidx(l, m)] * p0[m - 1] - tab.sq_minus[lidx(l, m)] * p0[m + 1];
+                dp[l] = tab.sq_plus[lidx(l, l)] * p0[l - 1] - tab.sq_minus[lidx(l, l)] * T(0);
+            }
+        }
+        begin(l);
+        {
+            T g0[3] = {T(0), T(0), T(0)};
+            if (GRAD && l > 0) {
+                const T lf = tab.sq_ll1[l] * p0[1];
+                g0[0] = cp * ct * lf;
+                g0[1] = sp * ct * lf;
+                g0[2] = -st * lf;
+            }
+            visit(l, 0, p0[0] / SQRT_2, T(0), g0, g0);
+        }
+#pragma unroll
+        for (int m = 1; m <= l; m++) {
+            const T yp = p0[m] * cm[m];
+            const T ym = p0[m] * sm[m];
+            T gp[3] = {T(0), T(0), T(0)}, gm[3] = {T(0), T(0), T(0)};
+            if (GRAD) {
+                const T pot = st > T(0.1) ? (T)m / st * p0[m] : T(-0.5) / ct * dp[m];
+                const T sdp = sm[m] * dp[m], cdp = cm[m] * dp[m];
+                gp[0] = sp * pot * sm[m] - T(0.5) * ct * cp * cdp;
+                gm[0] = -sp * pot * cm[m] - T(0.5) * ct * cp * sdp;
+                gp[1] = -cp * pot * sm[m] - T(0.5) * ct * sp * cdp;
+                gm[1] = cp * pot * cm[m] - T(0.5) * ct * sp * sdp;
+                gp[2] = T(0.5) * st * cdp;
+                gm[2] = T(0.5) * st * sdp;
+            }
+            visit(l, m, yp, ym, gp, gm);
+        }
+#pragma unroll
+        for (int m = 0; m <= LCAP; m++) {
+            p2[m] = p1[m];
+            p1[m] = p0[m];
+        }
+    }
+}
+
 // Radial integral of one angular channel in FP64: Hermite spline
 // (featomic/src/math/splines.rs:225-289) or the analytic GTO integral times
 // the orthonormalisation matrix (radial_integral/gto.rs:115-205).  Returns

@@ -126,10 +126,17 @@ def cases():
     box = workloads.random_box(300, density=0.1, min_distance=0.9, seed=21, strain=0.02)
     golden, hypers_g = load_input(os.path.join(GOLDEN, "soap-power-spectrum-gradients-input.json"))
     mols = workloads.molecules(6, seed=4, max_atoms=30)
+    small = workloads.random_box(120, density=0.1, min_distance=0.9, seed=23, strain=0.01)
     return [
+        # splined, lmax <= 8, nmax <= 8: the fused pair adjoint
         ("box_300_strained", [box], workloads.hypers(5.5, 7, 6)),
+        # analytic radial integral: features + pair adjoint kernels
         ("golden_gradients_input", golden, hypers_g),
         ("molecules_6", mols, workloads.hypers(5.0, 7, 6)),
+        # nmax 12: the fused pair adjoint with 16 radial registers
+        ("box_120_nmax12", [small], workloads.hypers(4.5, 11, 3)),
+        # lmax 10: features + pair adjoint kernels
+        ("box_120_lmax10", [small], workloads.hypers(4.0, 3, 10)),
     ]
 
 
