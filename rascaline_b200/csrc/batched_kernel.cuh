@@ -135,7 +135,7 @@ __device__ __forceinline__ Direction direction(const BatchArgs& a, double xi, do
 
 // Grid-wide barrier with a bounded wait.  Returns false (and sets bit 1 of
 // *status) when the other CTAs did not arrive in time.
-__device__ bool grid_barrier(unsigned int* bar, int32_t* status) {
+__device__ inline bool grid_barrier(unsigned int* bar, int32_t* status) {
     __shared__ int ok_shared;
     __syncthreads();
     if (threadIdx.x == 0) {

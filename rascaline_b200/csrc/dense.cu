@@ -10,17 +10,22 @@
 //   expansion    CTA per centre, thread per (l, m, n), segments reduced in
 //                registers (no atomics), inverse pairs with (-1)^l
 //                (spherical_expansion_pair.rs:130-163), self term on l = 0
-//   contraction  warp per (centre, species pair a <= b):
+//   contraction  CTA per centre, coefficients in shared memory, thread per
+//                (species pair a <= b, l, n1) with a register row over n2:
 //                P[l n1 n2] = sum_m c_a[l m n1] c_b[l m n2] / ((-1)^l sqrt(2l+1)),
 //                times sqrt(2) when a != b (power_spectrum.rs:529-780)
 //
 // Backward (adjoint of the above for a loss L with dL/dP given):
-//   dL/dc        CTA per centre: dL/dc_a[l m n] = sum over the species pairs
-//                containing a of scale * sum_n' G[n n'] c_b[l m n']
-//   dL/dr_ij     warp per pair, Y_lm, dY_lm, R_nl, dR_nl recomputed:
+//   dL/dc        CTA per centre, coefficients and dL/dP in shared memory,
+//                thread per (a, l, n) with a register row over m:
+//                dL/dc_a[l m n] = sum over the species pairs containing a of
+//                scale * sum_n' G[n n'] c_b[l m n']
+//   dL/dr_ij     thread per pair, Y_lm, dY_lm, R_nl, dR_nl recomputed in
+//                registers and contracted at once:
 //                D = dL/dc_i[s_j] + (-1)^l dL/dc_j[s_i],
 //                dL/dr_ij = sum_lm Y A u + f/r dY B, A = sum_n D (f' R + f R'),
 //                B = sum_n D R  (the pair gradient of spherical_expansion_pair.rs:323-422)
+//   (lmax > 8 or nmax > 16: warp-per-item kernels over stored pair records)
 //   atoms        thread per atom: dL/dr_a = sum over its directions of
 //                -+dL/dr_ij (self images cancel and are skipped), plus the
 //                strain (r_ij x dL/dr_ij) and cell (shift x dL/dr_ij) sums of
@@ -253,6 +258,104 @@ __global__ void __launch_bounds__(256) dense_grad_coef(DenseArgs<T> a) {
             }
         }
         a.grad_coef[c * S * K + o] = acc;
+    }
+}
+
+// The two per-centre contractions with the centre's coefficients (and, for
+// the adjoint, its dL/dP row) staged in shared memory and register tiles,
+// for nmax <= NCAP and 2 lmax + 1 <= MCAP.  Same sums in the same order as
+// dense_contraction / dense_grad_coef, so the results are identical; the
+// tiles cut the loads per multiply-add from 2 to about 1 / NCAP
+// (contraction) and 1 / (2l + 1) (adjoint).
+//
+// P_ab[l][n1][n2] = scale(l, a != b) sum_m c_a[l m n1] c_b[l m n2]
+// (power_spectrum.rs:529-780), one thread per (key, l, n1), NCAP outputs.
+template <typename T, int NCAP>
+__global__ void __launch_bounds__(128) dense_contraction_tiled(DenseArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char dense_smem[];
+    T* cs = reinterpret_cast<T*>(dense_smem);
+    const int64_t c = blockIdx.x;
+    const int S = a.n_species, K = a.K, N = a.nmax, NN = N * N, LN = (a.lmax + 1) * N;
+    for (int i = threadIdx.x; i < S * K; i += blockDim.x) cs[i] = a.coef[c * S * K + i];
+    __syncthreads();
+    const int items = a.n_keys * LN;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int key = it / LN;
+        const int rem = it - key * LN;
+        const int l = rem / N, n1 = rem - l * N;
+        int sa, sb;
+        key_species(key, S, &sa, &sb);
+        const T* ca = cs + sa * K + l * l * N;
+        const T* cb = cs + sb * K + l * l * N;
+        T acc[NCAP];
+#pragma unroll
+        for (int q = 0; q < NCAP; q++) acc[q] = T(0);
+        for (int m = 0; m < 2 * l + 1; m++) {
+            const T x = ca[m * N + n1];
+#pragma unroll
+            for (int q = 0; q < NCAP; q++)
+                if (q < N) acc[q] += x * cb[m * N + q];
+        }
+        const T scale = (T)ps_scale(l, sa != sb);
+        T* out = a.values + (c * a.n_keys + key) * a.n_props + l * NN + n1 * N;
+#pragma unroll
+        for (int q = 0; q < NCAP; q++)
+            if (q < N) out[q] = acc[q] * scale;
+    }
+}
+
+// dL/dc_a[l m n] = sum_b scale(l, a != b) sum_q G_ab[l](n, q) c_b[l m q], with
+// G_ab the dL/dP block of the key (min(a, b), max(a, b)) read as is (a < b),
+// transposed (a > b) or symmetrised (a == b); one thread per (a, l, n), all m.
+template <typename T, int MCAP>
+__global__ void __launch_bounds__(128) dense_grad_coef_tiled(DenseArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char dense_smem[];
+    T* cs = reinterpret_cast<T*>(dense_smem);
+    const int64_t c = blockIdx.x;
+    const int S = a.n_species, K = a.K, N = a.nmax, NN = N * N, LN = (a.lmax + 1) * N;
+    const int64_t KP = (int64_t)a.n_keys * a.n_props;
+    T* gs = cs + S * K;
+    for (int i = threadIdx.x; i < S * K; i += blockDim.x) cs[i] = a.coef[c * S * K + i];
+    for (int64_t i = threadIdx.x; i < KP; i += blockDim.x) gs[i] = a.grad_values[c * KP + i];
+    __syncthreads();
+    for (int it = threadIdx.x; it < S * LN; it += blockDim.x) {
+        const int sa = it / LN;
+        const int rem = it - sa * LN;
+        const int l = rem / N, n = rem - l * N;
+        const int M = 2 * l + 1;
+        T acc[MCAP];
+#pragma unroll
+        for (int m = 0; m < MCAP; m++) acc[m] = T(0);
+        for (int b = 0; b < S; b++) {
+            const T* cb = cs + b * K + l * l * N;
+            T s[MCAP];
+#pragma unroll
+            for (int m = 0; m < MCAP; m++) s[m] = T(0);
+            const T* g;
+            int row, col;
+            if (sa < b) {
+                g = gs + (int64_t)key_index(sa, b, S) * a.n_props + l * NN;
+                row = n * N;
+                col = 1;
+            } else {
+                g = gs + (int64_t)key_index(b, sa, S) * a.n_props + l * NN;
+                row = n;
+                col = N;
+            }
+            for (int q = 0; q < N; q++) {
+                const T gq = sa == b ? g[n * N + q] + g[q * N + n] : g[row + q * col];
+#pragma unroll
+                for (int m = 0; m < MCAP; m++)
+                    if (m < M) s[m] += gq * cb[m * N + q];
+            }
+            const T scale = (T)ps_scale(l, sa != b);
+#pragma unroll
+            for (int m = 0; m < MCAP; m++) acc[m] += scale * s[m];
+        }
+        T* out = a.grad_coef + c * S * K + sa * K + l * l * N + n;
+#pragma unroll
+        for (int m = 0; m < MCAP; m++)
+            if (m < M) out[m * N] = acc[m];
     }
 }
 
@@ -531,9 +634,15 @@ void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t s
     if (a.n_atoms == 0) return;
     dense_expansion<T><<<(unsigned)a.n_atoms, coefficient_threads(a.K), 0, stream>>>(a);
     CUDA_CHECK(cudaGetLastError());
-    const int64_t items = a.n_atoms * a.n_keys;
-    const int warps = 8;
-    dense_contraction<T><<<(unsigned)((items + warps - 1) / warps), 32 * warps, 0, stream>>>(a);
+    const size_t smem = sizeof(T) * (size_t)a.n_species * a.K;
+    if (a.nmax <= 16 && smem <= 48 * 1024) {
+        if (a.nmax <= 8) dense_contraction_tiled<T, 8><<<(unsigned)a.n_atoms, 128, smem, stream>>>(a);
+        else dense_contraction_tiled<T, 16><<<(unsigned)a.n_atoms, 128, smem, stream>>>(a);
+    } else {
+        const int64_t items = a.n_atoms * a.n_keys;
+        const int warps = 8;
+        dense_contraction<T><<<(unsigned)((items + warps - 1) / warps), 32 * warps, 0, stream>>>(a);
+    }
     CUDA_CHECK(cudaGetLastError());
 }
 
@@ -546,9 +655,16 @@ void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t 
     const int which = sizeof(T) == 8 ? 1 : 0;
     if (!configured[which]) {
         CUDA_CHECK(cudaFuncSetAttribute(dense_grad_coef<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(dense_grad_coef_tiled<T, 17>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024));
         configured[which] = true;
     }
-    dense_grad_coef<T><<<(unsigned)a.n_atoms, 256, smem, stream>>>(a);
+    const size_t tiled_smem = smem + sizeof(T) * (size_t)a.n_keys * a.n_props;
+    if (a.lmax <= DENSE_LMAX_SMALL && tiled_smem <= 200 * 1024) {
+        dense_grad_coef_tiled<T, 17><<<(unsigned)a.n_atoms, 128, tiled_smem, stream>>>(a);
+    } else {
+        dense_grad_coef<T><<<(unsigned)a.n_atoms, 256, smem, stream>>>(a);
+    }
     CUDA_CHECK(cudaGetLastError());
     bool fused = a.lmax <= DENSE_LMAX_SMALL && a.nmax <= 16 && a.tab.spline.splined;
     if constexpr (sizeof(T) == 4) fused = fused && a.surrogate == nullptr;
