@@ -413,7 +413,7 @@ def batched_form(steps, warmup):
     }
 
 
-def surrogate_form(steps, warmup):
+def surrogate_form(steps, warmup, train_steps=20000):
     """The learned radial surrogate on a 100 000-atom box (density 0.1 A^-3,
     minimum distance 0.9 A, 4 species; rc 6 A, max_radial 11, max_angular 8):
     the MLP 1 -> 64 -> 64 -> 108 (SiLU, BF16 weights, FP32 accumulation) is
@@ -437,7 +437,7 @@ def surrogate_form(steps, warmup):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s.make_dataset(1 << 20, seed=7)
-    loss = s.train(20000, 8192, 3e-3)
+    loss = s.train(train_steps, 8192, 3e-3)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     r = torch.linspace(0.9, 6.0, 20001, dtype=torch.float64, device="cuda")
@@ -501,7 +501,7 @@ def surrogate_form(steps, warmup):
     del vm, v64
     return {
         "workload": "random_box_100000_rho0.1_rc6_nmax11_lmax8_ps_values_fp32_spline_vs_mlp",
-        "training": {"samples": 1 << 20, "steps": 20000, "batch": 8192, "seconds": train_s, "final_loss": loss},
+        "training": {"samples": 1 << 20, "steps": train_steps, "batch": 8192, "seconds": train_s, "final_loss": loss},
         "radial_error_vs_exact": radial,
         "radial_evaluations_per_s": rates,
         "power_spectrum_error_vs_fp64": {
@@ -528,7 +528,18 @@ def main():
                         help="skip the FP32 adjoint form measured beside the drop-in")
     parser.add_argument("--atoms", type=int, default=1000,
                         help="atoms in the box (1000 is the benchmark; smaller boxes are for profiling)")
+    parser.add_argument("--only", choices=["adjoint", "batched", "surrogate"],
+                        help="run one chosen form alone and print its object (profiling)")
+    parser.add_argument("--train-steps", type=int, default=20000,
+                        help="training steps of the learned radial surrogate (20000 is the benchmark)")
     args = parser.parse_args()
+    if args.only:
+        import torch
+        torch.cuda.set_device(0)
+        form = {"adjoint": adjoint_form, "batched": batched_form,
+                "surrogate": lambda k, w: surrogate_form(k, w, args.train_steps)}[args.only]
+        print(json.dumps({args.only + "_form": form(args.steps, args.warmup)}), flush=True)
+        return
     global N_ATOMS, WORKLOAD
     if args.atoms != N_ATOMS:
         N_ATOMS = args.atoms
@@ -646,9 +657,10 @@ def main():
     }
     if not args.no_chosen_forms:
         line["adjoint_form"] = adjoint_form(args.steps, args.warmup)
-        line["adjoint_form"]["gpu_launches_per_step"] = 14
+        # 13 kernels of this library and 9 CUB sort / scan kernels it launches
+        line["adjoint_form"]["gpu_launches_per_step"] = 22
         line["batched_form"] = batched_form(args.steps, args.warmup)
-        line["surrogate_form"] = surrogate_form(min(args.steps, 5), args.warmup)
+        line["surrogate_form"] = surrogate_form(min(args.steps, 5), args.warmup, args.train_steps)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(system, hypers)
     print(json.dumps(line), flush=True)

@@ -10,7 +10,8 @@
  * signatures follow metatensor's C API where one exists) and the
  * `featomic_b200_block_values` accessor.
  *
- * Supported calculators: "spherical_expansion", "soap_power_spectrum"
+ * Supported calculators: "spherical_expansion", "spherical_expansion_by_pair",
+ * "soap_power_spectrum"
  * (Gaussian density, GTO radial basis, TensorProduct basis, ShiftedCosine or
  * Step smoothing, optional Willatt2018 radial scaling) and
  * "soap_radial_spectrum" (featomic/src/calculators/soap/radial_spectrum.rs:

@@ -248,7 +248,7 @@ def compute(calculator, hypers, systems, gradients=(), threads=1, se_over_centre
     "values", "gradients": {name: {"samples", "values"}}}]}``."""
     if calculator == "soap_radial_spectrum":
         return _radial_spectrum(compute("spherical_expansion", hypers, systems, gradients, threads, se_over_centres))
-    kind = {"spherical_expansion": 0, "soap_power_spectrum": 1}[calculator]
+    kind = {"spherical_expansion": 0, "soap_power_spectrum": 1, "spherical_expansion_by_pair": 2}[calculator]
     h = hypers_from_json(hypers)
     keep = []
     arr = (System * len(systems))()

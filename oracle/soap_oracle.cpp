@@ -18,6 +18,7 @@
 // digits) and tests/golden/known_answers.json (inline unit-test values).
 // ===========================================================================
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -1866,6 +1867,185 @@ static TensorMap power_spectrum(const Calculator& calc, std::vector<System>& sys
 // ===========================================================================
 using namespace oracle;
 
+// ---------------------------------------------------------------------------
+// Spherical expansion by pair: spherical_expansion_pair.rs:547-822 with the
+// samples of FullNeighborList (calculators/neighbor_list.rs:372-490)
+// ---------------------------------------------------------------------------
+static TensorMap spherical_expansion_by_pair(const Calculator& calc, std::vector<System>& systems, const Options& opt) {
+    const int lmax = calc.lmax;
+    const size_t nmax = calc.nmax;
+    // keys: every (first type, second type) of a pair in both orders, and
+    // (t, t) for every type present (neighbor_list.rs:374-400); l inner
+    std::set<std::pair<int32_t, int32_t>> tp;
+    for (auto& s : systems) {
+        for (const auto& p : s.nl.pairs) {
+            tp.insert({s.types[p.first], s.types[p.second]});
+            tp.insert({s.types[p.second], s.types[p.first]});
+        }
+        for (size_t i = 0; i < s.n; i++) tp.insert({s.types[i], s.types[i]});
+    }
+    TensorMap tm;
+    tm.keys.width = 4;
+    std::map<std::pair<int32_t, int32_t>, size_t> first_block;
+    for (auto& t : tp) {
+        first_block[t] = tm.blocks.size();
+        for (int l = 0; l <= lmax; l++) {
+            tm.keys.add({l, 1, t.first, t.second});
+            tm.blocks.emplace_back();
+        }
+    }
+    // samples (neighbor_list.rs:403-490): pairs of each system in pair order
+    // (both directions when the types are equal), then that system's self
+    // pairs; l = 0 keeps the self pairs, l > 0 does not
+    using Sample = std::array<int32_t, 6>;
+    std::map<std::pair<int32_t, int32_t>, std::vector<Sample>> samples0, samples1;
+    for (size_t si = 0; si < systems.size(); si++) {
+        const System& s = systems[si];
+        for (auto& t : tp) {
+            auto& s0 = samples0[t];
+            auto& s1 = samples1[t];
+            for (const auto& p : s.nl.pairs) {
+                const int32_t a = s.types[p.first], b = s.types[p.second];
+                const Sample fwd = {(int32_t)si, (int32_t)p.first, (int32_t)p.second, p.shift[0], p.shift[1], p.shift[2]};
+                const Sample inv = {(int32_t)si, (int32_t)p.second, (int32_t)p.first, -p.shift[0], -p.shift[1], -p.shift[2]};
+                if (t.first == t.second) {
+                    if (a == t.first && b == t.second) {
+                        s0.push_back(fwd);
+                        s1.push_back(fwd);
+                        s0.push_back(inv);
+                        s1.push_back(inv);
+                    }
+                } else if (a == t.first && b == t.second) {
+                    s0.push_back(fwd);
+                    s1.push_back(fwd);
+                } else if (b == t.first && a == t.second) {
+                    s0.push_back(inv);
+                    s1.push_back(inv);
+                }
+            }
+            if (t.first == t.second)
+                for (size_t i = 0; i < s.n; i++)
+                    if (s.types[i] == t.first) s0.push_back({(int32_t)si, (int32_t)i, (int32_t)i, 0, 0, 0});
+        }
+    }
+    // blocks, with the positions gradient samples of
+    // spherical_expansion_pair.rs:647-667 (self pairs have none; i == j
+    // images have one row)
+    std::vector<std::map<Sample, size_t>> row_of(tm.blocks.size());
+    std::vector<std::vector<size_t>> grad_row_of(tm.blocks.size());  // first positions row of each sample
+    for (auto& t : tp) {
+        for (int l = 0; l <= lmax; l++) {
+            const size_t bi = first_block[t] + l;
+            Block& b = tm.blocks[bi];
+            const auto& list = l == 0 ? samples0[t] : samples1[t];
+            b.samples.width = 6;
+            for (size_t k = 0; k < list.size(); k++) {
+                const Sample& x = list[k];
+                b.samples.add({x[0], x[1], x[2], x[3], x[4], x[5]});
+                row_of[bi][x] = k;
+            }
+            b.properties.width = 1;
+            for (size_t n = 0; n < nmax; n++) b.properties.add({(int32_t)n});
+            const size_t nm = 2 * l + 1;
+            b.components = {nm};
+            b.shape = {list.size(), nm, nmax};
+            b.values.assign(list.size() * nm * nmax, 0.0);
+            std::vector<int32_t> grad_rows;
+            size_t n_grad = 0;
+            grad_row_of[bi].assign(list.size(), SIZE_MAX);
+            for (size_t k = 0; k < list.size(); k++) {
+                const Sample& x = list[k];
+                if (x[1] == x[2] && x[3] == 0 && x[4] == 0 && x[5] == 0) continue;
+                grad_row_of[bi][k] = n_grad;
+                grad_rows.insert(grad_rows.end(), {(int32_t)k, x[0], x[1]});
+                n_grad++;
+                if (x[1] != x[2]) {
+                    grad_rows.insert(grad_rows.end(), {(int32_t)k, x[0], x[2]});
+                    n_grad++;
+                }
+            }
+            add_gradient_blocks(b, opt, grad_rows, n_grad, {nm}, nmax);
+        }
+    }
+    // self contributions on l = 0 (spherical_expansion_pair.rs:259-313)
+    const std::vector<double> self = calc.self_contribution();
+    for (auto& t : tp) {
+        if (t.first != t.second) continue;
+        Block& b = tm.blocks[first_block[t]];
+        for (size_t k = 0; k < b.samples.count(); k++) {
+            const int32_t* x = &b.samples.values[6 * k];
+            if (x[1] == x[2] && x[3] == 0 && x[4] == 0 && x[5] == 0)
+                for (size_t n = 0; n < nmax; n++) b.values[k * nmax + n] = self[n];
+        }
+    }
+    // pair contributions (spherical_expansion_pair.rs:731-822,
+    // accumulate_in_block :424-540)
+    const bool do_grad = opt.positions || opt.strain || opt.cell;
+    SphericalHarmonics sph(lmax);
+    const size_t L2 = (size_t)((lmax + 1) * (lmax + 1));
+    std::vector<double> Y(L2), GX(L2), GY(L2), GZ(L2), R((lmax + 1) * nmax), dR((lmax + 1) * nmax);
+    std::vector<std::vector<double>> vals(lmax + 1), grads(lmax + 1);
+    for (int l = 0; l <= lmax; l++) {
+        vals[l].assign((2 * l + 1) * nmax, 0.0);
+        grads[l].assign(3 * (2 * l + 1) * nmax, 0.0);
+    }
+    auto accumulate = [&](int l, size_t bi, const Sample& sample, const double* v, const double* g,
+                          const double vector[3]) {
+        Block& b = tm.blocks[bi];
+        const size_t k = row_of[bi].at(sample);
+        const size_t blk = (2 * l + 1) * nmax;
+        for (size_t q = 0; q < blk; q++) b.values[k * blk + q] += v[q];
+        if (!do_grad) return;
+        if (opt.positions) {
+            Block& gb = b.gradients.at("positions");
+            // rows (k, system, first) and (k, system, second): the same row
+            // when first == second
+            const size_t first_row = grad_row_of[bi][k];
+            const size_t second_row = sample[1] == sample[2] ? first_row : first_row + 1;
+            for (size_t q = 0; q < 3 * blk; q++) gb.values[first_row * 3 * blk + q] -= g[q];
+            for (size_t q = 0; q < 3 * blk; q++) gb.values[second_row * 3 * blk + q] += g[q];
+        }
+        if (opt.strain) {
+            Block& gb = b.gradients.at("strain");
+            for (int x1 = 0; x1 < 3; x1++)
+                for (int x2 = 0; x2 < 3; x2++)
+                    for (size_t q = 0; q < blk; q++)
+                        gb.values[((k * 3 + x1) * 3 + x2) * blk + q] += vector[x1] * g[x2 * blk + q];
+        }
+        if (opt.cell) {
+            Block& gb = b.gradients.at("cell");
+            const double shifts[3] = {(double)sample[3], (double)sample[4], (double)sample[5]};
+            for (int abc = 0; abc < 3; abc++)
+                for (int xyz = 0; xyz < 3; xyz++)
+                    for (size_t q = 0; q < blk; q++)
+                        gb.values[((k * 3 + abc) * 3 + xyz) * blk + q] += shifts[abc] * g[xyz * blk + q];
+        }
+    };
+    for (size_t si = 0; si < systems.size(); si++) {
+        const System& s = systems[si];
+        for (const auto& p : s.nl.pairs) {
+            double dir[3] = {p.vector[0] / p.distance, p.vector[1] / p.distance, p.vector[2] / p.distance};
+            calc.compute_for_pair(sph, p.distance, dir, do_grad, vals, grads, Y, GX, GY, GZ, R, dR);
+            const int32_t a = s.types[p.first], b = s.types[p.second];
+            const Sample fwd = {(int32_t)si, (int32_t)p.first, (int32_t)p.second, p.shift[0], p.shift[1], p.shift[2]};
+            const Sample inv = {(int32_t)si, (int32_t)p.second, (int32_t)p.first, -p.shift[0], -p.shift[1], -p.shift[2]};
+            const double vfwd[3] = {p.vector[0], p.vector[1], p.vector[2]};
+            const double vinv[3] = {-p.vector[0], -p.vector[1], -p.vector[2]};
+            for (int l = 0; l <= lmax; l++)
+                accumulate(l, first_block[{a, b}] + l, fwd, vals[l].data(), grads[l].data(), vfwd);
+            // PairContribution::inverse_pair (:130-163): values x (-1)^l,
+            // gradients x -(-1)^l
+            for (int l = 0; l <= lmax; l++) {
+                const double m1 = (l % 2 == 0) ? 1.0 : -1.0;
+                for (auto& v : vals[l]) v *= m1;
+                for (auto& g : grads[l]) g *= -m1;
+                accumulate(l, first_block[{b, a}] + l, inv, vals[l].data(), grads[l].data(), vinv);
+            }
+        }
+    }
+    return tm;
+}
+
 static thread_local std::string LAST_ERROR;
 
 struct oracle_result {
@@ -1981,7 +2161,9 @@ int oracle_compute(int32_t calculator, const oracle_hypers* h, const oracle_syst
         opt.threads = threads < 1 ? 1 : threads;
         opt.se_over_centres = se_over_centres != 0;
         auto* r = new oracle_result;
-        r->tm = calculator == 0 ? spherical_expansion(calc, sys, opt) : power_spectrum(calc, sys, opt);
+        if (calculator == 0) r->tm = spherical_expansion(calc, sys, opt);
+        else if (calculator == 1) r->tm = power_spectrum(calc, sys, opt);
+        else r->tm = spherical_expansion_by_pair(calc, sys, opt);
         *out = r;
         return 0;
     } catch (std::exception& e) { LAST_ERROR = e.what(); return 1; }

@@ -11,6 +11,7 @@ from .calculators import (  # noqa: F401
     SoapPowerSpectrum,
     SoapRadialSpectrum,
     SphericalExpansion,
+    SphericalExpansionByPair,
     System,
     TensorBlock,
     TensorMap,

@@ -384,6 +384,16 @@ class SphericalExpansion(CalculatorBase):
         super().__init__("spherical_expansion", {"cutoff": cutoff, "density": density, "basis": basis})
 
 
+class SphericalExpansionByPair(CalculatorBase):
+    """featomic's ``spherical_expansion_by_pair``: one row per pair and
+    direction, keys (o3_lambda, o3_sigma, first_atom_type, second_atom_type),
+    samples (system, first_atom, second_atom, cell_shift_a/b/c)
+    (featomic/src/calculators/soap/spherical_expansion_pair.rs)."""
+
+    def __init__(self, cutoff, density, basis):
+        super().__init__("spherical_expansion_by_pair", {"cutoff": cutoff, "density": density, "basis": basis})
+
+
 class SoapPowerSpectrum(CalculatorBase):
     def __init__(self, cutoff, density, basis):
         super().__init__("soap_power_spectrum", {"cutoff": cutoff, "density": density, "basis": basis})

@@ -1,6 +1,7 @@
 // Calculator facade: registry, construction from JSON and dispatch to the
 // engine (featomic/src/calculator.rs:243-526, registry :574-588): spherical
-// expansion, SOAP power spectrum and SOAP radial spectrum.
+// expansion, spherical expansion by pair, SOAP power spectrum and SOAP radial
+// spectrum.
 #include "engine.hpp"
 #include "host.hpp"
 
@@ -25,8 +26,12 @@ std::unique_ptr<CalculatorImpl> create_calculator(const std::string& name, const
         c->hypers = parse_hypers(json, /*deny_unknown_top=*/false, /*radial_spectrum_basis=*/true);
         c->power_spectrum = false;
         c->radial_spectrum = true;
-    } else if (name == "spherical_expansion_by_pair" ||
-               name == "lode_spherical_expansion" || name == "atomic_composition" || name == "dummy_calculator" ||
+    } else if (name == "spherical_expansion_by_pair") {
+        c->pretty_name = "spherical expansion by pair";
+        c->hypers = parse_hypers(json, /*deny_unknown_top=*/true);
+        c->power_spectrum = false;
+        c->by_pair = true;
+    } else if (name == "lode_spherical_expansion" || name == "atomic_composition" || name == "dummy_calculator" ||
                name == "neighbor_list" || name == "sorted_distances") {
         throw invalid_parameter("calculator '" + name + "' is not implemented by featomic-b200");
     } else {
@@ -72,8 +77,10 @@ void to_radial_spectrum(TensorMap& tm) {
 
 std::unique_ptr<TensorMap> compute(CalculatorImpl& calc, std::vector<HostSystem>& systems, const GradientOptions& grads,
                                    bool device_output, const double* positions_device, void* stream) {
-    auto tm = calc.engine->compute(calc.power_spectrum, systems, grads, device_output, positions_device,
-                                   (cudaStream_t)stream);
+    const int kind = calc.power_spectrum ? Engine::OUTPUT_POWER_SPECTRUM
+                     : calc.by_pair      ? Engine::OUTPUT_BY_PAIR
+                                         : Engine::OUTPUT_EXPANSION;
+    auto tm = calc.engine->compute(kind, systems, grads, device_output, positions_device, (cudaStream_t)stream);
     if (calc.radial_spectrum && tm) to_radial_spectrum(*tm);
     return tm;
 }

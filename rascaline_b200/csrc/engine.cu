@@ -317,9 +317,10 @@ void Engine::upload_tables() {
     tables_ready_ = true;
 }
 
-std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& systems, const GradientOptions& g,
+std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& systems, const GradientOptions& g,
                                            bool device_output, const double* d_positions_in, cudaStream_t stream) {
     auto t_start = std::chrono::steady_clock::now();
+    const bool ps = kind == OUTPUT_POWER_SPECTRUM, by_pair = kind == OUTPUT_BY_PAIR;
     upload_tables();
     cudaEvent_t ev[12];
     for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
@@ -400,10 +401,13 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
 
     // ---- pair indices to the host, then the per-pair features run on the GPU
     // while the host builds the metadata ----------------------------------------
-    std::vector<int32_t> h_first(pairs.count), h_second(pairs.count);
+    std::vector<int32_t> h_first(pairs.count), h_second(pairs.count), h_shift(by_pair ? 3 * pairs.count : 0);
     if (pairs.count) {
         CUDA_CHECK(cudaMemcpyAsync(h_first.data(), pairs.first, sizeof(int32_t) * pairs.count, cudaMemcpyDeviceToHost, stream));
         CUDA_CHECK(cudaMemcpyAsync(h_second.data(), pairs.second, sizeof(int32_t) * pairs.count, cudaMemcpyDeviceToHost, stream));
+        if (by_pair)
+            CUDA_CHECK(cudaMemcpyAsync(h_shift.data(), pairs.shift, sizeof(int32_t) * 3 * pairs.count,
+                                       cudaMemcpyDeviceToHost, stream));
     }
     CUDA_CHECK(cudaEventRecord(ev[6], stream));
 
@@ -419,7 +423,9 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
     CUDA_CHECK(cudaEventSynchronize(ev[6]));
     auto t_meta0 = std::chrono::steady_clock::now();
     Neighborhoods nh = build_neighborhoods(systems, pairs.count, h_first.data(), h_second.data());
-    OutputPlan plan = ps ? plan_power_spectrum(nh, h_, g) : plan_spherical_expansion(nh, h_, g);
+    OutputPlan plan = ps        ? plan_power_spectrum(nh, h_, g)
+                      : by_pair ? plan_by_pair(nh, h_, g, pairs.count, h_first.data(), h_second.data(), h_shift.data())
+                                : plan_spherical_expansion(nh, h_, g);
     auto t_meta1 = std::chrono::steady_clock::now();
     const int S = nh.n_species;
 
@@ -441,7 +447,48 @@ std::unique_ptr<TensorMap> Engine::compute(bool ps, std::vector<HostSystem>& sys
         d_out = arena_.alloc<double>("output", total);
     }
 
-    if (nh.n_atoms > 0 && !plan.blocks.empty()) {
+    if (by_pair && !plan.blocks.empty()) {
+        // ---- spherical expansion by pair: scatter of the pair records --------
+        CUDA_CHECK(cudaEventRecord(ev[7], stream));
+        CUDA_CHECK(cudaMemsetAsync(d_out, 0, sizeof(double) * (size_t)total, stream));
+        std::vector<int64_t> offv, offp, offs, offc;
+        for (auto& b : plan.blocks) {
+            offv.push_back(b.off_values);
+            offp.push_back(b.off_positions);
+            offs.push_back(b.off_strain);
+            offc.push_back(b.off_cell);
+        }
+        ByPairArgs bp{};
+        bp.layout = layout;
+        bp.n_dirs = 2 * pairs.count;
+        bp.pairs = pairs;
+        bp.features = features;
+        bp.dir_block0 = upload(arena_, "bp.block0", plan.bp_block0, stream);
+        bp.dir_row0 = upload(arena_, "bp.row0", plan.bp_row0, stream);
+        bp.dir_row1 = upload(arena_, "bp.row1", plan.bp_row1, stream);
+        bp.dir_grow = upload(arena_, "bp.grow", plan.bp_grow, stream);
+        bp.off_values = upload(arena_, "bp.offv", offv, stream);
+        bp.off_positions = upload(arena_, "bp.offp", offp, stream);
+        bp.off_strain = upload(arena_, "bp.offs", offs, stream);
+        bp.off_cell = upload(arena_, "bp.offc", offc, stream);
+        bp.n_self = (int64_t)plan.bp_self_row.size();
+        bp.self_block = upload(arena_, "bp.self_block", plan.bp_self_block, stream);
+        bp.self_row = upload(arena_, "bp.self_row", plan.bp_self_row, stream);
+        bp.self_contribution = d_self_;
+        bp.out = d_out;
+        CUDA_CHECK(cudaEventRecord(ev[3], stream));
+        CUDA_CHECK(cudaEventRecord(ev[8], stream));
+        CUDA_CHECK(cudaEventRecord(ev[9], stream));
+        launch_by_pair(bp, g.positions, g.strain, g.cell, stream);
+        CUDA_CHECK(cudaEventRecord(ev[4], stream));
+        int32_t h_status = 0;
+        CUDA_CHECK(cudaMemcpyAsync(&h_status, status, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        if (h_status != 0) {
+            throw internal_error("Failed to compute radial integral with GTO basis. Try increasing decreasing the "
+                                 "`cutoff`, or increasing the Gaussian's `width`.");
+        }
+    } else if (nh.n_atoms > 0 && !plan.blocks.empty() && !by_pair) {
         // ---- kernel (b): spherical expansion --------------------------------
         int K = layout.L2 * layout.nmax;
         SeArgs se{};

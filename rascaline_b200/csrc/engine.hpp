@@ -254,6 +254,27 @@ struct SeOutArgs {
 
 void launch_se_output(const SeOutArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream);
 
+// spherical_expansion_by_pair output: every direction's pair contribution
+// scattered into its rows (tables from plan_by_pair)
+struct ByPairArgs {
+    FeatureLayout layout;
+    int64_t n_dirs;                  // 2 x pairs
+    DevicePairs pairs;
+    const double* features;          // drop-in pair records
+    const int32_t* dir_block0;       // [n_dirs]
+    const int64_t* dir_row0;         // [n_dirs]
+    const int64_t* dir_row1;         // [n_dirs]
+    const int64_t* dir_grow;         // [n_dirs]
+    const int64_t *off_values, *off_positions, *off_strain, *off_cell;  // per block
+    int64_t n_self;
+    const int32_t* self_block;       // [n_self]
+    const int64_t* self_row;         // [n_self]
+    const double* self_contribution; // [nmax]
+    double* out;                     // zero-filled before the launch
+};
+
+void launch_by_pair(const ByPairArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream);
+
 }  // namespace fb200
 
 namespace fb200 {
@@ -273,10 +294,13 @@ struct PhaseTimes {
 // arena, and the compute pipeline.
 class Engine {
   public:
+    static constexpr int OUTPUT_EXPANSION = 0, OUTPUT_POWER_SPECTRUM = 1, OUTPUT_BY_PAIR = 2;
+
     explicit Engine(const Hypers& h);
     ~Engine();
 
-    std::unique_ptr<TensorMap> compute(bool power_spectrum, std::vector<HostSystem>& systems, const GradientOptions& g,
+    // kind: OUTPUT_EXPANSION, OUTPUT_POWER_SPECTRUM or OUTPUT_BY_PAIR
+    std::unique_ptr<TensorMap> compute(int kind, std::vector<HostSystem>& systems, const GradientOptions& g,
                                        bool device_output, const double* d_positions, cudaStream_t stream);
 
     const RadialTables& radial() const { return radial_; }

@@ -307,6 +307,128 @@ void launch_se_accumulate(const SeArgs& args, cudaStream_t stream) {
     CUDA_CHECK(cudaGetLastError());
 }
 
+namespace {
+
+// One warp per direction d = 2 pair + reversed.  The pair contribution of
+// spherical_expansion_pair.rs:323-422 from the pair record, reversed by
+// PairContribution::inverse_pair (:130-163: values x (-1)^l, gradients x
+// -(-1)^l, vector and shifts negated), written like accumulate_in_block
+// (:424-540) into rows that no other direction touches: values; positions
+// rows first -= g, second += g (one row, left at zero, for an i-i image);
+// strain vector[x1] g[x2]; cell shift[abc] g[xyz].  Each row receives one
+// contribution, so the sums of the reference reduce to these stores.
+template <bool POS, bool STRAIN, bool CELL>
+__global__ void __launch_bounds__(256) by_pair_kernel(ByPairArgs a) {
+    constexpr bool GRAD = POS || STRAIN || CELL;
+    const int warps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    const int64_t d = (int64_t)blockIdx.x * warps + (threadIdx.x >> 5);
+    if (d >= a.n_dirs) return;
+    const FeatureLayout L = a.layout;
+    const int64_t p = d >> 1;
+    const bool inv = d & 1;
+    const double* __restrict__ F = a.features + p * L.stride;
+    const double f = F[0];
+    const int N = L.nmax;
+    const int K = L.L2 * N;
+    const int blk0 = a.dir_block0[d];
+    const int64_t row0 = a.dir_row0[d], row1 = a.dir_row1[d];
+    const int64_t grow = GRAD ? a.dir_grow[d] : 0;
+    const bool same_atom = a.pairs.first[p] == a.pairs.second[p];
+    double fg = 0.0, r = 1.0, u[3] = {0.0, 0.0, 0.0}, vd[3] = {0.0, 0.0, 0.0}, sd[3] = {0.0, 0.0, 0.0};
+    if (GRAD) {
+        fg = F[1];
+        r = F[2];
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            u[x] = F[3 + x];
+            vd[x] = inv ? -a.pairs.vector[3 * p + x] : a.pairs.vector[3 * p + x];
+            sd[x] = (double)(inv ? -a.pairs.shift[3 * p + x] : a.pairs.shift[3 * p + x]);
+        }
+    }
+    for (int q = lane; q < K; q += 32) {
+        const int lm = q / N, n = q - lm * N;
+        int l = (int)sqrt((double)lm);
+        while (l * l > lm) l--;
+        while ((l + 1) * (l + 1) <= lm) l++;
+        const int mm = lm - l * l, w = 2 * l + 1;
+        const double m1 = (l & 1) ? -1.0 : 1.0;
+        const int blk = blk0 + l;
+        const int64_t row = l == 0 ? row0 : row1;
+        const double Yv = F[L.off_y + lm];
+        const double Rv = F[L.off_r + l * N + n];
+        double val = f * Yv * Rv;
+        if (inv) val *= m1;
+        a.out[a.off_values[blk] + (row * w + mm) * N + n] = val;
+        if (!GRAD) continue;
+        const double dR = F[L.off_dr + l * N + n];
+        double g[3];
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            const double dY = F[L.off_dy + x * L.L2 + lm];
+            g[x] = fg * u[x] * Rv * Yv + f * dR * u[x] * Yv + f * Rv * dY / r;
+            if (inv) g[x] *= -m1;
+        }
+        if (POS && !same_atom) {
+            double* o = a.out + a.off_positions[blk];
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                o[((grow * 3 + x) * w + mm) * N + n] = 0.0 - g[x];
+                o[(((grow + 1) * 3 + x) * w + mm) * N + n] = g[x];
+            }
+        }
+        if (STRAIN) {
+            double* o = a.out + a.off_strain[blk] + row * 9 * w * N + mm * N + n;
+#pragma unroll
+            for (int x1 = 0; x1 < 3; x1++)
+#pragma unroll
+                for (int x2 = 0; x2 < 3; x2++) o[(x1 * 3 + x2) * w * N] = vd[x1] * g[x2];
+        }
+        if (CELL) {
+            double* o = a.out + a.off_cell[blk] + row * 9 * w * N + mm * N + n;
+#pragma unroll
+            for (int x1 = 0; x1 < 3; x1++)
+#pragma unroll
+                for (int x2 = 0; x2 < 3; x2++) o[(x1 * 3 + x2) * w * N] = sd[x1] * g[x2];
+        }
+    }
+}
+
+// self pairs (i, i, 0 0 0) of the l = 0 blocks: the centre's own density
+// (spherical_expansion_pair.rs:222-313)
+__global__ void by_pair_self_kernel(ByPairArgs a, int nmax) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n_self * nmax) return;
+    const int64_t s = k / nmax;
+    const int n = (int)(k - s * nmax);
+    a.out[a.off_values[a.self_block[s]] + a.self_row[s] * nmax + n] = a.self_contribution[n];
+}
+
+}  // namespace
+
+void launch_by_pair(const ByPairArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream) {
+    if (args.n_dirs > 0) {
+        const int warps = 8;
+        const unsigned blocks = (unsigned)((args.n_dirs + warps - 1) / warps);
+        const int which = (positions ? 1 : 0) | (strain ? 2 : 0) | (cell ? 4 : 0);
+        switch (which) {
+            case 0: by_pair_kernel<false, false, false><<<blocks, 32 * warps, 0, stream>>>(args); break;
+            case 1: by_pair_kernel<true, false, false><<<blocks, 32 * warps, 0, stream>>>(args); break;
+            case 2: by_pair_kernel<false, true, false><<<blocks, 32 * warps, 0, stream>>>(args); break;
+            case 3: by_pair_kernel<true, true, false><<<blocks, 32 * warps, 0, stream>>>(args); break;
+            case 4: by_pair_kernel<false, false, true><<<blocks, 32 * warps, 0, stream>>>(args); break;
+            case 5: by_pair_kernel<true, false, true><<<blocks, 32 * warps, 0, stream>>>(args); break;
+            case 6: by_pair_kernel<false, true, true><<<blocks, 32 * warps, 0, stream>>>(args); break;
+            default: by_pair_kernel<true, true, true><<<blocks, 32 * warps, 0, stream>>>(args); break;
+        }
+        CUDA_CHECK(cudaGetLastError());
+    }
+    if (args.n_self > 0) {
+        const int64_t items = args.n_self * args.layout.nmax;
+        by_pair_self_kernel<<<(unsigned)((items + 255) / 256), 256, 0, stream>>>(args, args.layout.nmax);
+        CUDA_CHECK(cudaGetLastError());
+    }
+}
+
 void launch_se_output(const SeOutArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream) {
     if (args.n_rows > 0) {
         se_output_rows_kernel<<<(unsigned)args.n_rows, 128, 0, stream>>>(args, strain, cell);

@@ -167,6 +167,7 @@ struct CalculatorImpl {
     std::unique_ptr<Engine> engine;
     bool power_spectrum = false;
     bool radial_spectrum = false;  // spherical expansion l = 0, keys (center_type, neighbor_type)
+    bool by_pair = false;          // spherical_expansion_by_pair
     ~CalculatorImpl();
 };
 

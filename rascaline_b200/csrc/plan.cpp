@@ -320,4 +320,89 @@ OutputPlan plan_spherical_expansion(const Neighborhoods& nh, const Hypers& h, co
     return plan;
 }
 
+// spherical_expansion_by_pair (spherical_expansion_pair.rs:547-700) with the
+// samples of FullNeighborList (calculators/neighbor_list.rs:372-490): for
+// each (first type, second type) the pairs of each system in pair order
+// (both directions when the types are equal, else the matching one), then,
+// for l = 0 only, that system's self pairs (i, i, 0 0 0).  Every direction
+// lands in exactly one row of the blocks of its type pair.
+OutputPlan plan_by_pair(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g, int64_t n_pairs,
+                        const int32_t* first, const int32_t* second, const int32_t* shift) {
+    OutputPlan plan;
+    const int L = h.max_angular;
+    auto type_of = [&](int64_t atom) { return nh.species_types[nh.atom_species[atom]]; };
+    std::vector<std::pair<int32_t, int32_t>> tps;
+    for (int64_t p = 0; p < n_pairs; p++) {
+        tps.push_back({type_of(first[p]), type_of(second[p])});
+        tps.push_back({type_of(second[p]), type_of(first[p])});
+    }
+    for (int64_t a = 0; a < nh.n_atoms; a++) tps.push_back({type_of(a), type_of(a)});
+    std::sort(tps.begin(), tps.end());
+    tps.erase(std::unique(tps.begin(), tps.end()), tps.end());
+    auto tp_index = [&](int32_t a, int32_t b) {
+        return (int32_t)(std::lower_bound(tps.begin(), tps.end(), std::make_pair(a, b)) - tps.begin());
+    };
+    plan.keys.names = {"o3_lambda", "o3_sigma", "first_atom_type", "second_atom_type"};
+    for (auto& t : tps)
+        for (int l = 0; l <= L; l++) {
+            plan.keys.values.insert(plan.keys.values.end(), {l, 1, t.first, t.second});
+            plan.blocks.emplace_back();
+            BlockPlan& b = plan.blocks.back();
+            b.l = l;
+            b.samples.names = {"system", "first_atom", "second_atom", "cell_shift_a", "cell_shift_b", "cell_shift_c"};
+            b.gradient_samples.names = {"sample", "system", "atom"};
+        }
+    const size_t T = tps.size();
+    std::vector<int64_t> n0(T, 0), n1(T, 0), ngrad(T, 0);
+    plan.bp_block0.resize(2 * n_pairs);
+    plan.bp_row0.resize(2 * n_pairs);
+    plan.bp_row1.resize(2 * n_pairs);
+    plan.bp_grow.resize(2 * n_pairs);
+    auto add_direction = [&](int64_t d, int32_t system, int64_t a, int64_t b, int32_t s0, int32_t s1, int32_t s2) {
+        const int32_t ti = tp_index(type_of(a), type_of(b));
+        const int32_t la = nh.atom_local[a], lb = nh.atom_local[b];
+        const int64_t r0 = n0[ti]++, r1 = n1[ti]++;
+        plan.bp_block0[d] = ti * (L + 1);
+        plan.bp_row0[d] = r0;
+        plan.bp_row1[d] = r1;
+        plan.bp_grow[d] = ngrad[ti];
+        ngrad[ti] += la == lb ? 1 : 2;
+        for (int l = 0; l <= L; l++) {
+            BlockPlan& bp = plan.blocks[(size_t)ti * (L + 1) + l];
+            const int32_t row = (int32_t)(l == 0 ? r0 : r1);
+            bp.samples.values.insert(bp.samples.values.end(), {system, la, lb, s0, s1, s2});
+            if (!g.positions) continue;
+            bp.gradient_samples.values.insert(bp.gradient_samples.values.end(), {row, system, la});
+            if (la != lb) bp.gradient_samples.values.insert(bp.gradient_samples.values.end(), {row, system, lb});
+        }
+    };
+    int64_t p = 0;
+    const int64_t n_systems = (int64_t)nh.atom_offset.size() - 1;
+    for (int64_t s = 0; s < n_systems; s++) {
+        for (; p < n_pairs && nh.atom_system[first[p]] == s; p++) {
+            const int32_t* sh = shift + 3 * p;
+            add_direction(2 * p, (int32_t)s, first[p], second[p], sh[0], sh[1], sh[2]);
+            add_direction(2 * p + 1, (int32_t)s, second[p], first[p], -sh[0], -sh[1], -sh[2]);
+        }
+        for (int64_t a = nh.atom_offset[s]; a < nh.atom_offset[s + 1]; a++) {
+            const int32_t ti = tp_index(type_of(a), type_of(a));
+            BlockPlan& bp = plan.blocks[(size_t)ti * (L + 1)];
+            plan.bp_self_block.push_back(ti * (L + 1));
+            plan.bp_self_row.push_back(n0[ti]++);
+            bp.samples.values.insert(bp.samples.values.end(), {(int32_t)s, nh.atom_local[a], nh.atom_local[a], 0, 0, 0});
+        }
+    }
+    if (p != n_pairs) throw internal_error("spherical_expansion_by_pair: pairs are not grouped by system");
+    for (size_t ti = 0; ti < T; ti++)
+        for (int l = 0; l <= L; l++) {
+            BlockPlan& bp = plan.blocks[ti * (L + 1) + l];
+            bp.n_samples = l == 0 ? n0[ti] : n1[ti];
+            bp.n_grad_rows = g.positions ? ngrad[ti] : 0;
+        }
+    std::vector<int64_t> widths;
+    for (auto& bp : plan.blocks) widths.push_back((int64_t)(2 * bp.l + 1) * h.nmax());
+    assign_offsets(plan, g, widths);
+    return plan;
+}
+
 }  // namespace fb200

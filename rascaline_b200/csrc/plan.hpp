@@ -63,10 +63,20 @@ struct OutputPlan {
     std::vector<int32_t> grad_block, grad_centre, grad_atom, grad_d0, grad_d1;
     std::vector<int64_t> grad_row;
     std::vector<int32_t> block_l, block_species;
+    // spherical expansion by pair, per direction d = 2 pair + reversed: the
+    // block of l = 0 of its type pair (block of l = block0 + l), its row in
+    // the l = 0 and l > 0 blocks and its first positions gradient row; and
+    // the self pairs (l = 0 block, row)
+    std::vector<int32_t> bp_block0;
+    std::vector<int64_t> bp_row0, bp_row1, bp_grow;
+    std::vector<int32_t> bp_self_block;
+    std::vector<int64_t> bp_self_row;
 };
 
 OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g);
 OutputPlan plan_spherical_expansion(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g);
+OutputPlan plan_by_pair(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g, int64_t n_pairs,
+                        const int32_t* first, const int32_t* second, const int32_t* shift);
 
 // Labels of the properties of each calculator
 Labels ps_properties(const Hypers& h);

@@ -57,7 +57,8 @@ def compare_tensormaps(product, oracle_tm, gradients):
 
 def run_product(calculator, hypers, systems, gradients=(), use_native_system=True):
     cls = {"spherical_expansion": rb.SphericalExpansion, "soap_power_spectrum": rb.SoapPowerSpectrum,
-           "soap_radial_spectrum": rb.SoapRadialSpectrum}[calculator]
+           "soap_radial_spectrum": rb.SoapRadialSpectrum,
+           "spherical_expansion_by_pair": rb.SphericalExpansionByPair}[calculator]
     calc = cls(**hypers)
     tm = calc.compute([rb.System.from_dict(s) for s in systems], gradients=list(gradients),
                       use_native_system=use_native_system)
