@@ -27,6 +27,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # without contracting a*b+c into FMAs (rustc never contracts), so that sums
 # that cancel keep the reference's rounding.
 DEVICE = ["-fmad=false"]
+# The FP32 forms (dense adjoint, batched molecules, learned surrogate) are not
+# held to featomic's rounding: their kernels contract into FMAs.
+FMA_SOURCES = ("dense.cu", "surrogate.cu", "surrogate_mma.cu", "batched_kernels_")
 COMMON = [
     "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fopenmp",
     f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}", "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets",
@@ -69,7 +72,8 @@ def _compile(src, verbose, force=True):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
     if not force and not verbose and _object_current(src, obj):
         return obj, ""
-    cmd = [nvcc()] + ARCH + DEVICE + COMMON + ["-c", src, "-o", obj]
+    device = ["-fmad=true"] if os.path.basename(src).startswith(FMA_SOURCES) else DEVICE
+    cmd = [nvcc()] + ARCH + device + COMMON + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [nvcc(), "-x", "c++"] + COMMON + ["-c", src, "-o", obj]
     if verbose:

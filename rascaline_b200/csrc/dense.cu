@@ -33,6 +33,7 @@
 //   systems      CTA per system: strain and cell derivatives summed over atoms
 // Every reduction has a fixed order: results are deterministic.
 #include <cub/cub.cuh>
+#include <type_traits>
 
 #include "dense.hpp"
 #include "pair_math.cuh"
@@ -466,16 +467,37 @@ __global__ void __launch_bounds__(128) dense_pair_adjoint_fused(DenseArgs<T> a, 
     T R[NCAP], dR[NCAP], P[NCAP];
     T sign = T(1);
     T g0 = T(0), g1 = T(0), g2 = T(0);
+    // With N == NCAP the rows are read as 16-byte vectors (K N-aligned rows
+    // of 4 or 2 elements): the kernel is bound by L1 load throughput.
+    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    constexpr int W = 16 / sizeof(T);
+    const bool vec = N == NCAP && (a.K * (int)sizeof(T)) % 16 == 0;
     auto term = [&](int lm, T y, const T* gy) {
         T A = T(0), B = T(0);
         const T* di = Di + lm * N;
         const T* dj = Dj + lm * N;
+        if (vec) {
 #pragma unroll
-        for (int n = 0; n < NCAP; n++) {
-            if (n < N) {
-                const T D = di[n] + sign * dj[n];
-                A += D * P[n];
-                B += D * R[n];
+            for (int q = 0; q < NCAP / W; q++) {
+                const V x4 = __ldg(reinterpret_cast<const V*>(di) + q);
+                const V z4 = __ldg(reinterpret_cast<const V*>(dj) + q);
+                const T* xs = reinterpret_cast<const T*>(&x4);
+                const T* zs = reinterpret_cast<const T*>(&z4);
+#pragma unroll
+                for (int e = 0; e < W; e++) {
+                    const T D = xs[e] + sign * zs[e];
+                    A += D * P[q * W + e];
+                    B += D * R[q * W + e];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int n = 0; n < NCAP; n++) {
+                if (n < N) {
+                    const T D = di[n] + sign * dj[n];
+                    A += D * P[n];
+                    B += D * R[n];
+                }
             }
         }
         const T AY = A * y;

@@ -10,7 +10,8 @@
 //                         4 K-steps of 16, M = 128, N = 64, two TMEM regions
 //   epilogue              tcgen05.ld, h2 = silu(D + b2), dh2 = silu'(.) dD, split
 //   layer 3 (tcgen05)     Y = h2 W3^T, dY = dh2 W3^T, N = outputs rounded up to 16
-//   epilogue              R = s (Y + b3), dR/dr = s dY, stored per distance
+//   epilogue              R = s (Y + b3), dR/dr = s dY, staged in shared memory
+//                         and stored row-contiguously
 // One elected thread issues the MMAs and commits them to an mbarrier; every
 // wait is bounded and sets an error flag instead of hanging.
 //
@@ -247,20 +248,35 @@ __global__ void __launch_bounds__(TILE, 1) surrogate_mma_kernel(MmaArgs a) {
         __syncthreads();
         if (abort_flag) break;
         fence_after();
+        // The layer-3 MMAs have completed (mbarrier), so the A operands are
+        // free: each warp stages its 32 rows x 16 columns there and stores
+        // them row-contiguously (two rows of 64 bytes per instruction)
+        // instead of one scattered element per lane.
+        float* stage_v = reinterpret_cast<float*>(A_h) + warp * (2 * 32 * 17);
+        float* stage_d = stage_v + 32 * 17;
+        const int lane = tid & 31;
         for (int c = 0; c < a.out_pad; c += 16) {
             float y[16], t[16];
             tmem_load16(tmem + lane_base + c, y);
             tmem_load16(tmem + lane_base + 128 + c, t);
-            if (valid) {
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const int o = c + q;
-                    if (o < O) {
-                        a.values[i * a.ld + o] = sc[o] * (y[q] + b3[o]);
-                        if (a.derivs) a.derivs[i * a.ld + o] = sc[o] * t[q];
-                    }
+            for (int q = 0; q < 16; q++) {
+                const int o = c + q;
+                stage_v[lane * 17 + q] = sc[o] * (y[q] + b3[o]);
+                stage_d[lane * 17 + q] = sc[o] * t[q];
+            }
+            __syncwarp();
+            const int col = lane & 15, o = c + col;
+#pragma unroll 4
+            for (int it = 0; it < 16; it++) {
+                const int row = 2 * it + (lane >> 4);
+                const int64_t gi = tile * TILE + warp * 32 + row;
+                if (gi < a.n && o < O) {
+                    a.values[gi * a.ld + o] = stage_v[row * 17 + col];
+                    if (a.derivs) a.derivs[gi * a.ld + o] = stage_d[row * 17 + col];
                 }
             }
+            __syncwarp();
         }
         fence_before();
         __syncthreads();
@@ -334,6 +350,9 @@ void launch_surrogate_mma(const float* master, int hidden, int O, int out_pad, d
     const size_t smem_request = std::max<size_t>(smem, 228 * 1024 / 3 + 1024);
     CUDA_CHECK(cudaFuncSetAttribute(surrogate_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem_request));
+    // the largest shared-memory carveout, so that two CTAs fit on an SM
+    CUDA_CHECK(cudaFuncSetAttribute(surrogate_mma_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
     int per_sm = 0;
     CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, surrogate_mma_kernel, TILE, smem_request));
     if (per_sm < 1 || per_sm > 2) throw internal_error("unexpected residency of the tensor-core surrogate kernel");
