@@ -99,13 +99,11 @@ __global__ void dense_segments(const int32_t* __restrict__ sorted, int64_t n_dir
     seg_offset[k] = lo;
 }
 
+// The record of pair p (cutoff, direction, Y_lm [, dY_lm], R_nl [, dR_nl]) into f
 template <typename T, int LCAP, bool GRAD>
-__global__ void dense_pair_features(DevicePairs pairs, DeviceRadial exact, DenseTables<T> tab, CutoffParams cut,
-                                    FeatureLayout L, T* __restrict__ features, int32_t* __restrict__ status,
-                                    int radial_external) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= pairs.count) return;
-    T* f = features + p * L.stride;
+__device__ __forceinline__ void pair_record(const DevicePairs& pairs, int64_t p, const DeviceRadial& exact,
+                                            const DenseTables<T>& tab, const CutoffParams& cut, const FeatureLayout& L,
+                                            T* __restrict__ f, int32_t* __restrict__ status, int radial_external) {
     const double r = pairs.distance[p];
     const double v0 = pairs.vector[3 * p], v1 = pairs.vector[3 * p + 1], v2 = pairs.vector[3 * p + 2];
     double u0 = v0 / r, u1 = v1 / r, u2 = v2 / r;
@@ -153,6 +151,32 @@ __global__ void dense_pair_features(DevicePairs pairs, DeviceRadial exact, Dense
     for (int l = 0; l <= L.lmax; l++)
         ok &= radial_eval<T>(exact, tab.spline, l, r, f + L.off_r + l * L.nmax, GRAD ? f + L.off_dr + l * L.nmax : nullptr);
     if (!ok) atomicExch(status, 1);
+}
+
+// Thread per pair.  STAGED: the records of the CTA are built in shared
+// memory (row pitch stride + 1) and written out as one contiguous block, so
+// that the stores are coalesced instead of one scattered element per lane
+// (the records of consecutive pairs are adjacent in HBM).
+template <typename T, int LCAP, bool GRAD, bool STAGED>
+__global__ void dense_pair_features(DevicePairs pairs, DeviceRadial exact, DenseTables<T> tab, CutoffParams cut,
+                                    FeatureLayout L, T* __restrict__ features, int32_t* __restrict__ status,
+                                    int radial_external) {
+    extern __shared__ __align__(16) unsigned char feature_smem[];
+    const int64_t p0 = (int64_t)blockIdx.x * blockDim.x;
+    const int64_t p = p0 + threadIdx.x;
+    const int pitch = L.stride + 1;
+    T* f = STAGED ? reinterpret_cast<T*>(feature_smem) + threadIdx.x * pitch : features + p * L.stride;
+    if (p < pairs.count) pair_record<T, LCAP, GRAD>(pairs, p, exact, tab, cut, L, f, status, radial_external);
+    if (!STAGED) return;
+    __syncthreads();
+    const int count = (int)min((int64_t)blockDim.x, pairs.count - p0);
+    const int total = count * L.stride;
+    const T* src = reinterpret_cast<const T*>(feature_smem);
+    T* dst = features + p0 * L.stride;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        const int rec = i / L.stride;
+        dst[i] = src[rec * pitch + (i - rec * L.stride)];
+    }
 }
 
 template <typename T>
@@ -597,15 +621,25 @@ void launch_features(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream
     if (n_pairs == 0) return;
     DevicePairs pairs = a.pairs;
     pairs.count = n_pairs;
-    const int threads = 64;
-    const unsigned blocks = (unsigned)((n_pairs + threads - 1) / threads);
     const int external = a.surrogate != nullptr ? 1 : 0;
-    if (a.lmax <= DENSE_LMAX_SMALL) {
-        dense_pair_features<T, DENSE_LMAX_SMALL, GRAD>
-            <<<blocks, threads, 0, stream>>>(pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status, external);
+    // staged records: as many threads (multiple of 32, at most 128) as fit in
+    // 48 KB of shared memory
+    const size_t record = sizeof(T) * (size_t)(a.layout.stride + 1);
+    const int staged_threads = (int)std::min<size_t>(128, (48 * 1024 / record) / 32 * 32);
+    if (a.lmax <= DENSE_LMAX_SMALL && !external && staged_threads >= 32) {
+        const unsigned blocks = (unsigned)((n_pairs + staged_threads - 1) / staged_threads);
+        dense_pair_features<T, DENSE_LMAX_SMALL, GRAD, true><<<blocks, staged_threads, record * staged_threads, stream>>>(
+            pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status, external);
     } else {
-        dense_pair_features<T, DENSE_LMAX_LARGE, GRAD>
-            <<<blocks, threads, 0, stream>>>(pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status, external);
+        const int threads = 64;
+        const unsigned blocks = (unsigned)((n_pairs + threads - 1) / threads);
+        if (a.lmax <= DENSE_LMAX_SMALL) {
+            dense_pair_features<T, DENSE_LMAX_SMALL, GRAD, false><<<blocks, threads, 0, stream>>>(
+                pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status, external);
+        } else {
+            dense_pair_features<T, DENSE_LMAX_LARGE, GRAD, false><<<blocks, threads, 0, stream>>>(
+                pairs, a.exact, a.tab, a.cut, a.layout, a.features, a.status, external);
+        }
     }
     CUDA_CHECK(cudaGetLastError());
     if constexpr (sizeof(T) == 4) {

@@ -423,11 +423,40 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
     CUDA_CHECK(cudaEventSynchronize(ev[6]));
     auto t_meta0 = std::chrono::steady_clock::now();
     Neighborhoods nh = build_neighborhoods(systems, pairs.count, h_first.data(), h_second.data());
+    const int S = nh.n_species;
+
+    // ---- kernel (b): spherical expansion, launched as soon as the
+    // neighbourhoods are known, so that the host builds the output labels
+    // below while the GPU accumulates ------------------------------------------
+    SeArgs se{};
+    const bool run_se = !by_pair && nh.n_atoms > 0;
+    if (run_se) {
+        const int K = layout.L2 * layout.nmax;
+        se.layout = layout;
+        se.n_centres = nh.n_atoms;
+        se.n_species = S;
+        se.centre_species = upload(arena_, "meta.atom_species", nh.atom_species, stream);
+        se.seg_offset = upload(arena_, "meta.seg_offset", nh.seg_offset, stream);
+        se.dir_code = upload(arena_, "meta.dir_code", nh.dir_code, stream);
+        se.features = features;
+        se.self_contribution = d_self_;
+        se.do_positions = g.positions;
+        se.do_strain = g.strain;
+        se.do_cell = g.cell;
+        se.coef = arena_.alloc<double>("se.coef", nh.n_atoms * S * K);
+        se.pair_grad = g.positions ? arena_.alloc<double>("se.pair_grad", pairs.count * 3 * K) : nullptr;
+        se.self_grad = g.positions ? arena_.alloc<double>("se.self_grad", nh.n_atoms * S * 3 * K) : nullptr;
+        se.strain = g.strain ? arena_.alloc<double>("se.strain", nh.n_atoms * S * 9 * K) : nullptr;
+        se.cellg = g.cell ? arena_.alloc<double>("se.cell", nh.n_atoms * S * 9 * K) : nullptr;
+        CUDA_CHECK(cudaEventRecord(ev[7], stream));
+        launch_se_accumulate(se, stream);
+        CUDA_CHECK(cudaEventRecord(ev[3], stream));
+    }
+
     OutputPlan plan = ps        ? plan_power_spectrum(nh, h_, g)
                       : by_pair ? plan_by_pair(nh, h_, g, pairs.count, h_first.data(), h_second.data(), h_shift.data())
                                 : plan_spherical_expansion(nh, h_, g);
     auto t_meta1 = std::chrono::steady_clock::now();
-    const int S = nh.n_species;
 
     auto tm = std::make_unique<TensorMap>();
     tm->keys = plan.keys;
@@ -488,30 +517,7 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
             throw internal_error("Failed to compute radial integral with GTO basis. Try increasing decreasing the "
                                  "`cutoff`, or increasing the Gaussian's `width`.");
         }
-    } else if (nh.n_atoms > 0 && !plan.blocks.empty() && !by_pair) {
-        // ---- kernel (b): spherical expansion --------------------------------
-        int K = layout.L2 * layout.nmax;
-        SeArgs se{};
-        se.layout = layout;
-        se.n_centres = nh.n_atoms;
-        se.n_species = S;
-        se.centre_species = upload(arena_, "meta.atom_species", nh.atom_species, stream);
-        se.seg_offset = upload(arena_, "meta.seg_offset", nh.seg_offset, stream);
-        se.dir_code = upload(arena_, "meta.dir_code", nh.dir_code, stream);
-        se.features = features;
-        se.self_contribution = d_self_;
-        se.do_positions = g.positions;
-        se.do_strain = g.strain;
-        se.do_cell = g.cell;
-        se.coef = arena_.alloc<double>("se.coef", nh.n_atoms * S * K);
-        se.pair_grad = g.positions ? arena_.alloc<double>("se.pair_grad", pairs.count * 3 * K) : nullptr;
-        se.self_grad = g.positions ? arena_.alloc<double>("se.self_grad", nh.n_atoms * S * 3 * K) : nullptr;
-        se.strain = g.strain ? arena_.alloc<double>("se.strain", nh.n_atoms * S * 9 * K) : nullptr;
-        se.cellg = g.cell ? arena_.alloc<double>("se.cell", nh.n_atoms * S * 9 * K) : nullptr;
-        CUDA_CHECK(cudaEventRecord(ev[7], stream));
-        launch_se_accumulate(se, stream);
-        CUDA_CHECK(cudaEventRecord(ev[3], stream));
-
+    } else if (run_se && !plan.blocks.empty()) {
         std::vector<int64_t> offv, offp, offs, offc;
         for (auto& b : plan.blocks) {
             offv.push_back(b.off_values);

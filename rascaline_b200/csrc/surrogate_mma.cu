@@ -359,8 +359,11 @@ void launch_surrogate_mma(const float* master, int hidden, int O, int out_pad, d
     int device = 0, sms = 0;
     CUDA_CHECK(cudaGetDevice(&device));
     CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    // two CTAs per SM (the occupancy query may report one under the default
+    // carveout; a CTA that does not fit waits for a free slot, and the
+    // shared-memory request keeps a third off any SM)
     const int64_t tiles = (n + TILE - 1) / TILE;
-    const int blocks = (int)std::min<int64_t>(tiles, (int64_t)sms * per_sm);
+    const int blocks = (int)std::min<int64_t>(tiles, (int64_t)sms * 2);
     surrogate_mma_kernel<<<blocks, TILE, smem_request, stream>>>(a);
     CUDA_CHECK(cudaGetLastError());
 }
