@@ -7,7 +7,7 @@
 //                featomic's accumulate_all_pairs (spherical_expansion.rs:
 //                101-358); segment starts by binary search
 //   features     thread per pair: cutoff, Y_lm, R_nl in T
-//   expansion    CTA per centre, thread per (l, m, n), segments reduced in
+//   expansion    CTA per (centre, species), thread per (l, m, n), segment reduced in
 //                registers (no atomics), inverse pairs with (-1)^l
 //                (spherical_expansion_pair.rs:130-163), self term on l = 0
 //   contraction  CTA per centre, coefficients in shared memory, thread per
@@ -185,8 +185,10 @@ __global__ void __launch_bounds__(256) dense_expansion(DenseArgs<T> a) {
     __shared__ T dir_f[DENSE_CHUNK];
     __shared__ int dir_inv[DENSE_CHUNK];
     const FeatureLayout L = a.layout;
-    const int64_t c = blockIdx.x;
+    // one CTA per (centre, neighbour species) segment
     const int S = a.n_species;
+    const int64_t c = blockIdx.x / S;
+    const int t_block = (int)(blockIdx.x - c * S);
     const int K = a.K;
     const int tc = a.atom_species[c];
     for (int k0 = 0; k0 < K; k0 += blockDim.x) {
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(256) dense_expansion(DenseArgs<T> a) {
         const int l = isqrt_lm(lm);
         const T sign_l = (l & 1) ? T(-1) : T(1);
         const int ri = l * L.nmax + n;
-        for (int t = 0; t < S; t++) {
+        for (int t = t_block; t == t_block; t++) {
             const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
             T acc = T(0);
             for (int64_t dc = d0; dc < d1; dc += DENSE_CHUNK) {
@@ -286,6 +288,19 @@ __global__ void __launch_bounds__(256) dense_grad_coef(DenseArgs<T> a) {
     }
 }
 
+// global -> shared copy of n elements, in 16-byte vectors when both ends and
+// the length allow it
+template <typename T>
+__device__ __forceinline__ void stage_copy(T* __restrict__ dst, const T* __restrict__ src, int64_t n) {
+    if (((uintptr_t)dst % 16) == 0 && ((uintptr_t)src % 16) == 0 && (n * (int64_t)sizeof(T)) % 16 == 0) {
+        const int64_t nv = n * (int64_t)sizeof(T) / 16;
+        for (int64_t i = threadIdx.x; i < nv; i += blockDim.x)
+            reinterpret_cast<float4*>(dst)[i] = __ldg(reinterpret_cast<const float4*>(src) + i);
+    } else {
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+    }
+}
+
 // The two per-centre contractions with the centre's coefficients (and, for
 // the adjoint, its dL/dP row) staged in shared memory and register tiles,
 // for nmax <= NCAP and 2 lmax + 1 <= MCAP.  Same sums in the same order as
@@ -301,7 +316,7 @@ __global__ void __launch_bounds__(128) dense_contraction_tiled(DenseArgs<T> a) {
     T* cs = reinterpret_cast<T*>(dense_smem);
     const int64_t c = blockIdx.x;
     const int S = a.n_species, K = a.K, N = a.nmax, NN = N * N, LN = (a.lmax + 1) * N;
-    for (int i = threadIdx.x; i < S * K; i += blockDim.x) cs[i] = a.coef[c * S * K + i];
+    stage_copy(cs, a.coef + c * S * K, (int64_t)S * K);
     __syncthreads();
     const int items = a.n_keys * LN;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
@@ -340,8 +355,8 @@ __global__ void __launch_bounds__(128) dense_grad_coef_tiled(DenseArgs<T> a) {
     const int S = a.n_species, K = a.K, N = a.nmax, NN = N * N, LN = (a.lmax + 1) * N;
     const int64_t KP = (int64_t)a.n_keys * a.n_props;
     T* gs = cs + S * K;
-    for (int i = threadIdx.x; i < S * K; i += blockDim.x) cs[i] = a.coef[c * S * K + i];
-    for (int64_t i = threadIdx.x; i < KP; i += blockDim.x) gs[i] = a.grad_values[c * KP + i];
+    stage_copy(cs, a.coef + c * S * K, (int64_t)S * K);
+    stage_copy(gs, a.grad_values + c * KP, KP);
     __syncthreads();
     for (int it = threadIdx.x; it < S * LN; it += blockDim.x) {
         const int sa = it / LN;
@@ -688,7 +703,7 @@ template <typename T>
 void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream) {
     launch_features<T, false>(a, n_pairs, stream);
     if (a.n_atoms == 0) return;
-    dense_expansion<T><<<(unsigned)a.n_atoms, coefficient_threads(a.K), 0, stream>>>(a);
+    dense_expansion<T><<<(unsigned)(a.n_atoms * a.n_species), coefficient_threads(a.K), 0, stream>>>(a);
     CUDA_CHECK(cudaGetLastError());
     const size_t smem = sizeof(T) * (size_t)a.n_species * a.K;
     if (a.nmax <= 16 && smem <= 48 * 1024) {

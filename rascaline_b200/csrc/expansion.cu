@@ -10,7 +10,7 @@
 //   disabled, analytically (radial_integral/gto.rs:115-205).  The result is a
 //   per-pair feature record in HBM.
 //
-// * `se_accumulate` -- one CTA per centre, one thread per coefficient
+// * `se_accumulate` -- one CTA per (centre, neighbour species), one thread per coefficient
 //   (l, m, n).  Directions (pair, orientation) are sorted by
 //   (centre, neighbour species, pair), so every (centre, species) segment is a
 //   contiguous run reduced in registers: no atomics, deterministic order.  It
@@ -89,8 +89,11 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
     constexpr bool GRAD = POS || STRAIN || CELL;
     __shared__ DirScalars dirs[SE_CHUNK];
     const FeatureLayout L = a.layout;
-    const int64_t c = blockIdx.x;
+    // one CTA per (centre, neighbour species) segment: the segments are
+    // independent, and S times more CTAs keep more of them in flight
     const int S = a.n_species;
+    const int64_t c = blockIdx.x / S;
+    const int t_block = (int)(blockIdx.x - c * S);
     const int K = L.L2 * L.nmax;
     const int tc = a.centre_species[c];
 
@@ -105,7 +108,7 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
         const double sign_l = (l & 1) ? -1.0 : 1.0;
         const int ri = l * L.nmax + n;
 
-        for (int t = 0; t < S; t++) {
+        for (int t = t_block; t == t_block; t++) {
             const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
             double acc = 0.0;
             double sg[3] = {0.0, 0.0, 0.0};
@@ -293,7 +296,7 @@ void launch_se_accumulate(const SeArgs& args, cudaStream_t stream) {
     int threads = std::max(SE_CHUNK, std::min(256, (K + 31) / 32 * 32));
     const bool grad = args.layout.with_grad;
     const bool p = grad && args.do_positions, st = grad && args.do_strain, ce = grad && args.do_cell;
-    const unsigned blocks = (unsigned)args.n_centres;
+    const unsigned blocks = (unsigned)(args.n_centres * args.n_species);
 #define SE_LAUNCH(P, ST, CE) se_accumulate_kernel<P, ST, CE><<<blocks, threads, 0, stream>>>(args)
     if (!p && !st && !ce) SE_LAUNCH(false, false, false);
     else if (p && !st && !ce) SE_LAUNCH(true, false, false);
