@@ -270,14 +270,46 @@ class _CSystem:
         self.struct = C.featomic_system_t(None, *self._callbacks)
 
 
-def _options(gradients, use_native_system):
+def _c_labels(labels, keep):
+    """mts_labels_t view of a Labels (or (names, values)); `keep` holds the buffers."""
+    if not isinstance(labels, Labels):
+        labels = Labels(*labels)
+    names = (ctypes.c_char_p * max(1, len(labels.names)))(*[n.encode() for n in labels.names])
+    values = np.ascontiguousarray(labels.values, dtype=np.int32)
+    c = C.mts_labels_t()
+    c.names = ctypes.cast(names, ctypes.POINTER(ctypes.c_char_p))
+    c.values = values.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    c.size = len(labels.names)
+    c.count = values.shape[0]
+    keep += [names, values, c]
+    return ctypes.pointer(c)
+
+
+def _selection(selection, target, keep):
+    """featomic_labels_selection_t from None, Labels / (names, values) (a
+    subset) or a TensorMap (predefined labels per block)."""
+    if selection is None:
+        return
+    if isinstance(selection, TensorMap):
+        target.predefined = selection._handle.value
+        keep.append(selection)
+    else:
+        target.subset = _c_labels(selection, keep)
+
+
+def _options(gradients, use_native_system, selected_samples=None, selected_properties=None, selected_keys=None):
     gradients = list(gradients or [])
     arr = (ctypes.c_char_p * max(1, len(gradients)))(*[g.encode() for g in gradients])
     opts = C.featomic_calculation_options_t()
     opts.gradients = ctypes.cast(arr, ctypes.POINTER(ctypes.c_char_p))
     opts.gradients_count = len(gradients)
     opts.use_native_system = bool(use_native_system)
-    return opts, arr
+    keep = [arr]
+    _selection(selected_samples, opts.selected_samples, keep)
+    _selection(selected_properties, opts.selected_properties, keep)
+    if selected_keys is not None:
+        opts.selected_keys = _c_labels(selected_keys, keep)
+    return opts, keep
 
 
 class CalculatorBase:
@@ -320,13 +352,18 @@ class CalculatorBase:
         C.check(C.lib().featomic_calculator_cutoffs(self._handle, ctypes.byref(ptr), ctypes.byref(count)))
         return [ptr[i] for i in range(count.value)]
 
-    def compute(self, systems, gradients=None, use_native_system=True):
-        """Run the calculation on host systems; the result lives in host memory."""
+    def compute(self, systems, gradients=None, use_native_system=True, selected_samples=None,
+                selected_properties=None, selected_keys=None):
+        """Run the calculation on host systems; the result lives in host memory.
+        Selections follow featomic's ``CalculatorBase.compute``
+        (python/featomic/featomic/calculator_base.py:187+): ``Labels`` (or
+        ``(names, values)``) select a subset, a ``TensorMap`` gives the labels
+        of every block."""
         if isinstance(systems, (System, dict)):
             systems = [systems]
         csys = [_CSystem(System.from_dict(s)) for s in systems]
         arr = (C.featomic_system_t * max(1, len(csys)))(*[c.struct for c in csys])
-        opts, keep = _options(gradients, use_native_system)
+        opts, keep = _options(gradients, use_native_system, selected_samples, selected_properties, selected_keys)
         out = ctypes.c_void_p()
         C.check(C.lib().featomic_calculator_compute(self._handle, ctypes.byref(out), arr, len(csys), opts))
         if not out.value:

@@ -139,16 +139,51 @@ GradientOptions parse_options(const featomic_calculation_options_t& options) {
             throw invalid_parameter("unexpected gradient \"" + p +
                                     "\", should be one of \"positions\", \"cell\", or \"strain\"");
     }
-    if (options.selected_samples.subset || options.selected_samples.predefined || options.selected_properties.subset ||
-        options.selected_properties.predefined || options.selected_keys) {
-        throw invalid_parameter("samples / properties / keys selections are not supported by featomic-b200 yet");
-    }
     if (g.cell && std::getenv("FEATOMIC_NO_WARN_CELL_GRADIENTS") == nullptr) {
         log_message(FEATOMIC_LOG_LEVEL_WARN,
                     "The meaning of \"cell\" gradients has changed recently, you likely want \"strain\" gradients "
                     "instead. Please review the documentation carefully.");
     }
     return g;
+}
+
+Labels labels_from_c(const mts_labels_t* c, const char* what) {
+    Labels out;
+    if (c->size > 0) CHECK_POINTER(c->names);
+    if (c->count > 0 && c->size > 0) CHECK_POINTER(c->values);
+    for (uintptr_t k = 0; k < c->size; k++) {
+        if (!c->names[k]) throw invalid_parameter(std::string("NULL name in ") + what + " selection");
+        out.names.push_back(c->names[k]);
+    }
+    out.values.assign(c->values, c->values + c->size * c->count);
+    return out;
+}
+
+// featomic's selections in C form (featomic.h:245-277) -> owned labels
+struct SelectionStorage {
+    Labels keys, samples, properties;
+    Selection selection;
+};
+
+void parse_selections(const featomic_calculation_options_t& options, int max_angular, SelectionStorage& st) {
+    st.selection.max_angular = max_angular;
+    if (options.selected_keys) {
+        st.keys = labels_from_c(options.selected_keys, "keys");
+        st.selection.keys = &st.keys;
+    }
+    const featomic_labels_selection_t* which[2] = {&options.selected_samples, &options.selected_properties};
+    for (int k = 0; k < 2; k++) {
+        const featomic_labels_selection_t& s = *which[k];
+        const char* kind = k == 0 ? "samples" : "properties";
+        if (s.subset && s.predefined)
+            throw invalid_parameter(std::string("can not have both a subset and a predefined ") + kind + " selection");
+        if (s.subset) {
+            Labels& dst = k == 0 ? st.samples : st.properties;
+            dst = labels_from_c(s.subset, kind);
+            (k == 0 ? st.selection.samples : st.selection.properties) = &dst;
+        }
+        if (s.predefined) (k == 0 ? st.selection.samples_predefined : st.selection.properties_predefined) = s.predefined->tm.get();
+    }
 }
 
 mts_tensormap_t* wrap(std::unique_ptr<TensorMap> tm) {
@@ -299,10 +334,12 @@ featomic_status_t featomic_calculator_compute(featomic_calculator_t* calculator,
                 }
             }
         }
+        SelectionStorage selection;
+        parse_selections(options, calculator->impl->hypers.max_angular, selection);
         warn_close_pairs(host);
         auto tm = compute(*calculator->impl, host, g, false, nullptr, nullptr);
         record_profile(calculator->impl->engine->last_times());
-        *descriptor = wrap(std::move(tm));
+        *descriptor = wrap(apply_selection(std::move(tm), selection.selection));
     });
 }
 
@@ -338,6 +375,9 @@ featomic_status_t featomic_b200_calculator_compute_device(featomic_calculator_t*
                 throw invalid_parameter("featomic_b200_calculator_compute_device expects device positions");
             }
         }
+        if (options.selected_samples.subset || options.selected_samples.predefined ||
+            options.selected_properties.subset || options.selected_properties.predefined || options.selected_keys)
+            throw invalid_parameter("selections are supported by featomic_calculator_compute (host output) only");
         auto tm = compute(*calculator->impl, host, g, true, systems->positions, (cudaStream_t)stream);
         record_profile(calculator->impl->engine->last_times());
         *descriptor = wrap(std::move(tm));

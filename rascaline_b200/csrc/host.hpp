@@ -181,6 +181,20 @@ std::unique_ptr<TensorMap> compute(CalculatorImpl& calc, std::vector<HostSystem>
                                    const GradientOptions& grads, bool device_output,
                                    const double* positions_device, void* stream);
 
+// Samples / properties / keys selections (featomic's CalculationOptions,
+// calculator.rs:20-158), applied to the host output of a full calculation
+struct Selection {
+    const Labels* keys = nullptr;
+    const Labels* samples = nullptr;
+    const Labels* properties = nullptr;
+    const TensorMap* samples_predefined = nullptr;
+    const TensorMap* properties_predefined = nullptr;
+    int max_angular = 0;  // for the components of keys the systems do not produce
+    bool any() const { return keys || samples || properties || samples_predefined || properties_predefined; }
+};
+
+std::unique_ptr<TensorMap> apply_selection(std::unique_ptr<TensorMap> full, const Selection& selection);
+
 // run kernel (a) on one system given on the host, return the pairs
 std::vector<Pair> neighbor_list(const double* positions, int64_t n_atoms, const double* cell, double cutoff);
 
