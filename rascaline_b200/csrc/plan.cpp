@@ -179,7 +179,7 @@ void assign_offsets(OutputPlan& plan, const GradientOptions& g, const std::vecto
 
 }  // namespace
 
-OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g) {
+OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g, bool with_labels) {
     OutputPlan plan;
     const int S = nh.n_species;
     const int64_t N = nh.n_atoms;
@@ -222,6 +222,15 @@ OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const G
         plan.slot_offset[c + 1] = (int64_t)plan.slots.size();
     }
 
+    int64_t n_props = (int64_t)(h.max_angular + 1) * h.nmax() * h.nmax();
+    assign_offsets(plan, g, std::vector<int64_t>(nb, n_props));
+    if (with_labels) fill_power_spectrum_labels(nh, g, plan);
+    return plan;
+}
+
+void fill_power_spectrum_labels(const Neighborhoods& nh, const GradientOptions& g, OutputPlan& plan) {
+    const int64_t N = nh.n_atoms;
+    const int32_t nb = (int32_t)plan.blocks.size();
     // labels, written in place: every slot knows its sample row and its first
     // gradient row, so centres fill their rows independently
     std::vector<int32_t*> sample_w(nb), grad_w(nb);
@@ -256,9 +265,6 @@ OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const G
             }
         }
     }
-    int64_t n_props = (int64_t)(h.max_angular + 1) * h.nmax() * h.nmax();
-    assign_offsets(plan, g, std::vector<int64_t>(nb, n_props));
-    return plan;
 }
 
 OutputPlan plan_spherical_expansion(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g) {

@@ -73,7 +73,12 @@ struct OutputPlan {
     std::vector<int64_t> bp_self_row;
 };
 
-OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g);
+// without labels, the kernel tables and offsets only: the sample and
+// gradient-sample labels can then be written by fill_power_spectrum_labels
+// while the kernels run
+OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g,
+                               bool with_labels = true);
+void fill_power_spectrum_labels(const Neighborhoods& nh, const GradientOptions& g, OutputPlan& plan);
 OutputPlan plan_spherical_expansion(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g);
 OutputPlan plan_by_pair(const Neighborhoods& nh, const Hypers& h, const GradientOptions& g, int64_t n_pairs,
                         const int32_t* first, const int32_t* second, const int32_t* shift);
