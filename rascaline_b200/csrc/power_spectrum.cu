@@ -305,6 +305,11 @@ __device__ __forceinline__ const double* staged_source(const PsArgs& a, int64_t 
 }
 
 constexpr int POS_WARPS = 4;
+// per-centre slot tables staged in shared memory (centres with at most this
+// many slots; more read them from global memory), and per-warp entry counts
+constexpr int POS_SLOT_CAP = 64;
+constexpr int POS_CUM_CAP = 65;
+constexpr size_t POS_TABLE_BYTES = POS_SLOT_CAP * (8 + 2 * 4) + POS_WARPS * POS_CUM_CAP * 4;
 
 template <int MAXN>
 __global__ void __launch_bounds__(POS_WARPS * 32, 4) ps_positions_kernel(PsArgs a) {
@@ -316,10 +321,27 @@ __global__ void __launch_bounds__(POS_WARPS * 32, 4) ps_positions_kernel(PsArgs 
     double* coef_s = smem;
     double* scale_s = smem + S * K;
     double* stage = smem + ((S * K + 2 * (a.lmax + 1) + 1) & ~1) + (int64_t)warp * 3 * K;
+    // output-row tables: the first output element of every slot and its
+    // species pair, then each warp's copy of its entry's counts, so that the
+    // slot loop reads shared memory instead of a chain of dependent global
+    // loads (slot -> counts -> first row -> block offset)
+    int64_t* slot_base = reinterpret_cast<int64_t*>(smem + ((S * K + 2 * (a.lmax + 1) + 1) & ~1) +
+                                                    (int64_t)nwarps * 3 * K);
+    int32_t* slot_ab = reinterpret_cast<int32_t*>(slot_base + POS_SLOT_CAP);
+    int32_t* cum_w = slot_ab + 2 * POS_SLOT_CAP + warp * POS_CUM_CAP;
     load_coefficients(a, c, coef_s, S * K);
     load_scales(a.lmax, scale_s);
-    __syncthreads();
     const int64_t s0 = a.slot_offset[c], ns = a.slot_offset[c + 1] - s0;
+    const bool tables = ns <= POS_SLOT_CAP;
+    if (tables) {
+        for (int64_t i = threadIdx.x; i < ns; i += blockDim.x) {
+            const PsKeySlot slot = a.slots[s0 + i];
+            slot_base[i] = a.off_positions[slot.block] + a.slot_row[s0 + i] * 3 * a.n_props;
+            slot_ab[2 * i] = slot.a;
+            slot_ab[2 * i + 1] = slot.b;
+        }
+    }
+    __syncthreads();
     const int64_t e0 = a.entry_offset[c], ne = a.entry_offset[c + 1] - e0;
     for (int64_t e = warp; e < ne; e += nwarps) {
         double* cur = stage;
@@ -341,12 +363,25 @@ __global__ void __launch_bounds__(POS_WARPS * 32, 4) ps_positions_kernel(PsArgs 
             direct.p = cur;
             direct.flip = a.dir_code[entry.d0] & 1;
         }
+        if (tables) {
+            for (int i = lane; i <= S; i += 32) cum_w[i] = cum[i];
+            __syncwarp();
+        }
         for (int64_t s = 0; s < ns; s++) {
-            const PsKeySlot slot = a.slots[s0 + s];
-            if (!self && entry.species != slot.a && entry.species != slot.b) continue;
-            const int64_t rank = cum[slot.a] + (slot.a != slot.b ? cum[slot.b] : 0) + cum[S];
-            const int64_t row = a.slot_row[s0 + s] + rank;
-            double* out = a.out + a.off_positions[slot.block] + row * 3 * a.n_props;
+            PsKeySlot slot;
+            double* out;
+            if (tables) {
+                slot = PsKeySlot{0, 0, slot_ab[2 * s], slot_ab[2 * s + 1]};
+                if (!self && entry.species != slot.a && entry.species != slot.b) continue;
+                const int64_t rank = cum_w[slot.a] + (slot.a != slot.b ? cum_w[slot.b] : 0) + cum_w[S];
+                out = a.out + slot_base[s] + rank * 3 * a.n_props;
+            } else {
+                slot = a.slots[s0 + s];
+                if (!self && entry.species != slot.a && entry.species != slot.b) continue;
+                const int64_t rank = cum[slot.a] + (slot.a != slot.b ? cum[slot.b] : 0) + cum[S];
+                const int64_t row = a.slot_row[s0 + s] + rank;
+                out = a.out + a.off_positions[slot.block] + row * 3 * a.n_props;
+            }
             const double* self_a = a.self_grad + ((int64_t)c * S + slot.a) * 3 * K;
             const double* self_b = a.self_grad + ((int64_t)c * S + slot.b) * 3 * K;
             if (self || single) {
@@ -410,7 +445,8 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
     if (after_values) CUDA_CHECK(cudaEventRecord(after_values, stream));
     if (positions) {
         const size_t pos_bytes = sizeof(double) * (((size_t)args.n_species * K + 2 * (args.lmax + 1) + 1) / 2 * 2 +
-                                                   (size_t)POS_WARPS * 3 * K);
+                                                   (size_t)POS_WARPS * 3 * K) +
+                                 POS_TABLE_BYTES;
         if (pos_bytes > 200 * 1024) throw invalid_parameter("too many radial / angular functions for the positions gradient kernel");
         ps_positions_kernel<MAXN><<<(unsigned)args.n_centres, POS_WARPS * 32, pos_bytes, stream>>>(args);
         CUDA_CHECK(cudaGetLastError());
