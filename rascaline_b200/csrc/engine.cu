@@ -233,7 +233,10 @@ T* upload(DeviceArena& arena, const std::string& name, const std::vector<T>& hos
 
 double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0.0f;
-    cudaEventElapsedTime(&ms, a, b);
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();  // an event of a phase that did not run: not an error of the call
+        return 0.0;
+    }
     return (double)ms;
 }
 
@@ -551,7 +554,12 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
             pa.off_strain = upload(arena_, "ps.offs", offs, stream);
             pa.off_cell = upload(arena_, "ps.offc", offc, stream);
             pa.out = d_out;
-            launch_power_spectrum(pa, g.positions, g.strain, g.cell, stream, ev[8], ev[9]);
+            PsEvents pe;
+            pe.after_values = ev[8];
+            pe.after_strain_cell = ev[11];
+            pe.before_positions = ev[10];
+            pe.after_positions = ev[9];
+            launch_power_spectrum(pa, g.positions, g.strain, g.cell, stream, pe);
             // the labels only describe the output: written while the kernels run
             auto t_labels = std::chrono::steady_clock::now();
             fill_power_spectrum_labels(nh, g, plan);
@@ -674,9 +682,16 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
     times_.features = elapsed_ms(ev[6], ev[2]);
     times_.expansion = elapsed_ms(ev[7], ev[3]);
     times_.contraction = elapsed_ms(ev[3], ev[4]);
-    times_.ps_values = elapsed_ms(ev[3], ev[8]);
-    times_.ps_positions = elapsed_ms(ev[8], ev[9]);
-    times_.ps_strain_cell = elapsed_ms(ev[9], ev[4]);
+    if (ps && run_se) {
+        // values, strain and cell run beside the positions kernel
+        times_.ps_values = elapsed_ms(ev[3], ev[8]);
+        times_.ps_positions = elapsed_ms(ev[10], ev[9]);
+        times_.ps_strain_cell = elapsed_ms(ev[8], ev[11]);
+    } else {
+        times_.ps_values = elapsed_ms(ev[3], ev[8]);
+        times_.ps_positions = elapsed_ms(ev[8], ev[9]);
+        times_.ps_strain_cell = elapsed_ms(ev[9], ev[4]);
+    }
     times_.transfer = elapsed_ms(ev[4], ev[5]);
     times_.total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     return tm;

@@ -216,10 +216,18 @@ struct PsArgs {
     double* out;
 };
 
-// values, then positions / strain / cell rows; events (may be null) are
-// recorded after the values and after the positions kernels
+// timing events of launch_power_spectrum (each may be null)
+struct PsEvents {
+    cudaEvent_t after_values = nullptr;       // side stream
+    cudaEvent_t after_strain_cell = nullptr;  // side stream
+    cudaEvent_t before_positions = nullptr;   // caller's stream
+    cudaEvent_t after_positions = nullptr;    // caller's stream
+};
+
+// positions rows on `stream`; values, strain and cell rows beside it on a
+// second stream of the device; `stream` waits for both before later work
 void launch_power_spectrum(const PsArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream,
-                           cudaEvent_t after_values, cudaEvent_t after_positions);
+                           const PsEvents& events);
 
 // Spherical expansion output scatter (spherical_expansion calculator)
 struct SeOutArgs {

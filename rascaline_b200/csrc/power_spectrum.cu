@@ -25,6 +25,9 @@
 // sample (prefix counts per species).
 #include <cuda_pipeline.h>
 
+#include <map>
+#include <mutex>
+
 #include "engine.hpp"
 
 namespace fb200 {
@@ -424,9 +427,27 @@ __global__ void __launch_bounds__(256) ps_strain_cell_kernel(PsArgs a, int which
     }
 }
 
+// A second stream per device for the values and strain / cell kernels, which
+// run beside the positions kernel and fill the SMs its last wave leaves idle.
+// Dependencies go through events created per call, so concurrent callers that
+// share this stream stay correctly ordered.
+cudaStream_t side_stream() {
+    static std::mutex mutex;
+    static std::map<int, cudaStream_t> streams;
+    int device = 0;
+    CUDA_CHECK(cudaGetDevice(&device));
+    std::lock_guard<std::mutex> lock(mutex);
+    auto it = streams.find(device);
+    if (it != streams.end()) return it->second;
+    cudaStream_t s = nullptr;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    streams[device] = s;
+    return s;
+}
+
 template <int MAXN>
 void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bool cell, cudaStream_t stream,
-                cudaEvent_t after_values, cudaEvent_t after_positions) {
+                const PsEvents& events) {
     const int K = (args.lmax + 1) * (args.lmax + 1) * args.nmax;
     const size_t coef_bytes = sizeof(double) * ((size_t)args.n_species * K + 2 * (args.lmax + 1));
     const int threads = 256;
@@ -438,36 +459,54 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
         configured = true;
     }
     if (coef_bytes > 200 * 1024) throw invalid_parameter("too many species / radial / angular functions for the power spectrum kernels");
+    const size_t pos_bytes = sizeof(double) * (((size_t)args.n_species * K + 2 * (args.lmax + 1) + 1) / 2 * 2 +
+                                               (size_t)POS_WARPS * 3 * K) +
+                             POS_TABLE_BYTES;
+    if (positions && pos_bytes > 200 * 1024)
+        throw invalid_parameter("too many radial / angular functions for the positions gradient kernel");
+
+    // side stream: values, strain, cell
+    cudaStream_t side = side_stream();
+    cudaEvent_t fork = nullptr, join = nullptr;
+    CUDA_CHECK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CUDA_CHECK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    CUDA_CHECK(cudaEventRecord(fork, stream));
+    CUDA_CHECK(cudaStreamWaitEvent(side, fork, 0));
     if (values) {
-        ps_values_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, stream>>>(args);
+        ps_values_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args);
         CUDA_CHECK(cudaGetLastError());
     }
-    if (after_values) CUDA_CHECK(cudaEventRecord(after_values, stream));
-    if (positions) {
-        const size_t pos_bytes = sizeof(double) * (((size_t)args.n_species * K + 2 * (args.lmax + 1) + 1) / 2 * 2 +
-                                                   (size_t)POS_WARPS * 3 * K) +
-                                 POS_TABLE_BYTES;
-        if (pos_bytes > 200 * 1024) throw invalid_parameter("too many radial / angular functions for the positions gradient kernel");
-        ps_positions_kernel<MAXN><<<(unsigned)args.n_centres, POS_WARPS * 32, pos_bytes, stream>>>(args);
-        CUDA_CHECK(cudaGetLastError());
-    }
-    if (after_positions) CUDA_CHECK(cudaEventRecord(after_positions, stream));
+    if (events.after_values) CUDA_CHECK(cudaEventRecord(events.after_values, side));
     if (strain) {
-        ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, stream>>>(args, 0);
+        ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args, 0);
         CUDA_CHECK(cudaGetLastError());
     }
     if (cell) {
-        ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, stream>>>(args, 1);
+        ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args, 1);
         CUDA_CHECK(cudaGetLastError());
     }
+    if (events.after_strain_cell) CUDA_CHECK(cudaEventRecord(events.after_strain_cell, side));
+    CUDA_CHECK(cudaEventRecord(join, side));
+
+    // caller's stream: positions
+    if (events.before_positions) CUDA_CHECK(cudaEventRecord(events.before_positions, stream));
+    if (positions) {
+        ps_positions_kernel<MAXN><<<(unsigned)args.n_centres, POS_WARPS * 32, pos_bytes, stream>>>(args);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    if (events.after_positions) CUDA_CHECK(cudaEventRecord(events.after_positions, stream));
+    CUDA_CHECK(cudaStreamWaitEvent(stream, join, 0));
+    // released once the recorded work has completed
+    CUDA_CHECK(cudaEventDestroy(fork));
+    CUDA_CHECK(cudaEventDestroy(join));
 }
 
 }  // namespace
 
 void launch_power_spectrum(const PsArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream,
-                           cudaEvent_t after_values, cudaEvent_t after_positions) {
+                           const PsEvents& events) {
     if (args.n_centres == 0) return;
-    launch_all<0>(args, true, positions, strain, cell, stream, after_values, after_positions);
+    launch_all<0>(args, true, positions, strain, cell, stream, events);
 }
 
 }  // namespace fb200
