@@ -653,7 +653,9 @@ def main():
             "traffic": profile_traffic("ps_positions_random_box_1000"),
         },
         "clocks": clocks,
-        "gpu_launches": 11 * args.steps,
+        # per step: neighbour list 4 + its 4 CUB scan kernels, pair features,
+        # spherical expansion, power spectrum values / positions / strain
+        "gpu_launches": 13 * args.steps,
     }
     if not args.no_chosen_forms:
         line["adjoint_form"] = adjoint_form(args.steps, args.warmup)

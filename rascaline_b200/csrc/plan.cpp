@@ -62,7 +62,15 @@ Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_
         dir[fill[(size_t)first[p] * S + sp[second[p]]]++] = (int32_t)(p << 1);
         dir[fill[(size_t)second[p] * S + sp[first[p]]]++] = (int32_t)((p << 1) | 1);
     }
-    auto other_of = [&](int32_t code) { return (code & 1) ? first[code >> 1] : second[code >> 1]; };
+    // the other atom of every direction, in segment order: the merges below
+    // then read one contiguous array per segment
+    std::vector<int32_t> other_atom(2 * (size_t)n_pairs);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < 2 * n_pairs; k++) {
+        const int32_t code = dir[k];
+        other_atom[k] = (code & 1) ? first[code >> 1] : second[code >> 1];
+    }
+    const int32_t* other = other_atom.data();
 
     // unique neighbours.  Inside a segment the other atoms are sorted (pairs
     // with the centre second come first, ordered by first; then the centre's
@@ -95,7 +103,7 @@ Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_
             int32_t best_atom = 0;
             for (int t = 0; t < S; t++) {
                 if (pos[t] < end[t]) {
-                    int32_t o = other_of(dir[pos[t]]);
+                    int32_t o = other[pos[t]];
                     if (best < 0 || o < best_atom) {
                         best = t;
                         best_atom = o;
@@ -109,7 +117,7 @@ Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_
             }
             if (best < 0) break;
             int64_t d0 = pos[best], d = d0 + 1;
-            while (d < end[best] && other_of(dir[d]) == best_atom) d++;
+            while (d < end[best] && other[d] == best_atom) d++;
             pos[best] = d;
             if (best_atom == (int32_t)c) continue;  // periodic images of the centre itself
             emit(PsEntry{best_atom, best, (int32_t)d0, (int32_t)d});
