@@ -428,6 +428,8 @@ featomic_status_t featomic_b200_power_spectrum_dense(featomic_calculator_t* calc
         *state = nullptr;
         if (!calculator->impl->power_spectrum)
             throw invalid_parameter("featomic_b200_power_spectrum_dense needs a soap_power_spectrum calculator");
+        if (calculator->impl->hypers.explicit_basis())
+            throw invalid_parameter("the dense power spectrum does not support the Explicit basis");
         std::vector<HostSystem> host = device_systems(systems);
         std::vector<int32_t> sp;
         if (n_species > 0) {
@@ -499,6 +501,8 @@ featomic_status_t featomic_b200_batch_create(featomic_calculator_t* calculator, 
         *batch = nullptr;
         if (!calculator->impl->power_spectrum)
             throw invalid_parameter("featomic_b200_batch_create needs a soap_power_spectrum calculator");
+        if (calculator->impl->hypers.explicit_basis())
+            throw invalid_parameter("the batched form does not support the Explicit basis");
         if (n_systems > 0) CHECK_POINTER(system_sizes);
         std::vector<int64_t> sizes(n_systems);
         int64_t total = 0;
@@ -598,6 +602,8 @@ featomic_status_t featomic_b200_surrogate_create(featomic_calculator_t* calculat
         CHECK_POINTER(surrogate);
         *surrogate = nullptr;
         auto result = std::make_unique<featomic_b200_surrogate_t>();
+        if (calculator->impl->hypers.explicit_basis())
+            throw invalid_parameter("the learned radial surrogate does not support the Explicit basis");
         result->impl = std::make_shared<RadialSurrogate>(*calculator->impl->engine, hidden, seed);
         *surrogate = result.release();
     });

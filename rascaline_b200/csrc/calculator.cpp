@@ -73,15 +73,62 @@ void to_radial_spectrum(TensorMap& tm) {
     }
 }
 
+// Explicit basis (basis/mod.rs:95-116): the engine runs every channel with
+// max_radial + 1 functions, the channels with fewer padded with zero
+// functions; the output keeps the angular channels of the basis (keys with
+// their o3_lambda) and, per channel, its own radial functions (properties n,
+// or (l, n_1, n_2) of the power spectrum, power_spectrum.rs:512-523).
+std::unique_ptr<TensorMap> explicit_basis_output(std::unique_ptr<TensorMap> tm, const Hypers& h) {
+    if (!tm || tm->blocks.empty()) return tm;
+    const auto& size = h.radial_sizes;
+    size_t lc = 0;
+    while (lc < tm->keys.names.size() && tm->keys.names[lc] != "o3_lambda") lc++;
+    const bool has_lambda = lc < tm->keys.names.size();
+    const size_t kw = tm->keys.names.size();
+    Labels keys;
+    keys.names = tm->keys.names;
+    TensorMap props;
+    for (size_t k = 0; k < tm->keys.count(); k++) {
+        const Block& src = *tm->blocks[k];
+        auto blk = std::make_unique<Block>();
+        blk->properties.names = src.properties.names;
+        const size_t pw = src.properties.names.size();
+        if (has_lambda) {
+            const int l = tm->keys.values[k * kw + lc];
+            if (size[l] == 0) continue;  // channel absent from the basis
+            for (int n = 0; n < size[l]; n++) blk->properties.values.push_back(n);
+        } else if (pw == 3) {
+            for (size_t r = 0; r < src.properties.count(); r++) {
+                const int32_t* p = &src.properties.values[3 * r];
+                if (p[1] < size[p[0]] && p[2] < size[p[0]]) blk->properties.values.insert(blk->properties.values.end(), p, p + 3);
+            }
+        } else {
+            // l = 0 only (radial spectrum)
+            for (int n = 0; n < size[0]; n++) blk->properties.values.push_back(n);
+        }
+        keys.values.insert(keys.values.end(), tm->keys.values.begin() + k * kw, tm->keys.values.begin() + (k + 1) * kw);
+        props.blocks.push_back(std::move(blk));
+    }
+    props.keys = keys;
+    Selection sel;
+    sel.keys = &keys;
+    sel.properties_predefined = &props;
+    sel.max_angular = h.max_angular;
+    return apply_selection(std::move(tm), sel);
+}
+
 }  // namespace
 
 std::unique_ptr<TensorMap> compute(CalculatorImpl& calc, std::vector<HostSystem>& systems, const GradientOptions& grads,
                                    bool device_output, const double* positions_device, void* stream) {
+    if (calc.hypers.explicit_basis() && device_output)
+        throw invalid_parameter("the Explicit basis is supported with host output (featomic_calculator_compute) only");
     const int kind = calc.power_spectrum ? Engine::OUTPUT_POWER_SPECTRUM
                      : calc.by_pair      ? Engine::OUTPUT_BY_PAIR
                                          : Engine::OUTPUT_EXPANSION;
     auto tm = calc.engine->compute(kind, systems, grads, device_output, positions_device, (cudaStream_t)stream);
     if (calc.radial_spectrum && tm) to_radial_spectrum(*tm);
+    if (calc.hypers.explicit_basis()) tm = explicit_basis_output(std::move(tm), calc.hypers);
     return tm;
 }
 

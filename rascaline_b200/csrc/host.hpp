@@ -49,6 +49,11 @@ struct Hypers {
     int max_radial = 0;
     bool splined = true;
     double spline_accuracy = 1e-8;
+    // Explicit basis (basis/mod.rs:95-116): number of radial functions of each
+    // angular channel l = 0..max_angular, 0 for a channel absent from the
+    // basis; max_radial + 1 is the largest.  Empty for TensorProduct.
+    std::vector<int> radial_sizes;
+    bool explicit_basis() const { return !radial_sizes.empty(); }
 
     int nmax() const { return max_radial + 1; }
     int lm_count() const { return (max_angular + 1) * (max_angular + 1); }

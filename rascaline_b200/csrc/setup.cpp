@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <sstream>
 
 #include "host.hpp"
@@ -139,13 +140,51 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_
         basis_ptr = &object(field(root, "basis", "parameters"), "internally tagged enum SphericalExpansionBasis");
         std::string bt = tag(*basis_ptr, "SphericalExpansionBasis");
         if (bt == "Explicit") {
-            throw invalid_parameter("the 'Explicit' spherical expansion basis is not supported by featomic-b200 yet");
+            // one radial basis per angular channel (basis/mod.rs:60-116)
+            deny_unknown(*basis_ptr, {"type", "by_angular", "spline_accuracy"}, "ExplicitBasis");
+            const Value& by = object(field(*basis_ptr, "by_angular", "ExplicitBasis"), "a map");
+            if (by.object.empty()) throw invalid_parameter("the Explicit basis needs at least one angular channel");
+            std::map<int, int> sizes;
+            for (auto& kv : by.object) {
+                char* end = nullptr;
+                const long l = std::strtol(kv.first.c_str(), &end, 10);
+                if (kv.first.empty() || *end != '\0' || l < 0 || kv.first[0] == '-' || kv.first[0] == '+')
+                    throw json_error("invalid digit found in string `" + kv.first + "` for the by_angular keys");
+                const Value& radial = object(kv.second, "internally tagged enum SoapRadialBasis");
+                const std::string rt = tag(radial, "SoapRadialBasis");
+                if (rt == "Tabulated")
+                    throw invalid_parameter("the 'Tabulated' radial basis is not supported by featomic-b200 yet");
+                if (rt != "Gto") throw json_error("unknown variant `" + rt + "`, expected `Gto` or `Tabulated`");
+                deny_unknown(radial, {"type", "max_radial", "radius"}, "Gto");
+                if (const Value* rr = radial.get("radius"))
+                    if (rr->kind != Value::Null && as_f64(*rr, "radius") != h.cutoff)
+                        throw internal_error("GTO radius must be the same as the cutoff radius in SOAP, or should not provided");
+                sizes[(int)l] = (int)as_usize(field(radial, "max_radial", "Gto"), "max_radial") + 1;
+            }
+            h.max_angular = sizes.rbegin()->first;
+            if (h.max_angular > 24) throw invalid_parameter("max_angular larger than 24 is not supported by featomic-b200");
+            h.radial_sizes.assign(h.max_angular + 1, 0);
+            int largest = 0;
+            for (auto& kv : sizes) {
+                h.radial_sizes[kv.first] = kv.second;
+                largest = std::max(largest, kv.second);
+            }
+            h.max_radial = largest - 1;
+            if (const Value* sa = basis_ptr->get("spline_accuracy")) {
+                if (sa->kind == Value::Null) {
+                    throw invalid_parameter("the Explicit basis needs a splined radial integral in featomic-b200 "
+                                            "(spline_accuracy can not be null)");
+                }
+                h.spline_accuracy = as_f64(*sa, "spline_accuracy");
+            }
+            goto validate;
         } else if (bt != "TensorProduct") {
             throw json_error("unknown variant `" + bt + "`, expected `TensorProduct` or `Explicit`");
         }
         deny_unknown(*basis_ptr, {"type", "max_angular", "radial", "spline_accuracy"}, "TensorProduct");
         h.max_angular = (int)as_usize(field(*basis_ptr, "max_angular", "TensorProduct"), "max_angular");
     }
+    {
     const Value& basis = *basis_ptr;
     const Value& radial = object(field(basis, "radial", basis_name), "internally tagged enum SoapRadialBasis");
     std::string rt = tag(radial, "SoapRadialBasis");
@@ -171,6 +210,8 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_
         }
     }
 
+    }
+validate:
     // validation: cutoff.rs:32-45, density.rs:79-105, radial_integral/mod.rs:78-123
     if (h.smoothing == 0 && (h.smoothing_width <= 0.0 || !std::isfinite(h.smoothing_width))) {
         std::ostringstream m;
@@ -456,10 +497,27 @@ RadialTables build_radial_tables(const Hypers& h) {
     if (h.splined) {
         for (int l = 0; l <= h.max_angular; l++) {
             std::vector<double> pos, val, der;
+            // Explicit basis: channel l has its own GTO basis of radial_sizes[l]
+            // functions (its own widths and orthonormalisation), evaluated and
+            // splined with those functions only, then padded with zeros to N
+            RadialTables tl;
+            int NL = N;
+            if (h.explicit_basis()) {
+                NL = h.radial_sizes[l];
+                tl = t;
+                tl.nmax = NL;
+                tl.bn.clear();
+                for (double sw : gto_widths(std::max(NL, 1), h.cutoff)) tl.bn.push_back(1.0 / (2.0 * sw * sw));
+                tl.ortho = gto_orthonormalization(std::max(NL, 1), h.cutoff);
+            }
             auto eval = [&](double x, std::vector<double>& v, std::vector<double>& d) {
                 v.assign(N, 0.0);
                 d.assign(N, 0.0);
-                radial_integral_host(t, l, x, v.data(), d.data());
+                if (!h.explicit_basis()) {
+                    radial_integral_host(t, l, x, v.data(), d.data());
+                } else if (NL > 0) {
+                    radial_integral_host(tl, l, x, v.data(), d.data());
+                }
             };
             const int initial = 11;
             double step = (h.cutoff - 0.0) / (double)(initial - 1);
@@ -485,7 +543,7 @@ RadialTables build_radial_tables(const Hypers& h) {
                     double x = (pos[k] + pos[k + 1]) / 2.0;
                     eval(x, v, d);
                     auto w = soap::hermite_weights(pos[k], pos[k + 1], x);
-                    for (int n = 0; n < N; n++) {
+                    for (int n = 0; n < NL; n++) {
                         double s = soap::hermite_value(w, val[k * N + n], der[k * N + n], val[(k + 1) * N + n], der[(k + 1) * N + n]);
                         mean_abs += std::fabs(s - v[n]);
                         mean_rel += std::fabs((s - v[n]) / v[n]);
@@ -495,6 +553,7 @@ RadialTables build_radial_tables(const Hypers& h) {
                     mid_val.insert(mid_val.end(), v.begin(), v.end());
                     mid_der.insert(mid_der.end(), d.begin(), d.end());
                 }
+                if (count == 0) break;  // an angular channel absent from an Explicit basis
                 mean_abs /= (double)count;
                 mean_rel /= (double)count;
                 if (mean_abs < h.spline_accuracy || mean_rel < h.spline_accuracy) break;

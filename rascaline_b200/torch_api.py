@@ -96,6 +96,8 @@ def dense_power_spectrum(calculator, positions, types, cells, sizes, precision=6
         sp = np.unique(np.asarray(species, dtype=np.int32)).astype(np.int32)
     S = len(sp)
     params = json.loads(calculator._parameters)
+    if params["basis"].get("type") == "Explicit":
+        raise C.FeatomicError("the dense power spectrum does not support the Explicit basis", 1)
     L = params["basis"]["max_angular"]
     N = params["basis"]["radial"]["max_radial"] + 1
     n_keys, n_props = S * (S + 1) // 2, (L + 1) * N * N
