@@ -12,8 +12,9 @@
  *
  * Supported calculators: "spherical_expansion", "spherical_expansion_by_pair",
  * "soap_power_spectrum"
- * (Gaussian density, GTO radial basis, TensorProduct or Explicit basis,
- * ShiftedCosine or Step smoothing, optional Willatt2018 radial scaling) and
+ * (Gaussian density with GTO or Dirac density with Tabulated radial bases,
+ * TensorProduct or Explicit basis, ShiftedCosine or Step smoothing, optional
+ * Willatt2018 radial scaling) and
  * "soap_radial_spectrum" (featomic/src/calculators/soap/radial_spectrum.rs:
  * the same density and GTO radial basis, l = 0 only, keys
  * (center_type, neighbor_type), no components).

@@ -85,9 +85,18 @@ def _compile(src, verbose, force=True):
 
 
 def build(force=False, verbose=False, jobs=None):
+    os.makedirs(BUILD, exist_ok=True)
+    # one build at a time: a concurrent build could leave objects compiled
+    # against older headers that look up to date
+    import fcntl
+    with open(os.path.join(BUILD, ".lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        return _build_locked(force, verbose, jobs)
+
+
+def _build_locked(force, verbose, jobs):
     if not force and up_to_date():
         return LIBRARY
-    os.makedirs(BUILD, exist_ok=True)
     jobs = jobs or min(8, os.cpu_count() or 1)
     with concurrent.futures.ThreadPoolExecutor(jobs) as pool:
         results = list(pool.map(lambda s: _compile(s, verbose, force), sources()))

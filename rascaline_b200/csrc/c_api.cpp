@@ -602,8 +602,8 @@ featomic_status_t featomic_b200_surrogate_create(featomic_calculator_t* calculat
         CHECK_POINTER(surrogate);
         *surrogate = nullptr;
         auto result = std::make_unique<featomic_b200_surrogate_t>();
-        if (calculator->impl->hypers.explicit_basis())
-            throw invalid_parameter("the learned radial surrogate does not support the Explicit basis");
+        if (calculator->impl->hypers.explicit_basis() || calculator->impl->hypers.tabulated_basis())
+            throw invalid_parameter("the learned radial surrogate needs a GTO TensorProduct basis");
         result->impl = std::make_shared<RadialSurrogate>(*calculator->impl->engine, hidden, seed);
         *surrogate = result.release();
     });

@@ -37,6 +37,16 @@ inline Error internal_error(const std::string& m) { return Error(STATUS_INTERNAL
 // PowerSpectrumParameters, spherical_expansion_pair.rs:37-45,
 // power_spectrum.rs:35-43)
 // ---------------------------------------------------------------------------
+// A user-given spline of the radial integral (featomic's `Tabulated` radial
+// basis, basis/radial/tabulated.rs): control points sorted by position, each
+// with `size` values and derivatives
+struct TabulatedSpline {
+    int size = 0;
+    std::vector<double> positions;  // [points]
+    std::vector<double> values;     // [points][size]
+    std::vector<double> derivs;     // [points][size]
+};
+
 struct Hypers {
     double cutoff = 0.0;
     int smoothing = 0;  // 0 ShiftedCosine, 1 Step
@@ -54,6 +64,10 @@ struct Hypers {
     // basis; max_radial + 1 is the largest.  Empty for TensorProduct.
     std::vector<int> radial_sizes;
     bool explicit_basis() const { return !radial_sizes.empty(); }
+    // Tabulated radial basis: the spline of each angular channel (empty for
+    // GTO; an absent Explicit channel has size 0)
+    std::vector<TabulatedSpline> tabulated;
+    bool tabulated_basis() const { return !tabulated.empty(); }
 
     int nmax() const { return max_radial + 1; }
     int lm_count() const { return (max_angular + 1) * (max_angular + 1); }

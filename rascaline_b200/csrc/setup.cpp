@@ -70,6 +70,58 @@ std::string tag(const Value& v, const char* context) {
     return t->string;
 }
 
+// Tabulated radial basis: {"type": "Tabulated", "points": [{"position",
+// "values", "derivatives"}, ...]} with the checks of
+// basis/radial/tabulated.rs:174-210, points sorted by position
+TabulatedSpline parse_tabulated(const Value& radial) {
+    deny_unknown(radial, {"type", "points"}, "Tabulated");
+    const Value& points = field(radial, "points", "Tabulated");
+    if (points.kind != Value::Array) throw json_error(std::string("invalid type: ") + points.kind_name() + ", expected a sequence");
+    if (points.array.size() < 2)
+        throw invalid_parameter("we need at least two points to define a 'Tabulated' radial basis");
+    struct Point {
+        double position;
+        std::vector<double> values, derivs;
+    };
+    std::vector<Point> list;
+    size_t size = 0;
+    for (size_t k = 0; k < points.array.size(); k++) {
+        const Value& p = object(points.array[k], "struct SplinePoint");
+        deny_unknown(p, {"position", "values", "derivatives"}, "SplinePoint");
+        Point q;
+        q.position = as_f64(field(p, "position", "SplinePoint"), "position");
+        for (const char* name : {"values", "derivatives"}) {
+            const Value& arr = field(p, name, "SplinePoint");
+            if (arr.kind != Value::Array) throw json_error(std::string("invalid type: ") + arr.kind_name() + ", expected a sequence");
+            auto& dst = std::string(name) == "values" ? q.values : q.derivs;
+            for (auto& x : arr.array) dst.push_back(as_f64(x, name));
+        }
+        if (k == 0) size = q.values.size();
+        if (!std::isfinite(q.position)) {
+            std::ostringstream m;
+            m << "expected all points 'position' in 'Tabulated' radial basis to be finite numbers, got " << q.position;
+            throw invalid_parameter(m.str());
+        }
+        if (q.values.size() != size)
+            throw invalid_parameter("expected all points 'values' in 'Tabulated' radial basis to have the same size, got " +
+                                    std::to_string(q.values.size()) + " and " + std::to_string(size));
+        if (q.derivs.size() != size)
+            throw invalid_parameter("expected all points 'derivatives' in 'Tabulated' radial basis to have the same size, got " +
+                                    std::to_string(q.derivs.size()) + " and " + std::to_string(size));
+        list.push_back(std::move(q));
+    }
+    if (size == 0) throw invalid_parameter("a 'Tabulated' radial basis needs at least one function");
+    std::stable_sort(list.begin(), list.end(), [](const Point& a, const Point& b) { return a.position < b.position; });
+    TabulatedSpline t;
+    t.size = (int)size;
+    for (auto& q : list) {
+        t.positions.push_back(q.position);
+        t.values.insert(t.values.end(), q.values.begin(), q.values.end());
+        t.derivs.insert(t.derivs.end(), q.derivs.begin(), q.derivs.end());
+    }
+    return t;
+}
+
 }  // namespace
 
 Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_spectrum_basis) {
@@ -145,6 +197,7 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_
             const Value& by = object(field(*basis_ptr, "by_angular", "ExplicitBasis"), "a map");
             if (by.object.empty()) throw invalid_parameter("the Explicit basis needs at least one angular channel");
             std::map<int, int> sizes;
+            std::map<int, TabulatedSpline> tabulated;
             for (auto& kv : by.object) {
                 char* end = nullptr;
                 const long l = std::strtol(kv.first.c_str(), &end, 10);
@@ -152,8 +205,11 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_
                     throw json_error("invalid digit found in string `" + kv.first + "` for the by_angular keys");
                 const Value& radial = object(kv.second, "internally tagged enum SoapRadialBasis");
                 const std::string rt = tag(radial, "SoapRadialBasis");
-                if (rt == "Tabulated")
-                    throw invalid_parameter("the 'Tabulated' radial basis is not supported by featomic-b200 yet");
+                if (rt == "Tabulated") {
+                    tabulated[(int)l] = parse_tabulated(radial);
+                    sizes[(int)l] = tabulated[(int)l].size;
+                    continue;
+                }
                 if (rt != "Gto") throw json_error("unknown variant `" + rt + "`, expected `Gto` or `Tabulated`");
                 deny_unknown(radial, {"type", "max_radial", "radius"}, "Gto");
                 if (const Value* rr = radial.get("radius"))
@@ -170,11 +226,20 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_
                 largest = std::max(largest, kv.second);
             }
             h.max_radial = largest - 1;
+            if (!tabulated.empty()) {
+                // one kind of radial basis for every channel: Gto needs a
+                // Gaussian density, Tabulated a Dirac one
+                if (tabulated.size() != sizes.size())
+                    throw invalid_parameter("this combination of basis and density is not supported in SOAP");
+                h.tabulated.assign(h.max_angular + 1, TabulatedSpline());
+                for (auto& kv : tabulated) h.tabulated[kv.first] = kv.second;
+            }
             if (const Value* sa = basis_ptr->get("spline_accuracy")) {
-                if (sa->kind == Value::Null) {
+                if (sa->kind == Value::Null && tabulated.empty()) {
                     throw invalid_parameter("the Explicit basis needs a splined radial integral in featomic-b200 "
                                             "(spline_accuracy can not be null)");
                 }
+                if (sa->kind == Value::Null) goto validate;
                 h.spline_accuracy = as_f64(*sa, "spline_accuracy");
             }
             goto validate;
@@ -189,7 +254,11 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_
     const Value& radial = object(field(basis, "radial", basis_name), "internally tagged enum SoapRadialBasis");
     std::string rt = tag(radial, "SoapRadialBasis");
     if (rt == "Tabulated") {
-        throw invalid_parameter("the 'Tabulated' radial basis is not supported by featomic-b200 yet");
+        // the same user spline for every angular channel
+        const TabulatedSpline t = parse_tabulated(radial);
+        h.max_radial = t.size - 1;
+        h.tabulated.assign(h.max_angular + 1, t);
+        goto accuracy;
     } else if (rt != "Gto") {
         throw json_error("unknown variant `" + rt + "`, expected `Gto` or `Tabulated`");
     }
@@ -202,6 +271,7 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_
                 throw internal_error("GTO radius must be the same as the cutoff radius in SOAP, or should not provided");
         }
     }
+accuracy:
     if (const Value* sa = basis.get("spline_accuracy")) {
         if (sa->kind == Value::Null) {
             h.splined = false;
@@ -212,6 +282,8 @@ Hypers parse_hypers(const std::string& text, bool deny_unknown_top, bool radial_
 
     }
 validate:
+    // a Tabulated basis is its own spline
+    if (h.tabulated_basis()) h.splined = true;
     // validation: cutoff.rs:32-45, density.rs:79-105, radial_integral/mod.rs:78-123
     if (h.smoothing == 0 && (h.smoothing_width <= 0.0 || !std::isfinite(h.smoothing_width))) {
         std::ostringstream m;
@@ -223,8 +295,11 @@ validate:
         if (h.scaling_rate <= 0.0) throw invalid_parameter("expected positive rate for Willatt2018 radial scaling function");
         if (h.scaling_exponent <= 0.0) throw invalid_parameter("expected positive exponent for Willatt2018 radial scaling function");
     }
-    if (!gaussian) throw invalid_parameter("this combination of basis and density is not supported in SOAP");
-    if (!(h.density_width > 1e-16 && std::isfinite(h.density_width)))
+    // radial_integral/mod.rs:86-113: Gaussian density with GTO, Dirac density
+    // with Tabulated
+    if (h.tabulated_basis() ? dt != "DiracDelta" : !gaussian)
+        throw invalid_parameter("this combination of basis and density is not supported in SOAP");
+    if (gaussian && !(h.density_width > 1e-16 && std::isfinite(h.density_width)))
         throw invalid_parameter("expected positive and finite Gaussian width");
     if (!(h.cutoff > 0.0 && std::isfinite(h.cutoff))) throw invalid_parameter("cutoff must be positive and finite");
     if (h.splined && h.spline_accuracy < 0.0) {
@@ -486,7 +561,8 @@ RadialTables build_radial_tables(const Hypers& h) {
     t.lmax = h.max_angular;
     t.nmax = h.nmax();
     t.splined = false;  // evaluate analytically while building the knots
-    t.c = 1.0 / (2.0 * h.density_width * h.density_width);
+    // (the analytic GTO parameters are not used with a Tabulated basis)
+    t.c = h.tabulated_basis() ? 0.0 : 1.0 / (2.0 * h.density_width * h.density_width);
     t.width2 = h.density_width * h.density_width;
     for (double s : gto_widths(t.nmax, h.cutoff)) t.bn.push_back(1.0 / (2.0 * s * s));
     t.ortho = gto_orthonormalization(t.nmax, h.cutoff);
@@ -494,7 +570,35 @@ RadialTables build_radial_tables(const Hypers& h) {
 
     std::vector<double> all_pos, all_val, all_der;
     std::vector<int32_t> offsets, counts;
-    if (h.splined) {
+    if (h.tabulated_basis()) {
+        // the user's control points, each channel padded with zero functions
+        // to N (radial_integral/spline.rs from_tabulated)
+        for (int l = 0; l <= h.max_angular; l++) {
+            const TabulatedSpline& ts = h.tabulated[l];
+            offsets.push_back((int32_t)all_pos.size());
+            if (ts.size == 0) {
+                all_pos.insert(all_pos.end(), {0.0, h.cutoff});
+                all_val.insert(all_val.end(), 2 * (size_t)N, 0.0);
+                all_der.insert(all_der.end(), 2 * (size_t)N, 0.0);
+                counts.push_back(2);
+                continue;
+            }
+            counts.push_back((int32_t)ts.positions.size());
+            for (size_t k = 0; k < ts.positions.size(); k++) {
+                all_pos.push_back(ts.positions[k]);
+                for (int n = 0; n < N; n++) {
+                    all_val.push_back(n < ts.size ? ts.values[k * ts.size + n] : 0.0);
+                    all_der.push_back(n < ts.size ? ts.derivs[k * ts.size + n] : 0.0);
+                }
+            }
+        }
+        t.knot_offset = offsets;
+        t.knot_count = counts;
+        t.positions = all_pos;
+        t.values = all_val;
+        t.derivs = all_der;
+        t.splined = true;
+    } else if (h.splined) {
         for (int l = 0; l <= h.max_angular; l++) {
             std::vector<double> pos, val, der;
             // Explicit basis: channel l has its own GTO basis of radial_sizes[l]
