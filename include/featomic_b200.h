@@ -325,7 +325,9 @@ featomic_status_t featomic_b200_batch_tune(featomic_b200_batch_t* batch, const d
 
 /* The launch configuration: [warps per CTA, directions staged per warp,
  * coefficient layout (0: lane per (l, m, n), 1: lane per (l, m)), CTAs per
- * SM]. */
+ * SM, pipeline (0: the persistent kernel replayed from a CUDA graph; 1: the
+ * dense pipeline of featomic_b200_power_spectrum_dense and its backward,
+ * several launches with host synchronisation)].  The tuner times both. */
 featomic_status_t featomic_b200_batch_config(const featomic_b200_batch_t* batch, int32_t* config);
 featomic_status_t featomic_b200_batch_set_config(featomic_b200_batch_t* batch, const int32_t* config);
 

@@ -47,6 +47,10 @@ struct BatchConfig {
     int chunk = 32;       // neighbour directions staged per warp in the forward pass
     int layout = 1;       // 0: lane per (l, m, n) coefficient; 1: lane per (l, m), n in registers
     int ctas_per_sm = 1;  // resident CTAs per SM of the persistent grid
+    // 0: the persistent kernel above; 1: the dense pipeline of the adjoint
+    // form (several launches with host synchronisation, no graph), faster on
+    // large batches
+    int pipeline = 0;
 };
 
 class BatchPlan {
@@ -86,6 +90,11 @@ class BatchPlan {
     };
     BatchArgs args(const double* positions, const float* weights, const float* grad_values, float* values,
                    float* grad_positions, float* energies, float* grad_strain) const;
+    void run_dense(const double* positions, const float* weights, const float* grad_values, float* values,
+                   float* grad_positions, float* energies, float* grad_strain, cudaStream_t stream);
+    std::vector<HostSystem> systems_;   // types and zero cells, for the dense pipeline
+    float* d_values_scratch_ = nullptr;  // dense pipeline without a values output
+    float* d_grad_scratch_ = nullptr;    // dense pipeline without a positions output
     Shape shape(const BatchArgs& a, const BatchConfig& c) const;
     void enqueue(const BatchArgs& a, const Shape& sh, bool cooperative, cudaStream_t stream);
     Graph& graph_for(const Key& key, const BatchArgs& a, const BatchConfig& c);

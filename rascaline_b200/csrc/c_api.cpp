@@ -565,6 +565,7 @@ featomic_status_t featomic_b200_batch_config(const featomic_b200_batch_t* batch,
         config[1] = c.chunk;
         config[2] = c.layout;
         config[3] = c.ctas_per_sm;
+        config[4] = c.pipeline;
     });
 }
 
@@ -573,9 +574,9 @@ featomic_status_t featomic_b200_batch_set_config(featomic_b200_batch_t* batch, c
         CHECK_POINTER(batch);
         CHECK_POINTER(config);
         if ((config[0] != 4 && config[0] != 8) || (config[1] != 16 && config[1] != 32) ||
-            (config[2] != 0 && config[2] != 1) || config[3] < 1 || config[3] > 8)
+            (config[2] != 0 && config[2] != 1) || config[3] < 1 || config[3] > 8 || (config[4] != 0 && config[4] != 1))
             throw invalid_parameter("invalid batch configuration");
-        batch->plan->config = BatchConfig{config[0], config[1], config[2], config[3]};
+        batch->plan->config = BatchConfig{config[0], config[1], config[2], config[3], config[4]};
     });
 }
 

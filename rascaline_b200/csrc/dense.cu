@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256) dense_grad_coef(DenseArgs<T> a) {
     const int S = a.n_species, K = a.K, N = a.nmax, NN = N * N;
     for (int i = threadIdx.x; i < S * K; i += blockDim.x) cs[i] = a.coef[c * S * K + i];
     __syncthreads();
-    const T* G = a.grad_values + c * a.n_keys * a.n_props;
+    const T* G = a.grad_values + (a.grad_species ? (int64_t)a.grad_species[c] : c) * a.n_keys * a.n_props;
     for (int o = threadIdx.x; o < S * K; o += blockDim.x) {
         const int sa = o / K;
         const int k = o - sa * K;
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(128) dense_grad_coef_tiled(DenseArgs<T> a) {
     const int64_t KP = (int64_t)a.n_keys * a.n_props;
     T* gs = cs + S * K;
     stage_copy(cs, a.coef + c * S * K, (int64_t)S * K);
-    stage_copy(gs, a.grad_values + c * KP, KP);
+    stage_copy(gs, a.grad_values + (a.grad_species ? (int64_t)a.grad_species[c] : c) * KP, KP);
     __syncthreads();
     for (int it = threadIdx.x; it < S * LN; it += blockDim.x) {
         const int sa = it / LN;

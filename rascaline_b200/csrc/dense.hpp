@@ -36,6 +36,9 @@ struct DenseArgs {
     T* coef;              // [n_atoms][S][K]
     T* values;            // [n_atoms][n_keys][n_props]
     const T* grad_values; // same layout
+    // when set, the dL/dP row of centre c is grad_values[grad_species[c]]:
+    // one row per species (the weights of a linear model)
+    const int32_t* grad_species = nullptr;
     T* grad_coef;         // [n_atoms][S][K]
     T* pair_grad;         // [n_pairs][3] dL/dr_ij
     T* grad_positions;    // [n_atoms][3]

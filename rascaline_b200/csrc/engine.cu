@@ -861,7 +861,7 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
 }
 
 void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_positions, void* grad_strain,
-                            void* grad_cell, cudaStream_t stream) {
+                            void* grad_cell, cudaStream_t stream, bool by_species) {
     int dev = -1;
     CUDA_CHECK(cudaGetDevice(&dev));
     if (dev != st.device) throw invalid_parameter("the backward pass must run on the device of the forward pass");
@@ -886,6 +886,7 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
         dense_args(st, true, a);
         a.features = (double*)features;
         a.grad_values = (const double*)grad_values;
+        a.grad_species = by_species ? st.atom_species : nullptr;
         a.grad_coef = (double*)grad_coef;
         a.pair_grad = (double*)pair_grad;
         a.atom_partial = (double*)partial;
@@ -899,6 +900,7 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
         dense_args(st, true, a);
         a.features = (float*)features;
         a.grad_values = (const float*)grad_values;
+        a.grad_species = by_species ? st.atom_species : nullptr;
         a.grad_coef = (float*)grad_coef;
         a.pair_grad = (float*)pair_grad;
         a.atom_partial = (float*)partial;

@@ -323,8 +323,10 @@ class Engine {
                                               void* values, int64_t values_count, cudaStream_t stream);
     // dL/dpositions [n_atoms][3], and when not null dL/dstrain and dL/dcell
     // [n_systems][3][3], all device buffers of the forward precision
+    // `by_species`: grad_values holds one dL/dP row per species (the weights
+    // of a linear model) instead of one per atom
     void backward_dense(DenseState& state, const void* grad_values, void* grad_positions, void* grad_strain,
-                        void* grad_cell, cudaStream_t stream);
+                        void* grad_cell, cudaStream_t stream, bool by_species = false);
 
     // device tables for the kernels of the batched form (uploaded on first use)
     const DenseTables<float>& dense_tables_f() {

@@ -333,13 +333,14 @@ class Batch:
 
     @property
     def config(self):
-        c = (ctypes.c_int32 * 4)()
+        c = (ctypes.c_int32 * 5)()
         C.check(C.lib().featomic_b200_batch_config(self._handle, c))
-        return {"warps": c[0], "chunk": c[1], "layout": c[2], "ctas_per_sm": c[3]}
+        return {"warps": c[0], "chunk": c[1], "layout": c[2], "ctas_per_sm": c[3], "pipeline": c[4]}
 
     @config.setter
     def config(self, value):
-        c = (ctypes.c_int32 * 4)(value["warps"], value["chunk"], value["layout"], value["ctas_per_sm"])
+        c = (ctypes.c_int32 * 5)(value["warps"], value["chunk"], value["layout"], value["ctas_per_sm"],
+                                 value.get("pipeline", 0))
         C.check(C.lib().featomic_b200_batch_set_config(self._handle, c))
 
     def status(self):

@@ -112,9 +112,11 @@ def test_replays_are_deterministic_and_modes_agree(setup):
 def test_configurations_agree_and_tuner_picks_one(setup):
     batch, pos, weights, ref, _, _ = setup
     results = []
-    for config in ({"warps": 4, "chunk": 16, "layout": 0, "ctas_per_sm": 1},
-                   {"warps": 8, "chunk": 32, "layout": 1, "ctas_per_sm": 1},
-                   {"warps": 4, "chunk": 32, "layout": 1, "ctas_per_sm": 2}):
+    for config in ({"warps": 4, "chunk": 16, "layout": 0, "ctas_per_sm": 1, "pipeline": 0},
+                   {"warps": 8, "chunk": 32, "layout": 1, "ctas_per_sm": 1, "pipeline": 0},
+                   {"warps": 4, "chunk": 32, "layout": 1, "ctas_per_sm": 2, "pipeline": 0},
+                   # the dense pipeline of the adjoint form
+                   {"warps": 8, "chunk": 32, "layout": 1, "ctas_per_sm": 1, "pipeline": 1}):
         batch.config = config
         assert batch.config == config
         results.append(host(batch.run(pos, batch.outputs(), weights=weights)))
@@ -126,6 +128,7 @@ def test_configurations_agree_and_tuner_picks_one(setup):
     assert np.isfinite(best) and best > 0
     config = batch.config
     assert config["warps"] in (4, 8) and config["chunk"] in (16, 32) and config["layout"] in (0, 1)
+    assert config["pipeline"] in (0, 1)
     got = host(batch.run(pos, batch.outputs(), weights=weights))
     assert relative(got["gradients"], ref["gradients"]) <= 1e-4
 
