@@ -423,38 +423,57 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
     launch_pair_features(pairs, d_radial_, d_ylm_, cut, layout, features, status, stream);
     CUDA_CHECK(cudaEventRecord(ev[2], stream));
 
-    CUDA_CHECK(cudaEventSynchronize(ev[6]));
+    // ---- kernel (b): spherical expansion.  It needs the directions sorted by
+    // (centre, neighbour species) in pair order, which the GPU sorts itself,
+    // so it runs right after the pair features while the host builds the
+    // neighbourhood tables and the output plan -------------------------------
+    std::vector<int32_t> species_types, atom_species_h(n_atoms);
+    {
+        for (auto& s : systems) species_types.insert(species_types.end(), s.types.begin(), s.types.end());
+        std::sort(species_types.begin(), species_types.end());
+        species_types.erase(std::unique(species_types.begin(), species_types.end()), species_types.end());
+        int64_t a = 0;
+        for (auto& s : systems)
+            for (int32_t t : s.types)
+                atom_species_h[a++] =
+                    (int32_t)(std::lower_bound(species_types.begin(), species_types.end(), t) - species_types.begin());
+    }
+    const int S = (int)species_types.size();
     auto t_meta0 = std::chrono::steady_clock::now();
-    Neighborhoods nh = build_neighborhoods(systems, pairs.count, h_first.data(), h_second.data());
-    const int S = nh.n_species;
-
-    // ---- kernel (b): spherical expansion, launched as soon as the
-    // neighbourhoods are known, so that the host builds the output labels
-    // below while the GPU accumulates ------------------------------------------
     SeArgs se{};
-    const bool run_se = !by_pair && nh.n_atoms > 0;
+    const bool run_se = !by_pair && n_atoms > 0;
     if (run_se) {
         const int K = layout.L2 * layout.nmax;
         se.layout = layout;
-        se.n_centres = nh.n_atoms;
+        se.n_centres = n_atoms;
         se.n_species = S;
-        se.centre_species = upload(arena_, "meta.atom_species", nh.atom_species, stream);
-        se.seg_offset = upload(arena_, "meta.seg_offset", nh.seg_offset, stream);
-        se.dir_code = upload(arena_, "meta.dir_code", nh.dir_code, stream);
+        int32_t* d_species = upload(arena_, "meta.atom_species", atom_species_h, stream);
+        int32_t* d_dir = arena_.alloc<int32_t>("meta.dir_code", 2 * pairs.count);
+        int64_t* d_seg = arena_.alloc<int64_t>("meta.seg_offset", n_atoms * S + 1);
+        // the same order as the host's counting sort (stable radix sort of
+        // (centre, species) keys over pair << 1 | reversed)
+        launch_dense_directions(pairs, d_species, S, n_atoms, d_dir, d_seg, arena_, stream);
+        se.centre_species = d_species;
+        se.seg_offset = d_seg;
+        se.dir_code = d_dir;
         se.features = features;
         se.self_contribution = d_self_;
         se.do_positions = g.positions;
         se.do_strain = g.strain;
         se.do_cell = g.cell;
-        se.coef = arena_.alloc<double>("se.coef", nh.n_atoms * S * K);
+        se.coef = arena_.alloc<double>("se.coef", n_atoms * S * K);
         se.pair_grad = g.positions ? arena_.alloc<double>("se.pair_grad", pairs.count * 3 * K) : nullptr;
-        se.self_grad = g.positions ? arena_.alloc<double>("se.self_grad", nh.n_atoms * S * 3 * K) : nullptr;
-        se.strain = g.strain ? arena_.alloc<double>("se.strain", nh.n_atoms * S * 9 * K) : nullptr;
-        se.cellg = g.cell ? arena_.alloc<double>("se.cell", nh.n_atoms * S * 9 * K) : nullptr;
+        se.self_grad = g.positions ? arena_.alloc<double>("se.self_grad", n_atoms * S * 3 * K) : nullptr;
+        se.strain = g.strain ? arena_.alloc<double>("se.strain", n_atoms * S * 9 * K) : nullptr;
+        se.cellg = g.cell ? arena_.alloc<double>("se.cell", n_atoms * S * 9 * K) : nullptr;
         CUDA_CHECK(cudaEventRecord(ev[7], stream));
         launch_se_accumulate(se, stream);
         CUDA_CHECK(cudaEventRecord(ev[3], stream));
     }
+
+    CUDA_CHECK(cudaEventSynchronize(ev[6]));
+    Neighborhoods nh = build_neighborhoods(systems, pairs.count, h_first.data(), h_second.data());
+    if (nh.n_species != S) throw internal_error("species tables disagree");
 
     OutputPlan plan = ps        ? plan_power_spectrum(nh, h_, g, /*with_labels=*/false)
                       : by_pair ? plan_by_pair(nh, h_, g, pairs.count, h_first.data(), h_second.data(), h_shift.data())
