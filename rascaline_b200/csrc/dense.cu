@@ -179,6 +179,10 @@ __global__ void dense_pair_features(DevicePairs pairs, DeviceRadial exact, Dense
     }
 }
 
+// Thread per (l, m) and pair of radial functions (n0 = 2j, n1 = 2j + 1): the
+// direction scalars and Y_lm are loaded once for both, which halves the loads
+// of this load-issue-bound kernel; each coefficient is still summed over the
+// directions in pair order.
 template <typename T>
 __global__ void __launch_bounds__(256) dense_expansion(DenseArgs<T> a) {
     __shared__ int64_t dir_feature[DENSE_CHUNK];
@@ -188,42 +192,48 @@ __global__ void __launch_bounds__(256) dense_expansion(DenseArgs<T> a) {
     // one CTA per (centre, neighbour species) segment
     const int S = a.n_species;
     const int64_t c = blockIdx.x / S;
-    const int t_block = (int)(blockIdx.x - c * S);
-    const int K = a.K;
+    const int t = (int)(blockIdx.x - c * S);
+    const int K = a.K, N = L.nmax, NH = (N + 1) / 2;
+    const int items = L.L2 * NH;
     const int tc = a.atom_species[c];
-    for (int k0 = 0; k0 < K; k0 += blockDim.x) {
+    const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
+    for (int k0 = 0; k0 < items; k0 += blockDim.x) {
         const int k = k0 + threadIdx.x;
-        const bool active = k < K;
-        const int lm = active ? k / L.nmax : 0;
-        const int n = active ? k - lm * L.nmax : 0;
+        const bool active = k < items;
+        const int lm = active ? k / NH : 0;
+        const int n0 = active ? 2 * (k - lm * NH) : 0;
+        const bool has1 = n0 + 1 < N;
         const int l = isqrt_lm(lm);
         const T sign_l = (l & 1) ? T(-1) : T(1);
-        const int ri = l * L.nmax + n;
-        for (int t = t_block; t == t_block; t++) {
-            const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
-            T acc = T(0);
-            for (int64_t dc = d0; dc < d1; dc += DENSE_CHUNK) {
-                const int nd = (int)min((int64_t)DENSE_CHUNK, d1 - dc);
-                __syncthreads();
-                if (threadIdx.x < nd) {
-                    const int32_t code = a.dir_code[dc + threadIdx.x];
-                    const int64_t p = code >> 1;
-                    dir_feature[threadIdx.x] = p * L.stride;
-                    dir_inv[threadIdx.x] = code & 1;
-                    dir_f[threadIdx.x] = a.features[p * L.stride];
-                }
-                __syncthreads();
-                if (!active) continue;
-                for (int q = 0; q < nd; q++) {
-                    const T* __restrict__ F = a.features + dir_feature[q];
-                    const T val = dir_f[q] * F[L.off_y + lm] * F[L.off_r + ri];
-                    acc += dir_inv[q] ? sign_l * val : val;
-                }
+        const int ri = l * N + n0;
+        T acc0 = T(0), acc1 = T(0);
+        for (int64_t dc = d0; dc < d1; dc += DENSE_CHUNK) {
+            const int nd = (int)min((int64_t)DENSE_CHUNK, d1 - dc);
+            __syncthreads();
+            if (threadIdx.x < nd) {
+                const int32_t code = a.dir_code[dc + threadIdx.x];
+                const int64_t p = code >> 1;
+                dir_feature[threadIdx.x] = p * L.stride;
+                dir_inv[threadIdx.x] = code & 1;
+                dir_f[threadIdx.x] = a.features[p * L.stride];
             }
+            __syncthreads();
             if (!active) continue;
-            const T self = (t == tc && l == 0) ? a.tab.self_contribution[n] : T(0);
-            a.coef[(c * S + t) * K + k] = self + acc;
+            for (int q = 0; q < nd; q++) {
+                const T* __restrict__ F = a.features + dir_feature[q];
+                const T fy = dir_f[q] * F[L.off_y + lm];
+                const T v0 = fy * F[L.off_r + ri];
+                const T v1 = has1 ? fy * F[L.off_r + ri + 1] : T(0);
+                const bool inv = dir_inv[q];
+                acc0 += inv ? sign_l * v0 : v0;
+                acc1 += inv ? sign_l * v1 : v1;
+            }
         }
+        if (!active) continue;
+        const bool self = t == tc && l == 0;
+        T* out = a.coef + (c * S + t) * K + lm * N + n0;
+        out[0] = (self ? a.tab.self_contribution[n0] : T(0)) + acc0;
+        if (has1) out[1] = (self ? a.tab.self_contribution[n0 + 1] : T(0)) + acc1;
     }
 }
 
@@ -703,7 +713,8 @@ template <typename T>
 void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream) {
     launch_features<T, false>(a, n_pairs, stream);
     if (a.n_atoms == 0) return;
-    dense_expansion<T><<<(unsigned)(a.n_atoms * a.n_species), coefficient_threads(a.K), 0, stream>>>(a);
+    dense_expansion<T><<<(unsigned)(a.n_atoms * a.n_species),
+                         coefficient_threads(a.layout.L2 * ((a.nmax + 1) / 2)), 0, stream>>>(a);
     CUDA_CHECK(cudaGetLastError());
     const size_t smem = sizeof(T) * (size_t)a.n_species * a.K;
     if (a.nmax <= 16 && smem <= 48 * 1024) {
