@@ -406,6 +406,42 @@ featomic_status_t featomic_b200_radial_integral(const featomic_calculator_t* cal
 featomic_status_t featomic_b200_calculator_timings(const featomic_calculator_t* calculator, double* times,
                                                    uintptr_t count);
 
+/* ---- Clebsch-Gordan tensor products -------------------------------------
+ * The numerical core of featomic's Python clebsch_gordan module
+ * (python/featomic/featomic/clebsch_gordan/_coefficients.py): real CG
+ * coefficients and the coupling of two equivariant blocks.  No counterpart in
+ * featomic's C API (featomic does these in Python / torch). */
+
+/* Real Clebsch-Gordan coefficients coupling l1 and l2 to lambda, written as a
+ * dense [2 l1 + 1][2 l2 + 1][2 lambda + 1] array (`count` must be that size);
+ * the values of _coefficients.py:_build_dense_cg_coeff_dict (:137-224).
+ * Host computation, no device needed. */
+featomic_status_t featomic_b200_cg_coefficients(int32_t l1, int32_t l2, int32_t lambda, double* coefficients,
+                                                uintptr_t count);
+
+/* One block product: output[s][mu][p * n_second + q] =
+ *   sum_{m1, m2} C[m1][m2][mu] first[s][m1][p] second[s][m2][q]
+ * (_coefficients.py:_cg_tensor_product_dense, :677-709).  All three arrays are
+ * device memory, contiguous, of the precision given to
+ * featomic_b200_cg_product. */
+typedef struct featomic_b200_cg_task_t {
+    const void* first;   /* [n_samples][2 l1 + 1][n_first] */
+    const void* second;  /* [n_samples][2 l2 + 1][n_second] */
+    void* output;        /* [n_samples][2 lambda + 1][n_first * n_second] */
+    int64_t n_samples;
+    int32_t l1;
+    int32_t l2;
+    int32_t lambda;
+    int32_t n_first;
+    int32_t n_second;
+} featomic_b200_cg_task_t;
+
+/* Run `n_tasks` block products in one launch on `stream` (NULL = the legacy
+ * default stream); precision 32 (float) or 64 (double).  Returns once the
+ * products are queued; the tasks array may be freed on return. */
+featomic_status_t featomic_b200_cg_product(const featomic_b200_cg_task_t* tasks, uintptr_t n_tasks,
+                                           int32_t precision, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,20 @@ class featomic_b200_device_systems_t(ctypes.Structure):
     ]
 
 
+class featomic_b200_cg_task_t(ctypes.Structure):
+    _fields_ = [
+        ("first", ctypes.c_void_p),
+        ("second", ctypes.c_void_p),
+        ("output", ctypes.c_void_p),
+        ("n_samples", ctypes.c_int64),
+        ("l1", ctypes.c_int32),
+        ("l2", ctypes.c_int32),
+        ("lambda_", ctypes.c_int32),
+        ("n_first", ctypes.c_int32),
+        ("n_second", ctypes.c_int32),
+    ]
+
+
 # every symbol declared in include/featomic_b200.h: name -> (restype, argtypes)
 SIGNATURES = {
     "featomic_last_error": (ctypes.c_char_p, []),
@@ -163,6 +177,10 @@ SIGNATURES = {
                                                           ctypes.c_size_t, ctypes.POINTER(ctypes.c_double),
                                                           ctypes.POINTER(ctypes.c_double),
                                                           ctypes.POINTER(ctypes.c_int32)]),
+    "featomic_b200_cg_coefficients": (featomic_status_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                          ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
+    "featomic_b200_cg_product": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
+                                                     ctypes.c_void_p]),
     "featomic_b200_calculator_timings": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                              ctypes.c_size_t]),
 }

@@ -1,0 +1,362 @@
+"""Clebsch-Gordan tensor products and the equivariant power spectrum on the GPU.
+
+Mirrors featomic's ``featomic.clebsch_gordan`` Python module
+(python/featomic/featomic/clebsch_gordan/): ``ClebschGordanProduct``
+(_cg_product.py:29-436) and ``EquivariantPowerSpectrum``
+(_equivariant_power_spectrum.py:23-365, "lambda-SOAP").  The coefficients
+come from ``featomic_b200_cg_coefficients`` and every block product runs in
+one launch of the sm_100a kernel behind ``featomic_b200_cg_product``; the
+key / sample / property bookkeeping (metatensor operations in featomic) is
+done here, on the host.  Values live in torch CUDA tensors.
+"""
+import ctypes
+import json
+
+import numpy as np
+
+from . import _c_api as C
+from .calculators import Labels
+
+
+def cg_coefficients(l1, l2, o3_lambda):
+    """Real CG coefficients [2 l1 + 1, 2 l2 + 1, 2 o3_lambda + 1]
+    (_coefficients.py:137-224)."""
+    out = np.zeros(max(1, (2 * l1 + 1) * (2 * l2 + 1) * (2 * o3_lambda + 1)))
+    C.check(C.lib().featomic_b200_cg_coefficients(l1, l2, o3_lambda,
+                                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size))
+    return out.reshape(2 * l1 + 1, 2 * l2 + 1, 2 * o3_lambda + 1)
+
+
+def cg_tensor_products(tasks, stream=None):
+    """Run ``(first, second, output, o3_lambda)`` products (contiguous CUDA
+    tensors of one dtype, shapes [s, 2 l1 + 1, p], [s, 2 l2 + 1, q],
+    [s, 2 o3_lambda + 1, p * q]) in one launch."""
+    import torch
+
+    if not tasks:
+        return
+    dtype = tasks[0][0].dtype
+    if dtype not in (torch.float32, torch.float64):
+        raise TypeError("Clebsch-Gordan products take float32 or float64 tensors")
+    arr = (C.featomic_b200_cg_task_t * len(tasks))()
+    for k, (a, b, out, lam) in enumerate(tasks):
+        for t in (a, b, out):
+            if not t.is_cuda or t.dtype != dtype or not t.is_contiguous():
+                raise ValueError("Clebsch-Gordan tensors must be contiguous CUDA tensors of one dtype")
+        s, m1, p = a.shape
+        _, m2, q = b.shape
+        if b.shape[0] != s or tuple(out.shape) != (s, 2 * lam + 1, p * q):
+            raise ValueError("inconsistent shapes in a Clebsch-Gordan product")
+        arr[k] = C.featomic_b200_cg_task_t(a.data_ptr(), b.data_ptr(), out.data_ptr(), s, (m1 - 1) // 2,
+                                           (m2 - 1) // 2, lam, p, q)
+    if stream is None:
+        stream = torch.cuda.current_stream().cuda_stream
+    C.check(C.lib().featomic_b200_cg_product(arr, len(tasks), 64 if dtype == torch.float64 else 32,
+                                             ctypes.c_void_p(stream)))
+
+
+class Block:
+    """values (torch CUDA tensor [samples, components..., properties]) with its labels."""
+
+    def __init__(self, values, samples, components, properties):
+        self.values = values
+        self.samples = samples
+        self.components = components
+        self.properties = properties
+
+
+class EquivariantTensorMap:
+    """Keys and blocks of a Clebsch-Gordan product, with the accessors of the
+    calculators' TensorMap."""
+
+    def __init__(self, keys, blocks):
+        self.keys = keys
+        self._blocks = blocks
+
+    def __len__(self):
+        return len(self.keys)
+
+    def block_by_id(self, index):
+        return self._blocks[index]
+
+    def blocks(self):
+        return list(self._blocks)
+
+    def block(self, **selection):
+        matches = np.ones(len(self.keys), dtype=bool)
+        for name, value in selection.items():
+            matches &= self.keys.column(name) == value
+        idx = np.nonzero(matches)[0]
+        if len(idx) != 1:
+            raise ValueError(f"selection {selection} matches {len(idx)} blocks")
+        return self._blocks[int(idx[0])]
+
+
+def _rename(labels, old, new):
+    return Labels([new if n == old else n for n in labels.names], labels.values)
+
+
+def _to_device(tensor, suffix, dtype):
+    """A spherical expansion with "neighbor_type" / "n" renamed
+    (_equivariant_power_spectrum.py:312-320), values on the GPU."""
+    import torch
+
+    keys = _rename(tensor.keys, "neighbor_type", f"neighbor_{suffix}_type")
+    blocks = []
+    for b in tensor.blocks():
+        values = torch.as_tensor(np.ascontiguousarray(b.values) if isinstance(b.values, np.ndarray) else b.values)
+        blocks.append(Block(values.to(device="cuda", dtype=dtype).contiguous(), b.samples, b.components,
+                            _rename(b.properties, "n", f"n_{suffix}")))
+    return EquivariantTensorMap(keys, blocks)
+
+
+def _merge_blocks(members, moved_names, moved_values):
+    """Blocks of one merged key, properties (moved key values, block
+    properties) in the order of ``moved_values``; samples are the union in
+    order of first appearance and absent entries are zero (metatensor's
+    keys_to_properties)."""
+    import torch
+
+    present = [b for b in members.values() if b is not None]
+    rows, order = {}, []
+    for b in present:
+        for s in map(tuple, b.samples.values):
+            if s not in rows:
+                rows[s] = len(rows)
+                order.append(s)
+    ref = present[0]
+    comp_shape = tuple(ref.values.shape[1:-1])
+    nprop = ref.values.shape[-1]
+    prop_names = list(moved_names) + ref.properties.names
+    parts, prop_values = [], []
+    for mv in moved_values:
+        b = members.get(mv)
+        block_props = b.properties.values if b is not None else ref.properties.values
+        for p in block_props:
+            prop_values.append(list(mv) + list(p))
+        if b is None:
+            parts.append(torch.zeros((len(order),) + comp_shape + (nprop,), dtype=ref.values.dtype, device="cuda"))
+            continue
+        if len(b.samples) == len(order) and all(rows[tuple(s)] == i for i, s in enumerate(b.samples.values)):
+            parts.append(b.values)
+        else:
+            full = torch.zeros((len(order),) + comp_shape + (b.values.shape[-1],), dtype=ref.values.dtype,
+                               device="cuda")
+            idx = torch.as_tensor([rows[tuple(s)] for s in b.samples.values], device="cuda", dtype=torch.long)
+            full[idx] = b.values
+            parts.append(full)
+    sample_names = ref.samples.names
+    return Block(torch.cat(parts, dim=-1).contiguous(), Labels(sample_names, np.array(order, dtype=np.int32)),
+                 ref.components, Labels(prop_names, np.array(prop_values, dtype=np.int32)))
+
+
+def keys_to_properties(tensor, names, values=None):
+    """Move the key dimensions ``names`` to the properties: blocks that differ
+    only in them are merged.  ``values`` (rows of those dimensions) fixes the
+    merged entries and their order, zero-filling absent blocks; without it
+    each merged block holds the values its own blocks have, in increasing
+    order."""
+    keys = tensor.keys
+    move = [keys.names.index(n) for n in names]
+    keep = [i for i in range(len(keys.names)) if i not in move]
+    if values is not None:
+        values = [tuple(int(x) for x in np.atleast_1d(v)) for v in values]
+    groups, order = {}, []
+    for i, row in enumerate(keys.values):
+        rest = tuple(int(v) for v in row[keep])
+        if rest not in groups:
+            groups[rest] = {}
+            order.append(rest)
+        groups[rest][tuple(int(v) for v in row[move])] = tensor.block_by_id(i)
+    blocks = []
+    for rest in order:
+        group_values = values if values is not None else sorted(groups[rest])
+        members = {mv: groups[rest].get(mv) for mv in group_values}
+        blocks.append(_merge_blocks(members, names, group_values))
+    new_keys = Labels([keys.names[i] for i in keep], np.array(order, dtype=np.int32).reshape(len(order), len(keep)))
+    return EquivariantTensorMap(new_keys, blocks)
+
+
+def _filter_redundant_keys(keys):
+    """Keep keys with sorted angular orders l_1 <= l_2 <= ...
+    (_density_correlations.py:233-272)."""
+    nu = 1
+    while f"l_{nu + 1}" in keys.names:
+        nu += 1
+    cols = [keys.names.index(f"l_{k}") for k in range(1, nu + 1)]
+    return [i for i, row in enumerate(keys.values) if list(row[cols]) == sorted(row[cols])]
+
+
+def _select(keys, selected):
+    """Entries of ``keys`` matching any entry of ``selected`` on its dimensions
+    (metatensor Labels.select)."""
+    if not isinstance(selected, Labels):
+        selected = Labels(*selected)
+    cols = [keys.names.index(n) for n in selected.names]
+    wanted = {tuple(int(v) for v in row) for row in selected.values}
+    return [i for i, row in enumerate(keys.values) if tuple(int(v) for v in row[cols]) in wanted]
+
+
+def _match_samples(b1, b2):
+    """(samples, values_1, values_2) on common samples (_utils.py:272-350):
+    with the same sample names, the union (block 1's samples, then the new
+    ones of block 2, metatensor's union_and_mapping) with zeros where a block
+    has no entry; otherwise the block with fewer sample dimensions is
+    broadcast onto the other's samples."""
+    import torch
+
+    s1, s2 = b1.samples, b2.samples
+    if s1.names == s2.names:
+        if len(s1) == len(s2) and np.array_equal(s1.values, s2.values):
+            return s1, b1.values, b2.values
+        rows = {tuple(v): i for i, v in enumerate(s1.values)}
+        union = [tuple(v) for v in s1.values]
+        for v in map(tuple, s2.values):
+            if v not in rows:
+                rows[v] = len(union)
+                union.append(v)
+        samples = Labels(s1.names, np.array(union, dtype=np.int32).reshape(len(union), len(s1.names)))
+        out = []
+        for blk, labels in ((b1, s1), (b2, s2)):
+            full = torch.zeros((len(union),) + tuple(blk.values.shape[1:]), dtype=blk.values.dtype, device="cuda")
+            idx = torch.as_tensor([rows[tuple(v)] for v in labels.values], dtype=torch.long, device="cuda")
+            if len(idx):
+                full[idx] = blk.values
+            out.append(full)
+        return samples, out[0], out[1]
+    swapped = len(s1.names) > len(s2.names)
+    small, big = (b2, b1) if swapped else (b1, b2)
+    for name in small.samples.names:
+        if name not in big.samples.names:
+            raise ValueError("Samples dimensions of the two blocks are not compatible. The block with fewer "
+                             "samples dimensions must be a subset of the other block's dimensions. Got: "
+                             f"{small.samples.names} and {big.samples.names}. Offending dimension: {name}")
+    dims = [big.samples.names.index(n) for n in small.samples.names]
+    rows = {tuple(v): i for i, v in enumerate(small.samples.values)}
+    idx = torch.as_tensor([rows[tuple(v)] for v in big.samples.values[:, dims]], dtype=torch.long, device="cuda")
+    expanded = small.values[idx]
+    if swapped:
+        return big.samples, big.values, expanded
+    return big.samples, expanded, big.values
+
+
+class ClebschGordanProduct:
+    """CG tensor product of two equivariant TensorMaps (_cg_product.py:29-436);
+    no gradients, as in featomic."""
+
+    def __init__(self, *, max_angular, keys_filter=None):
+        self.max_angular = max_angular
+        self._keys_filter = keys_filter or (lambda keys: list(range(len(keys))))
+
+    def compute(self, tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys=None):
+        import torch
+
+        keys, combos = self._output_keys(tensor_1.keys, tensor_2.keys, o3_lambda_1_new_name, o3_lambda_2_new_name)
+        if selected_keys is not None:
+            idx = _select(keys, selected_keys)
+            keys, combos = Labels(keys.names, keys.values[idx]), [combos[i] for i in idx]
+        idx = self._keys_filter(keys)
+        keys, combos = Labels(keys.names, keys.values[idx]), [combos[i] for i in idx]
+        # all lambda of one block pair consecutive (_utils.py:160-216)
+        groups, order = {}, []
+        for i, c in enumerate(combos):
+            if c not in groups:
+                groups[c] = []
+                order.append(c)
+            groups[c].append(i)
+        lam_col = keys.names.index("o3_lambda")
+        new_values, blocks, tasks = [], [], []
+        for c in order:
+            b1, b2 = tensor_1.block_by_id(c[0]), tensor_2.block_by_id(c[1])
+            if b1.values.ndim != 3 or b2.values.ndim != 3:
+                raise ValueError("Clebsch-Gordan products take blocks with one o3_mu component")
+            samples, a, b = _match_samples(b1, b2)
+            a, b = a.contiguous(), b.to(a.dtype).contiguous()
+            props = Labels(b1.properties.names + b2.properties.names,
+                           np.array([list(p) + list(q) for p in b1.properties.values for q in b2.properties.values],
+                                    dtype=np.int32).reshape(-1, len(b1.properties.names) + len(b2.properties.names)))
+            for i in groups[c]:
+                lam = int(keys.values[i][lam_col])
+                out = torch.empty((a.shape[0], 2 * lam + 1, a.shape[2] * b.shape[2]), dtype=a.dtype, device="cuda")
+                tasks.append((a, b, out, lam))
+                mu = Labels(["o3_mu"], np.arange(-lam, lam + 1, dtype=np.int32).reshape(-1, 1))
+                blocks.append(Block(out, samples, [mu], props))
+                new_values.append(keys.values[i])
+        cg_tensor_products(tasks)
+        return EquivariantTensorMap(
+            Labels(keys.names, np.array(new_values, dtype=np.int32).reshape(-1, len(keys.names))), blocks)
+
+    @staticmethod
+    def _output_keys(keys_1, keys_2, name_1, name_2):
+        """_utils.py:30-157 (_compute_output_keys)."""
+        cg = ["o3_lambda", "o3_sigma"]
+        for n in cg:
+            if n not in keys_1.names or n not in keys_2.names:
+                raise ValueError(f"both tensors need the key dimension {n}")
+        match = [n for n in keys_1.names if n not in cg and n in keys_2.names]
+        other_1 = [n for n in keys_1.names if n not in cg and n not in match]
+        other_2 = [n for n in keys_2.names if n not in cg and n not in match]
+        names = cg + match + other_1 + [name_1] + other_2 + [name_2]
+        i1 = {n: keys_1.names.index(n) for n in keys_1.names}
+        i2 = {n: keys_2.names.index(n) for n in keys_2.names}
+        values, combos = [], []
+        for a, k1 in enumerate(keys_1.values):
+            for b, k2 in enumerate(keys_2.values):
+                if any(k1[i1[n]] != k2[i2[n]] for n in match):
+                    continue
+                l1, s1 = int(k1[i1["o3_lambda"]]), int(k1[i1["o3_sigma"]])
+                l2, s2 = int(k2[i2["o3_lambda"]]), int(k2[i2["o3_sigma"]])
+                for lam in range(abs(l1 - l2), l1 + l2 + 1):
+                    sigma = s1 * s2 * (-1) ** (l1 + l2 + lam)
+                    values.append([lam, sigma] + [int(k1[i1[n]]) for n in match] + [int(k1[i1[n]]) for n in other_1]
+                                  + [l1] + [int(k2[i2[n]]) for n in other_2] + [l2])
+                    combos.append((a, b))
+        return Labels(names, np.array(values, dtype=np.int32).reshape(-1, len(names))), combos
+
+
+class EquivariantPowerSpectrum:
+    """Equivariant power spectrum ("lambda-SOAP") of one or two spherical
+    expansions (_equivariant_power_spectrum.py:23-365)."""
+
+    def __init__(self, calculator_1, calculator_2=None, neighbor_types=None, *, dtype=None, device=None):
+        import torch
+
+        supported = ["spherical_expansion"]
+        for k, calc in ((1, calculator_1), (2, calculator_2)):
+            if calc is None:
+                continue
+            if calc._name not in supported:
+                raise ValueError(f"Only [{', '.join(supported)}] are supported for `calculator_{k}`, "
+                                 f"got '{calc._name}'")
+        p1 = json.loads(calculator_1.parameters)
+        p2 = p1 if calculator_2 is None else json.loads(calculator_2.parameters)
+        if calculator_2 is not None:
+            for k, p in ((1, p1), (2, p2)):
+                if p["basis"]["type"] != "TensorProduct":
+                    raise ValueError(f"only 'TensorProduct' basis is supported for calculator_{k}")
+        if device is not None and torch.device(device).type != "cuda":
+            raise ValueError("the equivariant power spectrum runs on CUDA devices only")
+        self.calculator_1 = calculator_1
+        self.calculator_2 = calculator_2
+        self.neighbor_types = neighbor_types
+        self.dtype = dtype if dtype is not None else torch.float64
+        self._cg_product = ClebschGordanProduct(
+            max_angular=p1["basis"]["max_angular"] + p2["basis"]["max_angular"],
+            keys_filter=_filter_redundant_keys)
+
+    @property
+    def name(self):
+        return "EquivariantPowerSpectrum"
+
+    def compute(self, systems, selected_keys=None, neighbors_to_properties=False):
+        """_equivariant_power_spectrum.py:215-256 / :296-365."""
+        d1 = _to_device(self.calculator_1.compute(systems), 1, self.dtype)
+        d2 = _to_device((self.calculator_2 or self.calculator_1).compute(systems), 2, self.dtype)
+        if neighbors_to_properties:
+            values = None if self.neighbor_types is None else [[t] for t in self.neighbor_types]
+            d1 = keys_to_properties(d1, ["neighbor_1_type"], values)
+            d2 = keys_to_properties(d2, ["neighbor_2_type"], values)
+        ps = self._cg_product.compute(d1, d2, "l_1", "l_2", selected_keys)
+        return keys_to_properties(ps, ["l_1", "l_2"])
+
+    forward = compute

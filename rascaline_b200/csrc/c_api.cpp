@@ -16,6 +16,7 @@
 
 #include "../../include/featomic_b200.h"
 #include "batched.hpp"
+#include "clebsch_gordan.hpp"
 #include "dense.hpp"
 #include "engine.hpp"
 #include "host.hpp"
@@ -934,6 +935,27 @@ featomic_status_t featomic_b200_block_values(const mts_block_t* block, double** 
         *shape = b->shape.data();
         *shape_count = b->shape.size();
         if (on_device) *on_device = b->on_device ? 1 : 0;
+    });
+}
+
+featomic_status_t featomic_b200_cg_coefficients(int32_t l1, int32_t l2, int32_t lambda, double* coefficients,
+                                                uintptr_t count) {
+    return guarded([&] {
+        CHECK_POINTER(coefficients);
+        const auto cg = fb200::real_cg_coefficients(l1, l2, lambda);
+        if (count != cg.size())
+            throw invalid_parameter("expected " + std::to_string(cg.size()) + " coefficients, got space for " +
+                                    std::to_string(count));
+        std::memcpy(coefficients, cg.data(), cg.size() * sizeof(double));
+    });
+}
+
+featomic_status_t featomic_b200_cg_product(const featomic_b200_cg_task_t* tasks, uintptr_t n_tasks,
+                                           int32_t precision, void* stream) {
+    return guarded([&] {
+        if (n_tasks == 0) return;
+        CHECK_POINTER(tasks);
+        fb200::cg_product(tasks, (size_t)n_tasks, precision, static_cast<cudaStream_t>(stream));
     });
 }
 
