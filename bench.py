@@ -22,6 +22,8 @@ contraction, every row materialised in featomic's TensorMap layout.
 * ``surrogate_form`` the learned radial surrogate (MLP trained on the GPU,
   tcgen05 inference) against the spline, on a 100 000-atom box, with errors
   against FP64.
+* ``--only cg`` the equivariant power spectrum (lambda-SOAP) of the same box:
+  every Clebsch-Gordan block product in one launch, FP64.
 * ``cpu_baseline`` / ``--impl reference``: featomic itself is Rust and cannot
   be built here (no cargo / crates), so the CPU side is the FP64 C++
   restatement in oracle/ (OpenMP, featomic's decomposition: spherical
@@ -536,6 +538,94 @@ def surrogate_form(steps, warmup, train_steps=20000):
     }
 
 
+def cg_form(steps, warmup):
+    """Equivariant power spectrum (lambda-SOAP) of the 1000-atom benchmark box
+    (rc 5.5 A, max_radial 7, max_angular 6, 4 species, neighbour types in the
+    properties): every Clebsch-Gordan block product with l_1 <= l_2, all
+    lambda, in one launch.  Timed: the product step on densities already on
+    the GPU (CUDA events, FP64); beside it the whole compute() (spherical
+    expansion through the C ABI, host->device copy, product) and the oracle's
+    numpy product on a 50-centre sample of every block."""
+    import torch
+    import rascaline_b200 as rb
+    from oracle import clebsch_gordan as ocg
+    from rascaline_b200 import clebsch_gordan as cg
+
+    system, hypers = workload()
+    se = rb.SphericalExpansion(**hypers)
+    calc = cg.EquivariantPowerSpectrum(se)
+    host = se.compute([system])
+    d1 = cg.keys_to_properties(cg._to_device(host, 1, torch.float64), ["neighbor_1_type"])
+    d2 = cg.keys_to_properties(cg._to_device(host, 2, torch.float64), ["neighbor_2_type"])
+    product = calc._cg_product
+    for _ in range(max(3, warmup)):
+        out = product.compute(d1, d2, "l_1", "l_2")
+    torch.cuda.synchronize()
+    in_bytes = sum(b.values.numel() * 8 for b in d1.blocks()) + sum(b.values.numel() * 8 for b in d2.blocks())
+    out_bytes = sum(b.values.numel() * 8 for b in out.blocks())
+    n_blocks = len(out)
+    centres = sum(len(b.samples) for k, b in zip(d1.keys.values, d1.blocks()) if k[0] == 0)
+    del out
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        starts[k].record()
+        out = product.compute(d1, d2, "l_1", "l_2")
+        ends[k].record()
+        del out
+    torch.cuda.synchronize()
+    step_ms = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)]))
+    # the kernel alone: the same tasks, planned once
+    out, tasks = product.plan(d1, d2, "l_1", "l_2")
+    for k in range(steps):
+        starts[k].record()
+        cg.cg_tensor_products(tasks)
+        ends[k].record()
+    torch.cuda.synchronize()
+    ms = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)]))
+    del out, tasks
+    t0 = time.perf_counter()
+    for _ in range(3):
+        full = calc.compute([system], neighbors_to_properties=True)
+        torch.cuda.synchronize()
+        del full
+    e2e_ms = (time.perf_counter() - t0) / 3 * 1000.0
+    # CPU: the oracle's numpy product of every block pair on the first 50 centres
+    t0 = time.perf_counter()
+    sample_centres = 0
+    for i, key in enumerate(d1.keys.values):
+        for j, key2 in enumerate(d2.keys.values):
+            if key[2] != key2[2] or key[0] > key2[0]:
+                continue
+            a = d1.block_by_id(i).values[:50].cpu().numpy()
+            b = d2.block_by_id(j).values[:50].cpu().numpy()
+            for lam in range(abs(int(key[0]) - int(key2[0])), int(key[0]) + int(key2[0]) + 1):
+                ocg.cg_tensor_product(a, b, lam)
+        sample_centres += min(50, len(d1.block_by_id(i).samples)) if key[0] == 0 else 0
+    cpu_s = time.perf_counter() - t0
+    peak, peak_kind = measured_peaks()
+    achieved = (in_bytes + out_bytes) / (ms / 1000.0) / 1e9
+    return {
+        "workload": "random_box_1000_rho0.1_rc5.5_nmax7_lmax6_lambda_soap_fp64_neighbors_to_properties",
+        "blocks": n_blocks,
+        "centres": centres,
+        "output_GB": out_bytes / 1e9,
+        "kernel_ms": ms,
+        "centres_per_s": centres / ms * 1e3,
+        "product_step_ms": step_ms,
+        "product_step_note": "compute() of the Clebsch-Gordan product on densities in HBM: key and label "
+                             "bookkeeping in Python plus the launch",
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "note": "input + output bytes of the product kernel per launch; 9.4 FMA per output value"},
+        "compute_e2e_ms": e2e_ms,
+        "cpu_baseline": {"value": sample_centres / cpu_s, "unit": "centres/s", "cores": 1, "kind": "port",
+                         "sample": "numpy einsum of every block pair on the first 50 centres of each block"},
+        "gpu_launches_per_step": 1,
+        "steps": steps,
+    }
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -547,7 +637,7 @@ def main():
                         help="skip the FP32 adjoint form measured beside the drop-in")
     parser.add_argument("--atoms", type=int, default=1000,
                         help="atoms in the box (1000 is the benchmark; smaller boxes are for profiling)")
-    parser.add_argument("--only", choices=["adjoint", "batched", "surrogate"],
+    parser.add_argument("--only", choices=["adjoint", "batched", "surrogate", "cg"],
                         help="run one chosen form alone and print its object (profiling)")
     parser.add_argument("--train-steps", type=int, default=20000,
                         help="training steps of the learned radial surrogate (20000 is the benchmark)")
@@ -555,7 +645,7 @@ def main():
     if args.only:
         import torch
         torch.cuda.set_device(0)
-        form = {"adjoint": adjoint_form, "batched": batched_form,
+        form = {"adjoint": adjoint_form, "batched": batched_form, "cg": cg_form,
                 "surrogate": lambda k, w: surrogate_form(k, w, args.train_steps)}[args.only]
         print(json.dumps({args.only + "_form": form(args.steps, args.warmup)}), flush=True)
         return

@@ -58,5 +58,9 @@ def cg_tensor_product(a, b, lam):
     a [s, 2 l1 + 1, p], b [s, 2 l2 + 1, q] -> [s, 2 lam + 1, p * q]."""
     l1 = (a.shape[1] - 1) // 2
     l2 = (b.shape[1] - 1) // 2
-    out = np.einsum("xyz,sxp,syq->szpq", real_cg(l1, l2, lam), a, b)
-    return out.reshape(a.shape[0], 2 * lam + 1, -1)
+    s, p, q = a.shape[0], a.shape[2], b.shape[2]
+    # outer product [s, p, q, m1, m2], then one matrix product with the
+    # coefficients [(m1 m2), mu], as the reference's dense backend does
+    outer = np.einsum("sxp,syq->spqxy", a, b).reshape(s * p * q, -1)
+    out = outer @ real_cg(l1, l2, lam).reshape(-1, 2 * lam + 1)
+    return out.reshape(s, p * q, 2 * lam + 1).transpose(0, 2, 1)

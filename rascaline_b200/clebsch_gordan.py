@@ -132,8 +132,8 @@ def _merge_blocks(members, moved_names, moved_values):
     for mv in moved_values:
         b = members.get(mv)
         block_props = b.properties.values if b is not None else ref.properties.values
-        for p in block_props:
-            prop_values.append(list(mv) + list(p))
+        prop_values.append(np.concatenate([np.tile(np.asarray(mv, dtype=np.int32), (len(block_props), 1)),
+                                           block_props], axis=1))
         if b is None:
             parts.append(torch.zeros((len(order),) + comp_shape + (nprop,), dtype=ref.values.dtype, device="cuda"))
             continue
@@ -147,7 +147,7 @@ def _merge_blocks(members, moved_names, moved_values):
             parts.append(full)
     sample_names = ref.samples.names
     return Block(torch.cat(parts, dim=-1).contiguous(), Labels(sample_names, np.array(order, dtype=np.int32)),
-                 ref.components, Labels(prop_names, np.array(prop_values, dtype=np.int32)))
+                 ref.components, Labels(prop_names, np.concatenate(prop_values, axis=0)))
 
 
 def keys_to_properties(tensor, names, values=None):
@@ -249,6 +249,14 @@ class ClebschGordanProduct:
         self._keys_filter = keys_filter or (lambda keys: list(range(len(keys))))
 
     def compute(self, tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys=None):
+        """The product TensorMap (_cg_product.py:139-212 / :262-334)."""
+        result, tasks = self.plan(tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys)
+        cg_tensor_products(tasks)
+        return result
+
+    def plan(self, tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys=None):
+        """(TensorMap with unfilled values, its block-product tasks for
+        ``cg_tensor_products``)."""
         import torch
 
         keys, combos = self._output_keys(tensor_1.keys, tensor_2.keys, o3_lambda_1_new_name, o3_lambda_2_new_name)
@@ -272,9 +280,9 @@ class ClebschGordanProduct:
                 raise ValueError("Clebsch-Gordan products take blocks with one o3_mu component")
             samples, a, b = _match_samples(b1, b2)
             a, b = a.contiguous(), b.to(a.dtype).contiguous()
+            p1, p2 = b1.properties.values, b2.properties.values
             props = Labels(b1.properties.names + b2.properties.names,
-                           np.array([list(p) + list(q) for p in b1.properties.values for q in b2.properties.values],
-                                    dtype=np.int32).reshape(-1, len(b1.properties.names) + len(b2.properties.names)))
+                           np.concatenate([np.repeat(p1, len(p2), axis=0), np.tile(p2, (len(p1), 1))], axis=1))
             for i in groups[c]:
                 lam = int(keys.values[i][lam_col])
                 out = torch.empty((a.shape[0], 2 * lam + 1, a.shape[2] * b.shape[2]), dtype=a.dtype, device="cuda")
@@ -282,9 +290,8 @@ class ClebschGordanProduct:
                 mu = Labels(["o3_mu"], np.arange(-lam, lam + 1, dtype=np.int32).reshape(-1, 1))
                 blocks.append(Block(out, samples, [mu], props))
                 new_values.append(keys.values[i])
-        cg_tensor_products(tasks)
         return EquivariantTensorMap(
-            Labels(keys.names, np.array(new_values, dtype=np.int32).reshape(-1, len(keys.names))), blocks)
+            Labels(keys.names, np.array(new_values, dtype=np.int32).reshape(-1, len(keys.names))), blocks), tasks
 
     @staticmethod
     def _output_keys(keys_1, keys_2, name_1, name_2):

@@ -136,6 +136,7 @@ struct DeviceCgTask {
     int32_t m1_count, m2_count;
     int32_t entries;      // offset of the task's (mu-sorted) coefficient list
     int32_t mu_offsets;   // offset of its [2 lambda + 2] per-mu starts
+    int32_t vector;       // rows of `second` / `output` take 4-wide vector accesses
 };
 
 struct CgEntry {
@@ -145,10 +146,31 @@ struct CgEntry {
 };
 
 constexpr int CG_THREADS = 256;
+constexpr int CG_PV = 4;  // first-block properties per thread
+constexpr int CG_QV = 4;  // second-block properties per thread
 
-// One thread per (sample, p, q) of one task: each output component mu is the
-// sum over the task's non-zero coefficients of that mu, so every output value
-// is written once, coalesced along q.
+__device__ inline void load4(const float* p, float (&x)[4]) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    x[0] = v.x, x[1] = v.y, x[2] = v.z, x[3] = v.w;
+}
+__device__ inline void load4(const double* p, double (&x)[4]) {
+    const double2 u = reinterpret_cast<const double2*>(p)[0], v = reinterpret_cast<const double2*>(p)[1];
+    x[0] = u.x, x[1] = u.y, x[2] = v.x, x[3] = v.y;
+}
+__device__ inline void store4(float* p, const float (&x)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(x[0], x[1], x[2], x[3]);
+}
+__device__ inline void store4(double* p, const double (&x)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(x[0], x[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(x[2], x[3]);
+}
+
+// One thread per (sample, 4 first-block properties, 4 second-block
+// properties) of one task: each coefficient and first-block value is loaded
+// once for 4 or 16 products, the second-block row and the output row are 4-wide
+// vector accesses when the task allows, and every output value is written
+// once.  Each output is sum_k (C_k * a[m1_k]) * b[m2_k] over the task's
+// non-zero coefficients of that mu, in the table order.
 template <typename T>
 __global__ void __launch_bounds__(CG_THREADS)
 cg_product_kernel(const DeviceCgTask* __restrict__ tasks, int n_tasks, const CgEntry* __restrict__ entries,
@@ -159,24 +181,57 @@ cg_product_kernel(const DeviceCgTask* __restrict__ tasks, int n_tasks, const CgE
         if (tasks[mid].block_start <= (int64_t)blockIdx.x) lo = mid; else hi = mid - 1;
     }
     const DeviceCgTask t = tasks[lo];
-    const int64_t PQ = (int64_t)t.n_first * t.n_second;
+    const int nqt = (t.n_second + CG_QV - 1) / CG_QV, npt = (t.n_first + CG_PV - 1) / CG_PV;
+    const int64_t tiles = (int64_t)npt * nqt;
     const int64_t item = ((int64_t)blockIdx.x - t.block_start) * CG_THREADS + threadIdx.x;
-    if (item >= t.n_samples * PQ) return;
-    const int64_t s = item / PQ;
-    const int64_t pq = item - s * PQ;
-    const int p = (int)(pq / t.n_second), q = (int)(pq - (int64_t)p * t.n_second);
-    const T* __restrict__ a = static_cast<const T*>(t.first) + s * t.m1_count * t.n_first + p;
-    const T* __restrict__ b = static_cast<const T*>(t.second) + s * t.m2_count * t.n_second + q;
-    T* __restrict__ out = static_cast<T*>(t.output) + s * (2 * t.lambda + 1) * PQ + pq;
+    if (item >= t.n_samples * tiles) return;
+    const int64_t s = item / tiles;
+    const int64_t r = item - s * tiles;
+    const int pt = (int)(r / nqt), qt = (int)(r - (int64_t)pt * nqt);
+    const int p0 = pt * CG_PV, q0 = qt * CG_QV;
+    const int np = min(CG_PV, t.n_first - p0), nq = min(CG_QV, t.n_second - q0);
+    const int64_t PQ = (int64_t)t.n_first * t.n_second;
+    const T* __restrict__ a = static_cast<const T*>(t.first) + s * t.m1_count * t.n_first + p0;
+    const T* __restrict__ b = static_cast<const T*>(t.second) + s * t.m2_count * t.n_second + q0;
+    T* __restrict__ out = static_cast<T*>(t.output) + s * (2 * t.lambda + 1) * PQ + (int64_t)p0 * t.n_second + q0;
+    const bool vec = t.vector && nq == CG_QV;
     const int32_t* starts = mu_starts + t.mu_offsets;
     const CgEntry* e = entries + t.entries;
     for (int mu = 0; mu <= 2 * t.lambda; mu++) {
-        T acc = T(0);
+        T acc[CG_PV][CG_QV];
+#pragma unroll
+        for (int i = 0; i < CG_PV; i++)
+#pragma unroll
+            for (int j = 0; j < CG_QV; j++) acc[i][j] = T(0);
         for (int k = starts[mu]; k < starts[mu + 1]; k++) {
             const CgEntry c = e[k];
-            acc += T(c.value) * a[(int64_t)c.m1 * t.n_first] * b[(int64_t)c.m2 * t.n_second];
+            const T* brow = b + (int64_t)c.m2 * t.n_second;
+            T bv[CG_QV];
+            if (vec) {
+                load4(brow, bv);
+            } else {
+#pragma unroll
+                for (int j = 0; j < CG_QV; j++) bv[j] = j < nq ? brow[j] : T(0);
+            }
+#pragma unroll
+            for (int i = 0; i < CG_PV; i++) {
+                const T ca = T(c.value) * (i < np ? a[(int64_t)c.m1 * t.n_first + i] : T(0));
+#pragma unroll
+                for (int j = 0; j < CG_QV; j++) acc[i][j] += ca * bv[j];
+            }
         }
-        out[mu * PQ] = acc;
+        T* orow = out + mu * PQ;
+#pragma unroll
+        for (int i = 0; i < CG_PV; i++) {
+            if (i >= np) break;
+            if (vec) {
+                store4(orow + (int64_t)i * t.n_second, acc[i]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < CG_QV; j++)
+                    if (j < nq) orow[(int64_t)i * t.n_second + j] = acc[i][j];
+            }
+        }
     }
 }
 
@@ -237,10 +292,14 @@ void cg_product(const featomic_b200_cg_task_t* tasks, size_t n_tasks, int precis
         d.m2_count = 2 * t.l2 + 1;
         d.entries = (int32_t)entries.size();
         d.mu_offsets = (int32_t)mu_starts.size();
+        const size_t align = 4 * (precision == 64 ? sizeof(double) : sizeof(float));
+        d.vector = t.n_second % CG_QV == 0 && reinterpret_cast<uintptr_t>(t.second) % std::min<size_t>(align, 16) == 0 &&
+                   reinterpret_cast<uintptr_t>(t.output) % std::min<size_t>(align, 16) == 0;
         entries.insert(entries.end(), sp.entries.begin(), sp.entries.end());
         mu_starts.insert(mu_starts.end(), sp.mu_starts.begin(), sp.mu_starts.end());
         dev.push_back(d);
-        blocks += (items + CG_THREADS - 1) / CG_THREADS;
+        const int64_t threads = t.n_samples * ((t.n_first + CG_PV - 1) / CG_PV) * ((t.n_second + CG_QV - 1) / CG_QV);
+        blocks += (threads + CG_THREADS - 1) / CG_THREADS;
     }
     if (dev.empty()) return;
     if (blocks > 0x7fffffffLL) throw invalid_parameter("Clebsch-Gordan product too large for one launch");
