@@ -146,7 +146,7 @@ struct CgEntry {
 };
 
 constexpr int CG_THREADS = 256;
-constexpr int CG_PV = 4;  // first-block properties per thread
+constexpr int CG_PV = 8;  // first-block properties per thread
 constexpr int CG_QV = 4;  // second-block properties per thread
 
 __device__ inline void load4(const float* p, float (&x)[4]) {
@@ -165,9 +165,9 @@ __device__ inline void store4(double* p, const double (&x)[4]) {
     reinterpret_cast<double2*>(p)[1] = make_double2(x[2], x[3]);
 }
 
-// One thread per (sample, 4 first-block properties, 4 second-block
+// One thread per (sample, 8 first-block properties, 4 second-block
 // properties) of one task: each coefficient and first-block value is loaded
-// once for 4 or 16 products, the second-block row and the output row are 4-wide
+// once for 4 or 32 products, the second-block row and the output row are 4-wide
 // vector accesses when the task allows, and every output value is written
 // once.  Each output is sum_k (C_k * a[m1_k]) * b[m2_k] over the task's
 // non-zero coefficients of that mu, in the table order.
