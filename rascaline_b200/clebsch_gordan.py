@@ -259,6 +259,8 @@ class ClebschGordanProduct:
         ``cg_tensor_products``)."""
         import torch
 
+        self._check_inputs(tensor_1, tensor_2, selected_keys)
+
         keys, combos = self._output_keys(tensor_1.keys, tensor_2.keys, o3_lambda_1_new_name, o3_lambda_2_new_name)
         if selected_keys is not None:
             idx = _select(keys, selected_keys)
@@ -292,6 +294,44 @@ class ClebschGordanProduct:
                 new_values.append(keys.values[i])
         return EquivariantTensorMap(
             Labels(keys.names, np.array(new_values, dtype=np.int32).reshape(-1, len(keys.names))), blocks), tasks
+
+    def _check_inputs(self, tensor_1, tensor_2, selected_keys):
+        """_cg_product.py:336-432."""
+        for tensor in (tensor_1, tensor_2):
+            if "o3_lambda" not in tensor.keys.names:
+                raise ValueError("input tensors must have a named key dimension `'o3_lambda`")
+            if "o3_sigma" not in tensor.keys.names:
+                raise ValueError("input tensors must have a named key dimension `'o3_sigma`")
+            for b in tensor.blocks():
+                if len(b.components) != 1 or b.components[0].names != ["o3_mu"]:
+                    raise ValueError("input tensors must have a single component axis with a single named "
+                                     "dimensions `'o3_mu'`")
+        max_angular = int(tensor_1.keys.column("o3_lambda").max(initial=0)
+                          + tensor_2.keys.column("o3_lambda").max(initial=0))
+        if selected_keys is not None:
+            if not isinstance(selected_keys, Labels):
+                selected_keys = Labels(*selected_keys)
+            if "o3_lambda" in selected_keys.names:
+                lams = selected_keys.column("o3_lambda")
+                if len(lams) and int(lams.max()) > self.max_angular:
+                    raise ValueError("the maximum angular momentum value found in key dimension `'o3_lambda'` in "
+                                     f"`selected_keys` exceeds `max_angular={self.max_angular}` used to calculate "
+                                     "the CG coefficients in the constructor.")
+                if len(lams):
+                    max_angular = min(max_angular, int(lams.max()))
+            if "o3_sigma" in selected_keys.names:
+                if any(int(v) not in (-1, 1) for v in selected_keys.column("o3_sigma")):
+                    raise ValueError("key dimension `'o3_sigma'` in `selected_keys` must only contain values of "
+                                     "-1 or 1.")
+        if max_angular > self.max_angular:
+            raise ValueError(f"the maximum angular momentum `{max_angular}` required by the input tensors (and "
+                             "perhaps lowered by angular selection via `selected_keys`) exceeds the value of "
+                             f"`max_angular={self.max_angular}` used to calculate the CG coefficients")
+        if len(tensor_1) and len(tensor_2):
+            shared = set(tensor_1.block_by_id(0).properties.names) & set(tensor_2.block_by_id(0).properties.names)
+            if shared:
+                raise ValueError(f"property names {sorted(shared)} are present in both input tensors; they must "
+                                 "be unique")
 
     @staticmethod
     def _output_keys(keys_1, keys_2, name_1, name_2):
@@ -357,8 +397,10 @@ class EquivariantPowerSpectrum:
 
     def compute(self, systems, selected_keys=None, neighbors_to_properties=False):
         """_equivariant_power_spectrum.py:215-256 / :296-365."""
-        d1 = _to_device(self.calculator_1.compute(systems), 1, self.dtype)
-        d2 = _to_device((self.calculator_2 or self.calculator_1).compute(systems), 2, self.dtype)
+        density_1 = self.calculator_1.compute(systems)
+        density_2 = density_1 if self.calculator_2 is None else self.calculator_2.compute(systems)
+        d1 = _to_device(density_1, 1, self.dtype)
+        d2 = _to_device(density_2, 2, self.dtype)
         if neighbors_to_properties:
             values = None if self.neighbor_types is None else [[t] for t in self.neighbor_types]
             d1 = keys_to_properties(d1, ["neighbor_1_type"], values)
@@ -367,3 +409,85 @@ class EquivariantPowerSpectrum:
         return keys_to_properties(ps, ["l_1", "l_2"])
 
     forward = compute
+
+
+def as_tensormap(tensor, dtype=None):
+    """An ``EquivariantTensorMap`` on the GPU from a calculator's TensorMap
+    (host or device), labels unchanged."""
+    import torch
+
+    blocks = []
+    for b in tensor.blocks():
+        values = b.values
+        values = torch.as_tensor(np.ascontiguousarray(values) if isinstance(values, np.ndarray) else values)
+        blocks.append(Block(values.to(device="cuda", dtype=dtype or values.dtype).contiguous(), b.samples,
+                            b.components, b.properties))
+    return EquivariantTensorMap(tensor.keys, blocks)
+
+
+def _increment_numeric_suffix(name, increment_by=1):
+    """_density_correlations.py:320-359: "n" -> "n_1", "n_1" -> "n_2",
+    "center_type" -> "center_1_type"."""
+    if not isinstance(increment_by, int):
+        raise ValueError("`increment_by` must be an integer.")
+    if name.endswith("type"):
+        prefix, suffix = name[: name.rfind("_type")], "_type"
+    else:
+        prefix, suffix = name, ""
+    number = "0"
+    if prefix.rfind("_") != -1:
+        tail = prefix[prefix.rfind("_") + 1:]
+        if tail.isdigit():
+            number = tail
+            prefix = prefix[: prefix.rfind("_")]
+    return prefix + "_" + str(int(number) + increment_by) + suffix
+
+
+def _increment_property_names(tensor, increment_by=1):
+    """_density_correlations.py:275-317."""
+    if increment_by < 0:
+        raise ValueError("`increment_by` must be a non-negative integer.")
+    blocks = [Block(b.values, b.samples, b.components,
+                    Labels([_increment_numeric_suffix(n, increment_by) for n in b.properties.names],
+                           b.properties.values))
+              for b in tensor.blocks()]
+    return EquivariantTensorMap(tensor.keys, blocks)
+
+
+class DensityCorrelations:
+    """Iterated Clebsch-Gordan products of a density with itself, to body
+    order n_correlations + 2 (_density_correlations.py:23-231)."""
+
+    def __init__(self, *, n_correlations, max_angular, skip_redundant=True, dtype=None, device=None):
+        import torch
+
+        if device is not None and torch.device(device).type != "cuda":
+            raise ValueError("density correlations run on CUDA devices only")
+        self._n_correlations = n_correlations
+        self._dtype = dtype
+        self._cg_product = ClebschGordanProduct(max_angular=max_angular,
+                                                keys_filter=_filter_redundant_keys if skip_redundant else None)
+
+    def compute(self, density, angular_cutoff=None, selected_keys=None):
+        """_density_correlations.py:70-120 / :160-231; ``density`` is a
+        calculator TensorMap or an ``EquivariantTensorMap``."""
+        if not isinstance(density, EquivariantTensorMap):
+            density = as_tensormap(density, self._dtype)
+        correlations = _increment_property_names(density, 1)
+        density = _increment_property_names(density, 1)
+        for i in range(self._n_correlations):
+            density = _increment_property_names(density, 1)
+            name_1 = f"l_{i + 1}" if i == 0 else f"k_{i + 1}"
+            name_2 = f"l_{i + 2}"
+            last = i == self._n_correlations - 1
+            if last and selected_keys is not None:
+                selection = selected_keys
+            elif angular_cutoff is None:
+                selection = None
+            else:
+                selection = Labels(["o3_lambda"], np.arange(angular_cutoff + 1, dtype=np.int32).reshape(-1, 1))
+            correlations = self._cg_product.compute(correlations, density, name_1, name_2, selection)
+        return correlations
+
+    forward = compute
+

@@ -9,8 +9,12 @@ _utils.py:_compute_output_keys and the redundant-key filter.
 GPU tests: block products against the oracle (FP64 and FP32, several tasks
 in one launch), the lambda = 0 blocks of the equivariant power spectrum
 against the drop-in SOAP power spectrum (itself pinned to featomic's
-goldens), the rotation of the lambda = 1 blocks of a molecule, and the
-neighbor-types-to-properties form against the keyed form."""
+goldens), the rotation of the lambda = 1 blocks of a molecule, the
+neighbor-types-to-properties form against the keyed form, and
+DensityCorrelations (_density_correlations.py): nu = 2 against the
+equivariant power spectrum, nu = 3 rotations and one block against the
+oracle.  The property-name rule and the input checks of
+_cg_product.py:336-432 run on the CPU."""
 import numpy as np
 import pytest
 
@@ -206,3 +210,104 @@ def test_neighbors_to_properties_matches_keyed_form():
     pb = padded.block(o3_lambda=0, o3_sigma=1, center_type=1)
     col = [j for j, p in enumerate(pb.properties.values) if p[2] == 7 or p[4] == 7]
     assert col and float(pb.values[:, :, col].abs().max()) == 0.0
+
+
+def test_increment_numeric_suffix():
+    # the examples of _density_correlations.py:_increment_numeric_suffix
+    f = cg._increment_numeric_suffix
+    assert f("n", 1) == "n_1"
+    assert f("n", 0) == "n_0"
+    assert f("n_1", 1) == "n_2"
+    assert f("center_type", 3) == "center_3_type"
+    assert f("first_atom_1_type") == "first_atom_2_type"
+    assert f("center_type_1_type", 7) == "center_type_8_type"
+
+
+def _host_tensor(lmax, prop_name):
+    import torch
+
+    keys = rb.Labels(["o3_lambda", "o3_sigma", "center_type"], [[l, 1, 1] for l in range(lmax + 1)])
+    blocks = [cg.Block(torch.zeros(2, 2 * l + 1, 3, dtype=torch.float64),
+                       rb.Labels(["system", "atom"], [[0, 0], [0, 1]]),
+                       [rb.Labels(["o3_mu"], np.arange(-l, l + 1).reshape(-1, 1))],
+                       rb.Labels([prop_name], [[0], [1], [2]])) for l in range(lmax + 1)]
+    return cg.EquivariantTensorMap(keys, blocks)
+
+
+def test_product_input_checks():
+    # _cg_product.py:336-432, checked before anything runs on a device
+    a, b = _host_tensor(2, "n_1"), _host_tensor(3, "n_2")
+    with pytest.raises(ValueError, match="exceeds the value of `max_angular=4`"):
+        cg.ClebschGordanProduct(max_angular=4).plan(a, b, "l_1", "l_2")
+    with pytest.raises(ValueError, match="present in both input tensors"):
+        cg.ClebschGordanProduct(max_angular=8).plan(a, _host_tensor(3, "n_1"), "l_1", "l_2")
+    with pytest.raises(ValueError, match="must only contain values of -1 or 1"):
+        cg.ClebschGordanProduct(max_angular=8).plan(a, b, "l_1", "l_2",
+                                                     selected_keys=rb.Labels(["o3_sigma"], [[2]]))
+    with pytest.raises(ValueError, match="in `selected_keys` exceeds `max_angular=5`"):
+        cg.ClebschGordanProduct(max_angular=5).plan(a, b, "l_1", "l_2",
+                                                     selected_keys=rb.Labels(["o3_lambda"], [[6]]))
+
+
+def _moved_density(system, hypers):
+    se = rb.SphericalExpansion(**hypers)
+    density = cg.as_tensormap(se.compute([system]), None)
+    return cg.keys_to_properties(density, ["neighbor_type"]), se
+
+
+@pytest.mark.gpu
+def test_density_correlations_nu2_is_the_equivariant_power_spectrum():
+    system = workloads.random_box(40, density=0.1, species=(1, 6, 8), seed=12)
+    hypers = workloads.hypers(3.5, 2, 2, spline_accuracy=None)
+    density, se = _moved_density(system, hypers)
+    nu2 = cg.DensityCorrelations(n_correlations=1, max_angular=4).compute(density)
+    assert nu2.keys.names == ["o3_lambda", "o3_sigma", "center_type", "l_1", "l_2"]
+    assert nu2.block_by_id(0).properties.names == ["neighbor_1_type", "n_1", "neighbor_2_type", "n_2"]
+    eps = cg.EquivariantPowerSpectrum(se).compute([system], neighbors_to_properties=True)
+    for key, blk in zip(nu2.keys.values, nu2.blocks()):
+        lam, sigma, ct, l1, l2 = (int(v) for v in key)
+        eb = eps.block(o3_lambda=lam, o3_sigma=sigma, center_type=ct)
+        cols = [j for j, p in enumerate(eb.properties.values) if p[0] == l1 and p[1] == l2]
+        np.testing.assert_array_equal(eb.properties.values[cols][:, 2:], blk.properties.values)
+        np.testing.assert_array_equal(eb.values[:, :, cols].cpu().numpy(), blk.values.cpu().numpy())
+
+
+@pytest.mark.gpu
+def test_density_correlations_nu3():
+    rng = np.random.default_rng(8)
+    mol = workloads.molecules(1, seed=9, min_atoms=10, max_atoms=10)[0]
+    rotated = dict(mol)
+    R = _rotation(rng)
+    rotated["positions"] = np.ascontiguousarray(mol["positions"] @ R.T)
+    hypers = workloads.hypers(4.0, 1, 2, spline_accuracy=None)
+    calc = cg.DensityCorrelations(n_correlations=2, max_angular=6)
+    density, _ = _moved_density(mol, hypers)
+    a = calc.compute(density, angular_cutoff=2)
+    b = calc.compute(_moved_density(rotated, hypers)[0], angular_cutoff=2)
+    assert a.keys.names == ["o3_lambda", "o3_sigma", "center_type", "l_1", "l_2", "k_2", "l_3"]
+    assert a.block_by_id(0).properties.names == ["neighbor_1_type", "n_1", "neighbor_2_type", "n_2",
+                                                 "neighbor_3_type", "n_3"]
+    # intermediate lambda <= 2, the redundant filter keeps l_1 <= l_2 <= l_3
+    assert a.keys.column("k_2").max() <= 2
+    assert all(k[3] <= k[4] <= k[6] for k in a.keys.values)
+    perm = np.array([1, 2, 0])
+    Rm = R[np.ix_(perm, perm)]
+    for i, key in enumerate(a.keys.values):
+        va, vb = a.block_by_id(i).values.cpu().numpy(), b.block_by_id(i).values.cpu().numpy()
+        tol = 1e-9 * max(1.0, np.abs(va).max())
+        if key[0] == 0:
+            np.testing.assert_allclose(vb, va, rtol=0, atol=tol)
+        elif key[0] == 1:
+            np.testing.assert_allclose(np.einsum("xy,syp->sxp", Rm, va), vb, rtol=0, atol=tol)
+    # one block recomputed with the oracle from the nu = 2 intermediate
+    nu2 = cg.DensityCorrelations(n_correlations=1, max_angular=6).compute(density, angular_cutoff=2)
+    key = next(k for k in a.keys.values if k[0] == 1 and k[5] == 1 and k[6] == 2)
+    lam, sigma, ct, l1, l2, k2, l3 = (int(v) for v in key)
+    # sigma = (-1)^(l_1 + l_2 + k_2) is fixed by the others
+    idx = [i for i, k in enumerate(nu2.keys.values) if k[0] == k2 and k[2] == ct and k[3] == l1 and k[4] == l2]
+    assert len(idx) == 1
+    left = nu2.block_by_id(idx[0])
+    right = density.block(o3_lambda=l3, center_type=ct)
+    ref = ocg.cg_tensor_product(left.values.cpu().numpy(), right.values.cpu().numpy(), lam)
+    got = a.block(o3_lambda=lam, o3_sigma=sigma, center_type=ct, l_1=l1, l_2=l2, k_2=k2, l_3=l3)
+    np.testing.assert_allclose(got.values.cpu().numpy(), ref, rtol=0, atol=1e-12 * max(1.0, np.abs(ref).max()))
