@@ -491,3 +491,80 @@ class DensityCorrelations:
 
     forward = compute
 
+
+
+class PowerSpectrum:
+    """The invariant power spectrum of featomic's Clebsch-Gordan module
+    (python/featomic/featomic/clebsch_gordan/_power_spectrum.py:27-352):
+    keys (center_type), properties (l, neighbor_1_type, n_1, neighbor_2_type,
+    n_2), values (-1)^l / sqrt(2l + 1) sum_m c1[m, a] c2[m, b] -- the
+    lambda = 0 product of the two l blocks, computed by the Clebsch-Gordan
+    kernel (its lambda = 0 coefficients are that factor).  Values only:
+    positions gradients are not built."""
+
+    def __init__(self, calculator_1, calculator_2=None, neighbor_types=None, *, dtype=None, device=None):
+        import torch
+
+        for k, calc in ((1, calculator_1), (2, calculator_2)):
+            if calc is not None and calc._name != "spherical_expansion":
+                raise ValueError(f"Only [spherical_expansion] are supported for `calculator_{k}`, "
+                                 f"got '{calc._name}'")
+        if device is not None and torch.device(device).type != "cuda":
+            raise ValueError("the power spectrum runs on CUDA devices only")
+        self.calculator_1 = calculator_1
+        self.calculator_2 = calculator_2
+        self.neighbor_types = neighbor_types
+        self.dtype = dtype if dtype is not None else torch.float64
+
+    @property
+    def name(self):
+        return "PowerSpectrum"
+
+    def _density(self, calc, systems, suffix):
+        tm = calc.compute(systems)
+        if tm.keys.names != ["o3_lambda", "o3_sigma", "center_type", "neighbor_type"]:
+            raise ValueError("expected a spherical expansion")
+        if self.neighbor_types is None:
+            values = [[int(t)] for t in np.unique(tm.keys.column("neighbor_type"))]
+        else:
+            values = [[t] for t in self.neighbor_types]
+        d = keys_to_properties(as_tensormap(tm, self.dtype), ["neighbor_type"], values)
+        return _increment_property_names(d, suffix)
+
+    def compute(self, systems, gradients=None, use_native_system=True):
+        """_power_spectrum.py:196-351."""
+        import torch
+
+        if gradients:
+            for parameter in gradients:
+                if parameter != "positions":
+                    raise NotImplementedError("PowerSpectrum currently only supports gradients w.r.t. to positions")
+            raise NotImplementedError("positions gradients of PowerSpectrum are not implemented in featomic-b200")
+        d1 = self._density(self.calculator_1, systems, 1)
+        d2 = d1 if self.calculator_2 is None else self._density(self.calculator_2, systems, 1)
+        d2 = _increment_property_names(d2, 1)
+        tasks, values, keys = [], [], []
+        for i, key in enumerate(d1.keys.values):
+            lam, ct = int(key[0]), int(key[2])
+            b1 = d1.block_by_id(i)
+            for j, key2 in enumerate(d2.keys.values):
+                if int(key2[0]) != lam or int(key2[2]) != ct:
+                    continue
+                b2 = d2.block_by_id(j)
+                if len(b1.samples) != len(b2.samples) or not np.array_equal(b1.samples.values, b2.samples.values):
+                    raise ValueError("the two spherical expansions have different samples")
+                out = torch.empty((len(b1.samples), 1, b1.values.shape[2] * b2.values.shape[2]),
+                                  dtype=b1.values.dtype, device="cuda")
+                tasks.append((b1.values.contiguous(), b2.values.contiguous(), out, 0))
+                p1, p2 = b1.properties.values, b2.properties.values
+                props = Labels(["neighbor_1_type", "n_1", "neighbor_2_type", "n_2"],
+                               np.concatenate([np.repeat(p1, len(p2), axis=0), np.tile(p2, (len(p1), 1))], axis=1))
+                values.append(Block(out, b1.samples, [], props))
+                keys.append([lam, ct])
+        cg_tensor_products(tasks)
+        blocks = [Block(b.values.reshape(b.values.shape[0], -1), b.samples, [], b.properties) for b in values]
+        tm = EquivariantTensorMap(Labels(["l", "center_type"], np.array(keys, dtype=np.int32).reshape(-1, 2)),
+                                  blocks)
+        return keys_to_properties(tm, ["l"])
+
+    forward = compute

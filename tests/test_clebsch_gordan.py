@@ -311,3 +311,41 @@ def test_density_correlations_nu3():
     ref = ocg.cg_tensor_product(left.values.cpu().numpy(), right.values.cpu().numpy(), lam)
     got = a.block(o3_lambda=lam, o3_sigma=sigma, center_type=ct, l_1=l1, l_2=l2, k_2=k2, l_3=l3)
     np.testing.assert_allclose(got.values.cpu().numpy(), ref, rtol=0, atol=1e-12 * max(1.0, np.abs(ref).max()))
+
+
+def test_power_spectrum_gradients_not_built():
+    se = rb.SphericalExpansion(**workloads.hypers(3.0, 2, 2))
+    ps = cg.PowerSpectrum(se)
+    with pytest.raises(NotImplementedError, match="only supports gradients w.r.t. to positions"):
+        ps.compute([workloads.random_box(10, seed=1)], gradients=["strain"])
+    with pytest.raises(NotImplementedError, match="not implemented in featomic-b200"):
+        ps.compute([workloads.random_box(10, seed=1)], gradients=["positions"])
+
+
+@pytest.mark.gpu
+def test_cg_power_spectrum_is_the_soap_power_spectrum():
+    # _power_spectrum.py: the same invariants as SoapPowerSpectrum without the
+    # sqrt(2) of mixed neighbour types, every neighbour type pair in the properties
+    system = workloads.random_box(48, density=0.1, species=(1, 6, 8), seed=13)
+    se = rb.SphericalExpansion(**_ps_hypers())
+    out = cg.PowerSpectrum(se).compute([system])
+    assert out.keys.names == ["center_type"]
+    blk = out.block_by_id(0)
+    assert blk.properties.names == ["l", "neighbor_1_type", "n_1", "neighbor_2_type", "n_2"]
+    assert blk.components == []
+    ps = rb.SoapPowerSpectrum(**_ps_hypers()).compute([system])
+    checked = 0
+    for key, pblk in zip(ps.keys.values, ps.blocks()):
+        ct, n1, n2 = (int(v) for v in key)
+        cblk = out.block(center_type=ct)
+        props = {tuple(p): i for i, p in enumerate(cblk.properties.values)}
+        rows = [{tuple(s): i for i, s in enumerate(cblk.samples.values)}[tuple(s)] for s in pblk.samples.values]
+        cv = cblk.values.cpu().numpy()[rows]
+        cols = [props[(l, n1, a, n2, b)] for l, a, b in pblk.properties.values]
+        factor = 1.0 if n1 == n2 else np.sqrt(2.0)
+        np.testing.assert_allclose(factor * cv[:, cols], np.asarray(pblk.values), rtol=1e-10, atol=1e-14)
+        # the (n2, n1) properties hold the transposed invariants
+        cols_t = [props[(l, n2, b, n1, a)] for l, a, b in pblk.properties.values]
+        np.testing.assert_allclose(factor * cv[:, cols_t], np.asarray(pblk.values), rtol=1e-10, atol=1e-14)
+        checked += cv[:, cols].size
+    assert checked > 1000
