@@ -137,6 +137,7 @@ struct DeviceCgTask {
     int32_t entries;      // offset of the task's (mu-sorted) coefficient list
     int32_t mu_offsets;   // offset of its [2 lambda + 2] per-mu starts
     int32_t vector;       // rows of `second` / `output` take 4-wide vector accesses
+    int32_t vector_first; // rows of `first` take 8-wide vector loads
 };
 
 struct CgEntry {
@@ -157,6 +158,17 @@ __device__ inline void load4(const double* p, double (&x)[4]) {
     const double2 u = reinterpret_cast<const double2*>(p)[0], v = reinterpret_cast<const double2*>(p)[1];
     x[0] = u.x, x[1] = u.y, x[2] = v.x, x[3] = v.y;
 }
+__device__ inline void load8(const float* p, float (&x)[8]) {
+    const float4 u = reinterpret_cast<const float4*>(p)[0], v = reinterpret_cast<const float4*>(p)[1];
+    x[0] = u.x, x[1] = u.y, x[2] = u.z, x[3] = u.w, x[4] = v.x, x[5] = v.y, x[6] = v.z, x[7] = v.w;
+}
+__device__ inline void load8(const double* p, double (&x)[8]) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double2 u = reinterpret_cast<const double2*>(p)[k];
+        x[2 * k] = u.x, x[2 * k + 1] = u.y;
+    }
+}
 __device__ inline void store4(float* p, const float (&x)[4]) {
     *reinterpret_cast<float4*>(p) = make_float4(x[0], x[1], x[2], x[3]);
 }
@@ -167,8 +179,8 @@ __device__ inline void store4(double* p, const double (&x)[4]) {
 
 // One thread per (sample, 8 first-block properties, 4 second-block
 // properties) of one task: each coefficient and first-block value is loaded
-// once for 4 or 32 products, the second-block row and the output row are 4-wide
-// vector accesses when the task allows, and every output value is written
+// once for 4 or 32 products, the first-block row (8 wide), the second-block
+// row and the output row (4 wide) are vector accesses when the task allows, and every output value is written
 // once.  Each output is sum_k (C_k * a[m1_k]) * b[m2_k] over the task's
 // non-zero coefficients of that mu, in the table order.
 template <typename T>
@@ -195,6 +207,7 @@ cg_product_kernel(const DeviceCgTask* __restrict__ tasks, int n_tasks, const CgE
     const T* __restrict__ b = static_cast<const T*>(t.second) + s * t.m2_count * t.n_second + q0;
     T* __restrict__ out = static_cast<T*>(t.output) + s * (2 * t.lambda + 1) * PQ + (int64_t)p0 * t.n_second + q0;
     const bool vec = t.vector && nq == CG_QV;
+    const bool vec_first = CG_PV == 8 && t.vector_first && np == CG_PV;
     const int32_t* starts = mu_starts + t.mu_offsets;
     const CgEntry* e = entries + t.entries;
     for (int mu = 0; mu <= 2 * t.lambda; mu++) {
@@ -213,9 +226,16 @@ cg_product_kernel(const DeviceCgTask* __restrict__ tasks, int n_tasks, const CgE
 #pragma unroll
                 for (int j = 0; j < CG_QV; j++) bv[j] = j < nq ? brow[j] : T(0);
             }
+            T av[CG_PV];
+            if (vec_first) {
+                load8(a + (int64_t)c.m1 * t.n_first, av);
+            } else {
+#pragma unroll
+                for (int i = 0; i < CG_PV; i++) av[i] = i < np ? a[(int64_t)c.m1 * t.n_first + i] : T(0);
+            }
 #pragma unroll
             for (int i = 0; i < CG_PV; i++) {
-                const T ca = T(c.value) * (i < np ? a[(int64_t)c.m1 * t.n_first + i] : T(0));
+                const T ca = T(c.value) * av[i];
 #pragma unroll
                 for (int j = 0; j < CG_QV; j++) acc[i][j] += ca * bv[j];
             }
@@ -295,6 +315,7 @@ void cg_product(const featomic_b200_cg_task_t* tasks, size_t n_tasks, int precis
         const size_t align = 4 * (precision == 64 ? sizeof(double) : sizeof(float));
         d.vector = t.n_second % CG_QV == 0 && reinterpret_cast<uintptr_t>(t.second) % std::min<size_t>(align, 16) == 0 &&
                    reinterpret_cast<uintptr_t>(t.output) % std::min<size_t>(align, 16) == 0;
+        d.vector_first = t.n_first % CG_PV == 0 && reinterpret_cast<uintptr_t>(t.first) % 16 == 0;
         entries.insert(entries.end(), sp.entries.begin(), sp.entries.end());
         mu_starts.insert(mu_starts.end(), sp.mu_starts.begin(), sp.mu_starts.end());
         dev.push_back(d);
