@@ -21,5 +21,6 @@ from .calculators import (  # noqa: F401
     profiling_get,
 )
 from ._c_api import FeatomicError, LIBRARY  # noqa: F401
+from . import clebsch_gordan  # noqa: F401
 
 __version__ = "0.1.0"
