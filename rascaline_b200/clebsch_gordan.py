@@ -110,6 +110,26 @@ def _to_device(tensor, suffix, dtype):
     return EquivariantTensorMap(keys, blocks)
 
 
+def _union_rows(arrays):
+    """Union of the rows of int32 arrays in order of first appearance, and for
+    each array the union index of each of its rows."""
+    if all(len(a) == len(arrays[0]) and np.array_equal(a, arrays[0]) for a in arrays[1:]):
+        same = np.arange(len(arrays[0]))
+        return arrays[0], [same] * len(arrays)
+    stacked = np.concatenate(arrays, axis=0)
+    _, first, inverse = np.unique(stacked, axis=0, return_index=True, return_inverse=True)
+    inverse = inverse.reshape(-1)
+    order = np.argsort(first, kind="stable")
+    position = np.empty(len(first), dtype=np.int64)
+    position[order] = np.arange(len(first))
+    union = stacked[first[order]]
+    out, start = [], 0
+    for a in arrays:
+        out.append(position[inverse[start:start + len(a)]])
+        start += len(a)
+    return union, out
+
+
 def _merge_blocks(members, moved_names, moved_values):
     """Blocks of one merged key, properties (moved key values, block
     properties) in the order of ``moved_values``; samples are the union in
@@ -118,12 +138,8 @@ def _merge_blocks(members, moved_names, moved_values):
     import torch
 
     present = [b for b in members.values() if b is not None]
-    rows, order = {}, []
-    for b in present:
-        for s in map(tuple, b.samples.values):
-            if s not in rows:
-                rows[s] = len(rows)
-                order.append(s)
+    union, index = _union_rows([b.samples.values for b in present])
+    rows_of = {id(b): idx for b, idx in zip(present, index)}
     ref = present[0]
     comp_shape = tuple(ref.values.shape[1:-1])
     nprop = ref.values.shape[-1]
@@ -135,18 +151,18 @@ def _merge_blocks(members, moved_names, moved_values):
         prop_values.append(np.concatenate([np.tile(np.asarray(mv, dtype=np.int32), (len(block_props), 1)),
                                            block_props], axis=1))
         if b is None:
-            parts.append(torch.zeros((len(order),) + comp_shape + (nprop,), dtype=ref.values.dtype, device="cuda"))
+            parts.append(torch.zeros((len(union),) + comp_shape + (nprop,), dtype=ref.values.dtype, device="cuda"))
             continue
-        if len(b.samples) == len(order) and all(rows[tuple(s)] == i for i, s in enumerate(b.samples.values)):
+        idx = rows_of[id(b)]
+        if len(idx) == len(union) and np.array_equal(idx, np.arange(len(union))):
             parts.append(b.values)
         else:
-            full = torch.zeros((len(order),) + comp_shape + (b.values.shape[-1],), dtype=ref.values.dtype,
+            full = torch.zeros((len(union),) + comp_shape + (b.values.shape[-1],), dtype=ref.values.dtype,
                                device="cuda")
-            idx = torch.as_tensor([rows[tuple(s)] for s in b.samples.values], device="cuda", dtype=torch.long)
-            full[idx] = b.values
+            full[torch.as_tensor(idx, device="cuda", dtype=torch.long)] = b.values
             parts.append(full)
     sample_names = ref.samples.names
-    return Block(torch.cat(parts, dim=-1).contiguous(), Labels(sample_names, np.array(order, dtype=np.int32)),
+    return Block(torch.cat(parts, dim=-1).contiguous(), Labels(sample_names, union),
                  ref.components, Labels(prop_names, np.concatenate(prop_values, axis=0)))
 
 
@@ -209,19 +225,13 @@ def _match_samples(b1, b2):
     if s1.names == s2.names:
         if len(s1) == len(s2) and np.array_equal(s1.values, s2.values):
             return s1, b1.values, b2.values
-        rows = {tuple(v): i for i, v in enumerate(s1.values)}
-        union = [tuple(v) for v in s1.values]
-        for v in map(tuple, s2.values):
-            if v not in rows:
-                rows[v] = len(union)
-                union.append(v)
-        samples = Labels(s1.names, np.array(union, dtype=np.int32).reshape(len(union), len(s1.names)))
+        union, index = _union_rows([s1.values, s2.values])
+        samples = Labels(s1.names, union)
         out = []
-        for blk, labels in ((b1, s1), (b2, s2)):
+        for blk, idx in ((b1, index[0]), (b2, index[1])):
             full = torch.zeros((len(union),) + tuple(blk.values.shape[1:]), dtype=blk.values.dtype, device="cuda")
-            idx = torch.as_tensor([rows[tuple(v)] for v in labels.values], dtype=torch.long, device="cuda")
             if len(idx):
-                full[idx] = blk.values
+                full[torch.as_tensor(idx, dtype=torch.long, device="cuda")] = blk.values
             out.append(full)
         return samples, out[0], out[1]
     swapped = len(s1.names) > len(s2.names)
