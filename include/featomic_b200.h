@@ -434,6 +434,10 @@ typedef struct featomic_b200_cg_task_t {
     int32_t lambda;
     int32_t n_first;
     int32_t n_second;
+    /* elements between consecutive (sample, mu) rows of `output`; 0 means
+     * n_first * n_second (a dense block).  A larger stride writes the
+     * product into columns of a wider block. */
+    int64_t output_stride;
 } featomic_b200_cg_task_t;
 
 /* Run `n_tasks` block products in one launch on `stream` (NULL = the legacy

@@ -88,6 +88,7 @@ class featomic_b200_cg_task_t(ctypes.Structure):
         ("lambda_", ctypes.c_int32),
         ("n_first", ctypes.c_int32),
         ("n_second", ctypes.c_int32),
+        ("output_stride", ctypes.c_int64),
     ]
 
 

@@ -30,7 +30,9 @@ def cg_coefficients(l1, l2, o3_lambda):
 def cg_tensor_products(tasks, stream=None):
     """Run ``(first, second, output, o3_lambda)`` products (contiguous CUDA
     tensors of one dtype, shapes [s, 2 l1 + 1, p], [s, 2 l2 + 1, q],
-    [s, 2 o3_lambda + 1, p * q]) in one launch."""
+    [s, 2 o3_lambda + 1, p * q]) in one launch.  A task
+    ``(first, second, output, o3_lambda, column)`` writes into the columns
+    ``column .. column + p * q`` of a wider output [s, 2 o3_lambda + 1, w]."""
     import torch
 
     if not tasks:
@@ -39,16 +41,25 @@ def cg_tensor_products(tasks, stream=None):
     if dtype not in (torch.float32, torch.float64):
         raise TypeError("Clebsch-Gordan products take float32 or float64 tensors")
     arr = (C.featomic_b200_cg_task_t * len(tasks))()
-    for k, (a, b, out, lam) in enumerate(tasks):
+    for k, task in enumerate(tasks):
+        a, b, out, lam = task[:4]
+        column = task[4] if len(task) > 4 else None
         for t in (a, b, out):
             if not t.is_cuda or t.dtype != dtype or not t.is_contiguous():
                 raise ValueError("Clebsch-Gordan tensors must be contiguous CUDA tensors of one dtype")
         s, m1, p = a.shape
         _, m2, q = b.shape
-        if b.shape[0] != s or tuple(out.shape) != (s, 2 * lam + 1, p * q):
-            raise ValueError("inconsistent shapes in a Clebsch-Gordan product")
-        arr[k] = C.featomic_b200_cg_task_t(a.data_ptr(), b.data_ptr(), out.data_ptr(), s, (m1 - 1) // 2,
-                                           (m2 - 1) // 2, lam, p, q)
+        if column is None:
+            if b.shape[0] != s or tuple(out.shape) != (s, 2 * lam + 1, p * q):
+                raise ValueError("inconsistent shapes in a Clebsch-Gordan product")
+            ptr, stride = out.data_ptr(), 0
+        else:
+            if b.shape[0] != s or tuple(out.shape[:2]) != (s, 2 * lam + 1) or column < 0 or \
+                    column + p * q > out.shape[2]:
+                raise ValueError("inconsistent shapes in a Clebsch-Gordan product")
+            ptr, stride = out.data_ptr() + column * out.element_size(), out.shape[2]
+        arr[k] = C.featomic_b200_cg_task_t(a.data_ptr(), b.data_ptr(), ptr, s, (m1 - 1) // 2,
+                                           (m2 - 1) // 2, lam, p, q, stride)
     if stream is None:
         stream = torch.cuda.current_stream().cuda_stream
     C.check(C.lib().featomic_b200_cg_product(arr, len(tasks), 64 if dtype == torch.float64 else 32,
@@ -193,6 +204,54 @@ def keys_to_properties(tensor, names, values=None):
     return EquivariantTensorMap(new_keys, blocks)
 
 
+def _products_into_properties(tensor, tasks, names):
+    """``keys_to_properties(tensor, names)`` for a planned, unallocated
+    product: each merged block is allocated once and every task writes its
+    columns of it (no copy of the product)."""
+    import torch
+
+    keys = tensor.keys
+    move = [keys.names.index(n) for n in names]
+    keep = [i for i in range(len(keys.names)) if i not in move]
+    groups, order = {}, []
+    for i, row in enumerate(keys.values):
+        rest = tuple(int(v) for v in row[keep])
+        if rest not in groups:
+            groups[rest] = []
+            order.append(rest)
+        groups[rest].append((tuple(int(v) for v in row[move]), i))
+    blocks, run = [], []
+    for rest in order:
+        members = sorted(groups[rest])
+        first = tensor.block_by_id(members[0][1])
+        for _, i in members[1:]:
+            b = tensor.block_by_id(i)
+            if len(b.samples) != len(first.samples) or not np.array_equal(b.samples.values, first.samples.values):
+                # different samples: allocate every product and merge with zero fill
+                for k, (a, bb, out, lam) in enumerate(tasks):
+                    tasks[k] = (a, bb, torch.empty(out, dtype=a.dtype, device="cuda"), lam)
+                    tensor.block_by_id(k).values = tasks[k][2]
+                cg_tensor_products(tasks)
+                return keys_to_properties(tensor, names)
+        width = sum(tensor.block_by_id(i).properties.values.shape[0] for _, i in members)
+        a0 = tasks[members[0][1]][0]
+        shape = tasks[members[0][1]][2]
+        merged = torch.empty((shape[0], shape[1], width), dtype=a0.dtype, device="cuda")
+        column, props = 0, []
+        for mv, i in members:
+            a, b, _, lam = tasks[i]
+            run.append((a, b, merged, lam, column))
+            p = tensor.block_by_id(i).properties.values
+            props.append(np.concatenate([np.tile(np.asarray(mv, dtype=np.int32), (len(p), 1)), p], axis=1))
+            column += len(p)
+        names_all = list(names) + first.properties.names
+        blocks.append(Block(merged, first.samples, first.components,
+                            Labels(names_all, np.concatenate(props, axis=0))))
+    cg_tensor_products(run)
+    new_keys = Labels([keys.names[i] for i in keep], np.array(order, dtype=np.int32).reshape(len(order), len(keep)))
+    return EquivariantTensorMap(new_keys, blocks)
+
+
 def _filter_redundant_keys(keys):
     """Keep keys with sorted angular orders l_1 <= l_2 <= ...
     (_density_correlations.py:233-272)."""
@@ -264,9 +323,11 @@ class ClebschGordanProduct:
         cg_tensor_products(tasks)
         return result
 
-    def plan(self, tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys=None):
+    def plan(self, tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys=None,
+             allocate=True):
         """(TensorMap with unfilled values, its block-product tasks for
-        ``cg_tensor_products``)."""
+        ``cg_tensor_products``); with ``allocate=False`` the blocks and tasks
+        carry the output shape instead of an output tensor."""
         import torch
 
         self._check_inputs(tensor_1, tensor_2, selected_keys)
@@ -297,7 +358,8 @@ class ClebschGordanProduct:
                            np.concatenate([np.repeat(p1, len(p2), axis=0), np.tile(p2, (len(p1), 1))], axis=1))
             for i in groups[c]:
                 lam = int(keys.values[i][lam_col])
-                out = torch.empty((a.shape[0], 2 * lam + 1, a.shape[2] * b.shape[2]), dtype=a.dtype, device="cuda")
+                shape = (a.shape[0], 2 * lam + 1, a.shape[2] * b.shape[2])
+                out = torch.empty(shape, dtype=a.dtype, device="cuda") if allocate else shape
                 tasks.append((a, b, out, lam))
                 mu = Labels(["o3_mu"], np.arange(-lam, lam + 1, dtype=np.int32).reshape(-1, 1))
                 blocks.append(Block(out, samples, [mu], props))
@@ -415,8 +477,8 @@ class EquivariantPowerSpectrum:
             values = None if self.neighbor_types is None else [[t] for t in self.neighbor_types]
             d1 = keys_to_properties(d1, ["neighbor_1_type"], values)
             d2 = keys_to_properties(d2, ["neighbor_2_type"], values)
-        ps = self._cg_product.compute(d1, d2, "l_1", "l_2", selected_keys)
-        return keys_to_properties(ps, ["l_1", "l_2"])
+        ps, tasks = self._cg_product.plan(d1, d2, "l_1", "l_2", selected_keys, allocate=False)
+        return _products_into_properties(ps, tasks, ["l_1", "l_2"])
 
     forward = compute
 

@@ -132,6 +132,7 @@ struct DeviceCgTask {
     void* output;
     int64_t n_samples;
     int64_t block_start;  // first CTA of this task
+    int64_t out_stride;   // elements between (sample, mu) rows of the output
     int32_t n_first, n_second, lambda;
     int32_t m1_count, m2_count;
     int32_t entries;      // offset of the task's (mu-sorted) coefficient list
@@ -202,10 +203,10 @@ cg_product_kernel(const DeviceCgTask* __restrict__ tasks, int n_tasks, const CgE
     const int pt = (int)(r / nqt), qt = (int)(r - (int64_t)pt * nqt);
     const int p0 = pt * CG_PV, q0 = qt * CG_QV;
     const int np = min(CG_PV, t.n_first - p0), nq = min(CG_QV, t.n_second - q0);
-    const int64_t PQ = (int64_t)t.n_first * t.n_second;
     const T* __restrict__ a = static_cast<const T*>(t.first) + s * t.m1_count * t.n_first + p0;
     const T* __restrict__ b = static_cast<const T*>(t.second) + s * t.m2_count * t.n_second + q0;
-    T* __restrict__ out = static_cast<T*>(t.output) + s * (2 * t.lambda + 1) * PQ + (int64_t)p0 * t.n_second + q0;
+    T* __restrict__ out = static_cast<T*>(t.output) + s * (2 * t.lambda + 1) * t.out_stride +
+                          (int64_t)p0 * t.n_second + q0;
     const bool vec = t.vector && nq == CG_QV;
     const bool vec_first = CG_PV == 8 && t.vector_first && np == CG_PV;
     const int32_t* starts = mu_starts + t.mu_offsets;
@@ -240,7 +241,7 @@ cg_product_kernel(const DeviceCgTask* __restrict__ tasks, int n_tasks, const CgE
                 for (int j = 0; j < CG_QV; j++) acc[i][j] += ca * bv[j];
             }
         }
-        T* orow = out + mu * PQ;
+        T* orow = out + mu * t.out_stride;
 #pragma unroll
         for (int i = 0; i < CG_PV; i++) {
             if (i >= np) break;
@@ -305,6 +306,11 @@ void cg_product(const featomic_b200_cg_task_t* tasks, size_t n_tasks, int precis
         d.output = t.output;
         d.n_samples = t.n_samples;
         d.block_start = blocks;
+        const int64_t pq = (int64_t)t.n_first * t.n_second;
+        if (t.output_stride != 0 && t.output_stride < pq)
+            throw invalid_parameter("output_stride of Clebsch-Gordan task " + std::to_string(i) +
+                                    " is smaller than n_first * n_second");
+        d.out_stride = t.output_stride == 0 ? pq : t.output_stride;
         d.n_first = t.n_first;
         d.n_second = t.n_second;
         d.lambda = t.lambda;
@@ -313,7 +319,7 @@ void cg_product(const featomic_b200_cg_task_t* tasks, size_t n_tasks, int precis
         d.entries = (int32_t)entries.size();
         d.mu_offsets = (int32_t)mu_starts.size();
         const size_t align = 4 * (precision == 64 ? sizeof(double) : sizeof(float));
-        d.vector = t.n_second % CG_QV == 0 && reinterpret_cast<uintptr_t>(t.second) % std::min<size_t>(align, 16) == 0 &&
+        d.vector = t.n_second % CG_QV == 0 && d.out_stride % CG_QV == 0 && reinterpret_cast<uintptr_t>(t.second) % std::min<size_t>(align, 16) == 0 &&
                    reinterpret_cast<uintptr_t>(t.output) % std::min<size_t>(align, 16) == 0;
         d.vector_first = t.n_first % CG_PV == 0 && reinterpret_cast<uintptr_t>(t.first) % 16 == 0;
         entries.insert(entries.end(), sp.entries.begin(), sp.entries.end());
