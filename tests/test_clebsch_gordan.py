@@ -349,3 +349,23 @@ def test_cg_power_spectrum_is_the_soap_power_spectrum():
         np.testing.assert_allclose(factor * cv[:, cols_t], np.asarray(pblk.values), rtol=1e-10, atol=1e-14)
         checked += cv[:, cols].size
     assert checked > 1000
+
+
+def test_cg_product_rejects_bad_tasks():
+    # checked on the host before anything is queued: no device memory is touched
+    import ctypes
+
+    from rascaline_b200 import _c_api as C
+
+    task = C.featomic_b200_cg_task_t(16, 32, 48, 2, 1, 1, 0, 4, 4, 8)
+    arr = (C.featomic_b200_cg_task_t * 1)(task)
+    assert C.lib().featomic_b200_cg_product(arr, 1, 64, None) == 1
+    assert "smaller than n_first * n_second" in C.lib().featomic_last_error().decode()
+    task.output_stride = 0
+    task.lambda_ = 3
+    arr = (C.featomic_b200_cg_task_t * 1)(task)
+    assert C.lib().featomic_b200_cg_product(arr, 1, 64, None) == 1
+    assert "can not couple" in C.lib().featomic_last_error().decode()
+    assert C.lib().featomic_b200_cg_product(arr, 1, 16, None) == 1
+    assert "precision must be 32 or 64" in C.lib().featomic_last_error().decode()
+    assert C.lib().featomic_b200_cg_product(None, 0, 64, None) == 0
