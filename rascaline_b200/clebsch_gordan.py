@@ -69,11 +69,20 @@ def cg_tensor_products(tasks, stream=None):
 class Block:
     """values (torch CUDA tensor [samples, components..., properties]) with its labels."""
 
-    def __init__(self, values, samples, components, properties):
+    def __init__(self, values, samples, components, properties, gradients=None):
         self.values = values
         self.samples = samples
         self.components = components
         self.properties = properties
+        self._gradients = dict(gradients or {})
+
+    def gradients_list(self):
+        return list(self._gradients)
+
+    def gradient(self, parameter):
+        if parameter not in self._gradients:
+            raise ValueError(f"this block has no gradient with respect to {parameter}")
+        return self._gradients[parameter]
 
 
 class EquivariantTensorMap:
@@ -565,14 +574,63 @@ class DensityCorrelations:
 
 
 
+def _moved_with_gradients(tm, types, dtype):
+    """keys_to_properties(neighbor_type) of a spherical expansion with its
+    positions gradients: per (o3_lambda, o3_sigma, center_type), values
+    [samples, 2l+1, types * n] and gradients [gradient samples, 3, 2l+1,
+    types * n], absent types zero; gradient samples (sample, system, atom)
+    are the union over the merged blocks, "sample" renumbered to the merged
+    samples."""
+    import torch
+
+    keys = tm.keys
+    nt = keys.names.index("neighbor_type")
+    groups, order = {}, []
+    for i, row in enumerate(keys.values):
+        rest = (int(row[0]), int(row[1]), int(row[2]))
+        if rest not in groups:
+            groups[rest] = {}
+            order.append(rest)
+        groups[rest][int(row[nt])] = i
+    out_keys, blocks = [], []
+    for rest in order:
+        present = [(k, tm.block_by_id(groups[rest][t])) for k, t in enumerate(types) if t in groups[rest]]
+        union, index = _union_rows([b.samples.values for _, b in present])
+        ref = present[0][1]
+        M, N = ref.values.shape[1], ref.values.shape[2]
+        values = torch.zeros((len(union), M, len(types) * N), dtype=dtype, device="cuda")
+        grads = []
+        for (k, b), ix in zip(present, index):
+            ixt = torch.as_tensor(ix, device="cuda", dtype=torch.long)
+            values[ixt, :, k * N:(k + 1) * N] = torch.as_tensor(np.ascontiguousarray(b.values)).to("cuda", dtype)
+            g = b.gradient("positions")
+            gs = np.array(g.samples.values, dtype=np.int32).reshape(-1, 3)
+            gs[:, 0] = ix[gs[:, 0]]
+            grads.append((k, gs, g.values))
+        gunion, gindex = _union_rows([gs for _, gs, _ in grads])
+        gvalues = torch.zeros((len(gunion), 3, M, len(types) * N), dtype=dtype, device="cuda")
+        for (k, gs, gv), gi in zip(grads, gindex):
+            if len(gi):
+                gvalues[torch.as_tensor(gi, device="cuda", dtype=torch.long), :, :, k * N:(k + 1) * N] = \
+                    torch.as_tensor(np.ascontiguousarray(gv)).to("cuda", dtype)
+        props = np.array([[t, int(n)] for t in types for n in ref.properties.values[:, 0]], dtype=np.int32)
+        grad = Block(gvalues, Labels(["sample", "system", "atom"], gunion.reshape(-1, 3)), [], None)
+        blocks.append(Block(values, Labels(ref.samples.names, union), ref.components,
+                            Labels(["neighbor_type", "n"], props), {"positions": grad}))
+        out_keys.append(list(rest))
+    return EquivariantTensorMap(Labels(["o3_lambda", "o3_sigma", "center_type"], np.array(out_keys, dtype=np.int32)),
+                                blocks)
+
+
 class PowerSpectrum:
     """The invariant power spectrum of featomic's Clebsch-Gordan module
     (python/featomic/featomic/clebsch_gordan/_power_spectrum.py:27-352):
     keys (center_type), properties (l, neighbor_1_type, n_1, neighbor_2_type,
     n_2), values (-1)^l / sqrt(2l + 1) sum_m c1[m, a] c2[m, b] -- the
     lambda = 0 product of the two l blocks, computed by the Clebsch-Gordan
-    kernel (its lambda = 0 coefficients are that factor).  Values only:
-    positions gradients are not built."""
+    kernel (its lambda = 0 coefficients are that factor).  Positions
+    gradients (_power_spectrum.py:373-435) are two more lambda = 0 products
+    per block: dc1 x c2 and c1 x dc2 on the gradient samples."""
 
     def __init__(self, calculator_1, calculator_2=None, neighbor_types=None, *, dtype=None, device=None):
         import torch
@@ -603,6 +661,11 @@ class PowerSpectrum:
         d = keys_to_properties(as_tensormap(tm, self.dtype), ["neighbor_type"], values)
         return _increment_property_names(d, suffix)
 
+    def _types(self, tm):
+        if self.neighbor_types is None:
+            return [int(t) for t in np.unique(tm.keys.column("neighbor_type"))]
+        return list(self.neighbor_types)
+
     def compute(self, systems, gradients=None, use_native_system=True):
         """_power_spectrum.py:196-351."""
         import torch
@@ -611,7 +674,7 @@ class PowerSpectrum:
             for parameter in gradients:
                 if parameter != "positions":
                     raise NotImplementedError("PowerSpectrum currently only supports gradients w.r.t. to positions")
-            raise NotImplementedError("positions gradients of PowerSpectrum are not implemented in featomic-b200")
+            return self._compute_with_gradients(systems)
         d1 = self._density(self.calculator_1, systems, 1)
         d2 = d1 if self.calculator_2 is None else self._density(self.calculator_2, systems, 1)
         d2 = _increment_property_names(d2, 1)
@@ -640,3 +703,85 @@ class PowerSpectrum:
         return keys_to_properties(tm, ["l"])
 
     forward = compute
+
+    def _compute_with_gradients(self, systems):
+        import torch
+
+        tm1 = self.calculator_1.compute(systems, gradients=["positions"])
+        d1 = _moved_with_gradients(tm1, self._types(tm1), self.dtype)
+        if self.calculator_2 is None:
+            d2 = d1
+        else:
+            tm2 = self.calculator_2.compute(systems, gradients=["positions"])
+            d2 = _moved_with_gradients(tm2, self._types(tm2), self.dtype)
+        tasks, pending = [], []
+        for i, key in enumerate(d1.keys.values):
+            lam, ct = int(key[0]), int(key[2])
+            b1 = d1.block_by_id(i)
+            for j, key2 in enumerate(d2.keys.values):
+                if int(key2[0]) != lam or int(key2[2]) != ct:
+                    continue
+                b2 = d2.block_by_id(j)
+                if len(b1.samples) != len(b2.samples) or not np.array_equal(b1.samples.values, b2.samples.values):
+                    raise ValueError("the two spherical expansions have different samples")
+                c1, c2 = b1.values, b2.values
+                S, M, P = c1.shape
+                Q = c2.shape[2]
+                out = torch.empty((S, 1, P * Q), dtype=c1.dtype, device="cuda")
+                tasks.append((c1, c2, out, 0))
+                g1, g2 = b1.gradient("positions"), b2.gradient("positions")
+                gs1, gs2 = g1.samples.values, g2.samples.values
+                grad = None
+                if len(gs1) and len(gs2):
+                    # dc1[g, x] x c2[sample(g)] and c1[sample(g)] x dc2[g, x], (g, x) as samples
+                    r1 = torch.as_tensor(gs1[:, 0], device="cuda", dtype=torch.long).repeat_interleave(3)
+                    r2 = torch.as_tensor(gs2[:, 0], device="cuda", dtype=torch.long).repeat_interleave(3)
+                    o1 = torch.empty((len(gs1) * 3, 1, P * Q), dtype=c1.dtype, device="cuda")
+                    o2 = torch.empty((len(gs2) * 3, 1, P * Q), dtype=c1.dtype, device="cuda")
+                    tasks.append((g1.values.reshape(-1, M, P), c2[r1].contiguous(), o1, 0))
+                    tasks.append((c1[r2].contiguous(), g2.values.reshape(-1, M, Q), o2, 0))
+                    grad = (gs1, gs2, o1, o2)
+                p1, p2 = b1.properties.values, b2.properties.values
+                props = np.concatenate([np.repeat(p1, len(p2), axis=0), np.tile(p2, (len(p1), 1))], axis=1)
+                pending.append((lam, ct, b1.samples, out, props, grad))
+        cg_tensor_products(tasks)
+        # keys_to_properties("l"): one block per centre type, l-major properties
+        groups, order = {}, []
+        for entry in pending:
+            if entry[1] not in groups:
+                groups[entry[1]] = []
+                order.append(entry[1])
+            groups[entry[1]].append(entry)
+        xyz = Labels(["xyz"], np.arange(3, dtype=np.int32).reshape(-1, 1))
+        blocks = []
+        for ct in order:
+            members = sorted(groups[ct], key=lambda e: e[0])
+            samples = members[0][2]
+            values = torch.cat([e[3].reshape(e[3].shape[0], -1) for e in members], dim=1)
+            props = np.concatenate([np.concatenate([np.full((len(e[4]), 1), e[0], dtype=np.int32), e[4]], axis=1)
+                                    for e in members], axis=0)
+            parts = []
+            for e in members:
+                if e[5] is None:
+                    parts.append((np.zeros((0, 3), dtype=np.int32), None, e[4].shape[0]))
+                    continue
+                gs1, gs2, o1, o2 = e[5]
+                gunion, (i1, i2) = _union_rows([gs1, gs2])
+                gv = torch.zeros((len(gunion), 3, o1.shape[2]), dtype=o1.dtype, device="cuda")
+                gv[torch.as_tensor(i1, device="cuda", dtype=torch.long)] += o1.reshape(len(gs1), 3, -1)
+                gv[torch.as_tensor(i2, device="cuda", dtype=torch.long)] += o2.reshape(len(gs2), 3, -1)
+                parts.append((gunion, gv, e[4].shape[0]))
+            gunion, gindex = _union_rows([p[0] for p in parts])
+            width = sum(p[2] for p in parts)
+            gvalues = torch.zeros((len(gunion), 3, width), dtype=values.dtype, device="cuda")
+            column = 0
+            for (rows, gv, w), gi in zip(parts, gindex):
+                if gv is not None and len(gi):
+                    gvalues[torch.as_tensor(gi, device="cuda", dtype=torch.long), :, column:column + w] = gv
+                column += w
+            names = ["l", "neighbor_1_type", "n_1", "neighbor_2_type", "n_2"]
+            prop_labels = Labels(names, props)
+            grad = Block(gvalues, Labels(["sample", "system", "atom"], gunion.reshape(-1, 3)), [xyz], prop_labels)
+            blocks.append(Block(values, samples, [], prop_labels, {"positions": grad}))
+        return EquivariantTensorMap(Labels(["center_type"], np.array(order, dtype=np.int32).reshape(-1, 1)), blocks)
+

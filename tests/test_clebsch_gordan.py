@@ -313,13 +313,11 @@ def test_density_correlations_nu3():
     np.testing.assert_allclose(got.values.cpu().numpy(), ref, rtol=0, atol=1e-12 * max(1.0, np.abs(ref).max()))
 
 
-def test_power_spectrum_gradients_not_built():
+def test_power_spectrum_gradient_parameters():
     se = rb.SphericalExpansion(**workloads.hypers(3.0, 2, 2))
     ps = cg.PowerSpectrum(se)
     with pytest.raises(NotImplementedError, match="only supports gradients w.r.t. to positions"):
         ps.compute([workloads.random_box(10, seed=1)], gradients=["strain"])
-    with pytest.raises(NotImplementedError, match="not implemented in featomic-b200"):
-        ps.compute([workloads.random_box(10, seed=1)], gradients=["positions"])
 
 
 @pytest.mark.gpu
@@ -369,3 +367,38 @@ def test_cg_product_rejects_bad_tasks():
     assert C.lib().featomic_b200_cg_product(arr, 1, 16, None) == 1
     assert "precision must be 32 or 64" in C.lib().featomic_last_error().decode()
     assert C.lib().featomic_b200_cg_product(None, 0, 64, None) == 0
+
+
+@pytest.mark.gpu
+def test_cg_power_spectrum_positions_gradients():
+    # _power_spectrum.py:373-435 against the drop-in power spectrum's gradient
+    # rows (pinned to featomic's goldens), matched by (centre, atom)
+    system = workloads.random_box(40, density=0.1, species=(1, 8), seed=14)
+    se = rb.SphericalExpansion(**_ps_hypers())
+    out = cg.PowerSpectrum(se).compute([system], gradients=["positions"])
+    ps = rb.SoapPowerSpectrum(**_ps_hypers()).compute([system], gradients=["positions"])
+    checked = 0
+    for key, pblk in zip(ps.keys.values, ps.blocks()):
+        ct, n1, n2 = (int(v) for v in key)
+        cblk = out.block(center_type=ct)
+        cgrad = cblk.gradient("positions")
+        assert cgrad.components[0].names == ["xyz"]
+        props = {tuple(p): i for i, p in enumerate(cblk.properties.values)}
+        cols = [props[(l, n1, a, n2, b)] for l, a, b in pblk.properties.values]
+        crow = {(tuple(cblk.samples.values[g[0]]), int(g[2])): i for i, g in enumerate(cgrad.samples.values)}
+        pgrad = pblk.gradient("positions")
+        pv = np.asarray(pgrad.values)
+        cv = cgrad.values.cpu().numpy()
+        factor = 1.0 if n1 == n2 else np.sqrt(2.0)
+        for i, g in enumerate(pgrad.samples.values):
+            row = crow[(tuple(pblk.samples.values[g[0]]), int(g[2]))]
+            np.testing.assert_allclose(factor * cv[row][:, cols], pv[i], rtol=1e-9,
+                                       atol=1e-12 * max(1.0, np.abs(pv).max()))
+            checked += 1
+    assert checked > 100
+    # the values are those of the values-only call
+    plain = cg.PowerSpectrum(se).compute([system])
+    for i in range(len(out)):
+        np.testing.assert_array_equal(out.block_by_id(i).values.cpu().numpy(),
+                                      plain.block_by_id(i).values.cpu().numpy())
+
