@@ -213,7 +213,7 @@ def keys_to_properties(tensor, names, values=None):
     return EquivariantTensorMap(new_keys, blocks)
 
 
-def _products_into_properties(tensor, tasks, names):
+def _products_into_properties(tensor, tasks, names, launch=True):
     """``keys_to_properties(tensor, names)`` for a planned, unallocated
     product: each merged block is allocated once and every task writes its
     columns of it (no copy of the product)."""
@@ -240,7 +240,8 @@ def _products_into_properties(tensor, tasks, names):
                 for k, (a, bb, out, lam) in enumerate(tasks):
                     tasks[k] = (a, bb, torch.empty(out, dtype=a.dtype, device="cuda"), lam)
                     tensor.block_by_id(k).values = tasks[k][2]
-                cg_tensor_products(tasks)
+                if launch:
+                    cg_tensor_products(tasks)
                 return keys_to_properties(tensor, names)
         width = sum(tensor.block_by_id(i).properties.values.shape[0] for _, i in members)
         a0 = tasks[members[0][1]][0]
@@ -256,7 +257,8 @@ def _products_into_properties(tensor, tasks, names):
         names_all = list(names) + first.properties.names
         blocks.append(Block(merged, first.samples, first.components,
                             Labels(names_all, np.concatenate(props, axis=0))))
-    cg_tensor_products(run)
+    if launch:
+        cg_tensor_products(run)
     new_keys = Labels([keys.names[i] for i in keep], np.array(order, dtype=np.int32).reshape(len(order), len(keep)))
     return EquivariantTensorMap(new_keys, blocks)
 
@@ -330,6 +332,14 @@ class ClebschGordanProduct:
         """The product TensorMap (_cg_product.py:139-212 / :262-334)."""
         result, tasks = self.plan(tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys)
         cg_tensor_products(tasks)
+        return result
+
+    def compute_metadata(self, tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name,
+                         selected_keys=None):
+        """The product's keys, samples, components and properties, with
+        uninitialised values of the right shapes and no product computed
+        (_cg_product.py:238-260)."""
+        result, _ = self.plan(tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys)
         return result
 
     def plan(self, tensor_1, tensor_2, o3_lambda_1_new_name, o3_lambda_2_new_name, selected_keys=None,
@@ -476,7 +486,12 @@ class EquivariantPowerSpectrum:
     def name(self):
         return "EquivariantPowerSpectrum"
 
-    def compute(self, systems, selected_keys=None, neighbors_to_properties=False):
+    def compute_metadata(self, systems, selected_keys=None, neighbors_to_properties=False):
+        """Metadata of ``compute`` with uninitialised values, without the
+        Clebsch-Gordan products (_equivariant_power_spectrum.py:276-294)."""
+        return self.compute(systems, selected_keys, neighbors_to_properties, _metadata=True)
+
+    def compute(self, systems, selected_keys=None, neighbors_to_properties=False, _metadata=False):
         """_equivariant_power_spectrum.py:215-256 / :296-365."""
         density_1 = self.calculator_1.compute(systems)
         density_2 = density_1 if self.calculator_2 is None else self.calculator_2.compute(systems)
@@ -487,7 +502,7 @@ class EquivariantPowerSpectrum:
             d1 = keys_to_properties(d1, ["neighbor_1_type"], values)
             d2 = keys_to_properties(d2, ["neighbor_2_type"], values)
         ps, tasks = self._cg_product.plan(d1, d2, "l_1", "l_2", selected_keys, allocate=False)
-        return _products_into_properties(ps, tasks, ["l_1", "l_2"])
+        return _products_into_properties(ps, tasks, ["l_1", "l_2"], launch=not _metadata)
 
     forward = compute
 
@@ -549,7 +564,12 @@ class DensityCorrelations:
         self._cg_product = ClebschGordanProduct(max_angular=max_angular,
                                                 keys_filter=_filter_redundant_keys if skip_redundant else None)
 
-    def compute(self, density, angular_cutoff=None, selected_keys=None):
+    def compute_metadata(self, density, angular_cutoff=None, selected_keys=None):
+        """Metadata of ``compute`` with uninitialised values
+        (_density_correlations.py:140-158)."""
+        return self.compute(density, angular_cutoff, selected_keys, _metadata=True)
+
+    def compute(self, density, angular_cutoff=None, selected_keys=None, _metadata=False):
         """_density_correlations.py:70-120 / :160-231; ``density`` is a
         calculator TensorMap or an ``EquivariantTensorMap``."""
         if not isinstance(density, EquivariantTensorMap):
@@ -567,7 +587,10 @@ class DensityCorrelations:
                 selection = None
             else:
                 selection = Labels(["o3_lambda"], np.arange(angular_cutoff + 1, dtype=np.int32).reshape(-1, 1))
-            correlations = self._cg_product.compute(correlations, density, name_1, name_2, selection)
+            if _metadata:
+                correlations = self._cg_product.compute_metadata(correlations, density, name_1, name_2, selection)
+            else:
+                correlations = self._cg_product.compute(correlations, density, name_1, name_2, selection)
         return correlations
 
     forward = compute

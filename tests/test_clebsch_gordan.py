@@ -402,3 +402,24 @@ def test_cg_power_spectrum_positions_gradients():
         np.testing.assert_array_equal(out.block_by_id(i).values.cpu().numpy(),
                                       plain.block_by_id(i).values.cpu().numpy())
 
+
+@pytest.mark.gpu
+def test_compute_metadata_matches_compute():
+    system = workloads.random_box(30, density=0.1, species=(1, 8), seed=15)
+    hypers = workloads.hypers(3.5, 2, 2, spline_accuracy=None)
+    se = rb.SphericalExpansion(**hypers)
+    eps = cg.EquivariantPowerSpectrum(se)
+    density, _ = _moved_density(system, hypers)
+    dc = cg.DensityCorrelations(n_correlations=2, max_angular=6)
+    for full, meta in ((eps.compute([system]), eps.compute_metadata([system])),
+                       (eps.compute([system], neighbors_to_properties=True),
+                        eps.compute_metadata([system], neighbors_to_properties=True)),
+                       (dc.compute(density, angular_cutoff=2), dc.compute_metadata(density, angular_cutoff=2))):
+        np.testing.assert_array_equal(full.keys.values, meta.keys.values)
+        assert full.keys.names == meta.keys.names
+        for a, b in zip(full.blocks(), meta.blocks()):
+            assert tuple(a.values.shape) == tuple(b.values.shape)
+            np.testing.assert_array_equal(a.samples.values, b.samples.values)
+            np.testing.assert_array_equal(a.properties.values, b.properties.values)
+            assert a.properties.names == b.properties.names
+
