@@ -22,7 +22,7 @@ contraction, every row materialised in featomic's TensorMap layout.
 * ``surrogate_form`` the learned radial surrogate (MLP trained on the GPU,
   tcgen05 inference) against the spline, on a 100 000-atom box, with errors
   against FP64.
-* ``--only cg`` the equivariant power spectrum (lambda-SOAP) of the same box:
+* ``cg_form`` the equivariant power spectrum (lambda-SOAP) of the same box:
   every Clebsch-Gordan block product in one launch, FP64.
 * ``cpu_baseline`` / ``--impl reference``: featomic itself is Rust and cannot
   be built here (no cargo / crates), so the CPU side is the FP64 C++
@@ -772,6 +772,7 @@ def main():
         line["adjoint_form"]["gpu_launches_per_step"] = 22
         line["batched_form"] = batched_form(args.steps, args.warmup)
         line["surrogate_form"] = surrogate_form(min(args.steps, 5), args.warmup, args.train_steps)
+        line["cg_form"] = cg_form(min(args.steps, 10), args.warmup)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(system, hypers)
     print(json.dumps(line), flush=True)
