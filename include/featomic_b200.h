@@ -446,6 +446,23 @@ typedef struct featomic_b200_cg_task_t {
 featomic_status_t featomic_b200_cg_product(const featomic_b200_cg_task_t* tasks, uintptr_t n_tasks,
                                            int32_t precision, void* stream);
 
+/* One coupling of two spherical axes (_coefficients.py:387-545, cg_couple):
+ * output[o][mu][i] = sum_{m1, m2} C[m1][m2][mu] input[o][m1][m2][i], all
+ * device memory, contiguous. */
+typedef struct featomic_b200_cg_couple_task_t {
+    const void* input;  /* [n_outer][2 l1 + 1][2 l2 + 1][n_inner] */
+    void* output;       /* [n_outer][2 lambda + 1][n_inner] */
+    int64_t n_outer;
+    int64_t n_inner;
+    int32_t l1;
+    int32_t l2;
+    int32_t lambda;
+} featomic_b200_cg_couple_task_t;
+
+/* Run `n_tasks` couplings in one launch on `stream`, precision 32 or 64. */
+featomic_status_t featomic_b200_cg_couple(const featomic_b200_cg_couple_task_t* tasks, uintptr_t n_tasks,
+                                          int32_t precision, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

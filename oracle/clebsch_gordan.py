@@ -64,3 +64,11 @@ def cg_tensor_product(a, b, lam):
     outer = np.einsum("sxp,syq->spqxy", a, b).reshape(s * p * q, -1)
     out = outer @ real_cg(l1, l2, lam).reshape(-1, 2 * lam + 1)
     return out.reshape(s, p * q, 2 * lam + 1).transpose(0, 2, 1)
+
+
+def cg_couple(x, lam):
+    """_coefficients.py:387-545 (cg_couple): x [b, 2 l1 + 1, 2 l2 + 1, a]
+    -> [b, 2 lam + 1, a]."""
+    l1 = (x.shape[1] - 1) // 2
+    l2 = (x.shape[2] - 1) // 2
+    return np.einsum("xyz,bxya->bza", real_cg(l1, l2, lam), x)

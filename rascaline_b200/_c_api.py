@@ -92,6 +92,19 @@ class featomic_b200_cg_task_t(ctypes.Structure):
     ]
 
 
+
+class featomic_b200_cg_couple_task_t(ctypes.Structure):
+    _fields_ = [
+        ("input", ctypes.c_void_p),
+        ("output", ctypes.c_void_p),
+        ("n_outer", ctypes.c_int64),
+        ("n_inner", ctypes.c_int64),
+        ("l1", ctypes.c_int32),
+        ("l2", ctypes.c_int32),
+        ("lambda_", ctypes.c_int32),
+    ]
+
+
 # every symbol declared in include/featomic_b200.h: name -> (restype, argtypes)
 SIGNATURES = {
     "featomic_last_error": (ctypes.c_char_p, []),
@@ -182,6 +195,8 @@ SIGNATURES = {
                                                           ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
     "featomic_b200_cg_product": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
                                                      ctypes.c_void_p]),
+    "featomic_b200_cg_couple": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
+                                                    ctypes.c_void_p]),
     "featomic_b200_calculator_timings": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                              ctypes.c_size_t]),
 }

@@ -808,3 +808,152 @@ class PowerSpectrum:
             blocks.append(Block(values, samples, [], prop_labels, {"positions": grad}))
         return EquivariantTensorMap(Labels(["center_type"], np.array(order, dtype=np.int32).reshape(-1, 1)), blocks)
 
+
+
+def cg_couple(tasks, stream=None):
+    """Run ``(input, output, l1, l2, o3_lambda)`` couplings (contiguous CUDA
+    tensors of one dtype, input [outer, 2 l1 + 1, 2 l2 + 1, inner], output
+    [outer, 2 o3_lambda + 1, inner]) in one launch
+    (_coefficients.py:387-545, cg_couple)."""
+    import torch
+
+    if not tasks:
+        return
+    dtype = tasks[0][0].dtype
+    if dtype not in (torch.float32, torch.float64):
+        raise TypeError("Clebsch-Gordan couplings take float32 or float64 tensors")
+    arr = (C.featomic_b200_cg_couple_task_t * len(tasks))()
+    for k, (x, out, l1, l2, lam) in enumerate(tasks):
+        for t in (x, out):
+            if not t.is_cuda or t.dtype != dtype or not t.is_contiguous():
+                raise ValueError("Clebsch-Gordan tensors must be contiguous CUDA tensors of one dtype")
+        if x.ndim != 4 or x.shape[1] != 2 * l1 + 1 or x.shape[2] != 2 * l2 + 1 or \
+                tuple(out.shape) != (x.shape[0], 2 * lam + 1, x.shape[3]):
+            raise ValueError("inconsistent shapes in a Clebsch-Gordan coupling")
+        arr[k] = C.featomic_b200_cg_couple_task_t(x.data_ptr(), out.data_ptr(), x.shape[0], x.shape[3], l1, l2, lam)
+    if stream is None:
+        stream = torch.cuda.current_stream().cuda_stream
+    C.check(C.lib().featomic_b200_cg_couple(arr, len(tasks), 64 if dtype == torch.float64 else 32,
+                                            ctypes.c_void_p(stream)))
+
+
+def _insert(labels, name, value):
+    return Labels([name] + labels.names,
+                  np.concatenate([np.full((len(labels), 1), value, dtype=np.int32), labels.values], axis=1))
+
+
+def cartesian_to_spherical(tensor, components, keep_l_in_keys=None, remove_blocks_threshold=1e-9):
+    """A tensor with Cartesian (xyz) components in spherical form
+    (_cartesian_spherical.py:21-304): the xyz axes become (y, z, x) = real
+    l = 1 components, then the last two converted axes are coupled with
+    Clebsch-Gordan coefficients until one o3_mu axis is left; keys gain
+    o3_lambda, o3_sigma (and l_i / k_i with ``keep_l_in_keys``); blocks whose
+    squared norm is at most ``remove_blocks_threshold`` are dropped."""
+    import torch
+
+    if len(tensor) == 0 or len(components) == 0:
+        return tensor
+    if not isinstance(components, list):
+        raise TypeError(f"`components` should be a list, got {type(components)}")
+    if keep_l_in_keys is None:
+        keep_l_in_keys = len(components) >= 3
+    first = tensor.block_by_id(0)
+    names = [c.names[0] for c in first.components]
+    axes = []
+    for component in components:
+        if component not in names:
+            raise ValueError(f"'{component}' is not part of this tensor components")
+        axes.append(names.index(component) + 1)
+    for key, block in zip(tensor.keys.values, tensor.blocks()):
+        for idx in axes:
+            values = [int(v) for v in block.components[idx - 1].values[:, 0]]
+            if values != [0, 1, 2]:
+                raise ValueError(f"component '{block.components[idx - 1].names[0]}' in block for key {list(key)} "
+                                 f"should have [0, 1, 2] as values, got {values} instead")
+    if list(range(axes[0], axes[-1] + 1)) != axes:
+        raise ValueError(f"this function only supports consecutive components, {components} are not")
+    if "o3_lambda" in tensor.keys.names:
+        raise ValueError("this tensor already has an `o3_lambda` key, is it already in spherical form?")
+    for i in range(len(components)):
+        if f"l_{i}" in tensor.keys.names:
+            raise ValueError(f"this tensor already has an `l_{i}` key, is it already in spherical form?")
+    if len(components) > 2 and not keep_l_in_keys:
+        raise ValueError("`keep_l_in_keys` must be `True` for tensors of rank 3 and above")
+
+    blocks = []
+    for block in tensor.blocks():
+        values = block.values
+        if isinstance(values, np.ndarray):
+            values = torch.as_tensor(np.ascontiguousarray(values))
+        values = values.to("cuda")
+        values = torch.roll(values, shifts=[-1] * len(axes), dims=axes).contiguous()
+        comps = []
+        for idx, comp in enumerate(block.components):
+            if idx + 1 in axes:
+                name = "o3_mu" if len(axes) == 1 else f"__internal_to_convert_{idx}"
+                comps.append(Labels([name], np.array([[-1], [0], [1]], dtype=np.int32)))
+            else:
+                comps.append(comp)
+        blocks.append(Block(values, block.samples, comps, block.properties))
+    keys = tensor.keys
+    if len(axes) == 1:
+        if keep_l_in_keys:
+            keys = _insert(keys, "l_1", 1)
+        keys = _insert(_insert(keys, "o3_sigma", 1), "o3_lambda", 1)
+        return EquivariantTensorMap(keys, blocks)
+    current = EquivariantTensorMap(keys, blocks)
+    iteration = 0
+    while len(axes) > 1:
+        current = _do_coupling(current, axes[-2] - 1, axes[-1] - 1, keep_l_in_keys, iteration)
+        axes.pop()
+        iteration += 1
+    if remove_blocks_threshold is None:
+        return current
+    kept = [i for i, b in enumerate(current.blocks()) if float((b.values * b.values).sum()) > remove_blocks_threshold]
+    return EquivariantTensorMap(Labels(current.keys.names, current.keys.values[kept]),
+                                [current.block_by_id(i) for i in kept])
+
+
+def _do_coupling(tensor, component_1, component_2, keep_l_in_keys, iteration):
+    """_cartesian_spherical.py:307-444: couple two consecutive spherical
+    component axes of every block to every allowed lambda."""
+    import torch
+
+    assert component_2 == component_1 + 1
+    keys = tensor.keys
+    if "o3_lambda" in keys.names:
+        old_sigmas = keys.column("o3_sigma").copy()
+        keep = [i for i, n in enumerate(keys.names) if n != "o3_sigma"]
+        keys = Labels([keys.names[i] for i in keep], keys.values[:, keep])
+    else:
+        old_sigmas = np.ones(len(keys), dtype=np.int32)
+    if keep_l_in_keys:
+        if "o3_lambda" in keys.names:
+            keys = Labels([f"k_{iteration}" if n == "o3_lambda" else n for n in keys.names], keys.values)
+            keys = _insert(keys, f"l_{iteration + 2}", 1)
+        else:
+            keys = _insert(_insert(keys, "l_1", 1), "l_2", 1)
+    new_values, new_blocks, tasks = [], [], []
+    for k, block in enumerate(tensor.blocks()):
+        shape = tuple(block.values.shape)
+        l1 = (shape[component_1 + 1] - 1) // 2
+        l2 = (shape[component_2 + 1] - 1) // 2
+        before = int(np.prod(shape[:component_1 + 1]))
+        after = int(np.prod(shape[component_2 + 2:]))
+        x = block.values.reshape(before, shape[component_1 + 1], shape[component_2 + 1], after)
+        for lam in range(abs(l1 - l2), l1 + l2 + 1):
+            sigma = int(old_sigmas[k]) * (-1) ** (l1 + l2 + lam)
+            new_values.append([lam, sigma] + [int(v) for v in keys.values[k]])
+            out = torch.empty((before, 2 * lam + 1, after), dtype=x.dtype, device="cuda")
+            tasks.append((x, out, l1, l2, lam))
+            new_shape = list(shape)
+            new_shape.pop(component_2 + 1)
+            new_shape[component_1 + 1] = 2 * lam + 1
+            comps = list(block.components)
+            comps.pop(component_2)
+            comps[component_1] = Labels(["o3_mu"], np.arange(-lam, lam + 1, dtype=np.int32).reshape(-1, 1))
+            new_blocks.append(Block(out.view(new_shape), block.samples, comps, block.properties))
+    cg_couple(tasks)
+    return EquivariantTensorMap(Labels(["o3_lambda", "o3_sigma"] + keys.names,
+                                       np.array(new_values, dtype=np.int32).reshape(len(new_values), -1)),
+                                new_blocks)

@@ -959,4 +959,13 @@ featomic_status_t featomic_b200_cg_product(const featomic_b200_cg_task_t* tasks,
     });
 }
 
+featomic_status_t featomic_b200_cg_couple(const featomic_b200_cg_couple_task_t* tasks, uintptr_t n_tasks,
+                                          int32_t precision, void* stream) {
+    return guarded([&] {
+        if (n_tasks == 0) return;
+        CHECK_POINTER(tasks);
+        fb200::cg_couple(tasks, (size_t)n_tasks, precision, static_cast<cudaStream_t>(stream));
+    });
+}
+
 }  // extern "C"

@@ -256,6 +256,46 @@ cg_product_kernel(const DeviceCgTask* __restrict__ tasks, int n_tasks, const CgE
     }
 }
 
+struct DeviceCoupleTask {
+    const void* input;
+    void* output;
+    int64_t n_outer, n_inner;
+    int64_t block_start;
+    int32_t m1_count, m2_count, lambda;
+    int32_t entries, mu_offsets;
+};
+
+// Coupling of two spherical axes of one array: one thread per (outer,
+// inner) index, out[o, mu, i] = sum_k C_k * x[o, m1_k, m2_k, i] over the
+// non-zero coefficients of mu in table order; loads and stores coalesced
+// along the inner index.
+template <typename T>
+__global__ void __launch_bounds__(CG_THREADS)
+cg_couple_kernel(const DeviceCoupleTask* __restrict__ tasks, int n_tasks, const CgEntry* __restrict__ entries,
+                 const int32_t* __restrict__ mu_starts) {
+    int lo = 0, hi = n_tasks - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (tasks[mid].block_start <= (int64_t)blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    const DeviceCoupleTask t = tasks[lo];
+    const int64_t item = ((int64_t)blockIdx.x - t.block_start) * CG_THREADS + threadIdx.x;
+    if (item >= t.n_outer * t.n_inner) return;
+    const int64_t o = item / t.n_inner, i = item - o * t.n_inner;
+    const T* __restrict__ x = static_cast<const T*>(t.input) + o * t.m1_count * t.m2_count * t.n_inner + i;
+    T* __restrict__ out = static_cast<T*>(t.output) + o * (2 * t.lambda + 1) * t.n_inner + i;
+    const int32_t* starts = mu_starts + t.mu_offsets;
+    const CgEntry* e = entries + t.entries;
+    for (int mu = 0; mu <= 2 * t.lambda; mu++) {
+        T acc = T(0);
+        for (int k = starts[mu]; k < starts[mu + 1]; k++) {
+            const CgEntry c = e[k];
+            acc += T(c.value) * x[((int64_t)c.m1 * t.m2_count + c.m2) * t.n_inner];
+        }
+        out[mu * t.n_inner] = acc;
+    }
+}
+
 // Non-zero real CG coefficients of (l1, l2, lambda), grouped by mu, cached.
 struct SparseCg {
     std::vector<CgEntry> entries;
@@ -351,6 +391,62 @@ void cg_product(const featomic_b200_cg_task_t* tasks, size_t n_tasks, int precis
         cg_product_kernel<double><<<(unsigned)blocks, CG_THREADS, 0, stream>>>(d_tasks, (int)dev.size(), d_entries, d_mu);
     else
         cg_product_kernel<float><<<(unsigned)blocks, CG_THREADS, 0, stream>>>(d_tasks, (int)dev.size(), d_entries, d_mu);
+    CUDA_CHECK(cudaGetLastError());
+    CUDA_CHECK(cudaFreeAsync(buffer, stream));
+}
+
+void cg_couple(const featomic_b200_cg_couple_task_t* tasks, size_t n_tasks, int precision, cudaStream_t stream) {
+    if (precision != 32 && precision != 64) throw invalid_parameter("precision must be 32 or 64");
+    std::vector<DeviceCoupleTask> dev;
+    std::vector<CgEntry> entries;
+    std::vector<int32_t> mu_starts;
+    int64_t blocks = 0;
+    for (size_t i = 0; i < n_tasks; i++) {
+        const auto& t = tasks[i];
+        if (t.n_outer < 0 || t.n_inner < 0)
+            throw invalid_parameter("negative size in Clebsch-Gordan coupling task " + std::to_string(i));
+        const int64_t items = t.n_outer * t.n_inner;
+        const SparseCg& sp = sparse_cg(t.l1, t.l2, t.lambda);
+        if (items == 0) continue;
+        if (!t.input || !t.output)
+            throw invalid_parameter("NULL array in Clebsch-Gordan coupling task " + std::to_string(i));
+        DeviceCoupleTask d;
+        d.input = t.input;
+        d.output = t.output;
+        d.n_outer = t.n_outer;
+        d.n_inner = t.n_inner;
+        d.block_start = blocks;
+        d.m1_count = 2 * t.l1 + 1;
+        d.m2_count = 2 * t.l2 + 1;
+        d.lambda = t.lambda;
+        d.entries = (int32_t)entries.size();
+        d.mu_offsets = (int32_t)mu_starts.size();
+        entries.insert(entries.end(), sp.entries.begin(), sp.entries.end());
+        mu_starts.insert(mu_starts.end(), sp.mu_starts.begin(), sp.mu_starts.end());
+        dev.push_back(d);
+        blocks += (items + CG_THREADS - 1) / CG_THREADS;
+    }
+    if (dev.empty()) return;
+    if (blocks > 0x7fffffffLL) throw invalid_parameter("Clebsch-Gordan coupling too large for one launch");
+    const size_t tb = dev.size() * sizeof(DeviceCoupleTask);
+    const size_t eb = std::max<size_t>(entries.size(), 1) * sizeof(CgEntry);
+    const size_t mb = mu_starts.size() * sizeof(int32_t);
+    const size_t e_off = (tb + 15) / 16 * 16, m_off = e_off + (eb + 15) / 16 * 16, total = m_off + mb;
+    std::vector<unsigned char> host(total, 0);
+    std::memcpy(host.data(), dev.data(), tb);
+    if (!entries.empty()) std::memcpy(host.data() + e_off, entries.data(), entries.size() * sizeof(CgEntry));
+    std::memcpy(host.data() + m_off, mu_starts.data(), mb);
+    unsigned char* buffer = nullptr;
+    CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&buffer), total, stream));
+    CUDA_CHECK(cudaMemcpyAsync(buffer, host.data(), total, cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    const auto* d_tasks = reinterpret_cast<const DeviceCoupleTask*>(buffer);
+    const auto* d_entries = reinterpret_cast<const CgEntry*>(buffer + e_off);
+    const auto* d_mu = reinterpret_cast<const int32_t*>(buffer + m_off);
+    if (precision == 64)
+        cg_couple_kernel<double><<<(unsigned)blocks, CG_THREADS, 0, stream>>>(d_tasks, (int)dev.size(), d_entries, d_mu);
+    else
+        cg_couple_kernel<float><<<(unsigned)blocks, CG_THREADS, 0, stream>>>(d_tasks, (int)dev.size(), d_entries, d_mu);
     CUDA_CHECK(cudaGetLastError());
     CUDA_CHECK(cudaFreeAsync(buffer, stream));
 }

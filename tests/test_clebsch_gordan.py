@@ -423,3 +423,76 @@ def test_compute_metadata_matches_compute():
             np.testing.assert_array_equal(a.properties.values, b.properties.values)
             assert a.properties.names == b.properties.names
 
+
+
+def _cartesian_tensor(values, rank):
+    import torch
+
+    S, P = values.shape[0], values.shape[-1]
+    keys = rb.Labels(["key"], [[0]])
+    comps = [rb.Labels([f"xyz_{i + 1}"], [[0], [1], [2]]) for i in range(rank)]
+    block = cg.Block(torch.tensor(values, device="cuda"), rb.Labels(["sample"], np.arange(S).reshape(-1, 1)), comps,
+                     rb.Labels(["p"], np.arange(P).reshape(-1, 1)))
+    return cg.EquivariantTensorMap(keys, [block])
+
+
+@pytest.mark.gpu
+def test_cg_couple_matches_oracle():
+    import torch
+
+    rng = np.random.default_rng(21)
+    tasks, expected = [], []
+    for l1, l2 in ((1, 1), (2, 1), (3, 2)):
+        x = rng.standard_normal((7, 2 * l1 + 1, 2 * l2 + 1, 5))
+        tx = torch.tensor(x, device="cuda")
+        for lam in range(abs(l1 - l2), l1 + l2 + 1):
+            out = torch.full((7, 2 * lam + 1, 5), float("nan"), dtype=torch.float64, device="cuda")
+            tasks.append((tx, out, l1, l2, lam))
+            expected.append(ocg.cg_couple(x, lam))
+    cg.cg_couple(tasks)
+    for (_, out, _, _, _), ref in zip(tasks, expected):
+        np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=0, atol=1e-13)
+
+
+@pytest.mark.gpu
+def test_cartesian_to_spherical():
+    rng = np.random.default_rng(22)
+    # rank 1: (x, y, z) -> (y, z, x) as the o3_mu = -1, 0, 1 components
+    v = rng.standard_normal((4, 3, 2))
+    out = cg.cartesian_to_spherical(_cartesian_tensor(v, 1), ["xyz_1"])
+    assert out.keys.names == ["o3_lambda", "o3_sigma", "key"]
+    np.testing.assert_array_equal(out.keys.values, [[1, 1, 0]])
+    np.testing.assert_array_equal(out.block_by_id(0).values.cpu().numpy(), v[:, [1, 2, 0], :])
+    # rank 2: a symmetric matrix has no o3_sigma = -1 block; values from the oracle
+    m = rng.standard_normal((5, 3, 3, 2))
+    sym = m + m.transpose(0, 2, 1, 3)
+    out = cg.cartesian_to_spherical(_cartesian_tensor(sym, 2), ["xyz_1", "xyz_2"])
+    assert out.keys.names == ["o3_lambda", "o3_sigma", "key"]
+    np.testing.assert_array_equal(out.keys.values, [[0, 1, 0], [2, 1, 0]])
+    rolled = sym[:, [1, 2, 0]][:, :, [1, 2, 0]]
+    for key, blk in zip(out.keys.values, out.blocks()):
+        np.testing.assert_allclose(blk.values.cpu().numpy(), ocg.cg_couple(rolled, int(key[0])), atol=1e-13)
+        assert blk.components[0].names == ["o3_mu"]
+    # lambda = 0 is -trace / sqrt(3); rotations leave it and the lambda = 2 norm unchanged
+    np.testing.assert_allclose(out.block_by_id(0).values.cpu().numpy()[:, 0, :],
+                               -np.trace(sym, axis1=1, axis2=2) / np.sqrt(3), atol=1e-13)
+    R = _rotation(rng)
+    rot = np.einsum("ij,sjkp,lk->silp", R, sym, R)
+    out_r = cg.cartesian_to_spherical(_cartesian_tensor(rot, 2), ["xyz_1", "xyz_2"])
+    for a, b in zip(out.blocks(), out_r.blocks()):
+        np.testing.assert_allclose(np.linalg.norm(b.values.cpu().numpy(), axis=1),
+                                   np.linalg.norm(a.values.cpu().numpy(), axis=1), atol=1e-12)
+    # rank 3: l / k dimensions in the keys, invariant lambda = 0 block
+    t = rng.standard_normal((3, 3, 3, 3, 1))
+    out = cg.cartesian_to_spherical(_cartesian_tensor(t, 3), ["xyz_1", "xyz_2", "xyz_3"])
+    assert out.keys.names == ["o3_lambda", "o3_sigma", "l_3", "k_1", "l_2", "l_1", "key"]
+    assert sorted(int(k[0]) for k in out.keys.values) == [0, 1, 1, 1, 2, 2, 3]
+    rot = np.einsum("ia,jb,kc,sabcp->sijkp", R, R, R, t)
+    out_r = cg.cartesian_to_spherical(_cartesian_tensor(rot, 3), ["xyz_1", "xyz_2", "xyz_3"])
+    for key, a, b in zip(out.keys.values, out.blocks(), out_r.blocks()):
+        va, vb = a.values.cpu().numpy(), b.values.cpu().numpy()
+        np.testing.assert_allclose(np.linalg.norm(vb, axis=1), np.linalg.norm(va, axis=1), atol=1e-12)
+        if key[0] == 0:
+            np.testing.assert_allclose(vb, va, atol=1e-12)
+    with pytest.raises(ValueError, match="must be `True` for tensors of rank 3"):
+        cg.cartesian_to_spherical(_cartesian_tensor(t, 3), ["xyz_1", "xyz_2", "xyz_3"], keep_l_in_keys=False)
