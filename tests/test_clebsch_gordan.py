@@ -496,3 +496,39 @@ def test_cartesian_to_spherical():
             np.testing.assert_allclose(vb, va, atol=1e-12)
     with pytest.raises(ValueError, match="must be `True` for tensors of rank 3"):
         cg.cartesian_to_spherical(_cartesian_tensor(t, 3), ["xyz_1", "xyz_2", "xyz_3"], keep_l_in_keys=False)
+
+
+def _host_cartesian(rank, values=(0, 1, 2), keys=("key",)):
+    comps = [rb.Labels([f"xyz_{i + 1}"], np.array(values).reshape(-1, 1)) for i in range(rank)]
+    block = cg.Block(np.zeros((2,) + (len(values),) * rank + (1,)), rb.Labels(["sample"], [[0], [1]]), comps,
+                     rb.Labels(["p"], [[0]]))
+    return cg.EquivariantTensorMap(rb.Labels(list(keys), [[0] * len(keys)]), [block])
+
+
+def test_cartesian_to_spherical_input_checks():
+    # _cartesian_spherical.py:86-130, all raised before anything runs on a device
+    with pytest.raises(ValueError, match="'xyz_9' is not part of this tensor components"):
+        cg.cartesian_to_spherical(_host_cartesian(2), ["xyz_9"])
+    with pytest.raises(ValueError, match=r"should have \[0, 1, 2\] as values"):
+        cg.cartesian_to_spherical(_host_cartesian(1, values=(0, 1, 3)), ["xyz_1"])
+    with pytest.raises(ValueError, match="only supports consecutive components"):
+        cg.cartesian_to_spherical(_host_cartesian(3), ["xyz_1", "xyz_3"])
+    with pytest.raises(ValueError, match="already has an `o3_lambda` key"):
+        cg.cartesian_to_spherical(_host_cartesian(1, keys=("o3_lambda",)), ["xyz_1"])
+    with pytest.raises(TypeError, match="should be a list"):
+        cg.cartesian_to_spherical(_host_cartesian(1), "xyz_1")
+    empty = _host_cartesian(1)
+    assert cg.cartesian_to_spherical(empty, []) is empty
+
+
+def test_cg_couple_rejects_bad_tasks():
+    # host-side checks before anything is queued: no device memory is touched
+    from rascaline_b200 import _c_api as C
+
+    task = C.featomic_b200_cg_couple_task_t(16, 32, 2, 3, 1, 1, 3)
+    arr = (C.featomic_b200_cg_couple_task_t * 1)(task)
+    assert C.lib().featomic_b200_cg_couple(arr, 1, 64, None) == 1
+    assert "can not couple" in C.lib().featomic_last_error().decode()
+    assert C.lib().featomic_b200_cg_couple(arr, 1, 8, None) == 1
+    assert "precision must be 32 or 64" in C.lib().featomic_last_error().decode()
+    assert C.lib().featomic_b200_cg_couple(None, 0, 64, None) == 0
