@@ -441,17 +441,18 @@ def test_cg_couple_matches_oracle():
     import torch
 
     rng = np.random.default_rng(21)
-    tasks, expected = [], []
-    for l1, l2 in ((1, 1), (2, 1), (3, 2)):
-        x = rng.standard_normal((7, 2 * l1 + 1, 2 * l2 + 1, 5))
-        tx = torch.tensor(x, device="cuda")
-        for lam in range(abs(l1 - l2), l1 + l2 + 1):
-            out = torch.full((7, 2 * lam + 1, 5), float("nan"), dtype=torch.float64, device="cuda")
-            tasks.append((tx, out, l1, l2, lam))
-            expected.append(ocg.cg_couple(x, lam))
-    cg.cg_couple(tasks)
-    for (_, out, _, _, _), ref in zip(tasks, expected):
-        np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=0, atol=1e-13)
+    for dtype, tol in ((torch.float64, 1e-13), (torch.float32, 2e-6)):
+        tasks, expected = [], []
+        for l1, l2 in ((1, 1), (2, 1), (3, 2)):
+            x = rng.standard_normal((7, 2 * l1 + 1, 2 * l2 + 1, 5))
+            tx = torch.tensor(x, dtype=dtype, device="cuda")
+            for lam in range(abs(l1 - l2), l1 + l2 + 1):
+                out = torch.full((7, 2 * lam + 1, 5), float("nan"), dtype=dtype, device="cuda")
+                tasks.append((tx, out, l1, l2, lam))
+                expected.append(ocg.cg_couple(tx.double().cpu().numpy(), lam))
+        cg.cg_couple(tasks)
+        for (_, out, _, _, _), ref in zip(tasks, expected):
+            np.testing.assert_allclose(out.double().cpu().numpy(), ref, rtol=0, atol=tol * max(1.0, np.abs(ref).max()))
 
 
 @pytest.mark.gpu
