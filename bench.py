@@ -236,8 +236,9 @@ def run_reference(args):
     barrier(world)
 
 
-def adjoint_form(steps, warmup):
-    """The adjoint form on the 20 000-atom strained box: dense power spectrum
+def adjoint_form(steps, warmup, n=20000):
+    """The adjoint form on the 20 000-atom strained box (``n`` atoms, for
+    profiling smaller cases of the same workload): dense power spectrum
     in FP32 arithmetic, then forces and virial of a linear energy model through
     the CUDA adjoint (no gradient blocks materialised).  One step = forward +
     backward; errors are measured once against the same calculation in FP64."""
@@ -246,7 +247,6 @@ def adjoint_form(steps, warmup):
     from rascaline_b200 import workloads
     from rascaline_b200.torch_api import dense_backward, dense_power_spectrum
 
-    n = 20000
     system = workloads.random_box(n, density=0.1, min_distance=0.9, seed=5, strain=0.02)
     calc = rb.SoapPowerSpectrum(**workloads.hypers(5.0, 7, 6))
     positions = torch.tensor(system["positions"], device="cuda")
@@ -297,7 +297,7 @@ def adjoint_form(steps, warmup):
         return float((a - b).abs().max() / b.abs().max())
 
     return {
-        "workload": "random_box_20000_rho0.1_strain0.02_rc5_nmax7_lmax6_ps+forces+virial_adjoint",
+        "workload": f"random_box_{n}_rho0.1_strain0.02_rc5_nmax7_lmax6_ps+forces+virial_adjoint",
         "metric": "atom-envs/s (power spectrum + forces + virial)",
         "value": n / (r32["ms"] / 1000.0),
         "ms_per_step": r32["ms"],
@@ -639,13 +639,15 @@ def main():
                         help="atoms in the box (1000 is the benchmark; smaller boxes are for profiling)")
     parser.add_argument("--only", choices=["adjoint", "batched", "surrogate", "cg"],
                         help="run one chosen form alone and print its object (profiling)")
+    parser.add_argument("--adjoint-atoms", type=int, default=20000,
+                        help="atoms of the adjoint form's box with --only adjoint (20000 is the benchmark)")
     parser.add_argument("--train-steps", type=int, default=20000,
                         help="training steps of the learned radial surrogate (20000 is the benchmark)")
     args = parser.parse_args()
     if args.only:
         import torch
         torch.cuda.set_device(0)
-        form = {"adjoint": adjoint_form, "batched": batched_form, "cg": cg_form,
+        form = {"adjoint": lambda k, w: adjoint_form(k, w, args.adjoint_atoms), "batched": batched_form, "cg": cg_form,
                 "surrogate": lambda k, w: surrogate_form(k, w, args.train_steps)}[args.only]
         print(json.dumps({args.only + "_form": form(args.steps, args.warmup)}), flush=True)
         return

@@ -279,6 +279,17 @@ featomic_status_t featomic_b200_power_spectrum_dense_backward(featomic_b200_dens
 
 featomic_status_t featomic_b200_dense_free(featomic_b200_dense_t* state);
 
+/* Engine of the FP32 per-centre contractions of the dense forms (the power
+ * spectrum P_l = X_l^T X_l and the adjoint dL/dc): `tensor_cores` = 1 (the
+ * default) runs them on the tcgen05 tensor cores with TF32 hi + lo operands
+ * and FP32 accumulation, 0 on the CUDA cores; the value of the environment
+ * variable FEATOMIC_B200_DENSE_MMA ("0" or "1") is the initial setting.
+ * Process-wide; FP64 always uses the CUDA cores.  `channels_per_round`
+ * (1 to 4, or 0 to keep the current value) is the number of angular channels
+ * of one tensor-core round; FEATOMIC_B200_MMA_CHANNELS gives its initial
+ * value.  No counterpart in featomic. */
+featomic_status_t featomic_b200_set_contraction_engine(int32_t tensor_cores, int32_t channels_per_round);
+
 /* ---- batched form: many molecules in one persistent launch ------------------
  *
  * Non-periodic systems (molecules) of up to 4096 atoms each, computed with

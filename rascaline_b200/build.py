@@ -29,7 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 DEVICE = ["-fmad=false"]
 # The FP32 forms (dense adjoint, batched molecules, learned surrogate) are not
 # held to featomic's rounding: their kernels contract into FMAs.
-FMA_SOURCES = ("dense.cu", "surrogate.cu", "surrogate_mma.cu", "batched_kernels_")
+FMA_SOURCES = ("dense.cu", "dense_mma.cu", "surrogate.cu", "surrogate_mma.cu", "batched_kernels_")
 COMMON = [
     "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fopenmp",
     f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}", "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets",

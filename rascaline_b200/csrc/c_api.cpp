@@ -488,6 +488,16 @@ featomic_status_t featomic_b200_dense_free(featomic_b200_dense_t* state) {
     return guarded([&] { delete state; });
 }
 
+featomic_status_t featomic_b200_set_contraction_engine(int32_t tensor_cores, int32_t channels_per_round) {
+    return guarded([&] {
+        if (tensor_cores != 0 && tensor_cores != 1) throw fb200::invalid_parameter("tensor_cores must be 0 or 1");
+        if (channels_per_round < 0 || channels_per_round > 4)
+            throw fb200::invalid_parameter("channels_per_round must be between 1 and 4 (0 keeps the current value)");
+        fb200::set_dense_mma_enabled(tensor_cores == 1);
+        if (channels_per_round > 0) fb200::dense_mma_channels_per_round = channels_per_round;
+    });
+}
+
 struct featomic_b200_batch_t {
     std::unique_ptr<fb200::BatchPlan> plan;
 };

@@ -33,6 +33,7 @@
 //   systems      CTA per system: strain and cell derivatives summed over atoms
 // Every reduction has a fixed order: results are deterministic.
 #include <cub/cub.cuh>
+#include <cstdlib>
 #include <type_traits>
 
 #include "dense.hpp"
@@ -680,6 +681,22 @@ int coefficient_threads(int K) { return std::max(DENSE_CHUNK, std::min(256, (K +
 
 }  // namespace
 
+namespace {
+int mma_state = -1;  // -1: not read from the environment yet
+}
+
+bool dense_mma_enabled() {
+    if (mma_state < 0) {
+        const char* env = std::getenv("FEATOMIC_B200_DENSE_MMA");
+        mma_state = (env && env[0] == '0') ? 0 : 1;
+        const char* channels = std::getenv("FEATOMIC_B200_MMA_CHANNELS");
+        if (channels && channels[0] >= '1' && channels[0] <= '4') dense_mma_channels_per_round = channels[0] - '0';
+    }
+    return mma_state == 1;
+}
+
+void set_dense_mma_enabled(bool enabled) { mma_state = enabled ? 1 : 0; }
+
 void launch_dense_directions(const DevicePairs& pairs, const int32_t* atom_species, int n_species, int64_t n_atoms,
                              int32_t* dir_code, int64_t* seg_offset, DeviceArena& arena, cudaStream_t stream) {
     const int64_t n_dirs = 2 * pairs.count;
@@ -716,6 +733,12 @@ void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t s
     dense_expansion<T><<<(unsigned)(a.n_atoms * a.n_species),
                          coefficient_threads(a.layout.L2 * ((a.nmax + 1) / 2)), 0, stream>>>(a);
     CUDA_CHECK(cudaGetLastError());
+    if constexpr (sizeof(T) == 4) {
+        if (dense_mma_enabled() && dense_mma_supported(a)) {
+            launch_dense_contraction_mma(a, stream);
+            return;
+        }
+    }
     const size_t smem = sizeof(T) * (size_t)a.n_species * a.K;
     if (a.nmax <= 16 && smem <= 48 * 1024) {
         if (a.nmax <= 8) dense_contraction_tiled<T, 8><<<(unsigned)a.n_atoms, 128, smem, stream>>>(a);
@@ -742,7 +765,11 @@ void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t 
         configured[which] = true;
     }
     const size_t tiled_smem = smem + sizeof(T) * (size_t)a.n_keys * a.n_props;
-    if (a.lmax <= DENSE_LMAX_SMALL && tiled_smem <= 200 * 1024) {
+    bool mma = false;
+    if constexpr (sizeof(T) == 4) mma = dense_mma_enabled() && dense_mma_supported(a);
+    if (mma) {
+        if constexpr (sizeof(T) == 4) launch_dense_grad_coef_mma(a, stream);
+    } else if (a.lmax <= DENSE_LMAX_SMALL && tiled_smem <= 200 * 1024) {
         dense_grad_coef_tiled<T, 17><<<(unsigned)a.n_atoms, 128, tiled_smem, stream>>>(a);
     } else {
         dense_grad_coef<T><<<(unsigned)a.n_atoms, 256, smem, stream>>>(a);

@@ -83,6 +83,18 @@ struct DenseState {
     std::vector<void*> allocations_;
 };
 
+// FP32 contractions on the tensor cores (dense_mma.cu): the power spectrum
+// P_l = X_l^T X_l and dL/dc; supported when S nmax <= 128 and 2 lmax + 1 <= 32
+bool dense_mma_supported(const DenseArgs<float>& a);
+void launch_dense_contraction_mma(const DenseArgs<float>& a, cudaStream_t stream);
+void launch_dense_grad_coef_mma(const DenseArgs<float>& a, cudaStream_t stream);
+// angular channels per round of the tensor-core kernels (1 to 4)
+extern int dense_mma_channels_per_round;
+// whether the FP32 contractions use the tensor cores (default) or the CUDA
+// cores; FEATOMIC_B200_DENSE_MMA=0 in the environment selects the CUDA cores
+bool dense_mma_enabled();
+void set_dense_mma_enabled(bool enabled);
+
 template <typename T>
 void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream);
 template <typename T>

@@ -22,6 +22,7 @@
 #include <cuda_bf16.h>
 
 #include "engine.hpp"
+#include "tcgen05.cuh"
 
 namespace fb200 {
 
@@ -30,77 +31,23 @@ namespace {
 constexpr int SH = 64;          // hidden units
 constexpr int TILE = 128;       // distances per tile (MMA M)
 constexpr int TMEM_COLS = 256;  // [0, N) values, [128, 128 + N) derivatives
-constexpr long long MMA_SPINS = 1ll << 24;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+using tc::fence_after;
+using tc::fence_async_smem;
+using tc::fence_before;
+using tc::mbar_wait;
+using tc::mma_bf16;
+using tc::mma_commit;
+using tc::smem_addr;
+using tc::tmem_load16;
 
 // byte offset of element (row, k) in a K-major [rows x 64] BF16 operand
-__host__ __device__ __forceinline__ uint32_t core_offset(int row, int k) {
-    return (uint32_t)((row >> 3) * (SH / 8) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
-}
+__host__ __device__ __forceinline__ uint32_t core_offset(int row, int k) { return tc::core_offset(row, k, SH * 2, 2); }
 
-__device__ __forceinline__ uint64_t operand_desc(uint32_t addr) {
-    const uint32_t lbo = 128, sbo = (SH / 8) * 128;
-    uint64_t d = 0;
-    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
-    return d;                // base offset 0, no swizzle
-}
+__device__ __forceinline__ uint64_t operand_desc(uint32_t addr) { return tc::operand_desc(addr, 128, (SH / 8) * 128); }
 
 // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
 // K-major, M = 128, N = n
-__device__ __forceinline__ uint32_t mma_idesc(int n) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-    const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-    for (long long spin = 0; spin < MMA_SPINS; spin++) {
-        uint32_t done = 0;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(phase)
-            : "memory");
-        if (done) return true;
-        __nanosleep(32);
-    }
-    return false;
-}
-
-__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_load16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
-}
+__device__ __forceinline__ uint32_t mma_idesc(int n) { return tc::instr_desc(tc::FORMAT_BF16, TILE, n); }
 
 __device__ __forceinline__ float sigmoid(float z) { return 1.0f / (1.0f + __expf(-z)); }
 
