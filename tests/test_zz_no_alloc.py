@@ -112,3 +112,47 @@ def test_sizes_beyond_the_limits_are_rejected():
     assert status == INVALID_PARAMETER
     assert "2048 pairs per atom" in C.lib().featomic_last_error().decode()
     assert not pairs.view(np.uint8).any()
+
+
+def test_calls_allocate_no_device_memory():
+    """After the one-time set-up of the first call, calls leave the device's
+    free memory (cudaMemGetInfo) unchanged, and the device's default memory
+    pool records no allocation while they run, not even one freed before the
+    call returns (its used-memory high watermark, reset before the calls,
+    stays at the current use)."""
+    torch = _torch()
+    from cuda.bindings import driver
+    from cuda.bindings import runtime as rt
+
+    stream = torch.cuda.Stream()
+    box = workloads.random_box(1000, density=0.1, min_distance=0.9, seed=2)
+    n = len(rb.neighbor_list(box["positions"], box["cell"], 5.5)["first"])
+    pos = torch.as_tensor(np.ascontiguousarray(box["positions"], dtype=np.float64)).cuda()
+    out = torch.zeros(n * PAIR.itemsize, dtype=torch.uint8, device="cuda")
+    cell = np.ascontiguousarray(box["cell"], dtype=np.float64).reshape(9)
+    count = ctypes.c_size_t(0)
+
+    def call():
+        status = C.lib().featomic_b200_neighbor_list_noalloc(
+            pos.data_ptr(), len(pos), cell.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 5.5,
+            out.data_ptr(), n, ctypes.byref(count), stream.cuda_stream)
+        assert status == 0, C.lib().featomic_last_error()
+        assert count.value == n
+
+    call()  # the first call on a device may do its one-time set-up
+    torch.cuda.synchronize()
+    err, pool = rt.cudaDeviceGetDefaultMemPool(torch.cuda.current_device())
+    assert err == rt.cudaError_t.cudaSuccess
+    high = rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh
+    current = rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent
+    err, = rt.cudaMemPoolSetAttribute(pool, high, driver.cuuint64_t(0))  # resets the watermark to the current use
+    assert err == rt.cudaError_t.cudaSuccess
+    err, used_before = rt.cudaMemPoolGetAttribute(pool, current)
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        call()
+    stream.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    err, used_high = rt.cudaMemPoolGetAttribute(pool, high)
+    assert free_after == free_before
+    assert int(used_high) == int(used_before)
