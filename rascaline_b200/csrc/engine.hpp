@@ -318,15 +318,27 @@ class Engine {
     // dense power spectrum with its adjoint (dense.hpp); `species` empty means
     // the sorted atomic types of the systems; `values` is a device buffer of
     // n_atoms x n_keys x n_properties elements of the precision (32 / 64)
+    // `expansion`: `values` receives the spherical expansion coefficients
+    // [n_atoms][n_species][(lmax + 1)^2 nmax] instead, with no contraction
     std::unique_ptr<DenseState> forward_dense(int precision, std::vector<HostSystem>& systems,
                                               const double* d_positions, const std::vector<int32_t>& species,
-                                              void* values, int64_t values_count, cudaStream_t stream);
+                                              void* values, int64_t values_count, cudaStream_t stream,
+                                              bool expansion = false);
     // dL/dpositions [n_atoms][3], and when not null dL/dstrain and dL/dcell
     // [n_systems][3][3], all device buffers of the forward precision
     // `by_species`: grad_values holds one dL/dP row per species (the weights
     // of a linear model) instead of one per atom
+    // `coefficients`: grad_values is dL/dc [n_atoms][n_species][K] of the
+    // spherical expansion instead of dL/dP
     void backward_dense(DenseState& state, const void* grad_values, void* grad_positions, void* grad_strain,
-                        void* grad_cell, cudaStream_t stream, bool by_species = false);
+                        void* grad_cell, cudaStream_t stream, bool by_species = false, bool coefficients = false);
+    // forward-mode derivative along a displacement of the positions
+    // ([n_atoms][3]) and cells ([n_systems][3][3] or null): the tangent of the
+    // coefficients (when `tangent_coef` is not null) and of the power spectrum
+    // (when `tangent_values` is not null), device buffers of the forward
+    // precision
+    void jvp_dense(DenseState& state, const void* tangent_positions, const void* tangent_cell, void* tangent_coef,
+                   void* tangent_values, cudaStream_t stream);
 
     // device tables for the kernels of the batched form (uploaded on first use)
     const DenseTables<float>& dense_tables_f() {

@@ -25,7 +25,6 @@
 // inside a block is
 // the slot's first row plus the rank of the neighbour among the rows of that
 // sample (prefix counts per species).
-#include <cuda_pipeline.h>
 
 #include <map>
 #include <mutex>
@@ -290,52 +289,140 @@ __device__ __forceinline__ void positions_row(const PsArgs& a, int lane, int K, 
     }
 }
 
-// The gradient record of a neighbour that shares one pair with the centre
-// (3 K doubles, the common case) is copied to shared memory asynchronously
-// before the warp contracts it.  One buffer per warp: the smaller footprint
-// keeps 16 warps per SM resident, which hides the copy better than a second
-// buffer (measured: 14 % faster than double buffering at 8 warps per SM).
-__device__ __forceinline__ void stage_record(double* dst, const double* src, int n, int lane) {
-    if ((n & 1) == 0) {
-        for (int i = 2 * lane; i < n; i += 64) __pipeline_memcpy_async(dst + i, src + i, 16);
-    } else {
-        for (int i = lane; i < n; i += 32) __pipeline_memcpy_async(dst + i, src + i, 8);
+// D[n1][n2] += sum_k A[n1][k] B[k][n2] on the FP64 tensor cores (DMMA,
+// 8 x 8 x 4): lane t holds A[t / 4][t % 4] and B[t % 4][t / 4] and the two
+// outputs D[t / 4][2 (t % 4) + {0, 1}]
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+constexpr int DMMA_SLOTS = 4;
+
+// Positions-gradient rows of one neighbour entry that shares a single pair
+// with the centre, nmax <= 8, on the FP64 tensor cores.  For a slot (a, b)
+// and the entry's species s, per l:
+//   s == a:  rows += G^T C_b   (sum_m g[x][l m][n1] c_b[l m][n2])
+//   s == b:  rows += C_a^T G   (sum_m c_a[l m][n1] g[x][l m][n2])
+// with G the pair gradient (times -(-1)^l for a reversed pair).  Lane t owns
+// m = m0 + t % 4, n = t / 4 of every fragment: the same register of G is the
+// A operand of the first product and the B operand of the second.  Up to
+// DMMA_SLOTS slots share the loads of G.
+__device__ void positions_entry_dmma(const PsArgs& a, int lane, int K, const double* __restrict__ coef_s,
+                                     const double* __restrict__ scale_s, const double* __restrict__ g, bool flip,
+                                     int species, const int32_t* slot_ab, const int64_t* slot_base,
+                                     const int32_t* cum_w, int64_t ns) {
+    const int S = a.n_species, N = a.nmax;
+    const int tm = lane & 3, tn = lane >> 2;
+    const bool n_ok = tn < N;
+    const int n2 = 2 * tm;
+    int64_t s = 0;
+    while (s < ns) {
+        // the next chunk of slots that contain the entry's species
+        int sa[DMMA_SLOTS], sb[DMMA_SLOTS];
+        double* out[DMMA_SLOTS];
+        int count = 0;
+#pragma unroll
+        for (int i = 0; i < DMMA_SLOTS; i++) {
+            sa[i] = sb[i] = -1;
+            out[i] = nullptr;
+            while (s < ns) {
+                const int x = slot_ab[2 * s], y = slot_ab[2 * s + 1];
+                const int64_t here = s++;
+                if (species != x && species != y) continue;
+                const int64_t rank = cum_w[x] + (x != y ? cum_w[y] : 0) + cum_w[S];
+                sa[i] = x;
+                sb[i] = y;
+                out[i] = a.out + slot_base[here] + rank * 3 * a.n_props;
+                count = i + 1;
+                break;
+            }
+        }
+        if (count == 0) break;
+        for (int l = 0; l <= a.lmax; l++) {
+            const int M = 2 * l + 1, base = l * l * N;
+            const double sign = (flip && (l & 1) == 0) ? -1.0 : 1.0;
+            double acc[DMMA_SLOTS][3][2];
+#pragma unroll
+            for (int i = 0; i < DMMA_SLOTS; i++)
+#pragma unroll
+                for (int x = 0; x < 3; x++) acc[i][x][0] = acc[i][x][1] = 0.0;
+            for (int m0 = 0; m0 < M; m0 += 4) {
+                const int m = m0 + tm;
+                const bool ok = n_ok && m < M;
+                const int idx = base + m * N + tn;
+                double gx[3];
+#pragma unroll
+                for (int x = 0; x < 3; x++) gx[x] = ok ? sign * g[x * K + idx] : 0.0;
+#pragma unroll
+                for (int i = 0; i < DMMA_SLOTS; i++) {
+                    if (i < count) {
+                        if (species == sa[i]) {
+                            const double cb = ok ? coef_s[sb[i] * K + idx] : 0.0;
+#pragma unroll
+                            for (int x = 0; x < 3; x++) dmma_8x8x4(acc[i][x], gx[x], cb);
+                        }
+                        if (species == sb[i]) {
+                            const double ca = ok ? coef_s[sa[i] * K + idx] : 0.0;
+#pragma unroll
+                            for (int x = 0; x < 3; x++) dmma_8x8x4(acc[i][x], ca, gx[x]);
+                        }
+                    }
+                }
+            }
+            const int64_t o = (int64_t)l * N * N + (int64_t)tn * N + n2;
+#pragma unroll
+            for (int i = 0; i < DMMA_SLOTS; i++) {
+                if (i < count && n_ok) {
+                    const double scale = scale_s[(sa[i] != sb[i] ? a.lmax + 1 : 0) + l];
+#pragma unroll
+                    for (int x = 0; x < 3; x++) {
+                        double* dst = out[i] + x * a.n_props + o;
+                        if (N == 8) {
+                            double2 w;
+                            w.x = acc[i][x][0] * scale;
+                            w.y = acc[i][x][1] * scale;
+                            __stcs(reinterpret_cast<double2*>(dst), w);
+                        } else {
+                            if (n2 < N) dst[0] = acc[i][x][0] * scale;
+                            if (n2 + 1 < N) dst[1] = acc[i][x][1] * scale;
+                        }
+                    }
+                }
+            }
+        }
     }
 }
 
-__device__ __forceinline__ const double* staged_source(const PsArgs& a, int64_t c, int64_t entry_index, int K) {
-    const PsEntry entry = a.entries[entry_index];
-    if (entry.atom == (int32_t)c || entry.d1 - entry.d0 != 1) return nullptr;
-    return a.pair_grad + (int64_t)(a.dir_code[entry.d0] >> 1) * 3 * K;
-}
-
 constexpr int POS_WARPS = 4;
+// resident CTAs per SM the register budget is set for (128 registers)
+constexpr int POS_MIN_BLOCKS = 4;
 // CTAs per centre, each taking every POS_SPLIT-th group of POS_WARPS entries:
 // more, smaller CTAs shorten the last wave
 constexpr int POS_SPLIT = 2;
 // per-centre slot tables staged in shared memory (centres with at most this
-// many slots; more read them from global memory), and per-warp entry counts
+// many slots; more read them from global memory) and per-warp entry counts
 constexpr int POS_SLOT_CAP = 64;
 constexpr int POS_CUM_CAP = 65;
 constexpr size_t POS_TABLE_BYTES = POS_SLOT_CAP * (8 + 2 * 4) + POS_WARPS * POS_CUM_CAP * 4;
 
 template <int MAXN>
-__global__ void __launch_bounds__(POS_WARPS * 32, 4) ps_positions_kernel(PsArgs a) {
+__global__ void __launch_bounds__(POS_WARPS * 32, POS_MIN_BLOCKS) ps_positions_kernel(PsArgs a) {
     extern __shared__ double smem[];
     const int64_t c = blockIdx.x / POS_SPLIT;
     const int part = (int)(blockIdx.x - c * POS_SPLIT);
     const int S = a.n_species;
     const int K = (a.lmax + 1) * (a.lmax + 1) * a.nmax;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int64_t head = (S * K + 2 * (a.lmax + 1) + 1) & ~1;
     double* coef_s = smem;
     double* scale_s = smem + S * K;
-    double* stage = smem + ((S * K + 2 * (a.lmax + 1) + 1) & ~1) + (int64_t)warp * 3 * K;
     // output-row tables: the first output element of every slot and its
     // species pair, then each warp's copy of its entry's counts, so that the
     // slot loop reads shared memory instead of a chain of dependent global
     // loads (slot -> counts -> first row -> block offset)
-    int64_t* slot_base = reinterpret_cast<int64_t*>(smem + ((S * K + 2 * (a.lmax + 1) + 1) & ~1) +
-                                                    (int64_t)nwarps * 3 * K);
+    int64_t* slot_base = reinterpret_cast<int64_t*>(smem + head);
     int32_t* slot_ab = reinterpret_cast<int32_t*>(slot_base + POS_SLOT_CAP);
     int32_t* cum_w = slot_ab + 2 * POS_SLOT_CAP + warp * POS_CUM_CAP;
     load_coefficients(a, c, coef_s, S * K);
@@ -352,29 +439,29 @@ __global__ void __launch_bounds__(POS_WARPS * 32, 4) ps_positions_kernel(PsArgs 
     }
     __syncthreads();
     const int64_t e0 = a.entry_offset[c], ne = a.entry_offset[c + 1] - e0;
-    for (int64_t e = warp + part * nwarps; e < ne; e += nwarps * POS_SPLIT) {
-        double* cur = stage;
-        {
-            const double* src = staged_source(a, c, e0 + e, K);
-            if (src) stage_record(stage, src, 3 * K, lane);
-            __pipeline_commit();
-            __pipeline_wait_prior(0);
-        }
-        __syncwarp();
-
+    for (int64_t e = warp + part * nwarps; e < ne; e += (int64_t)nwarps * POS_SPLIT) {
         const PsEntry entry = a.entries[e0 + e];
         const bool self = entry.atom == (int32_t)c;
         const int32_t* cum = a.entry_cum + (e0 + e) * (S + 1);
         const bool single = entry.d1 - entry.d0 <= 1;
-        DirectSource direct{nullptr, false};
-        ImagesSource images{a.dir_code + entry.d0, entry.d1 - entry.d0, a.pair_grad, 3 * (int64_t)K};
-        if (!self && single) {
-            direct.p = cur;
-            direct.flip = a.dir_code[entry.d0] & 1;
-        }
         if (tables) {
             for (int i = lane; i <= S; i += 32) cum_w[i] = cum[i];
             __syncwarp();
+        }
+        if (tables && !self && entry.d1 - entry.d0 == 1 && a.nmax <= 8) {
+            // the common entry: FP64 tensor cores, the pair gradient read in place
+            const int32_t code = a.dir_code[entry.d0];
+            positions_entry_dmma(a, lane, K, coef_s, scale_s, a.pair_grad + (int64_t)(code >> 1) * 3 * K, code & 1,
+                                 entry.species, slot_ab, slot_base, cum_w, ns);
+            __syncwarp();
+            continue;
+        }
+        DirectSource direct{nullptr, false};
+        ImagesSource images{a.dir_code + entry.d0, entry.d1 - entry.d0, a.pair_grad, 3 * (int64_t)K};
+        if (!self && single && entry.d1 > entry.d0) {
+            const int32_t code = a.dir_code[entry.d0];
+            direct.p = a.pair_grad + (int64_t)(code >> 1) * 3 * K;
+            direct.flip = code & 1;
         }
         for (int64_t s = 0; s < ns; s++) {
             PsKeySlot slot;
@@ -401,7 +488,6 @@ __global__ void __launch_bounds__(POS_WARPS * 32, 4) ps_positions_kernel(PsArgs 
         }
         __syncwarp();
     }
-    __pipeline_wait_prior(0);
 }
 
 // strain (which = 0) or cell (which = 1) rows: 9 components, done as three
@@ -465,9 +551,8 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
         configured = true;
     }
     if (coef_bytes > 200 * 1024) throw invalid_parameter("too many species / radial / angular functions for the power spectrum kernels");
-    const size_t pos_bytes = sizeof(double) * (((size_t)args.n_species * K + 2 * (args.lmax + 1) + 1) / 2 * 2 +
-                                               (size_t)POS_WARPS * 3 * K) +
-                             POS_TABLE_BYTES;
+    const size_t pos_bytes =
+        sizeof(double) * (((size_t)args.n_species * K + 2 * (args.lmax + 1) + 1) / 2 * 2) + POS_TABLE_BYTES;
     if (positions && pos_bytes > 200 * 1024)
         throw invalid_parameter("too many radial / angular functions for the positions gradient kernel");
 
