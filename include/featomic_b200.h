@@ -279,6 +279,45 @@ featomic_status_t featomic_b200_power_spectrum_dense_backward(featomic_b200_dens
 
 featomic_status_t featomic_b200_dense_free(featomic_b200_dense_t* state);
 
+/* The spherical expansion of every atom as one dense row per neighbour
+ * species, [atom][species][(l, m), n] with (l, m) = l^2 + l + m over
+ * l <= max_angular and n over max_radial + 1 (zero for species absent around
+ * the atom), for a spherical_expansion calculator, in FP64 or FP32 arithmetic.
+ * featomic's block (o3_lambda = l, center_type, neighbor_type) holds the rows
+ * [atom][neighbor species][l^2 .. l^2 + 2l][n] of the atoms of center_type
+ * that have neighbour type (the atom itself counts).  `values_count` must be
+ * n_atoms x n_species x (max_angular + 1)^2 (max_radial + 1).  The state is
+ * the one of featomic_b200_power_spectrum_dense (free it with
+ * featomic_b200_dense_free).  Replaces the explicit-gradient autograd of
+ * featomic-torch's SphericalExpansion (featomic-torch/src/autograd.cpp). */
+featomic_status_t featomic_b200_spherical_expansion_dense(featomic_calculator_t* calculator,
+                                                          const featomic_b200_device_systems_t* systems,
+                                                          const int32_t* species, uintptr_t n_species,
+                                                          int32_t precision, void* values, uintptr_t values_count,
+                                                          featomic_b200_dense_t** state, void* stream);
+
+/* Backward pass of featomic_b200_spherical_expansion_dense: dL/dcoefficients
+ * in the layout of its `values` to dL/dpositions, dL/dstrain and dL/dcell (as
+ * featomic_b200_power_spectrum_dense_backward). */
+featomic_status_t featomic_b200_spherical_expansion_dense_backward(featomic_b200_dense_t* state,
+                                                                   const void* grad_coefficients, void* grad_positions,
+                                                                   void* grad_strain, void* grad_cell, void* stream);
+
+/* Forward-mode derivative of a dense forward pass along a displacement of
+ * the positions (`tangent_positions` [n_atoms][3]) and of the cells
+ * (`tangent_cell` [n_systems][3][3], rows = cell vectors, NULL for none;
+ * positions are held fixed when the cell moves, as in featomic's cell
+ * gradient): the tangent of the expansion coefficients (`tangent_coefficients`,
+ * layout of featomic_b200_spherical_expansion_dense) and/or of the power
+ * spectrum (`tangent_values`, layout of featomic_b200_power_spectrum_dense),
+ * device buffers of the forward precision, either may be NULL.  This is the
+ * derivative of the backward pass's output with respect to its input dL/dX,
+ * i.e. what the double backward of featomic-torch's PositionsGrad / CellGrad
+ * computes (featomic-torch/src/autograd.cpp:318-426). */
+featomic_status_t featomic_b200_dense_jvp(featomic_b200_dense_t* state, const void* tangent_positions,
+                                          const void* tangent_cell, void* tangent_coefficients, void* tangent_values,
+                                          void* stream);
+
 /* Engine of the FP32 per-centre contractions of the dense forms (the power
  * spectrum P_l = X_l^T X_l and the adjoint dL/dc): `tensor_cores` = 1 (the
  * default) runs them on the tcgen05 tensor cores with TF32 hi + lo operands

@@ -153,6 +153,16 @@ SIGNATURES = {
                                                         ctypes.POINTER(ctypes.c_int32)]),
     "featomic_b200_power_spectrum_dense_backward": (featomic_status_t, [ctypes.c_void_p] + [ctypes.c_void_p] * 5),
     "featomic_b200_dense_free": (featomic_status_t, [ctypes.c_void_p]),
+    "featomic_b200_spherical_expansion_dense": (featomic_status_t, [ctypes.c_void_p,
+                                                                    ctypes.POINTER(featomic_b200_device_systems_t),
+                                                                    ctypes.POINTER(ctypes.c_int32), ctypes.c_size_t,
+                                                                    ctypes.c_int32, ctypes.c_void_p, ctypes.c_size_t,
+                                                                    ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
+    "featomic_b200_spherical_expansion_dense_backward": (featomic_status_t, [ctypes.c_void_p, ctypes.c_void_p,
+                                                                             ctypes.c_void_p, ctypes.c_void_p,
+                                                                             ctypes.c_void_p, ctypes.c_void_p]),
+    "featomic_b200_dense_jvp": (featomic_status_t, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p]),
     "featomic_b200_set_contraction_engine": (featomic_status_t, [ctypes.c_int32, ctypes.c_int32]),
     "featomic_b200_batch_create": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t,
                                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int32),

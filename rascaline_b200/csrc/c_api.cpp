@@ -444,6 +444,34 @@ featomic_status_t featomic_b200_power_spectrum_dense(featomic_calculator_t* calc
     });
 }
 
+featomic_status_t featomic_b200_spherical_expansion_dense(featomic_calculator_t* calculator,
+                                                          const featomic_b200_device_systems_t* systems,
+                                                          const int32_t* species, uintptr_t n_species,
+                                                          int32_t precision, void* values, uintptr_t values_count,
+                                                          featomic_b200_dense_t** state, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(systems);
+        CHECK_POINTER(state);
+        *state = nullptr;
+        const auto& impl = *calculator->impl;
+        if (impl.power_spectrum || impl.radial_spectrum || impl.by_pair)
+            throw invalid_parameter("featomic_b200_spherical_expansion_dense needs a spherical_expansion calculator");
+        if (impl.hypers.explicit_basis())
+            throw invalid_parameter("the dense spherical expansion does not support the Explicit basis");
+        std::vector<HostSystem> host = device_systems(systems);
+        std::vector<int32_t> sp;
+        if (n_species > 0) {
+            CHECK_POINTER(species);
+            sp.assign(species, species + n_species);
+        }
+        auto result = std::make_unique<featomic_b200_dense_t>();
+        result->state = impl.engine->forward_dense(precision, host, systems->positions, sp, values, (int64_t)values_count,
+                                                   (cudaStream_t)stream, /*expansion=*/true);
+        *state = result.release();
+    });
+}
+
 featomic_status_t featomic_b200_dense_shape(const featomic_b200_dense_t* state, uintptr_t* n_atoms,
                                             uintptr_t* n_species, uintptr_t* n_keys, uintptr_t* n_properties,
                                             uintptr_t* n_pairs) {
@@ -481,6 +509,31 @@ featomic_status_t featomic_b200_power_spectrum_dense_backward(featomic_b200_dens
         CHECK_POINTER(state);
         DenseState& st = *state->state;
         st.engine->backward_dense(st, grad_values, grad_positions, grad_strain, grad_cell, (cudaStream_t)stream);
+    });
+}
+
+featomic_status_t featomic_b200_spherical_expansion_dense_backward(featomic_b200_dense_t* state,
+                                                                   const void* grad_coefficients, void* grad_positions,
+                                                                   void* grad_strain, void* grad_cell, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(state);
+        DenseState& st = *state->state;
+        if (st.n_atoms > 0) CHECK_POINTER(grad_coefficients);
+        st.engine->backward_dense(st, grad_coefficients, grad_positions, grad_strain, grad_cell, (cudaStream_t)stream,
+                                  /*by_species=*/false, /*coefficients=*/true);
+    });
+}
+
+featomic_status_t featomic_b200_dense_jvp(featomic_b200_dense_t* state, const void* tangent_positions,
+                                          const void* tangent_cell, void* tangent_coefficients, void* tangent_values,
+                                          void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(state);
+        DenseState& st = *state->state;
+        if (!tangent_coefficients && !tangent_values)
+            throw invalid_parameter("one of tangent_coefficients and tangent_values must not be NULL");
+        st.engine->jvp_dense(st, tangent_positions, tangent_cell, tangent_coefficients, tangent_values,
+                             (cudaStream_t)stream);
     });
 }
 

@@ -642,6 +642,108 @@ __global__ void __launch_bounds__(256) dense_system_reduce(DenseArgs<T> a) {
     }
 }
 
+// Forward-mode derivative (tangent) of the expansion along a displacement of
+// the positions (tangent_positions [atoms][3]) and cells (tangent_cell
+// [systems][3][3], rows = cell vectors, may be null): the pair vector moves by
+//   delta_ij = t[second] - t[first] + shift . T_cell[system]
+// (positions held fixed when the cell moves, as in featomic's cell gradient),
+// and each pair term c_ij[l m n] = f R_ln Y_lm moves by
+//   (f' R_ln + f R'_ln) Y_lm (u . delta) + f / r R_ln (dY_lm . delta)
+// (spherical_expansion_pair.rs:323-422).  Thread per (pair, lm), from the
+// pair records with gradients; writes tangent[pair][lm][n].
+template <typename T>
+__global__ void dense_pair_tangent(DenseArgs<T> a, int64_t n_pairs, const T* __restrict__ tpos,
+                                   const T* __restrict__ tcell, T* __restrict__ tangent) {
+    const FeatureLayout L = a.layout;
+    const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= n_pairs * L.L2) return;
+    const int64_t p = item / L.L2;
+    const int lm = (int)(item - p * L.L2);
+    const int l = isqrt_lm(lm);
+    const int N = a.nmax;
+    const int i = a.pairs.first[p], j = a.pairs.second[p];
+    T d[3];
+#pragma unroll
+    for (int x = 0; x < 3; x++) d[x] = tpos[3 * j + x] - tpos[3 * i + x];
+    if (tcell) {
+        // system of the pair: the last system that starts at or before atom i
+        int64_t lo = 0, hi = a.n_systems - 1;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) >> 1;
+            if (a.atom_offset[mid] <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        const T* U = tcell + 9 * lo;
+#pragma unroll
+        for (int x = 0; x < 3; x++)
+            d[x] += (T)a.pairs.shift[3 * p] * U[x] + (T)a.pairs.shift[3 * p + 1] * U[3 + x] +
+                    (T)a.pairs.shift[3 * p + 2] * U[6 + x];
+    }
+    const T* __restrict__ F = a.features + p * L.stride;
+    const T f = F[0], fg = F[1], r = F[2];
+    const T ud = F[3] * d[0] + F[4] * d[1] + F[5] * d[2];
+    const T yd = F[L.off_dy + lm] * d[0] + F[L.off_dy + L.L2 + lm] * d[1] + F[L.off_dy + 2 * L.L2 + lm] * d[2];
+    const T y = F[L.off_y + lm];
+    const T A = y * ud, B = f / r * yd;
+    T* out = tangent + p * a.K + lm * N;
+    for (int n = 0; n < N; n++) {
+        const T R = F[L.off_r + l * N + n], dR = F[L.off_dr + l * N + n];
+        out[n] = (fg * R + f * dR) * A + R * B;
+    }
+}
+
+// tangent of the coefficients: sum over each (centre, species) segment of
+// the pair tangents in pair order, (-1)^l for the reversed direction
+template <typename T>
+__global__ void __launch_bounds__(256) dense_tangent_expansion(DenseArgs<T> a, const T* __restrict__ tangent,
+                                                               T* __restrict__ tcoef) {
+    const int S = a.n_species, N = a.nmax;
+    const int64_t c = blockIdx.x / S;
+    const int t = (int)(blockIdx.x - c * S);
+    const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
+    for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+        const int l = isqrt_lm(k / N);
+        const T sign = (l & 1) ? T(-1) : T(1);
+        T acc = T(0);
+        for (int64_t d = d0; d < d1; d++) {
+            const int32_t code = a.dir_code[d];
+            const T v = tangent[(int64_t)(code >> 1) * a.K + k];
+            acc += (code & 1) ? sign * v : v;
+        }
+        tcoef[(c * S + t) * a.K + k] = acc;
+    }
+}
+
+// tangent of the power spectrum: warp per (centre, key), lane per property
+//   dP[l n1 n2] = scale sum_m (dc_a[l m n1] c_b[l m n2] + c_a[l m n1] dc_b[l m n2])
+template <typename T>
+__global__ void __launch_bounds__(256) dense_tangent_contraction(DenseArgs<T> a, const T* __restrict__ tcoef,
+                                                                 T* __restrict__ tvalues) {
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t item = (int64_t)blockIdx.x * warps + warp;
+    if (item >= a.n_atoms * a.n_keys) return;
+    const int64_t c = item / a.n_keys;
+    const int key = (int)(item - c * a.n_keys);
+    int sa, sb;
+    key_species(key, a.n_species, &sa, &sb);
+    const int N = a.nmax, NN = N * N;
+    const T* ca = a.coef + (c * a.n_species + sa) * a.K;
+    const T* cb = a.coef + (c * a.n_species + sb) * a.K;
+    const T* ta = tcoef + (c * a.n_species + sa) * a.K;
+    const T* tb = tcoef + (c * a.n_species + sb) * a.K;
+    T* out = tvalues + item * a.n_props;
+    for (int o = lane; o < a.n_props; o += 32) {
+        const int l = o / NN;
+        const int rem = o - l * NN;
+        const int n1 = rem / N, n2 = rem - n1 * N;
+        const int base = l * l * N;
+        T s = T(0);
+        for (int m = 0; m < 2 * l + 1; m++)
+            s += ta[base + m * N + n1] * cb[base + m * N + n2] + ca[base + m * N + n1] * tb[base + m * N + n2];
+        out[o] = s * (T)ps_scale(l, sa != sb);
+    }
+}
+
 template <typename T, bool GRAD>
 void launch_features(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream) {
     if (n_pairs == 0) return;
@@ -733,6 +835,7 @@ void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t s
     dense_expansion<T><<<(unsigned)(a.n_atoms * a.n_species),
                          coefficient_threads(a.layout.L2 * ((a.nmax + 1) / 2)), 0, stream>>>(a);
     CUDA_CHECK(cudaGetLastError());
+    if (a.values == nullptr) return;  // the expansion alone
     if constexpr (sizeof(T) == 4) {
         if (dense_mma_enabled() && dense_mma_supported(a)) {
             launch_dense_contraction_mma(a, stream);
@@ -752,8 +855,7 @@ void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t s
 }
 
 template <typename T>
-void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream) {
-    if (a.n_atoms == 0) return;
+void launch_dense_grad_coef(const DenseArgs<T>& a, cudaStream_t stream) {
     const size_t smem = sizeof(T) * (size_t)a.n_species * a.K;
     if (smem > 200 * 1024) throw invalid_parameter("too many species x coefficients for the adjoint kernel");
     static bool configured[2] = {false, false};
@@ -775,6 +877,12 @@ void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t 
         dense_grad_coef<T><<<(unsigned)a.n_atoms, 256, smem, stream>>>(a);
     }
     CUDA_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream, bool coef_grad_given) {
+    if (a.n_atoms == 0) return;
+    if (!coef_grad_given) launch_dense_grad_coef(a, stream);
     bool fused = a.lmax <= DENSE_LMAX_SMALL && a.nmax <= 16 && a.tab.spline.splined;
     if constexpr (sizeof(T) == 4) fused = fused && a.surrogate == nullptr;
     if (n_pairs > 0 && fused) {
@@ -799,9 +907,36 @@ void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t 
     }
 }
 
+template <typename T>
+void launch_dense_jvp(const DenseArgs<T>& a, int64_t n_pairs, const T* tangent_positions, const T* tangent_cell,
+                      T* pair_tangent, T* tangent_coef, T* tangent_values, cudaStream_t stream) {
+    if (a.n_atoms == 0) return;
+    if (n_pairs > 0) {
+        launch_features<T, true>(a, n_pairs, stream);
+        const int threads = 128;
+        const int64_t items = n_pairs * a.layout.L2;
+        dense_pair_tangent<T><<<(unsigned)((items + threads - 1) / threads), threads, 0, stream>>>(
+            a, n_pairs, tangent_positions, tangent_cell, pair_tangent);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    dense_tangent_expansion<T><<<(unsigned)(a.n_atoms * a.n_species), 128, 0, stream>>>(a, pair_tangent, tangent_coef);
+    CUDA_CHECK(cudaGetLastError());
+    if (tangent_values) {
+        const int warps = 8;
+        const int64_t items = a.n_atoms * a.n_keys;
+        dense_tangent_contraction<T><<<(unsigned)((items + warps - 1) / warps), 32 * warps, 0, stream>>>(
+            a, tangent_coef, tangent_values);
+        CUDA_CHECK(cudaGetLastError());
+    }
+}
+
 template void launch_dense_forward<float>(const DenseArgs<float>&, int64_t, cudaStream_t);
 template void launch_dense_forward<double>(const DenseArgs<double>&, int64_t, cudaStream_t);
-template void launch_dense_backward<float>(const DenseArgs<float>&, int64_t, cudaStream_t);
-template void launch_dense_backward<double>(const DenseArgs<double>&, int64_t, cudaStream_t);
+template void launch_dense_backward<float>(const DenseArgs<float>&, int64_t, cudaStream_t, bool);
+template void launch_dense_backward<double>(const DenseArgs<double>&, int64_t, cudaStream_t, bool);
+template void launch_dense_jvp<float>(const DenseArgs<float>&, int64_t, const float*, const float*, float*, float*,
+                                      float*, cudaStream_t);
+template void launch_dense_jvp<double>(const DenseArgs<double>&, int64_t, const double*, const double*, double*,
+                                       double*, double*, cudaStream_t);
 
 }  // namespace fb200

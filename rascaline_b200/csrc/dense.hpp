@@ -97,8 +97,16 @@ void set_dense_mma_enabled(bool enabled);
 
 template <typename T>
 void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream);
+// the adjoint; with coef_grad_given, a.grad_coef already holds dL/dc (the
+// spherical expansion's own backward pass) and dL/dP is not read
 template <typename T>
-void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream);
+void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream, bool coef_grad_given = false);
+// forward-mode derivative along (tangent_positions [atoms][3], tangent_cell
+// [systems][9] or null): pair_tangent [pairs][K] scratch, tangent_coef
+// [atoms][S][K] and, when not null, tangent_values [atoms][keys][props]
+template <typename T>
+void launch_dense_jvp(const DenseArgs<T>& a, int64_t n_pairs, const T* tangent_positions, const T* tangent_cell,
+                      T* pair_tangent, T* tangent_coef, T* tangent_values, cudaStream_t stream);
 void launch_dense_directions(const DevicePairs& pairs, const int32_t* atom_species, int n_species, int64_t n_atoms,
                              int32_t* dir_code, int64_t* seg_offset, DeviceArena& arena, cudaStream_t stream);
 

@@ -762,7 +762,8 @@ void Engine::dense_args(const DenseState& st, bool grad, DenseArgs<T>& a) {
 
 std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<HostSystem>& systems,
                                                   const double* d_positions, const std::vector<int32_t>& species,
-                                                  void* values, int64_t values_count, cudaStream_t stream) {
+                                                  void* values, int64_t values_count, cudaStream_t stream,
+                                                  bool expansion) {
     if (precision != 32 && precision != 64) throw invalid_parameter("precision must be 32 or 64");
     upload_tables();
     const std::shared_ptr<RadialSurrogate> hold = surrogate_.lock();
@@ -802,9 +803,11 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
     st->n_keys = S * (S + 1) / 2;
     st->n_props = (int64_t)(h_.max_angular + 1) * h_.nmax() * h_.nmax();
     st->K = (h_.max_angular + 1) * (h_.max_angular + 1) * h_.nmax();
-    const int64_t expected = n_atoms * st->n_keys * st->n_props;
+    const int64_t expected = expansion ? n_atoms * S * st->K : n_atoms * st->n_keys * st->n_props;
     if (values_count != expected) {
-        throw invalid_parameter("the values buffer must hold n_atoms x n_keys x n_properties = " +
+        throw invalid_parameter(std::string("the values buffer must hold ") +
+                                (expansion ? "n_atoms x n_species x (max_angular + 1)^2 (max_radial + 1) = "
+                                           : "n_atoms x n_keys x n_properties = ") +
                                 std::to_string(expected) + " elements, got " + std::to_string(values_count));
     }
     if (n_atoms > 0 && !values) throw invalid_parameter("values must not be NULL");
@@ -859,16 +862,20 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
         DenseArgs<double> a;
         dense_args(*st, false, a);
         a.features = (double*)features;
-        a.values = (double*)values;
+        a.values = expansion ? nullptr : (double*)values;
         a.status = status;
         launch_dense_forward<double>(a, P, stream);
     } else {
         DenseArgs<float> a;
         dense_args(*st, false, a);
         a.features = (float*)features;
-        a.values = (float*)values;
+        a.values = expansion ? nullptr : (float*)values;
         a.status = status;
         launch_dense_forward<float>(a, P, stream);
+    }
+    if (expansion) {
+        CUDA_CHECK(cudaMemcpyAsync(values, st->coef, T_size * (size_t)n_atoms * S * st->K, cudaMemcpyDeviceToDevice,
+                                   stream));
     }
     if (!radial_.splined) {
         int32_t h_status = 0;
@@ -879,8 +886,47 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
     return st;
 }
 
+void Engine::jvp_dense(DenseState& st, const void* tangent_positions, const void* tangent_cell, void* tangent_coef,
+                       void* tangent_values, cudaStream_t stream) {
+    int dev = -1;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev != st.device) throw invalid_parameter("the derivative must run on the device of the forward pass");
+    const std::shared_ptr<RadialSurrogate> hold = surrogate_.lock();
+    active_surrogate_ = hold.get();
+    struct Release {
+        RadialSurrogate** p;
+        ~Release() { *p = nullptr; }
+    } release{&active_surrogate_};
+    if (st.n_atoms == 0) return;
+    if (!tangent_positions) throw invalid_parameter("tangent_positions must not be NULL");
+    const size_t T_size = st.precision == 64 ? 8 : 4;
+    const int64_t P = st.n_pairs;
+    const FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), true);
+    void* features = arena_.alloc_bytes("dense.features_grad", T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride);
+    void* pair_tangent = arena_.alloc_bytes("dense.pair_tangent", T_size * (size_t)std::max<int64_t>(P, 1) * st.K);
+    void* tcoef = tangent_coef ? tangent_coef
+                               : arena_.alloc_bytes("dense.tangent_coef", T_size * (size_t)st.n_atoms * st.n_species * st.K);
+    int32_t* status = arena_.alloc<int32_t>("dense.status", 1);
+    CUDA_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t), stream));
+    if (st.precision == 64) {
+        DenseArgs<double> a;
+        dense_args(st, true, a);
+        a.features = (double*)features;
+        a.status = status;
+        launch_dense_jvp<double>(a, P, (const double*)tangent_positions, (const double*)tangent_cell,
+                                 (double*)pair_tangent, (double*)tcoef, (double*)tangent_values, stream);
+    } else {
+        DenseArgs<float> a;
+        dense_args(st, true, a);
+        a.features = (float*)features;
+        a.status = status;
+        launch_dense_jvp<float>(a, P, (const float*)tangent_positions, (const float*)tangent_cell, (float*)pair_tangent,
+                                (float*)tcoef, (float*)tangent_values, stream);
+    }
+}
+
 void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_positions, void* grad_strain,
-                            void* grad_cell, cudaStream_t stream, bool by_species) {
+                            void* grad_cell, cudaStream_t stream, bool by_species, bool coefficients) {
     int dev = -1;
     CUDA_CHECK(cudaGetDevice(&dev));
     if (dev != st.device) throw invalid_parameter("the backward pass must run on the device of the forward pass");
@@ -896,7 +942,8 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
     const int64_t P = st.n_pairs;
     const FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), true);
     void* features = arena_.alloc_bytes("dense.features_grad", T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride);
-    void* grad_coef = arena_.alloc_bytes("dense.grad_coef", T_size * (size_t)st.n_atoms * st.n_species * st.K);
+    void* grad_coef = coefficients ? const_cast<void*>(grad_values)
+                                   : arena_.alloc_bytes("dense.grad_coef", T_size * (size_t)st.n_atoms * st.n_species * st.K);
     void* pair_grad = arena_.alloc_bytes("dense.pair_grad", T_size * 3 * (size_t)std::max<int64_t>(P, 1));
     void* partial = arena_.alloc_bytes("dense.atom_partial", T_size * 18 * (size_t)st.n_atoms);
     int32_t* status = arena_.alloc<int32_t>("dense.status", 1);
@@ -913,7 +960,7 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
         a.grad_strain = (double*)grad_strain;
         a.grad_cell = (double*)grad_cell;
         a.status = status;
-        launch_dense_backward<double>(a, P, stream);
+        launch_dense_backward<double>(a, P, stream, coefficients);
     } else {
         DenseArgs<float> a;
         dense_args(st, true, a);
@@ -927,7 +974,7 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
         a.grad_strain = (float*)grad_strain;
         a.grad_cell = (float*)grad_cell;
         a.status = status;
-        launch_dense_backward<float>(a, P, stream);
+        launch_dense_backward<float>(a, P, stream, coefficients);
     }
 }
 

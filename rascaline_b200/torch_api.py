@@ -12,10 +12,18 @@ explicit gradient blocks.  Here the backward pass is
 ``featomic_b200_power_spectrum_dense_backward``: a CUDA adjoint that recomputes
 the per-pair terms and never builds the gradient blocks.  The forward runs in
 FP64 (``precision=64``, the drop-in values) or in FP32 (``precision=32``).
-The backward pass is not itself differentiable (no double backward).
+
+Double backward follows featomic-torch (``PositionsGrad`` / ``CellGrad`` are
+themselves autograd functions, ``autograd.cpp:22-54``, ``:318-426``): the
+backward pass is differentiable with respect to its input dL/dX, through the
+forward-mode derivative of X (``featomic_b200_dense_jvp``), so that losses on
+forces and virials train the model that produced dL/dX.  Second derivatives
+with respect to positions and cell are not computed; a warning says so, as in
+featomic-torch.
 """
 import ctypes
 import json
+import warnings
 
 import numpy as np
 import torch
@@ -23,7 +31,8 @@ import torch
 from . import _c_api as C
 from .calculators import CalculatorBase, Labels
 
-__all__ = ["System", "Calculator", "SoapPowerSpectrum", "TorchTensorMap", "TorchBlock", "Batch", "dense_power_spectrum"]
+__all__ = ["System", "Calculator", "SoapPowerSpectrum", "SphericalExpansion", "TorchTensorMap", "TorchBlock", "Batch",
+           "dense_power_spectrum", "dense_spherical_expansion", "dense_jvp"]
 
 
 class System:
@@ -127,37 +136,147 @@ def dense_backward(state, grad_values, n_systems, strain=False, cell=True):
     return gpos, gstrain, gcell
 
 
-class _DensePowerSpectrum(torch.autograd.Function):
-    """positions [atoms, 3], cells [systems, 3, 3] -> dense power spectrum;
-    the backward pass is the CUDA adjoint."""
+def dense_spherical_expansion(calculator, positions, types, cells, sizes, precision=64, species=None):
+    """Forward pass of a spherical_expansion calculator without autograd:
+    (coefficients [n_atoms, n_species, (lmax + 1)^2 nmax] torch tensor on the
+    GPU, DenseState); arguments as dense_power_spectrum."""
+    if not (positions.is_cuda and positions.dtype == torch.float64 and positions.is_contiguous()):
+        raise ValueError("positions must be a contiguous CUDA float64 tensor")
+    types = np.ascontiguousarray(types, dtype=np.int32)
+    cells = np.ascontiguousarray(cells, dtype=np.float64).reshape(-1, 9)
+    sizes = np.ascontiguousarray(sizes, dtype=np.uintp)
+    if species is None:
+        sp = np.unique(types).astype(np.int32)
+    else:
+        sp = np.unique(np.asarray(species, dtype=np.int32)).astype(np.int32)
+    params = json.loads(calculator._parameters)
+    if params["basis"].get("type") == "Explicit":
+        raise C.FeatomicError("the dense spherical expansion does not support the Explicit basis", 1)
+    L = params["basis"]["max_angular"]
+    N = params["basis"]["radial"]["max_radial"] + 1
+    dtype = torch.float64 if precision == 64 else torch.float32
+    values = torch.empty((len(types), len(sp), (L + 1) ** 2 * N), dtype=dtype, device=positions.device)
+    dev = _device_systems(positions, types, cells, sizes)
+    handle = ctypes.c_void_p()
+    stream = torch.cuda.current_stream(positions.device).cuda_stream
+    C.check(C.lib().featomic_b200_spherical_expansion_dense(
+        calculator._handle, ctypes.byref(dev), sp.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(sp), precision,
+        values.data_ptr(), values.numel(), ctypes.byref(handle), ctypes.c_void_p(stream)))
+    return values, DenseState(handle)
+
+
+def expansion_backward(state, grad_coefficients, n_systems, strain=False, cell=True):
+    """dense_backward for a spherical-expansion state: dL/dcoefficients to
+    (dL/dpositions, dL/dstrain or None, dL/dcell or None)."""
+    grad_coefficients = grad_coefficients.contiguous()
+    device, dtype = grad_coefficients.device, grad_coefficients.dtype
+    gpos = torch.empty((state.n_atoms, 3), dtype=dtype, device=device)
+    gstrain = torch.empty((n_systems, 3, 3), dtype=dtype, device=device) if strain else None
+    gcell = torch.empty((n_systems, 3, 3), dtype=dtype, device=device) if cell else None
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else None)  # noqa: E731
+    stream = torch.cuda.current_stream(device).cuda_stream
+    C.check(C.lib().featomic_b200_spherical_expansion_dense_backward(
+        state._handle, ptr(grad_coefficients), ptr(gpos), ptr(gstrain), ptr(gcell), ctypes.c_void_p(stream)))
+    return gpos, gstrain, gcell
+
+
+def dense_jvp(state, tangent_positions, tangent_cell=None, values=True, coefficients=False, dtype=None):
+    """Forward-mode derivative of a dense forward pass along a displacement
+    of the positions [atoms, 3] (and cells [systems, 3, 3]): (tangent of the
+    power spectrum or None, tangent of the expansion coefficients or None)."""
+    dtype = dtype or tangent_positions.dtype
+    device = tangent_positions.device
+    tpos = tangent_positions.to(dtype).contiguous()
+    tcell = tangent_cell.to(dtype).contiguous() if tangent_cell is not None else None
+    n = state.n_atoms
+    tv = torch.empty((n, state.n_keys, state.n_properties), dtype=dtype, device=device) if values else None
+    tc = None
+    if coefficients:
+        tc = torch.empty((n, state.n_species, state.expansion_width), dtype=dtype, device=device)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else None)  # noqa: E731
+    stream = torch.cuda.current_stream(device).cuda_stream
+    C.check(C.lib().featomic_b200_dense_jvp(state._handle, ptr(tpos), ptr(tcell), ptr(tc), ptr(tv),
+                                            ctypes.c_void_p(stream)))
+    return tv, tc
+
+
+SECOND_DERIVATIVE_WARNING = ("second derivatives with respect to {} are not implemented and will not be accumulated "
+                             "during backward() calls")
+
+
+class _DenseAdjoint(torch.autograd.Function):
+    """The adjoint backward pass as a function of dL/dX (the power spectrum
+    or the expansion coefficients), differentiable with respect to dL/dX: its
+    own backward pass is the forward-mode derivative of X along the incoming
+    gradients of dL/dpositions and dL/dcell."""
 
     @staticmethod
-    def forward(ctx, positions, cells, calculator, types, sizes, precision, species, holder):
+    def forward(ctx, grad_out, positions, cells, state, n_systems, need_cell, expansion):
+        if expansion:
+            gpos, _, gcell = expansion_backward(state, grad_out, n_systems, strain=False, cell=need_cell)
+        else:
+            gpos, _, gcell = dense_backward(state, grad_out, n_systems, strain=False, cell=need_cell)
+        if gcell is None:
+            gcell = torch.zeros((n_systems, 3, 3), dtype=gpos.dtype, device=gpos.device)
+        ctx.state = state
+        ctx.expansion = expansion
+        ctx.need_cell = need_cell
+        ctx.precision_dtype = grad_out.dtype
+        return gpos.to(positions.dtype), gcell.to(cells.dtype)
+
+    @staticmethod
+    def backward(ctx, d_gpos, d_gcell):
+        if ctx.needs_input_grad[1]:
+            warnings.warn(SECOND_DERIVATIVE_WARNING.format("positions"), stacklevel=2)
+        if ctx.needs_input_grad[2]:
+            warnings.warn(SECOND_DERIVATIVE_WARNING.format("cell matrix"), stacklevel=2)
+        d_grad_out = None
+        if ctx.needs_input_grad[0]:
+            st = ctx.state
+            dtype = ctx.precision_dtype
+            if d_gpos is None:
+                d_gpos = torch.zeros((st.n_atoms, 3), dtype=dtype, device="cuda")
+            if not ctx.need_cell:
+                d_gcell = None  # the cell output was zeros, not a function of dL/dX
+            tv, tc = dense_jvp(st, d_gpos, d_gcell, values=not ctx.expansion, coefficients=ctx.expansion, dtype=dtype)
+            d_grad_out = tc if ctx.expansion else tv
+        return d_grad_out, None, None, None, None, None, None
+
+
+class _DenseForward(torch.autograd.Function):
+    """positions [atoms, 3], cells [systems, 3, 3] -> dense power spectrum or
+    expansion coefficients; the backward pass is the CUDA adjoint."""
+
+    @staticmethod
+    def forward(ctx, positions, cells, calculator, types, sizes, precision, species, holder, expansion):
         pos = positions.detach().to(torch.float64).contiguous()
         cell_host = cells.detach().to(torch.float64).cpu().numpy().reshape(-1, 9)
-        values, state = dense_power_spectrum(calculator, pos, types, cell_host, sizes, precision, species)
+        run = dense_spherical_expansion if expansion else dense_power_spectrum
+        values, state = run(calculator, pos, types, cell_host, sizes, precision, species)
+        if expansion:
+            state.expansion_width = values.shape[2]
         holder.append(state)
         ctx.state = state
         ctx.n_systems = len(sizes)
-        ctx.dtypes = (positions.dtype, cells.dtype)
+        ctx.expansion = expansion
+        ctx.save_for_backward(positions, cells)
         return values
 
     @staticmethod
-    @torch.autograd.function.once_differentiable
     def backward(ctx, grad_values):
         need_pos, need_cell = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
-        gpos, _, gcell = dense_backward(ctx.state, grad_values, ctx.n_systems, strain=False, cell=need_cell)
-        gpos = gpos.to(ctx.dtypes[0]) if need_pos else None
-        gcell = gcell.to(ctx.dtypes[1]) if need_cell else None
-        return gpos, gcell, None, None, None, None, None, None
+        positions, cells = ctx.saved_tensors
+        gpos, gcell = _DenseAdjoint.apply(grad_values.contiguous(), positions, cells, ctx.state, ctx.n_systems,
+                                          need_cell, ctx.expansion)
+        return gpos if need_pos else None, gcell if need_cell else None, None, None, None, None, None, None, None
 
 
 class TorchBlock:
-    def __init__(self, values, samples, properties):
+    def __init__(self, values, samples, properties, components=None):
         self.values = values
         self.samples = samples
         self.properties = properties
-        self.components = []
+        self.components = components or []
 
 
 class TorchTensorMap:
@@ -176,14 +295,17 @@ class TorchTensorMap:
 
 
 class Calculator:
-    """featomic-torch's CalculatorHolder for the SOAP power spectrum."""
+    """featomic-torch's CalculatorHolder for the SOAP power spectrum and the
+    spherical expansion."""
 
     def __init__(self, name, parameters, precision=64, species=None):
-        if name != "soap_power_spectrum":
-            raise ValueError(f"the torch interface of featomic-b200 supports soap_power_spectrum, not {name}")
+        if name not in ("soap_power_spectrum", "spherical_expansion"):
+            raise ValueError("the torch interface of featomic-b200 supports soap_power_spectrum and "
+                             f"spherical_expansion, not {name}")
         if precision not in (32, 64):
             raise ValueError("precision must be 32 or 64")
         self._calculator = CalculatorBase(name, parameters)
+        self._registry_name = name
         self.hypers = parameters if isinstance(parameters, dict) else json.loads(parameters)
         self.precision = precision
         self.species = None if species is None else sorted(set(int(s) for s in species))
@@ -205,22 +327,30 @@ class Calculator:
         sizes = np.array([len(s) for s in systems], dtype=np.uintp)
         return systems, positions, cells, types, sizes
 
+    @property
+    def _expansion(self):
+        return self._registry_name == "spherical_expansion"
+
     def dense(self, systems):
-        """Dense power spectrum [atoms, n_keys, n_properties] of all systems
+        """Dense power spectrum [atoms, n_keys, n_properties] (or expansion
+        coefficients [atoms, n_species, (lmax + 1)^2 nmax]) of all systems
         (see featomic_b200_power_spectrum_dense for the layout), differentiable
         w.r.t. the positions and cells."""
         systems, positions, cells, types, sizes = self._gather(systems)
-        return _DensePowerSpectrum.apply(positions, cells, self._calculator, types, sizes, self.precision,
-                                         self.species, [])
+        return _DenseForward.apply(positions, cells, self._calculator, types, sizes, self.precision, self.species, [],
+                                   self._expansion)
 
     def compute(self, systems):
-        """The power spectrum in featomic's TensorMap layout: keys
-        (center_type, neighbor_1_type, neighbor_2_type), samples (system, atom)
-        of the centres that have both neighbour types, properties (l, n_1, n_2)."""
+        """featomic's TensorMap layout.  Power spectrum: keys (center_type,
+        neighbor_1_type, neighbor_2_type), samples (system, atom) of the
+        centres that have both neighbour types, properties (l, n_1, n_2).
+        Spherical expansion: keys (o3_lambda, o3_sigma, center_type,
+        neighbor_type), samples (system, atom) of the centres that have the
+        neighbour type, components (o3_mu), properties (n)."""
         systems, positions, cells, types, sizes = self._gather(systems)
         holder = []
-        values = _DensePowerSpectrum.apply(positions, cells, self._calculator, types, sizes, self.precision,
-                                           self.species, holder)
+        values = _DenseForward.apply(positions, cells, self._calculator, types, sizes, self.precision, self.species,
+                                     holder, self._expansion)
         # which neighbour species every atom has, from the forward pass
         species, counts = holder[0].species(with_counts=True)
         S = len(species)
@@ -231,6 +361,8 @@ class Calculator:
         atom_of = np.concatenate([np.arange(n) for n in sizes.astype(np.int64)]) if len(types) else np.zeros(0, int)
         L = self.hypers["basis"]["max_angular"]
         N = self.hypers["basis"]["radial"]["max_radial"] + 1
+        if self._expansion:
+            return self._expansion_blocks(values, species, present, own, system_of, atom_of, L, N)
         properties = Labels(["l", "n_1", "n_2"],
                             [[l, n1, n2] for l in range(L + 1) for n1 in range(N) for n2 in range(N)])
         keys, blocks = [], []
@@ -254,10 +386,37 @@ class Calculator:
                     blocks.append(TorchBlock(block_values, samples, properties))
         return TorchTensorMap(Labels(["center_type", "neighbor_1_type", "neighbor_2_type"], keys), blocks)
 
+    @staticmethod
+    def _expansion_blocks(values, species, present, own, system_of, atom_of, L, N):
+        # keys (l, 1, center, neighbour) with l varying fastest
+        # (featomic/src/calculators/soap/spherical_expansion.rs:662-742)
+        S = len(species)
+        properties = Labels(["n"], [[n] for n in range(N)])
+        keys, blocks = [], []
+        for c in range(S):
+            for t in range(S):
+                rows = np.nonzero((own == c) & present[:, t])[0]
+                if len(rows) == 0:
+                    continue
+                index = torch.as_tensor(rows, device=values.device)
+                samples = Labels(["system", "atom"], np.stack([system_of[rows], atom_of[rows]], axis=1))
+                for l in range(L + 1):
+                    block_values = values[index, t, l * l * N:(l + 1) * (l + 1) * N].reshape(len(rows), 2 * l + 1, N)
+                    components = [Labels(["o3_mu"], [[m] for m in range(-l, l + 1)])]
+                    keys.append([l, 1, species[c], species[t]])
+                    blocks.append(TorchBlock(block_values, samples, properties, components))
+        return TorchTensorMap(Labels(["o3_lambda", "o3_sigma", "center_type", "neighbor_type"], keys), blocks)
+
 
 class SoapPowerSpectrum(Calculator):
     def __init__(self, cutoff, density, basis, precision=64, species=None):
         super().__init__("soap_power_spectrum", {"cutoff": cutoff, "density": density, "basis": basis},
+                         precision=precision, species=species)
+
+
+class SphericalExpansion(Calculator):
+    def __init__(self, cutoff, density, basis, precision=64, species=None):
+        super().__init__("spherical_expansion", {"cutoff": cutoff, "density": density, "basis": basis},
                          precision=precision, species=species)
 
 
