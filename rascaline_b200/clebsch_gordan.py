@@ -27,6 +27,56 @@ def cg_coefficients(l1, l2, o3_lambda):
     return out.reshape(2 * l1 + 1, 2 * l2 + 1, 2 * o3_lambda + 1)
 
 
+CG_BACKENDS = ("python-dense", "python-sparse")
+
+
+def _check_cg_backend(cg_backend):
+    if cg_backend not in CG_BACKENDS:
+        raise ValueError(f"invalid `cg_backend`, got '{cg_backend}', only 'python-dense', or 'python-sparse' are "
+                         "supported")
+
+
+def calculate_cg_coefficients(lambda_max, cg_backend, arrays_backend, dtype, device):
+    """The real Clebsch-Gordan coefficients of every (l1, l2, lambda) with
+    l1, l2 <= lambda_max and |l1 - l2| <= lambda <= min(lambda_max, l1 + l2),
+    in featomic's cache layout (_coefficients.py:35-134, 225-335): keys
+    (l1, l2, lambda); "python-dense" blocks [1, 2 l1 + 1, 2 l2 + 1, 2 lambda + 1,
+    1] with components m1, m2, mu; "python-sparse" blocks [n, 1] of the
+    non-zero coefficients with samples (m1, m2, mu).  ``arrays_backend`` is
+    "numpy" or "torch".  This library's own products take their coefficients
+    from the GPU directly, so the cache is only for callers that read it."""
+    _check_cg_backend(cg_backend)
+    if arrays_backend == "torch":
+        import torch
+
+        if dtype not in (torch.float32, torch.float64):
+            raise ValueError(f"invalid dtype ({dtype}), only torch.float32 and torch.float64 are supported")
+        convert = lambda a: torch.as_tensor(a, dtype=dtype, device=device)  # noqa: E731
+    elif arrays_backend == "numpy":
+        if np.dtype(dtype) not in (np.float32, np.float64):
+            raise ValueError(f"invalid dtype ({dtype}), only np.float32 and np.float64 are supported")
+        convert = lambda a: np.ascontiguousarray(a, dtype=dtype)  # noqa: E731
+    else:
+        raise ValueError(f"invalid arrays_backend '{arrays_backend}', only 'numpy' and 'torch' are supported")
+    keys, blocks = [], []
+    for l1 in range(lambda_max + 1):
+        for l2 in range(lambda_max + 1):
+            for lam in range(abs(l1 - l2), min(lambda_max, l1 + l2) + 1):
+                dense = cg_coefficients(l1, l2, lam)
+                keys.append([l1, l2, lam])
+                if cg_backend == "python-dense":
+                    comps = [Labels([name], np.arange(n, dtype=np.int32).reshape(-1, 1))
+                             for name, n in zip(("m1", "m2", "mu"), dense.shape)]
+                    blocks.append(Block(convert(dense.reshape((1,) + dense.shape + (1,))), Labels(["_"], [[0]]),
+                                        comps, Labels(["cg_coefficient"], [[0]])))
+                else:
+                    nonzero = np.argwhere(np.abs(dense) > 1e-15)
+                    values = dense[tuple(nonzero.T)].reshape(-1, 1)
+                    blocks.append(Block(convert(values), Labels(["m1", "m2", "mu"], nonzero.astype(np.int32)), [],
+                                        Labels(["cg_coefficient"], [[0]])))
+    return EquivariantTensorMap(Labels(["l1", "l2", "lambda"], np.array(keys, dtype=np.int32)), blocks)
+
+
 def cg_tensor_products(tasks, stream=None):
     """Run ``(first, second, output, o3_lambda)`` products (contiguous CUDA
     tensors of one dtype, shapes [s, 2 l1 + 1, p], [s, 2 l2 + 1, q],
@@ -842,17 +892,38 @@ def _insert(labels, name, value):
                   np.concatenate([np.full((len(labels), 1), value, dtype=np.int32), labels.values], axis=1))
 
 
-def cartesian_to_spherical(tensor, components, keep_l_in_keys=None, remove_blocks_threshold=1e-9):
+def cartesian_to_spherical(tensor, components, keep_l_in_keys=None, remove_blocks_threshold=1e-9, cg_backend=None,
+                           cg_coefficients=None):
     """A tensor with Cartesian (xyz) components in spherical form
     (_cartesian_spherical.py:21-304): the xyz axes become (y, z, x) = real
     l = 1 components, then the last two converted axes are coupled with
     Clebsch-Gordan coefficients until one o3_mu axis is left; keys gain
     o3_lambda, o3_sigma (and l_i / k_i with ``keep_l_in_keys``); blocks whose
-    squared norm is at most ``remove_blocks_threshold`` are dropped."""
+    squared norm is at most ``remove_blocks_threshold`` are dropped.
+
+    ``cg_backend`` follows featomic: "python-sparse" (the default for numpy
+    values) couples x[m1, m2] with C[m1, m2, mu]; "python-dense" (the default
+    for torch values) swaps the two coupled axes before contracting, which
+    multiplies every coupled block by (-1)^(l1 + l2 + lambda), i.e. flips the
+    sign of the o3_sigma = -1 blocks (_coefficients.py:440-455).  The
+    coupling always runs on the GPU; ``cg_coefficients`` is accepted for
+    featomic's signature and not needed (the coefficients are computed here).
+    Values come back with the input's array type and device."""
     import torch
 
     if len(tensor) == 0 or len(components) == 0:
         return tensor
+    values0 = tensor.block_by_id(0).values
+    if isinstance(values0, np.ndarray):
+        out_numpy, out_device = True, None
+    elif isinstance(values0, torch.Tensor):
+        out_numpy, out_device = False, values0.device
+    else:
+        raise TypeError(f"unknown array type in tensor ({type(values0)}), only numpy and torch are supported")
+    if cg_backend is None:
+        cg_backend = "python-sparse" if out_numpy else "python-dense"
+    _check_cg_backend(cg_backend)
+    dense_backend = cg_backend == "python-dense"
     if not isinstance(components, list):
         raise TypeError(f"`components` should be a list, got {type(components)}")
     if keep_l_in_keys is None:
@@ -900,23 +971,35 @@ def cartesian_to_spherical(tensor, components, keep_l_in_keys=None, remove_block
         if keep_l_in_keys:
             keys = _insert(keys, "l_1", 1)
         keys = _insert(_insert(keys, "o3_sigma", 1), "o3_lambda", 1)
-        return EquivariantTensorMap(keys, blocks)
+        return _to_input_arrays(EquivariantTensorMap(keys, blocks), out_numpy, out_device)
     current = EquivariantTensorMap(keys, blocks)
     iteration = 0
     while len(axes) > 1:
-        current = _do_coupling(current, axes[-2] - 1, axes[-1] - 1, keep_l_in_keys, iteration)
+        current = _do_coupling(current, axes[-2] - 1, axes[-1] - 1, keep_l_in_keys, iteration, dense_backend)
         axes.pop()
         iteration += 1
-    if remove_blocks_threshold is None:
-        return current
-    kept = [i for i, b in enumerate(current.blocks()) if float((b.values * b.values).sum()) > remove_blocks_threshold]
-    return EquivariantTensorMap(Labels(current.keys.names, current.keys.values[kept]),
-                                [current.block_by_id(i) for i in kept])
+    if remove_blocks_threshold is not None:
+        kept = [i for i, b in enumerate(current.blocks())
+                if float((b.values * b.values).sum()) > remove_blocks_threshold]
+        current = EquivariantTensorMap(Labels(current.keys.names, current.keys.values[kept]),
+                                       [current.block_by_id(i) for i in kept])
+    return _to_input_arrays(current, out_numpy, out_device)
 
 
-def _do_coupling(tensor, component_1, component_2, keep_l_in_keys, iteration):
+def _to_input_arrays(tensor, numpy_values, device):
+    """The blocks' values as numpy arrays, or torch tensors on ``device``."""
+    blocks = []
+    for b in tensor.blocks():
+        values = b.values.cpu().numpy() if numpy_values else b.values.to(device)
+        blocks.append(Block(values, b.samples, b.components, b.properties))
+    return EquivariantTensorMap(tensor.keys, blocks)
+
+
+def _do_coupling(tensor, component_1, component_2, keep_l_in_keys, iteration, dense_backend=False):
     """_cartesian_spherical.py:307-444: couple two consecutive spherical
-    component axes of every block to every allowed lambda."""
+    component axes of every block to every allowed lambda; with
+    ``dense_backend`` the result of featomic's "python-dense" backend, the
+    coupled block times (-1)^(l1 + l2 + lambda)."""
     import torch
 
     assert component_2 == component_1 + 1
@@ -954,6 +1037,10 @@ def _do_coupling(tensor, component_1, component_2, keep_l_in_keys, iteration):
             comps[component_1] = Labels(["o3_mu"], np.arange(-lam, lam + 1, dtype=np.int32).reshape(-1, 1))
             new_blocks.append(Block(out.view(new_shape), block.samples, comps, block.properties))
     cg_couple(tasks)
+    if dense_backend:
+        for x, out, l1, l2, lam in tasks:
+            if (l1 + l2 + lam) % 2 == 1:
+                out.neg_()
     return EquivariantTensorMap(Labels(["o3_lambda", "o3_sigma"] + keys.names,
                                        np.array(new_values, dtype=np.int32).reshape(len(new_values), -1)),
                                 new_blocks)

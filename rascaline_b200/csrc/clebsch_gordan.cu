@@ -381,9 +381,9 @@ void cg_product(const featomic_b200_cg_task_t* tasks, size_t n_tasks, int precis
     std::memcpy(host.data() + m_off, mu_starts.data(), mb);
     unsigned char* buffer = nullptr;
     CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&buffer), total, stream));
+    // a copy from pageable host memory returns once the source has been
+    // staged, so `host` may be released when this function returns
     CUDA_CHECK(cudaMemcpyAsync(buffer, host.data(), total, cudaMemcpyHostToDevice, stream));
-    // the pageable source of the copy must outlive it
-    CUDA_CHECK(cudaStreamSynchronize(stream));
     const auto* d_tasks = reinterpret_cast<const DeviceCgTask*>(buffer);
     const auto* d_entries = reinterpret_cast<const CgEntry*>(buffer + e_off);
     const auto* d_mu = reinterpret_cast<const int32_t*>(buffer + m_off);
@@ -438,8 +438,8 @@ void cg_couple(const featomic_b200_cg_couple_task_t* tasks, size_t n_tasks, int 
     std::memcpy(host.data() + m_off, mu_starts.data(), mb);
     unsigned char* buffer = nullptr;
     CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&buffer), total, stream));
+    // staged before the call returns (pageable source), as above
     CUDA_CHECK(cudaMemcpyAsync(buffer, host.data(), total, cudaMemcpyHostToDevice, stream));
-    CUDA_CHECK(cudaStreamSynchronize(stream));
     const auto* d_tasks = reinterpret_cast<const DeviceCoupleTask*>(buffer);
     const auto* d_entries = reinterpret_cast<const CgEntry*>(buffer + e_off);
     const auto* d_mu = reinterpret_cast<const int32_t*>(buffer + m_off);

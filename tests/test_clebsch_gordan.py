@@ -533,3 +533,59 @@ def test_cg_couple_rejects_bad_tasks():
     assert C.lib().featomic_b200_cg_couple(arr, 1, 8, None) == 1
     assert "precision must be 32 or 64" in C.lib().featomic_last_error().decode()
     assert C.lib().featomic_b200_cg_couple(None, 0, 64, None) == 0
+
+
+@pytest.mark.gpu
+def test_cartesian_to_spherical_backends():
+    """featomic's coupling backends differ on the o3_sigma = -1 blocks: the
+    "python-sparse" backend (default for numpy values) couples x[m1, m2]
+    with C[m1, m2, mu], the "python-dense" backend (default for torch values)
+    swaps the coupled axes first, which multiplies each block by
+    (-1)^(l1 + l2 + lambda) (_coefficients.py:440-455).  A non-symmetric
+    rank-2 tensor has a lambda = 1, o3_sigma = -1 block: sparse equals the
+    oracle's coupling, dense equals minus it (1e-13)."""
+    rng = np.random.default_rng(31)
+    m = rng.standard_normal((5, 3, 3, 2))
+    rolled = m[:, [1, 2, 0]][:, :, [1, 2, 0]]
+    sparse = cg.cartesian_to_spherical(_cartesian_tensor(m, 2), ["xyz_1", "xyz_2"], cg_backend="python-sparse")
+    dense = cg.cartesian_to_spherical(_cartesian_tensor(m, 2), ["xyz_1", "xyz_2"])
+    np.testing.assert_array_equal(sparse.keys.values, [[0, 1, 0], [1, -1, 0], [2, 1, 0]])
+    np.testing.assert_array_equal(dense.keys.values, sparse.keys.values)
+    for key, bs, bd in zip(sparse.keys.values, sparse.blocks(), dense.blocks()):
+        ref = ocg.cg_couple(rolled, int(key[0]))
+        np.testing.assert_allclose(bs.values.cpu().numpy(), ref, rtol=0, atol=1e-13)
+        np.testing.assert_allclose(bd.values.cpu().numpy(), int(key[1]) * ref, rtol=0, atol=1e-13)
+    # numpy values: the sparse default, numpy values back
+    host = cg.EquivariantTensorMap(rb.Labels(["key"], [[0]]), [cg.Block(
+        m, rb.Labels(["sample"], np.arange(5).reshape(-1, 1)),
+        [rb.Labels([f"xyz_{i + 1}"], [[0], [1], [2]]) for i in range(2)], rb.Labels(["p"], [[0], [1]]))])
+    out = cg.cartesian_to_spherical(host, ["xyz_1", "xyz_2"])
+    assert isinstance(out.block_by_id(1).values, np.ndarray)
+    np.testing.assert_allclose(out.block_by_id(1).values, ocg.cg_couple(rolled, 1), rtol=0, atol=1e-13)
+    with pytest.raises(ValueError, match="invalid `cg_backend`"):
+        cg.cartesian_to_spherical(host, ["xyz_1", "xyz_2"], cg_backend="python-fast")
+
+
+def test_calculate_cg_coefficients_layout():
+    """featomic's coefficient cache (_coefficients.py:35-134, 225-335): keys
+    (l1, l2, lambda) for l1, l2 <= lambda_max and |l1 - l2| <= lambda <=
+    min(lambda_max, l1 + l2); dense blocks [1, 2 l1 + 1, 2 l2 + 1, 2 lambda +
+    1, 1], sparse blocks of the non-zero coefficients with (m1, m2, mu)
+    samples; values equal cg_coefficients."""
+    dense = cg.calculate_cg_coefficients(2, "python-dense", "numpy", np.float64, "cpu")
+    sparse = cg.calculate_cg_coefficients(2, "python-sparse", "numpy", np.float64, "cpu")
+    expected = [[l1, l2, lam] for l1 in range(3) for l2 in range(3) for lam in range(abs(l1 - l2), min(2, l1 + l2) + 1)]
+    assert dense.keys.names == ["l1", "l2", "lambda"]
+    np.testing.assert_array_equal(dense.keys.values, expected)
+    np.testing.assert_array_equal(sparse.keys.values, expected)
+    for (l1, l2, lam), bd, bs in zip(expected, dense.blocks(), sparse.blocks()):
+        ref = cg.cg_coefficients(l1, l2, lam)
+        assert bd.values.shape == (1,) + ref.shape + (1,)
+        np.testing.assert_array_equal(bd.values[0, ..., 0], ref)
+        assert [c.names[0] for c in bd.components] == ["m1", "m2", "mu"]
+        assert bs.samples.names == ["m1", "m2", "mu"]
+        rebuilt = np.zeros_like(ref)
+        rebuilt[tuple(bs.samples.values.T)] = bs.values[:, 0]
+        np.testing.assert_array_equal(rebuilt, np.where(np.abs(ref) > 1e-15, ref, 0.0))
+    with pytest.raises(ValueError, match="invalid `cg_backend`"):
+        cg.calculate_cg_coefficients(1, "python-fast", "numpy", np.float64, "cpu")
