@@ -391,8 +391,10 @@ featomic_status_t featomic_b200_batch_free(featomic_b200_batch_t* batch);
  *
  * A small MLP r -> R_nl(r), 1 -> 64 -> 64 -> (max_angular + 1) (max_radial + 1)
  * with SiLU activations, trained on the GPU by this library's own kernels on
- * exact (analytic GTO) radial integrals of the calculator, evaluated with
- * BF16 weights and FP32 accumulation on the tensor cores.  Attached to a
+ * exact (analytic GTO) radial integrals of the calculator (Adam, then a
+ * least-squares refit of the output layer), evaluated on the tensor cores
+ * with BF16 operands (weights and activations each stored as three BF16
+ * parts) and FP32 accumulation.  Attached to a
  * calculator it replaces the spline in the FP32 dense power spectrum and its
  * adjoint.  featomic's radial basis does not depend on the atomic species, so
  * one network serves every species pair.  No counterpart in featomic. */
@@ -407,11 +409,22 @@ featomic_status_t featomic_b200_surrogate_shape(const featomic_b200_surrogate_t*
  * radial integrals, computed on the GPU */
 featomic_status_t featomic_b200_surrogate_dataset(featomic_b200_surrogate_t* surrogate, uintptr_t n_samples,
                                                   uint64_t seed, void* stream);
+/* weight lambda of the derivative term of the training loss (default 0.1) */
+featomic_status_t featomic_b200_surrogate_set_derivative_weight(featomic_b200_surrogate_t* surrogate,
+                                                                double derivative_weight);
 /* `steps` Adam steps on random minibatches (one captured CUDA graph per step);
- * `loss` receives the mean squared error of the normalised outputs of the last
- * minibatch */
+ * `loss` receives the loss of the last minibatch: the mean squared error of
+ * the normalised outputs plus lambda times that of their derivatives with
+ * respect to x = 2 r / cutoff - 1 */
 featomic_status_t featomic_b200_surrogate_train(featomic_b200_surrogate_t* surrogate, uintptr_t steps,
                                                 uintptr_t batch, double learning_rate, double* loss, void* stream);
+/* Least-squares refit of the output layer (the last linear layer, W3 and
+ * b3) over the whole training set: minimises the squared error of the
+ * normalised outputs plus `derivative_weight` times that of their
+ * r-derivatives, through FP64 normal equations solved on the GPU (Cholesky).
+ * Call after featomic_b200_surrogate_train. */
+featomic_status_t featomic_b200_surrogate_fit_output_layer(featomic_b200_surrogate_t* surrogate,
+                                                           double derivative_weight, void* stream);
 /* loss and gradient (host, n_parameters) on the first `n` training samples */
 featomic_status_t featomic_b200_surrogate_gradient(featomic_b200_surrogate_t* surrogate, uintptr_t n,
                                                    float* gradient, double* loss, void* stream);
@@ -424,9 +437,11 @@ featomic_status_t featomic_b200_surrogate_scales(const featomic_b200_surrogate_t
 featomic_status_t featomic_b200_surrogate_samples(const featomic_b200_surrogate_t* surrogate, float* r,
                                                   uintptr_t count, void* stream);
 /* R_o(r) and dR_o/dr (o = l (max_radial + 1) + n) for `n` device distances,
- * written to device float32 rows of stride `ld`; `method` 0: tensor cores,
- * 1: CUDA cores (same network), 2: the calculator's FP64 spline, 3: the exact
- * analytic integral */
+ * written to device float32 rows of stride `ld`; `method` 0: tensor cores
+ * (W2, W3 and the activations as sums of three BF16 parts), 1: CUDA cores
+ * (same network, FP32 weights), 2: the calculator's FP64 spline, 3: the exact
+ * analytic integral, 4: CUDA cores with W2 and W3 rounded to one BF16 each
+ * (the single-BF16 control of the error) */
 featomic_status_t featomic_b200_surrogate_evaluate(featomic_b200_surrogate_t* surrogate, const double* r,
                                                    uintptr_t n, float* values, float* derivs, uintptr_t ld,
                                                    int32_t method, void* stream);

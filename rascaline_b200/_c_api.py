@@ -184,6 +184,8 @@ SIGNATURES = {
     "featomic_b200_surrogate_train": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
                                                           ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                                           ctypes.c_void_p]),
+    "featomic_b200_surrogate_set_derivative_weight": (featomic_status_t, [ctypes.c_void_p, ctypes.c_double]),
+    "featomic_b200_surrogate_fit_output_layer": (featomic_status_t, [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]),
     "featomic_b200_surrogate_gradient": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t,
                                                              ctypes.POINTER(ctypes.c_float),
                                                              ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),

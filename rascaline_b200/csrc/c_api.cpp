@@ -703,6 +703,22 @@ featomic_status_t featomic_b200_surrogate_train(featomic_b200_surrogate_t* surro
     });
 }
 
+featomic_status_t featomic_b200_surrogate_set_derivative_weight(featomic_b200_surrogate_t* surrogate,
+                                                                double derivative_weight) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        surrogate->impl->set_derivative_weight(derivative_weight);
+    });
+}
+
+featomic_status_t featomic_b200_surrogate_fit_output_layer(featomic_b200_surrogate_t* surrogate,
+                                                           double derivative_weight, void* stream) {
+    return guarded([&] {
+        CHECK_POINTER(surrogate);
+        surrogate->impl->fit_output_layer(derivative_weight, (cudaStream_t)stream);
+    });
+}
+
 featomic_status_t featomic_b200_surrogate_gradient(featomic_b200_surrogate_t* surrogate, uintptr_t n,
                                                    float* gradient, double* loss, void* stream) {
     return guarded([&] {
@@ -767,7 +783,8 @@ featomic_status_t featomic_b200_surrogate_evaluate(featomic_b200_surrogate_t* su
             case 1: surrogate->impl->evaluate(r, (int64_t)n, values, derivs, (int64_t)ld, false, s); break;
             case 2: surrogate->impl->evaluate_reference(r, (int64_t)n, values, derivs, (int64_t)ld, false, s); break;
             case 3: surrogate->impl->evaluate_reference(r, (int64_t)n, values, derivs, (int64_t)ld, true, s); break;
-            default: throw invalid_parameter("method must be 0, 1, 2 or 3");
+            case 4: surrogate->impl->evaluate(r, (int64_t)n, values, derivs, (int64_t)ld, false, s, true, true); break;
+            default: throw invalid_parameter("method must be 0, 1, 2, 3 or 4");
         }
     });
 }

@@ -3,9 +3,12 @@
 An MLP r -> R_nl(r) for every (l, n) of a calculator's radial basis,
 1 -> 64 -> 64 -> (max_angular + 1)(max_radial + 1) with SiLU activations,
 trained on the GPU by this library's own kernels on exact (analytic GTO)
-radial integrals, evaluated with BF16 weights on the tensor cores.  Attached
-to a calculator with :meth:`RadialSurrogate.attach`, it replaces the spline in
-the FP32 dense power spectrum and its adjoint.
+radial integrals (Adam, then :meth:`RadialSurrogate.fit_output_layer`, a
+least-squares refit of the linear output layer on values and derivatives),
+evaluated on the tensor cores with BF16 operands, each weight and activation
+a sum of three BF16 parts, and FP32 accumulation.  Attached to a calculator
+with :meth:`RadialSurrogate.attach`, it replaces the spline in the FP32 dense
+power spectrum and its adjoint.
 """
 import ctypes
 
@@ -13,7 +16,9 @@ import numpy as np
 
 from . import _c_api as C
 
-METHODS = {"tensor_cores": 0, "cuda_cores": 1, "spline": 2, "analytic": 3}
+# "bf16_single": the CUDA cores with W2 and W3 rounded to one BF16 each, the
+# control that shows what three-part operands buy
+METHODS = {"tensor_cores": 0, "cuda_cores": 1, "spline": 2, "analytic": 3, "bf16_single": 4}
 
 
 def _stream():
@@ -56,13 +61,24 @@ class RadialSurrogate:
     def make_dataset(self, n_samples=1 << 20, seed=7):
         C.check(C.lib().featomic_b200_surrogate_dataset(self._handle, n_samples, seed, _stream()))
 
-    def train(self, steps, batch=8192, learning_rate=3e-3):
+    def train(self, steps, batch=8192, learning_rate=3e-3, derivative_weight=0.1):
+        """Adam steps; the loss is the mean squared error of the normalised
+        outputs plus ``derivative_weight`` times that of their derivatives
+        with respect to x = 2 r / cutoff - 1.  Returns the last loss."""
+        C.check(C.lib().featomic_b200_surrogate_set_derivative_weight(self._handle, float(derivative_weight)))
         loss = ctypes.c_double()
         C.check(C.lib().featomic_b200_surrogate_train(self._handle, steps, batch, learning_rate, ctypes.byref(loss),
                                                        _stream()))
         return loss.value
 
-    def loss_and_gradient(self, n):
+    def fit_output_layer(self, derivative_weight=0.01):
+        """Refit W3 and b3 by least squares over the whole training set:
+        squared error of the normalised outputs plus ``derivative_weight``
+        times that of their r-derivatives (FP64 normal equations on the GPU)."""
+        C.check(C.lib().featomic_b200_surrogate_fit_output_layer(self._handle, float(derivative_weight), _stream()))
+
+    def loss_and_gradient(self, n, derivative_weight=0.1):
+        C.check(C.lib().featomic_b200_surrogate_set_derivative_weight(self._handle, float(derivative_weight)))
         grad = np.zeros(self.n_parameters, dtype=np.float32)
         loss = ctypes.c_double()
         C.check(C.lib().featomic_b200_surrogate_gradient(self._handle, n,
