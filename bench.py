@@ -236,6 +236,37 @@ def run_reference(args):
     barrier(world)
 
 
+DENSE_PHASES = ("pair_features", "expansion", "contraction", "dl_dc", "pair_adjoint", "reductions")
+
+
+def dense_phase_times(calc):
+    """Device times (ms) of the phases of the calculator's last dense forward
+    and backward passes (featomic_b200_dense_timings)."""
+    import ctypes
+    from rascaline_b200 import _c_api as C
+    t = (ctypes.c_double * 6)()
+    C.check(C.lib().featomic_b200_dense_timings(calc._handle, t, 6))
+    return dict(zip(DENSE_PHASES, [float(x) for x in t]))
+
+
+def dense_rooflines(phases, n_atoms, S, K, n_keys, n_props, grad_rows, peak, peak_kind, word=4):
+    """HBM rooflines of the two tensor-core contractions of an FP32 dense
+    pass: the power spectrum (coefficients read, values written) and dL/dc
+    (coefficients and dL/dP rows read, dL/dc written); `grad_rows` dL/dP rows
+    are read (one per atom, or one per species for a linear model)."""
+    out = {}
+    contraction = word * n_atoms * (S * K + n_keys * n_props)
+    grad = word * (2 * n_atoms * S * K + grad_rows * n_keys * n_props)
+    for name, phase, bytes_ in (("contraction", "contraction", contraction), ("dl_dc", "dl_dc", grad)):
+        ms = phases.get(phase, 0.0)
+        achieved = bytes_ / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        out[name] = {"kernel": "dense_contraction_mma" if name == "contraction" else "dense_grad_coef_mma",
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes_per_launch": bytes_,
+                     "time_ms": ms}
+    return out
+
+
 def adjoint_form(steps, warmup, n=20000):
     """The adjoint form on the 20 000-atom strained box (``n`` atoms, for
     profiling smaller cases of the same workload): dense power spectrum
@@ -287,11 +318,15 @@ def adjoint_form(steps, warmup, n=20000):
         torch.cuda.synchronize()
         fwd = float(np.mean([s.elapsed_time(m) for s, m in zip(starts, mids)]))
         bwd = float(np.mean([m.elapsed_time(e) for m, e in zip(mids, ends)]))
+        phases = dense_phase_times(calc)
         values, forces, virial = run(precision, g)
         energy = float((values.double() * grad).sum())
-        results[precision] = dict(ms=fwd + bwd, forward_ms=fwd, backward_ms=bwd, energy=energy,
+        results[precision] = dict(ms=fwd + bwd, forward_ms=fwd, backward_ms=bwd, energy=energy, phases=phases,
                                   values=values.double(), forces=forces.double(), virial=virial.double())
     r32, r64 = results[32], results[64]
+    peak, peak_kind = measured_peaks()
+    K = 49 * 8
+    rooflines = dense_rooflines(r32["phases"], n, S, K, n_keys, n_props, n, peak, peak_kind)
 
     def rel(a, b):
         return float((a - b).abs().max() / b.abs().max())
@@ -304,6 +339,9 @@ def adjoint_form(steps, warmup, n=20000):
         "forward_ms": r32["forward_ms"],
         "backward_ms": r32["backward_ms"],
         "dtype": "f32",
+        "phases_ms": r32["phases"],
+        "roofline": rooflines["contraction"],
+        "roofline_dl_dc": rooflines["dl_dc"],
         "fp64_value": n / (r64["ms"] / 1000.0),
         "fp64_ms_per_step": r64["ms"],
         "error_vs_fp64": {
@@ -362,6 +400,7 @@ def batched_form(steps, warmup):
     ms = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)]))
     if batch.status() != 0:
         raise RuntimeError("the batched form reported an error")
+    phases = dense_phase_times(calc) if batch.config["pipeline"] == 1 else None
 
     # end to end: positions from pinned host memory, gradients and energies back
     host_pos = torch.as_tensor(positions).pin_memory()
@@ -428,6 +467,9 @@ def batched_form(steps, warmup):
                 "d2h_bytes_per_step": n * 12 + batch.n_systems * 4},
         "error_vs_fp64": errors,
         "gpu_launches_per_step": 1 if chosen["pipeline"] == 0 else 24,
+        "phases_ms": phases,
+        "roofline": dense_rooflines(phases, n, len(species), 49 * 8, batch.n_keys, batch.n_properties,
+                                    len(species), *measured_peaks())["contraction"] if phases else None,
         "steps": steps,
         "l2": "flushed between steps (256 MiB write); the 2.4 GB FP32 output also exceeds L2",
         "energy_model": "E = sum over atoms of w[centre species] . P, w ~ N(0, 1/sqrt(d)) seeded",
@@ -458,12 +500,15 @@ def surrogate_form(steps, warmup, train_steps=20000):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s.make_dataset(1 << 20, seed=7)
-    loss = s.train(train_steps, 8192, 3e-3)
+    loss = s.train(train_steps, 8192, 3e-3, derivative_weight=0.1)
+    s.fit_output_layer(0.01)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     r = torch.linspace(0.9, 6.0, 20001, dtype=torch.float64, device="cuda")
     exact, dexact = s.evaluate(r, "analytic")
     mlp, dmlp = s.evaluate(r, "tensor_cores")
+    fp32w, dfp32w = s.evaluate(r, "cuda_cores")
+    bf1, dbf1 = s.evaluate(r, "bf16_single")
     spl, dspl = s.evaluate(r, "spline")
     scale, dscale = exact.abs().amax(dim=0), dexact.abs().amax(dim=0)
 
@@ -476,6 +521,12 @@ def surrogate_form(steps, warmup, train_steps=20000):
     radial = {
         "mlp_values_rms": rms(mlp, exact, scale), "mlp_values_max": mx(mlp, exact, scale),
         "mlp_derivatives_rms": rms(dmlp, dexact, dscale), "mlp_derivatives_max": mx(dmlp, dexact, dscale),
+        # the same network with FP32 weights on the CUDA cores, and with one
+        # BF16 per weight: what three-part BF16 operands buy
+        "fp32_weights_control_values_max": mx(fp32w, exact, scale),
+        "fp32_weights_control_derivatives_max": mx(dfp32w, dexact, dscale),
+        "single_bf16_control_values_max": mx(bf1, exact, scale),
+        "single_bf16_control_derivatives_max": mx(dbf1, dexact, dscale),
         "spline_values_max": mx(spl, exact, scale), "spline_derivatives_max": mx(dspl, dexact, dscale),
         "normalisation": "each output divided by its largest magnitude over r in [0.9, 6] A",
     }
@@ -520,9 +571,31 @@ def surrogate_form(steps, warmup, train_steps=20000):
     mlp_err = float((vm.double() - v64).abs().max()) / v64_max
     mlp_rms = float(((vm.double() - v64) ** 2).mean().sqrt()) / float((v64 ** 2).mean().sqrt())
     del vm, v64
+    # forces (adjoint of a seeded random dL/dP) on a 5000-atom box of the same
+    # density and hypers: spline and MLP in FP32 against FP64
+    from rascaline_b200.torch_api import dense_backward
+    small = workloads.random_box(5000, density=0.1, min_distance=0.9, seed=16)
+    spos = torch.tensor(small["positions"], device="cuda")
+    scell = np.asarray(small["cell"]).reshape(1, 9)
+    sv64, st64 = dense_power_spectrum(calc, spos, small["types"], scell, [5000], 64)
+    G = torch.randn(sv64.shape, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+    f64, _, _ = dense_backward(st64, G, 1, cell=False)
+    _, st32 = dense_power_spectrum(calc, spos, small["types"], scell, [5000], 32)
+    f32, _, _ = dense_backward(st32, G.float(), 1, cell=False)
+    s.attach()
+    try:
+        _, stm = dense_power_spectrum(calc, spos, small["types"], scell, [5000], 32)
+        fm, _, _ = dense_backward(stm, G.float(), 1, cell=False)
+    finally:
+        s.attach(False)
+    forces = {"spline_fp32_max_abs_over_max": float((f32.double() - f64).abs().max() / f64.abs().max()),
+              "mlp_fp32_max_abs_over_max": float((fm.double() - f64).abs().max() / f64.abs().max()),
+              "workload": "random_box_5000_rho0.1_rc6_nmax11_lmax8, dL/dP ~ N(0, 1) seeded"}
+    del sv64, st64, st32, stm, G
     return {
         "workload": "random_box_100000_rho0.1_rc6_nmax11_lmax8_ps_values_fp32_spline_vs_mlp",
-        "training": {"samples": 1 << 20, "steps": train_steps, "batch": 8192, "seconds": train_s, "final_loss": loss},
+        "training": {"samples": 1 << 20, "steps": train_steps, "batch": 8192, "seconds": train_s, "final_loss": loss,
+                     "seconds_includes": "training set, Adam steps and the output-layer fit"},
         "radial_error_vs_exact": radial,
         "radial_evaluations_per_s": rates,
         "power_spectrum_error_vs_fp64": {
@@ -530,11 +603,119 @@ def surrogate_form(steps, warmup, train_steps=20000):
             "mlp_fp32_max_abs_over_max": mlp_err,
             "mlp_fp32_rms_over_rms": mlp_rms,
         },
+        "forces_error_vs_fp64": forces,
+        "training_recipe": "Adam on values + 0.1 x-derivatives, then least-squares output layer (lambda 0.01) on "
+                           "the tensor-core features; W2, W3 and activations as three BF16 parts on the tensor cores",
         "ms_per_step": {"fp64_spline": ms64, "fp32_spline": ms_spline, "fp32_mlp": ms_mlp},
         "atom_envs_per_s": {"fp64_spline": n / ms64 * 1e3, "fp32_spline": n / ms_spline * 1e3,
                             "fp32_mlp": n / ms_mlp * 1e3},
         "steps": steps,
         "note": "power spectrum values only (no gradients); the MLP replaces the spline in the FP32 pair features",
+    }
+
+
+def combined_form(steps, warmup, train_steps=20000, dropin_value=None):
+    """batched + surrogate + adjoint on the 4096 molecules of the batched
+    form: the learned radial surrogate (trained for these hypers: rc 5 A,
+    max_radial 7, max_angular 6, 56 outputs) replaces the spline in the
+    batch's dense pipeline (FP32 forward with the tensor-core contraction,
+    then the adjoint of a linear energy model and the energies), timed like
+    the batched form; errors against the FP64 spline path.  `vs_dropin` is
+    this value over the FP64 drop-in's atom-envs/s of the same run."""
+    import torch
+    import rascaline_b200 as rb
+    from rascaline_b200 import workloads
+    from rascaline_b200.surrogate import RadialSurrogate
+    from rascaline_b200.torch_api import Batch, dense_backward, dense_power_spectrum
+
+    mols = workloads.molecules(4096, seed=3)
+    positions = np.concatenate([m["positions"] for m in mols])
+    types = np.concatenate([m["types"] for m in mols]).astype(np.int32)
+    sizes = np.array([len(m["types"]) for m in mols])
+    species = [1, 6, 7, 8]
+    calc = rb.SoapPowerSpectrum(**workloads.hypers(5.0, 7, 6))
+    s = RadialSurrogate(calc, seed=3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.make_dataset(1 << 20, seed=7)
+    s.train(train_steps, 8192, 3e-3, derivative_weight=0.1)
+    s.fit_output_layer(0.01)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    batch = Batch(calc, sizes, types, species)
+    rng = np.random.default_rng(17)
+    W = rng.normal(0.0, 1.0 / np.sqrt(batch.n_keys * batch.n_properties),
+                   size=(len(species), batch.n_keys, batch.n_properties))
+    weights = torch.as_tensor(W, dtype=torch.float32, device="cuda").contiguous()
+    pos = torch.as_tensor(positions, device="cuda")
+    out = batch.outputs()
+    batch.config = {"warps": 4, "chunk": 32, "layout": 1, "ctas_per_sm": 2, "pipeline": 1}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    s.attach()
+    try:
+        for _ in range(max(3, warmup)):
+            batch.run(pos, out, weights=weights)
+        torch.cuda.synchronize()
+        stream = torch.cuda.current_stream()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            batch.run(pos, out, weights=weights)
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        ms = float(np.mean([a.elapsed_time(b) for a, b in zip(starts, ends)]))
+        phases = dense_phase_times(calc)
+        host_pos = torch.as_tensor(positions).pin_memory()
+        host_grad = torch.empty((batch.n_atoms, 3), dtype=torch.float32).pin_memory()
+        host_energy = torch.empty(batch.n_systems, dtype=torch.float32).pin_memory()
+        e2e = []
+        for k in range(max(3, steps // 2) + 2):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            pos.copy_(host_pos, non_blocking=True)
+            batch.run(pos, out, weights=weights)
+            host_grad.copy_(out["gradients"], non_blocking=True)
+            host_energy.copy_(out["energies"], non_blocking=True)
+            torch.cuda.synchronize()
+            if k >= 2:
+                e2e.append(time.perf_counter() - t1)
+        e2e_ms = 1000.0 * float(np.mean(e2e))
+    finally:
+        s.attach(False)
+    values64, state = dense_power_spectrum(calc, pos, types, np.zeros((len(mols), 9)), sizes, 64, species)
+    G = torch.as_tensor(W[np.searchsorted(species, types)], device="cuda")
+    grad64, _, _ = dense_backward(state, G, len(mols), strain=False, cell=False)
+    atom_energy = (values64 * G).sum(dim=(1, 2))
+    system = torch.as_tensor(np.repeat(np.arange(len(mols)), sizes), device="cuda")
+    energy64 = torch.zeros(len(mols), dtype=torch.float64, device="cuda").index_add_(0, system, atom_energy)
+
+    def rel(a, b):
+        return float((a.double() - b).abs().max() / b.abs().max())
+
+    errors = {
+        "values_max_abs_over_max": rel(out["values"], values64),
+        "gradients_max_abs_over_max": rel(out["gradients"], grad64),
+        "energies_max_abs_over_max": rel(out["energies"], energy64),
+    }
+    n = batch.n_atoms
+    value = n / (ms / 1000.0)
+    return {
+        "workload": "molecules_4096_sizes5-60_rc5_nmax7_lmax6_ps+gradients+energies_mlp_radial",
+        "metric": "atom-envs/s (power spectrum + forces)",
+        "value": value,
+        "ms_per_step": ms,
+        "vs_dropin": value / dropin_value if dropin_value else None,
+        "n_atoms": n,
+        "dtype": "f32 (radial integral: BF16 tensor-core MLP)",
+        "phases_ms": phases,
+        "e2e": {"value": n / (e2e_ms / 1000.0), "unit": "atom-envs/s", "h2d_bytes_per_step": n * 24,
+                "d2h_bytes_per_step": n * 12 + batch.n_systems * 4},
+        "error_vs_fp64": errors,
+        "surrogate_training_seconds": train_s,
+        "steps": steps,
+        "l2": "flushed between steps (256 MiB write)",
     }
 
 
@@ -637,7 +818,7 @@ def main():
                         help="skip the FP32 adjoint form measured beside the drop-in")
     parser.add_argument("--atoms", type=int, default=1000,
                         help="atoms in the box (1000 is the benchmark; smaller boxes are for profiling)")
-    parser.add_argument("--only", choices=["adjoint", "batched", "surrogate", "cg"],
+    parser.add_argument("--only", choices=["adjoint", "batched", "surrogate", "combined", "cg"],
                         help="run one chosen form alone and print its object (profiling)")
     parser.add_argument("--adjoint-atoms", type=int, default=20000,
                         help="atoms of the adjoint form's box with --only adjoint (20000 is the benchmark)")
@@ -648,7 +829,8 @@ def main():
         import torch
         torch.cuda.set_device(0)
         form = {"adjoint": lambda k, w: adjoint_form(k, w, args.adjoint_atoms), "batched": batched_form, "cg": cg_form,
-                "surrogate": lambda k, w: surrogate_form(k, w, args.train_steps)}[args.only]
+                "surrogate": lambda k, w: surrogate_form(k, w, args.train_steps),
+                "combined": lambda k, w: combined_form(k, w, args.train_steps)}[args.only]
         print(json.dumps({args.only + "_form": form(args.steps, args.warmup)}), flush=True)
         return
     global N_ATOMS, WORKLOAD
@@ -774,10 +956,27 @@ def main():
         line["adjoint_form"]["gpu_launches_per_step"] = 22
         line["batched_form"] = batched_form(args.steps, args.warmup)
         line["surrogate_form"] = surrogate_form(min(args.steps, 5), args.warmup, args.train_steps)
+        line["combined_form"] = combined_form(args.steps, args.warmup, args.train_steps, line["value"])
         line["cg_form"] = cg_form(min(args.steps, 10), args.warmup)
+        # a compact summary of the chosen forms placed before the long objects
+        forms = {}
+        for name in ("adjoint_form", "batched_form", "combined_form"):
+            f = line[name]
+            forms[name] = {"value": f["value"], "ms_per_step": f["ms_per_step"],
+                           "errors_vs_fp64": f["error_vs_fp64"],
+                           "roofline_frac": (f.get("roofline") or {}).get("frac")}
+        forms["combined_form"]["vs_dropin"] = line["combined_form"]["vs_dropin"]
+        sf = line["surrogate_form"]
+        forms["surrogate_form"] = {"power_spectrum_error_vs_fp64": sf["power_spectrum_error_vs_fp64"],
+                                   "forces_error_vs_fp64": sf["forces_error_vs_fp64"],
+                                   "radial_evaluations_per_s": sf["radial_evaluations_per_s"]}
+        line["forms"] = forms
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(system, hypers)
-    print(json.dumps(line), flush=True)
+    # the contract's keys and the forms' summary first, the long objects last
+    head = {k: v for k, v in line.items() if not k.endswith("_form")}
+    tail = {k: v for k, v in line.items() if k.endswith("_form")}
+    print(json.dumps({**head, **tail}), flush=True)
 
 
 if __name__ == "__main__":

@@ -464,6 +464,17 @@ featomic_status_t featomic_b200_surrogate_free(featomic_b200_surrogate_t* surrog
 featomic_status_t featomic_b200_radial_integral(const featomic_calculator_t* calculator, const double* r,
                                                 uintptr_t n_r, double* values, double* gradients, int32_t* knots);
 
+/* Device times (ms, CUDA events on the caller's stream) of the phases of the
+ * last dense forward and backward passes of this calculator
+ * (featomic_b200_power_spectrum_dense, ..._spherical_expansion_dense and
+ * their backward passes, the batched form's dense pipeline): [0] pair
+ * features, [1] expansion, [2] contraction, [3] dL/dc, [4] pair adjoint,
+ * [5] reductions; `count` entries at most are written.  Waits for the last
+ * backward pass; concurrent passes of one calculator overwrite each other's
+ * times.  No counterpart in featomic. */
+featomic_status_t featomic_b200_dense_timings(const featomic_calculator_t* calculator, double* times,
+                                             uintptr_t count);
+
 /* Per-phase device time (ms) of the last compute call of this calculator:
  * [neighbours, host metadata, pair features, expansion, contraction,
  *  device->host transfer, total wall, power-spectrum values kernel,

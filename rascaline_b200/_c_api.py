@@ -210,6 +210,8 @@ SIGNATURES = {
                                                      ctypes.c_void_p]),
     "featomic_b200_cg_couple": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32,
                                                     ctypes.c_void_p]),
+    "featomic_b200_dense_timings": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                                        ctypes.c_size_t]),
     "featomic_b200_calculator_timings": (featomic_status_t, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                              ctypes.c_size_t]),
 }

@@ -866,6 +866,16 @@ featomic_status_t featomic_b200_radial_integral(const featomic_calculator_t* cal
     });
 }
 
+featomic_status_t featomic_b200_dense_timings(const featomic_calculator_t* calculator, double* times,
+                                             uintptr_t count) {
+    return guarded([&] {
+        CHECK_POINTER(calculator);
+        CHECK_POINTER(times);
+        const std::vector<double> t = calculator->impl->engine->dense_times();
+        for (uintptr_t k = 0; k < count && k < t.size(); k++) times[k] = t[k];
+    });
+}
+
 featomic_status_t featomic_b200_calculator_timings(const featomic_calculator_t* calculator, double* times,
                                                    uintptr_t count) {
     return guarded([&] {

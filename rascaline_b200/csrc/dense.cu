@@ -830,15 +830,29 @@ void launch_dense_directions(const DevicePairs& pairs, const int32_t* atom_speci
 
 template <typename T>
 void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream) {
+    auto mark = [&](int k) {
+        if (a.marks) CUDA_CHECK(cudaEventRecord(a.marks[k], stream));
+    };
+    mark(0);
     launch_features<T, false>(a, n_pairs, stream);
-    if (a.n_atoms == 0) return;
+    mark(1);
+    if (a.n_atoms == 0) {
+        mark(2);
+        mark(3);
+        return;
+    }
     dense_expansion<T><<<(unsigned)(a.n_atoms * a.n_species),
                          coefficient_threads(a.layout.L2 * ((a.nmax + 1) / 2)), 0, stream>>>(a);
     CUDA_CHECK(cudaGetLastError());
-    if (a.values == nullptr) return;  // the expansion alone
+    mark(2);
+    if (a.values == nullptr) {  // the expansion alone
+        mark(3);
+        return;
+    }
     if constexpr (sizeof(T) == 4) {
         if (dense_mma_enabled() && dense_mma_supported(a)) {
             launch_dense_contraction_mma(a, stream);
+            mark(3);
             return;
         }
     }
@@ -852,6 +866,7 @@ void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t s
         dense_contraction<T><<<(unsigned)((items + warps - 1) / warps), 32 * warps, 0, stream>>>(a);
     }
     CUDA_CHECK(cudaGetLastError());
+    mark(3);
 }
 
 template <typename T>
@@ -881,8 +896,16 @@ void launch_dense_grad_coef(const DenseArgs<T>& a, cudaStream_t stream) {
 
 template <typename T>
 void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t stream, bool coef_grad_given) {
-    if (a.n_atoms == 0) return;
+    auto mark = [&](int k) {
+        if (a.marks) CUDA_CHECK(cudaEventRecord(a.marks[k], stream));
+    };
+    mark(4);
+    if (a.n_atoms == 0) {
+        for (int k = 5; k < 8; k++) mark(k);
+        return;
+    }
     if (!coef_grad_given) launch_dense_grad_coef(a, stream);
+    mark(5);
     bool fused = a.lmax <= DENSE_LMAX_SMALL && a.nmax <= 16 && a.tab.spline.splined;
     if constexpr (sizeof(T) == 4) fused = fused && a.surrogate == nullptr;
     if (n_pairs > 0 && fused) {
@@ -897,6 +920,7 @@ void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t 
         dense_pair_adjoint<T><<<(unsigned)((n_pairs + warps - 1) / warps), 32 * warps, 0, stream>>>(a, n_pairs);
         CUDA_CHECK(cudaGetLastError());
     }
+    mark(6);
     const bool partials = a.grad_strain || a.grad_cell;
     const int threads = 128;
     dense_atom_reduce<T><<<(unsigned)((a.n_atoms + threads - 1) / threads), threads, 0, stream>>>(a, partials ? 1 : 0);
@@ -905,6 +929,7 @@ void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t 
         dense_system_reduce<T><<<(unsigned)a.n_systems, 256, 0, stream>>>(a);
         CUDA_CHECK(cudaGetLastError());
     }
+    mark(7);
 }
 
 template <typename T>

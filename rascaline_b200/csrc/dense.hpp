@@ -49,6 +49,11 @@ struct DenseArgs {
     // FP32 only: R_nl and dR_nl/dr from the learned radial surrogate instead
     // of the spline
     RadialSurrogate* surrogate = nullptr;
+    // when set, events recorded on the stream between the phases: [0] before
+    // the pair features, [1] after them, [2] after the expansion, [3] after
+    // the contraction (forward); [4] before dL/dc, [5] after it, [6] after the
+    // pair adjoint, [7] after the reductions (backward)
+    cudaEvent_t* marks = nullptr;
 };
 
 // write the surrogate's R_nl(r) (and dR/dr when `derivs`) of every pair into

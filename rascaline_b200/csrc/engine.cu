@@ -259,6 +259,29 @@ Engine::Engine(const Hypers& h) : h_(h) {
 
 Engine::~Engine() {
     for (void* p : table_buffers_) cudaFree(p);
+    if (dense_marks_ready_)
+        for (auto& e : dense_marks_) cudaEventDestroy(e);
+}
+
+cudaEvent_t* Engine::dense_marks() {
+    if (!dense_marks_ready_) {
+        for (auto& e : dense_marks_) CUDA_CHECK(cudaEventCreate(&e));
+        dense_marks_ready_ = true;
+    }
+    return dense_marks_;
+}
+
+std::vector<double> Engine::dense_times() {
+    std::vector<double> t(6, 0.0);
+    if (!dense_marks_ready_) return t;
+    // the last marks of the forward and backward passes
+    if (cudaEventSynchronize(dense_marks_[3]) != cudaSuccess || cudaEventSynchronize(dense_marks_[7]) != cudaSuccess) {
+        cudaGetLastError();  // a pass that never ran: no times
+        return t;
+    }
+    for (int k = 0; k < 3; k++) t[k] = elapsed_ms(dense_marks_[k], dense_marks_[k + 1]);
+    for (int k = 0; k < 3; k++) t[3 + k] = elapsed_ms(dense_marks_[4 + k], dense_marks_[5 + k]);
+    return t;
 }
 
 void Engine::upload_tables() {
@@ -858,9 +881,11 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
     CUDA_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t), stream));
     const FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), false);
     void* features = arena_.alloc_bytes("dense.features", T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride);
+    cudaEvent_t* marks = dense_marks();
     if (precision == 64) {
         DenseArgs<double> a;
         dense_args(*st, false, a);
+        a.marks = marks;
         a.features = (double*)features;
         a.values = expansion ? nullptr : (double*)values;
         a.status = status;
@@ -868,6 +893,7 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
     } else {
         DenseArgs<float> a;
         dense_args(*st, false, a);
+        a.marks = marks;
         a.features = (float*)features;
         a.values = expansion ? nullptr : (float*)values;
         a.status = status;
@@ -947,9 +973,11 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
     void* pair_grad = arena_.alloc_bytes("dense.pair_grad", T_size * 3 * (size_t)std::max<int64_t>(P, 1));
     void* partial = arena_.alloc_bytes("dense.atom_partial", T_size * 18 * (size_t)st.n_atoms);
     int32_t* status = arena_.alloc<int32_t>("dense.status", 1);
+    cudaEvent_t* marks = dense_marks();
     if (st.precision == 64) {
         DenseArgs<double> a;
         dense_args(st, true, a);
+        a.marks = marks;
         a.features = (double*)features;
         a.grad_values = (const double*)grad_values;
         a.grad_species = by_species ? st.atom_species : nullptr;
@@ -964,6 +992,7 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
     } else {
         DenseArgs<float> a;
         dense_args(st, true, a);
+        a.marks = marks;
         a.features = (float*)features;
         a.grad_values = (const float*)grad_values;
         a.grad_species = by_species ? st.atom_species : nullptr;

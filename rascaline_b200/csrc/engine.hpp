@@ -339,6 +339,10 @@ class Engine {
     // precision
     void jvp_dense(DenseState& state, const void* tangent_positions, const void* tangent_cell, void* tangent_coef,
                    void* tangent_values, cudaStream_t stream);
+    // device times (ms) of the phases of the last dense forward and backward
+    // passes: pair features, expansion, contraction, dL/dc, pair adjoint,
+    // reductions (waits for the last backward pass; 0 for a phase not run)
+    std::vector<double> dense_times();
 
     // device tables for the kernels of the batched form (uploaded on first use)
     const DenseTables<float>& dense_tables_f() {
@@ -356,6 +360,11 @@ class Engine {
     void set_surrogate(const std::shared_ptr<RadialSurrogate>& s) { surrogate_ = s; }
 
   private:
+    // events between the phases of the dense forms (dense_times), created on
+    // first use on the engine's device
+    cudaEvent_t dense_marks_[8] = {};
+    bool dense_marks_ready_ = false;
+    cudaEvent_t* dense_marks();
     void upload_tables();
     template <typename T>
     void dense_args(const DenseState& st, bool grad, DenseArgs<T>& a);
