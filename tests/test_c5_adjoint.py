@@ -19,7 +19,7 @@ import pytest
 import rascaline_b200 as rb
 from rascaline_b200 import workloads
 
-from test_dense_adjoint import assert_close, dense_grad_values, key_of, linear_weights
+from test_dense_adjoint import assert_close, dense_grad_values, linear_weights
 
 pytestmark = pytest.mark.gpu
 
