@@ -329,6 +329,15 @@ featomic_status_t featomic_b200_dense_jvp(featomic_b200_dense_t* state, const vo
  * value.  No counterpart in featomic. */
 featomic_status_t featomic_b200_set_contraction_engine(int32_t tensor_cores, int32_t channels_per_round);
 
+/* Kernels of the FP64 spherical expansion (featomic_calculator_compute and
+ * featomic_b200_calculator_compute_device): `fused` = 1 (the default) builds
+ * every pair's cutoff, Y_lm and R_nl in shared memory inside the expansion
+ * kernel (max_angular <= 8 with splined radial integrals), 0 writes them to a
+ * per-pair record in device memory first and reads them back.  Both give
+ * identical results.  The environment variable FEATOMIC_B200_FUSED_SE ("0" or
+ * "1") is the initial setting.  Process-wide.  No counterpart in featomic. */
+featomic_status_t featomic_b200_set_expansion_engine(int32_t fused);
+
 /* ---- batched form: many molecules in one persistent launch ------------------
  *
  * Non-periodic systems (molecules) of up to 4096 atoms each, computed with
@@ -478,7 +487,9 @@ featomic_status_t featomic_b200_dense_timings(const featomic_calculator_t* calcu
 /* Per-phase device time (ms) of the last compute call of this calculator:
  * [neighbours, host metadata, pair features, expansion, contraction,
  *  device->host transfer, total wall, power-spectrum values kernel,
- *  power-spectrum positions-gradient kernel, strain / cell kernels] */
+ *  power-spectrum positions-gradient kernel, strain / cell kernels,
+ *  host metadata built before the contraction kernels launch, host labels
+ *  written while they run] */
 featomic_status_t featomic_b200_calculator_timings(const featomic_calculator_t* calculator, double* times,
                                                    uintptr_t count);
 

@@ -164,6 +164,7 @@ SIGNATURES = {
     "featomic_b200_dense_jvp": (featomic_status_t, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p]),
     "featomic_b200_set_contraction_engine": (featomic_status_t, [ctypes.c_int32, ctypes.c_int32]),
+    "featomic_b200_set_expansion_engine": (featomic_status_t, [ctypes.c_int32]),
     "featomic_b200_batch_create": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t,
                                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int32),
                                                        ctypes.POINTER(ctypes.c_int32), ctypes.c_size_t,

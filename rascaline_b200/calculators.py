@@ -409,10 +409,10 @@ class CalculatorBase:
 
     def timings(self):
         """Per-phase time (ms) of the last call."""
-        out = (ctypes.c_double * 10)()
-        C.check(C.lib().featomic_b200_calculator_timings(self._handle, out, 10))
+        out = (ctypes.c_double * 12)()
+        C.check(C.lib().featomic_b200_calculator_timings(self._handle, out, 12))
         names = ["neighbors", "metadata", "features", "expansion", "contraction", "transfer", "total",
-                 "ps_values", "ps_positions", "ps_strain_cell"]
+                 "ps_values", "ps_positions", "ps_strain_cell", "metadata_before_launch", "labels"]
         return dict(zip(names, list(out)))
 
 

@@ -551,6 +551,13 @@ featomic_status_t featomic_b200_set_contraction_engine(int32_t tensor_cores, int
     });
 }
 
+featomic_status_t featomic_b200_set_expansion_engine(int32_t fused) {
+    return guarded([&] {
+        if (fused != 0 && fused != 1) throw fb200::invalid_parameter("fused must be 0 or 1");
+        fb200::set_se_fused_enabled(fused == 1);
+    });
+}
+
 struct featomic_b200_batch_t {
     std::unique_ptr<fb200::BatchPlan> plan;
 };
@@ -882,9 +889,11 @@ featomic_status_t featomic_b200_calculator_timings(const featomic_calculator_t* 
         CHECK_POINTER(calculator);
         CHECK_POINTER(times);
         const PhaseTimes& t = calculator->impl->engine->last_times();
-        double all[10] = {t.neighbors, t.metadata,  t.features,     t.expansion,    t.contraction,
-                          t.transfer,  t.total,     t.ps_values,    t.ps_positions, t.ps_strain_cell};
-        for (uintptr_t k = 0; k < count && k < 10; k++) times[k] = all[k];
+        double all[12] = {t.neighbors,    t.metadata,       t.features,
+                          t.expansion,    t.contraction,    t.transfer,
+                          t.total,        t.ps_values,      t.ps_positions,
+                          t.ps_strain_cell, t.metadata_before_launch, t.labels};
+        for (uintptr_t k = 0; k < count && k < 12; k++) times[k] = all[k];
     });
 }
 

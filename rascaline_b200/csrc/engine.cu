@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include "dense.hpp"
@@ -231,6 +232,35 @@ T* upload(DeviceArena& arena, const std::string& name, const std::vector<T>& hos
     return d;
 }
 
+// A non-blocking stream per device for the metadata work beside the
+// spherical-expansion kernel (neighbourhood tables, uploads).  It has the
+// highest priority: its small kernels take SMs as soon as blocks of the
+// expansion retire instead of waiting for the whole grid.
+cudaStream_t copy_stream() {
+    static std::mutex mutex;
+    static std::map<int, cudaStream_t> streams;
+    int device = 0;
+    CUDA_CHECK(cudaGetDevice(&device));
+    std::lock_guard<std::mutex> lock(mutex);
+    auto it = streams.find(device);
+    if (it != streams.end()) return it->second;
+    cudaStream_t s = nullptr;
+    int least = 0, greatest = 0;
+    CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CUDA_CHECK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest));
+    streams[device] = s;
+    return s;
+}
+
+// makes `stream` wait for the uploads issued on the copy stream so far
+void join_uploads(cudaStream_t stream) {
+    cudaEvent_t done = nullptr;
+    CUDA_CHECK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    CUDA_CHECK(cudaEventRecord(done, copy_stream()));
+    CUDA_CHECK(cudaStreamWaitEvent(stream, done, 0));
+    CUDA_CHECK(cudaEventDestroy(done));  // released once the recorded work has completed
+}
+
 double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
@@ -259,8 +289,20 @@ Engine::Engine(const Hypers& h) : h_(h) {
 
 Engine::~Engine() {
     for (void* p : table_buffers_) cudaFree(p);
+    if (staging_) cudaFreeHost(staging_);
     if (dense_marks_ready_)
         for (auto& e : dense_marks_) cudaEventDestroy(e);
+}
+
+void* Engine::staging(size_t bytes) {
+    if (bytes > staging_bytes_) {
+        if (staging_) CUDA_CHECK(cudaFreeHost(staging_));
+        staging_ = nullptr;
+        staging_bytes_ = 0;
+        CUDA_CHECK(cudaHostAlloc(&staging_, bytes, cudaHostAllocDefault));
+        staging_bytes_ = bytes;
+    }
+    return staging_;
 }
 
 cudaEvent_t* Engine::dense_marks() {
@@ -348,12 +390,12 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
     auto t_start = std::chrono::steady_clock::now();
     const bool ps = kind == OUTPUT_POWER_SPECTRUM, by_pair = kind == OUTPUT_BY_PAIR;
     upload_tables();
-    cudaEvent_t ev[12];
+    cudaEvent_t ev[15];
     for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
     struct EventGuard {
         cudaEvent_t* e;
         ~EventGuard() {
-            for (int k = 0; k < 12; k++) cudaEventDestroy(e[k]);
+            for (int k = 0; k < 15; k++) cudaEventDestroy(e[k]);
         }
     } guard{ev};
     CUDA_CHECK(cudaEventRecord(ev[0], stream));
@@ -385,6 +427,22 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
         }
         d_positions = d;
     }
+
+    // atomic types -> species indices, uploaded while the stream is idle (a
+    // copy from pageable memory waits for the stream)
+    std::vector<int32_t> species_types, atom_species_h(n_atoms);
+    {
+        for (auto& s : systems) species_types.insert(species_types.end(), s.types.begin(), s.types.end());
+        std::sort(species_types.begin(), species_types.end());
+        species_types.erase(std::unique(species_types.begin(), species_types.end()), species_types.end());
+        int64_t a = 0;
+        for (auto& s : systems)
+            for (int32_t t : s.types)
+                atom_species_h[a++] =
+                    (int32_t)(std::lower_bound(species_types.begin(), species_types.end(), t) - species_types.begin());
+    }
+    const int S = (int)species_types.size();
+    int32_t* d_species = (!by_pair && n_atoms > 0) ? upload(arena_, "meta.atom_species", atom_species_h, stream) : nullptr;
 
     // ---- kernel (a): neighbour list ------------------------------------------
     DevicePairs pairs;
@@ -427,8 +485,12 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
 
     // ---- pair indices to the host, then the per-pair features run on the GPU
     // while the host builds the metadata ----------------------------------------
-    std::vector<int32_t> h_first(pairs.count), h_second(pairs.count), h_shift(by_pair ? 3 * pairs.count : 0);
-    if (pairs.count) {
+    // the power spectrum builds its neighbourhood tables on the device: the
+    // host needs no pair list
+    const bool device_tables = ps && n_atoms > 0;
+    std::vector<int32_t> h_first(device_tables ? 0 : pairs.count), h_second(device_tables ? 0 : pairs.count),
+        h_shift(by_pair ? 3 * pairs.count : 0);
+    if (pairs.count && !device_tables) {
         CUDA_CHECK(cudaMemcpyAsync(h_first.data(), pairs.first, sizeof(int32_t) * pairs.count, cudaMemcpyDeviceToHost, stream));
         CUDA_CHECK(cudaMemcpyAsync(h_second.data(), pairs.second, sizeof(int32_t) * pairs.count, cudaMemcpyDeviceToHost, stream));
         if (by_pair)
@@ -438,44 +500,68 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
     CUDA_CHECK(cudaEventRecord(ev[6], stream));
 
     FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), g.any());
-    double* features = arena_.alloc<double>("features", pairs.count * layout.stride);
+    // the spherical expansion builds its pair terms itself (fused kernel) or
+    // reads them from per-pair records
+    const bool fused_se = !by_pair && n_atoms > 0 && se_fused_enabled() && se_fused_supported(layout, d_radial_);
+    double* features = fused_se ? nullptr : arena_.alloc<double>("features", pairs.count * layout.stride);
     int32_t* status = arena_.alloc<int32_t>("status", 1);
     CUDA_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t), stream));
     CutoffParams cut{h_.cutoff, h_.smoothing_width, h_.smoothing, h_.scaling ? 1 : 0,
                      h_.scaling_scale, h_.scaling_rate, h_.scaling_exponent};
-    launch_pair_features(pairs, d_radial_, d_ylm_, cut, layout, features, status, stream);
+    if (!fused_se) launch_pair_features(pairs, d_radial_, d_ylm_, cut, layout, features, status, stream);
     CUDA_CHECK(cudaEventRecord(ev[2], stream));
 
     // ---- kernel (b): spherical expansion.  It needs the directions sorted by
     // (centre, neighbour species) in pair order, which the GPU sorts itself,
     // so it runs right after the pair features while the host builds the
     // neighbourhood tables and the output plan -------------------------------
-    std::vector<int32_t> species_types, atom_species_h(n_atoms);
-    {
-        for (auto& s : systems) species_types.insert(species_types.end(), s.types.begin(), s.types.end());
-        std::sort(species_types.begin(), species_types.end());
-        species_types.erase(std::unique(species_types.begin(), species_types.end()), species_types.end());
-        int64_t a = 0;
-        for (auto& s : systems)
-            for (int32_t t : s.types)
-                atom_species_h[a++] =
-                    (int32_t)(std::lower_bound(species_types.begin(), species_types.end(), t) - species_types.begin());
-    }
-    const int S = (int)species_types.size();
     auto t_meta0 = std::chrono::steady_clock::now();
     SeArgs se{};
     const bool run_se = !by_pair && n_atoms > 0;
+    DeviceNeighborhoods nb;
+    int32_t* nb_host_count = nullptr;
+    uint8_t* nb_host_mask = nullptr;
+    int64_t nb_capacity = 0;
+    int64_t* nb_host_offset = nullptr;
+    PsEntry* nb_host_entries = nullptr;
     if (run_se) {
         const int K = layout.L2 * layout.nmax;
         se.layout = layout;
         se.n_centres = n_atoms;
         se.n_species = S;
-        int32_t* d_species = upload(arena_, "meta.atom_species", atom_species_h, stream);
         int32_t* d_dir = arena_.alloc<int32_t>("meta.dir_code", 2 * pairs.count);
         int64_t* d_seg = arena_.alloc<int64_t>("meta.seg_offset", n_atoms * S + 1);
         // the same order as the host's counting sort (stable radix sort of
         // (centre, species) keys over pair << 1 | reversed)
         launch_dense_directions(pairs, d_species, S, n_atoms, d_dir, d_seg, arena_, stream);
+        if (device_tables) {
+            // the power spectrum's neighbourhood tables, built on the copy
+            // stream beside the expansion: the per-centre species counts come
+            // back first (the output plan needs them), then the entries (the
+            // labels need them); the contraction kernels wait for the copy
+            // stream (join_uploads)
+            cudaStream_t up = copy_stream();
+            CUDA_CHECK(cudaEventRecord(ev[14], stream));
+            CUDA_CHECK(cudaStreamWaitEvent(up, ev[14], 0));
+            nb = launch_neighborhoods(pairs, d_species, d_dir, d_seg, S, n_atoms, arena_, up);
+            // pinned staging: [entry offsets][entries][species counts][species mask]
+            nb_capacity = 2 * pairs.count + n_atoms;
+            const size_t b_offset = sizeof(int64_t) * (n_atoms + 1), b_entries = sizeof(PsEntry) * nb_capacity;
+            const size_t b_count = sizeof(int32_t) * n_atoms * S;
+            char* host = (char*)staging(b_offset + b_entries + b_count + n_atoms * S);
+            nb_host_offset = (int64_t*)host;
+            nb_host_entries = (PsEntry*)(host + b_offset);
+            nb_host_count = (int32_t*)(host + b_offset + b_entries);
+            nb_host_mask = (uint8_t*)(host + b_offset + b_entries + b_count);
+            CUDA_CHECK(cudaMemcpyAsync(nb_host_count, nb.species_count, b_count, cudaMemcpyDeviceToHost, up));
+            CUDA_CHECK(cudaMemcpyAsync(nb_host_mask, nb.species_mask, n_atoms * S, cudaMemcpyDeviceToHost, up));
+            CUDA_CHECK(cudaEventRecord(ev[12], up));
+            CUDA_CHECK(cudaMemcpyAsync(nb_host_offset, nb.entry_offset, sizeof(int64_t) * (n_atoms + 1),
+                                       cudaMemcpyDeviceToHost, up));
+            CUDA_CHECK(cudaMemcpyAsync(nb_host_entries, nb.entries, sizeof(PsEntry) * nb_capacity,
+                                       cudaMemcpyDeviceToHost, up));
+            CUDA_CHECK(cudaEventRecord(ev[13], up));
+        }
         se.centre_species = d_species;
         se.seg_offset = d_seg;
         se.dir_code = d_dir;
@@ -490,18 +576,55 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
         se.strain = g.strain ? arena_.alloc<double>("se.strain", n_atoms * S * 9 * K) : nullptr;
         se.cellg = g.cell ? arena_.alloc<double>("se.cell", n_atoms * S * 9 * K) : nullptr;
         CUDA_CHECK(cudaEventRecord(ev[7], stream));
-        launch_se_accumulate(se, stream);
+        if (fused_se) launch_se_fused(se, pairs, d_radial_, d_ylm_, cut, stream);
+        else launch_se_accumulate(se, stream);
         CUDA_CHECK(cudaEventRecord(ev[3], stream));
     }
 
-    CUDA_CHECK(cudaEventSynchronize(ev[6]));
-    Neighborhoods nh = build_neighborhoods(systems, pairs.count, h_first.data(), h_second.data());
-    if (nh.n_species != S) throw internal_error("species tables disagree");
+    if (!nh_) nh_ = std::make_unique<Neighborhoods>();
+    Neighborhoods& nh = *nh_;
+    if (device_tables) {
+        // the atoms' bookkeeping here, the per-centre species tables from the
+        // device; the entries follow before the labels are written
+        CUDA_CHECK(cudaEventSynchronize(ev[12]));
+        nh.n_atoms = n_atoms;
+        nh.n_species = S;
+        nh.species_types = species_types;
+        nh.atom_species = atom_species_h;
+        nh.atom_offset.resize(systems.size() + 1);
+        nh.atom_system.resize(n_atoms);
+        nh.atom_local.resize(n_atoms);
+        int64_t a = 0;
+        nh.atom_offset[0] = 0;
+        for (size_t s = 0; s < systems.size(); s++) {
+            for (int64_t i = 0; i < systems[s].n_atoms; i++, a++) {
+                nh.atom_system[a] = (int32_t)s;
+                nh.atom_local[a] = (int32_t)i;
+            }
+            nh.atom_offset[s + 1] = a;
+        }
+        nh.species_count.assign(nb_host_count, nb_host_count + n_atoms * S);
+        nh.species_mask.assign(nb_host_mask, nb_host_mask + n_atoms * S);
+    } else {
+        CUDA_CHECK(cudaEventSynchronize(ev[6]));
+        build_neighborhoods(systems, pairs.count, h_first.data(), h_second.data(), nh);
+        if (nh.n_species != S) throw internal_error("species tables disagree");
+    }
 
     OutputPlan plan = ps        ? plan_power_spectrum(nh, h_, g, /*with_labels=*/false)
                       : by_pair ? plan_by_pair(nh, h_, g, pairs.count, h_first.data(), h_second.data(), h_shift.data())
                                 : plan_spherical_expansion(nh, h_, g);
+    // the device's entries into the host tables, for the labels
+    auto load_entries = [&]() {
+        if (!device_tables) return;
+        CUDA_CHECK(cudaEventSynchronize(ev[13]));
+        nh.entry_offset.assign(nb_host_offset, nb_host_offset + n_atoms + 1);
+        const int64_t n_entries = nh.entry_offset[n_atoms];
+        if (n_entries > nb_capacity) throw internal_error("neighbour tables overflow");
+        nh.entries.assign(nb_host_entries, nb_host_entries + n_entries);
+    };
     auto t_meta1 = std::chrono::steady_clock::now();
+    auto t_launch = t_meta1;  // host time when the contraction kernels are queued
     double meta_extra = 0.0;  // host metadata work done later, overlapped with kernels
 
     auto tm = std::make_unique<TensorMap>();
@@ -564,6 +687,8 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
                                  "`cutoff`, or increasing the Gaussian's `width`.");
         }
     } else if (run_se && !plan.blocks.empty()) {
+        // the metadata goes up on the copy stream while the expansion runs
+        cudaStream_t up = copy_stream();
         std::vector<int64_t> offv, offp, offs, offc;
         for (auto& b : plan.blocks) {
             offv.push_back(b.off_values);
@@ -585,25 +710,28 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
             pa.strain = se.strain;
             pa.cellg = se.cellg;
             pa.dir_code = se.dir_code;
-            pa.slot_offset = upload(arena_, "ps.slot_offset", plan.slot_offset, stream);
-            pa.slots = upload(arena_, "ps.slots", plan.slots, stream);
-            pa.entry_offset = upload(arena_, "ps.entry_offset", nh.entry_offset, stream);
-            pa.entries = upload(arena_, "ps.entries", nh.entries, stream);
-            pa.entry_cum = upload(arena_, "ps.entry_cum", nh.entry_cum, stream);
-            pa.slot_row = upload(arena_, "ps.slot_row", plan.slot_row, stream);
-            pa.off_values = upload(arena_, "ps.offv", offv, stream);
-            pa.off_positions = upload(arena_, "ps.offp", offp, stream);
-            pa.off_strain = upload(arena_, "ps.offs", offs, stream);
-            pa.off_cell = upload(arena_, "ps.offc", offc, stream);
+            pa.slot_offset = upload(arena_, "ps.slot_offset", plan.slot_offset, up);
+            pa.slots = upload(arena_, "ps.slots", plan.slots, up);
+            pa.entry_offset = nb.entry_offset;
+            pa.entries = nb.entries;
+            pa.entry_cum = nb.entry_cum;
+            pa.slot_row = upload(arena_, "ps.slot_row", plan.slot_row, up);
+            pa.off_values = upload(arena_, "ps.offv", offv, up);
+            pa.off_positions = upload(arena_, "ps.offp", offp, up);
+            pa.off_strain = upload(arena_, "ps.offs", offs, up);
+            pa.off_cell = upload(arena_, "ps.offc", offc, up);
             pa.out = d_out;
+            join_uploads(stream);
             PsEvents pe;
             pe.after_values = ev[8];
             pe.after_strain_cell = ev[11];
             pe.before_positions = ev[10];
             pe.after_positions = ev[9];
+            t_launch = std::chrono::steady_clock::now();
             launch_power_spectrum(pa, g.positions, g.strain, g.cell, stream, pe);
             // the labels only describe the output: written while the kernels run
             auto t_labels = std::chrono::steady_clock::now();
+            load_entries();
             fill_power_spectrum_labels(nh, g, plan);
             meta_extra += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_labels).count();
         } else {
@@ -618,25 +746,27 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
             so.cellg = se.cellg;
             so.dir_code = se.dir_code;
             so.n_rows = (int64_t)plan.row_centre.size();
-            so.row_centre = upload(arena_, "so.row_centre", plan.row_centre, stream);
-            so.row_block = upload(arena_, "so.row_block", plan.row_block, stream);
-            so.row_sample = upload(arena_, "so.row_sample", plan.row_sample, stream);
+            so.row_centre = upload(arena_, "so.row_centre", plan.row_centre, up);
+            so.row_block = upload(arena_, "so.row_block", plan.row_block, up);
+            so.row_sample = upload(arena_, "so.row_sample", plan.row_sample, up);
             so.n_grad_rows = (int64_t)plan.grad_block.size();
-            so.grad_block = upload(arena_, "so.grad_block", plan.grad_block, stream);
-            so.grad_row = upload(arena_, "so.grad_row", plan.grad_row, stream);
-            so.grad_centre = upload(arena_, "so.grad_centre", plan.grad_centre, stream);
-            so.grad_atom = upload(arena_, "so.grad_atom", plan.grad_atom, stream);
+            so.grad_block = upload(arena_, "so.grad_block", plan.grad_block, up);
+            so.grad_row = upload(arena_, "so.grad_row", plan.grad_row, up);
+            so.grad_centre = upload(arena_, "so.grad_centre", plan.grad_centre, up);
+            so.grad_atom = upload(arena_, "so.grad_atom", plan.grad_atom, up);
             so.grad_d0 = upload(arena_, "so.grad_d0", plan.grad_d0, stream);
             so.grad_d1 = upload(arena_, "so.grad_d1", plan.grad_d1, stream);
-            so.block_l = upload(arena_, "so.block_l", plan.block_l, stream);
-            so.block_species = upload(arena_, "so.block_species", plan.block_species, stream);
-            so.off_values = upload(arena_, "so.offv", offv, stream);
-            so.off_positions = upload(arena_, "so.offp", offp, stream);
-            so.off_strain = upload(arena_, "so.offs", offs, stream);
-            so.off_cell = upload(arena_, "so.offc", offc, stream);
+            so.block_l = upload(arena_, "so.block_l", plan.block_l, up);
+            so.block_species = upload(arena_, "so.block_species", plan.block_species, up);
+            so.off_values = upload(arena_, "so.offv", offv, up);
+            so.off_positions = upload(arena_, "so.offp", offp, up);
+            so.off_strain = upload(arena_, "so.offs", offs, up);
+            so.off_cell = upload(arena_, "so.offc", offc, up);
             so.out = d_out;
+            join_uploads(stream);
             CUDA_CHECK(cudaEventRecord(ev[8], stream));
             CUDA_CHECK(cudaEventRecord(ev[9], stream));
+            t_launch = std::chrono::steady_clock::now();
             launch_se_output(so, g.positions, g.strain, g.cell, stream);
         }
         CUDA_CHECK(cudaEventRecord(ev[4], stream));
@@ -648,7 +778,10 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
                                  "`cutoff`, or increasing the Gaussian's `width`.");
         }
     } else {
-        if (ps) fill_power_spectrum_labels(nh, g, plan);
+        if (ps) {
+            load_entries();
+            fill_power_spectrum_labels(nh, g, plan);
+        }
         for (int k : {7, 3, 8, 9, 4}) CUDA_CHECK(cudaEventRecord(ev[k], stream));
     }
 
@@ -720,7 +853,9 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
     }
 
     times_.neighbors = elapsed_ms(ev[0], ev[1]);
-    times_.metadata = std::chrono::duration<double, std::milli>(t_meta1 - t_meta0).count() + meta_extra;
+    times_.metadata_before_launch = std::chrono::duration<double, std::milli>(t_launch - t_meta0).count();
+    times_.labels = meta_extra;
+    times_.metadata = times_.metadata_before_launch + meta_extra;
     times_.features = elapsed_ms(ev[6], ev[2]);
     times_.expansion = elapsed_ms(ev[7], ev[3]);
     times_.contraction = elapsed_ms(ev[3], ev[4]);

@@ -174,6 +174,16 @@ void launch_pair_features(const DevicePairs& pairs, const DeviceRadial& radial, 
                           const CutoffParams& cut, const FeatureLayout& layout, double* features, int32_t* status,
                           cudaStream_t stream);
 void launch_se_accumulate(const SeArgs& args, cudaStream_t stream);
+// pair_features + se_accumulate in one kernel (the pair terms built in shared
+// memory, args.features unused), for lmax <= 8 and splined radial
+// integrals; bit-identical results
+bool se_fused_supported(const FeatureLayout& layout, const DeviceRadial& radial);
+void launch_se_fused(const SeArgs& args, const DevicePairs& pairs, const DeviceRadial& radial, const DeviceYlm& ylm,
+                     const CutoffParams& cut, cudaStream_t stream);
+// whether the drop-in's spherical expansion uses the fused kernel (default)
+// or the two-kernel path; FEATOMIC_B200_FUSED_SE=0 selects the two kernels
+bool se_fused_enabled();
+void set_se_fused_enabled(bool enabled);
 
 // ---------------------------------------------------------------------------
 // Power spectrum (kernel c)
@@ -228,6 +238,23 @@ struct PsEvents {
 // second stream of the device; `stream` waits for both before later work
 void launch_power_spectrum(const PsArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream,
                            const PsEvents& events);
+
+// The power-spectrum kernels' neighbourhood tables built on the device from
+// the sorted directions: for every centre its unique neighbours (and itself)
+// by atom index, with the per-species prefix counts, the number of unique
+// neighbours of each species and the species present around it.  The merge
+// of the host's build_neighborhoods, one thread per centre, so the tables
+// are identical to the host's.
+struct DeviceNeighborhoods {
+    int64_t* entry_offset = nullptr;   // [n_atoms + 1]
+    PsEntry* entries = nullptr;        // [entry_offset[n_atoms]]
+    int32_t* entry_cum = nullptr;      // [entries][S + 1]
+    int32_t* species_count = nullptr;  // [n_atoms * S]
+    uint8_t* species_mask = nullptr;   // [n_atoms * S]
+};
+DeviceNeighborhoods launch_neighborhoods(const DevicePairs& pairs, const int32_t* atom_species, const int32_t* dir_code,
+                                         const int64_t* seg_offset, int n_species, int64_t n_atoms, DeviceArena& arena,
+                                         cudaStream_t stream);
 
 // Spherical expansion output scatter (spherical_expansion calculator)
 struct SeOutArgs {
@@ -288,6 +315,7 @@ void launch_by_pair(const ByPairArgs& args, bool positions, bool strain, bool ce
 namespace fb200 {
 
 struct DenseState;
+struct Neighborhoods;
 template <typename T>
 struct DenseArgs;
 class RadialSurrogate;
@@ -296,6 +324,9 @@ struct PhaseTimes {
     double neighbors = 0, metadata = 0, features = 0, expansion = 0, contraction = 0, transfer = 0, total = 0;
     // kernels of the contraction phase
     double ps_values = 0, ps_positions = 0, ps_strain_cell = 0;
+    // host metadata split: built before the contraction kernels can launch,
+    // and the output labels written while they run
+    double metadata_before_launch = 0, labels = 0;
 };
 
 // One calculator's GPU state: constant tables on the device, the workspace
@@ -384,6 +415,13 @@ class Engine {
     double* d_self_ = nullptr;
     std::vector<void*> table_buffers_;
     PhaseTimes times_;
+    // host neighbourhood tables of the power spectrum (labels), kept between
+    // calls for their storage, and a pinned buffer their device copy comes
+    // back through
+    std::unique_ptr<Neighborhoods> nh_;
+    void* staging_ = nullptr;
+    size_t staging_bytes_ = 0;
+    void* staging(size_t bytes);
 };
 
 }  // namespace fb200

@@ -1,6 +1,8 @@
 // Kernel (b): SOAP spherical expansion on the GPU, FP64.
 //
-// Two launches:
+// Two launches (or, for lmax <= 8, one: se_fused_kernel builds the pair
+// terms of each chunk of directions in shared memory instead of reading the
+// per-pair records from HBM):
 //
 // * `pair_features` -- one thread per half pair: cutoff / radial scaling,
 //   real spherical harmonics Y_lm (and their Cartesian gradients) by the
@@ -19,6 +21,8 @@
 //   first->second orientation, the self (centre) gradient, and the strain and
 //   cell gradients, with the (-1)^l / -(-1)^l factors of the reversed pair
 //   (spherical_expansion_pair.rs:130-163).
+#include <cstdlib>
+
 #include "engine.hpp"
 #include "pair_math.cuh"
 #include "soap_math.cuh"
@@ -213,6 +217,210 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
     }
 }
 
+// Fused form of pair_features + se_accumulate (lmax <= 8): one CTA per
+// (centre, neighbour species) segment.  For each chunk of FUSED_CHUNK
+// directions the pair terms are built in shared memory instead of being read
+// back from per-pair records in HBM: one thread per (direction, m) evaluates
+// column m of the Legendre table and then Y_l^{+-m} (+ gradients), one thread
+// per (direction, l) the radial integral R_nl (+ dR/dr), one thread per
+// direction the cutoff and radial scaling; then every thread accumulates two
+// radial functions of one (l, m) over the chunk's directions in pair order.
+// The same functions in the same order as the two-kernel path, so the results
+// are bit-identical to it; no atomics.
+constexpr int FUSED_CHUNK = 16;
+
+struct FusedDir {
+    double f, fg, r, u[3], v[3], sh[3];
+    int64_t pair;
+    int inv, self_image;
+};
+
+__host__ __device__ inline size_t fused_shared_doubles(int lmax, int nmax, bool grad) {
+    const int L2 = (lmax + 1) * (lmax + 1), LR = (lmax + 1) * nmax, NP = (lmax + 1) * (lmax + 2) / 2;
+    return (size_t)FUSED_CHUNK * (L2 * (grad ? 4 : 1) + LR * (grad ? 2 : 1) + NP);
+}
+
+template <bool POS, bool STRAIN, bool CELL>
+__global__ void __launch_bounds__(256, 2) se_fused_kernel(SeArgs a, DevicePairs pairs, DeviceRadial radial, DeviceYlm ylm,
+                                                        CutoffParams cut) {
+    constexpr bool GRAD = POS || STRAIN || CELL;
+    extern __shared__ double fsm[];
+    __shared__ FusedDir dirs[FUSED_CHUNK];
+    const FeatureLayout L = a.layout;
+    const int L2 = L.L2, N = L.nmax, LR = (L.lmax + 1) * N, NH = (N + 1) / 2, NP = (L.lmax + 1) * (L.lmax + 2) / 2;
+    double* Ys = fsm;                                      // [chunk][L2]
+    double* dYs = Ys + FUSED_CHUNK * L2;                   // [chunk][3][L2]
+    double* Rs = dYs + (GRAD ? FUSED_CHUNK * 3 * L2 : 0);  // [chunk][LR]
+    double* dRs = Rs + FUSED_CHUNK * LR;                   // [chunk][LR]
+    double* Ps = dRs + (GRAD ? FUSED_CHUNK * LR : 0);      // [chunk][NP] Legendre table
+    const int S = a.n_species;
+    const int64_t c = blockIdx.x / S;
+    const int t = (int)(blockIdx.x - c * S);
+    const int K = L2 * N;
+    const int tc = a.centre_species[c];
+    const int64_t d0 = a.seg_offset[c * S + t], d1 = a.seg_offset[c * S + t + 1];
+    // this thread's coefficients: (l, m) = lm and n = n0, n0 + 1
+    const int item = threadIdx.x;
+    const bool active = item < L2 * NH;
+    const int lm = active ? item / NH : 0;
+    const int n0 = active ? 2 * (item - lm * NH) : 0;
+    const bool has1 = n0 + 1 < N;
+    int l = (int)sqrt((double)lm);
+    while (l * l > lm) l--;
+    while ((l + 1) * (l + 1) <= lm) l++;
+    const double sign_l = (l & 1) ? -1.0 : 1.0;
+    const int ri = l * N + n0;
+    double acc[2] = {0.0, 0.0};
+    double sg[2][3], st[2][9], ce[2][9];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+#pragma unroll
+        for (int x = 0; x < 3; x++) sg[j][x] = 0.0;
+#pragma unroll
+        for (int x = 0; x < 9; x++) {
+            st[j][x] = 0.0;
+            ce[j][x] = 0.0;
+        }
+    }
+    for (int64_t dc = d0; dc < d1; dc += FUSED_CHUNK) {
+        const int nd = (int)min((int64_t)FUSED_CHUNK, d1 - dc);
+        const int lcols = L.lmax + 1;
+        __syncthreads();
+        // threads [0, nd * lcols): direction q, Legendre column m (the m = 0
+        // thread also writes the direction's scalars); threads
+        // [nd * lcols, 2 nd * lcols): direction q, radial channel l
+        for (int w = threadIdx.x; w < 2 * nd * lcols; w += blockDim.x) {
+            const bool column = w < nd * lcols;
+            const int wq = column ? w : w - nd * lcols;
+            const int q = wq / lcols, j = wq - q * lcols;
+            const int32_t code = a.dir_code[dc + q];
+            const int64_t p = code >> 1;
+            const double r = pairs.distance[p];
+            if (!column) {
+                radial_spline_compute(radial, j, r, Rs + q * LR + j * N, GRAD ? dRs + q * LR + j * N : nullptr);
+                continue;
+            }
+            // the direction's unit vector and scalars, as pair_features_kernel computes them
+            const double v0 = pairs.vector[3 * p], v1 = pairs.vector[3 * p + 1], v2 = pairs.vector[3 * p + 2];
+            double u0 = v0 / r, u1 = v1 / r, u2 = v2 / r;
+            if (r < 1e-6) {
+                // coincident atoms: spherical_expansion_pair.rs:337-339
+                u0 = 0.0;
+                u1 = 0.0;
+                u2 = 1.0;
+            }
+            ylm_legendre_column(ylm, ylm_angles(u0, u1, u2), j, Ps + q * NP);
+            if (j != 0) continue;
+            double fc, dfc;
+            soap::cutoff_function(cut.smoothing, cut.rc, cut.width, r, &fc, &dfc);
+            double sc = 1.0, dsc = 0.0;
+            if (cut.scaling) soap::willatt2018(cut.scale, cut.rate, cut.exponent, r, &sc, &dsc);
+            FusedDir& D = dirs[q];
+            D.f = sc * fc;
+            D.fg = dfc * sc + fc * dsc;
+            D.r = r;
+            D.u[0] = u0;
+            D.u[1] = u1;
+            D.u[2] = u2;
+            D.v[0] = v0;
+            D.v[1] = v1;
+            D.v[2] = v2;
+            for (int x = 0; x < 3; x++) D.sh[x] = (double)pairs.shift[3 * p + x];
+            D.pair = p;
+            D.inv = code & 1;
+            D.self_image = pairs.first[p] == pairs.second[p];
+        }
+        __syncthreads();
+        // Y_l^{+-m} (+ gradients) of every (direction, m) from the complete table
+        for (int w = threadIdx.x; w < nd * lcols; w += blockDim.x) {
+            const int q = w / lcols, m = w - q * lcols;
+            const FusedDir& D = dirs[q];
+            double* Y = Ys + q * L2;
+            double* G = GRAD ? dYs + q * 3 * L2 : nullptr;
+            ylm_column_outputs(ylm, ylm_angles(D.u[0], D.u[1], D.u[2]), m, Ps + q * NP, Y, G,
+                               GRAD ? G + L2 : nullptr, GRAD ? G + 2 * L2 : nullptr);
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int q = 0; q < nd; q++) {
+            const FusedDir& D = dirs[q];
+            const double Yv = Ys[q * L2 + lm];
+            double dY[3] = {0.0, 0.0, 0.0};
+            if (GRAD) {
+#pragma unroll
+                for (int x = 0; x < 3; x++) dY[x] = dYs[(q * 3 + x) * L2 + lm];
+            }
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                if (j == 1 && !has1) break;
+                const double Rv = Rs[q * LR + ri + j];
+                const double val = D.f * Yv * Rv;
+                acc[j] += D.inv ? sign_l * val : val;
+                if (!GRAD) continue;
+                const double dR = dRs[q * LR + ri + j];
+                double g[3];
+#pragma unroll
+                for (int x = 0; x < 3; x++) g[x] = D.fg * D.u[x] * Rv * Yv + D.f * dR * D.u[x] * Yv + D.f * Rv * dY[x] / D.r;
+                const int k = lm * N + n0 + j;
+                if (POS && !D.inv) {
+                    double* pg = a.pair_grad + D.pair * 3 * K;
+                    pg[k] = g[0];
+                    pg[K + k] = g[1];
+                    pg[2 * K + k] = g[2];
+                }
+                const double gf = D.inv ? -sign_l : 1.0;
+                const double gi[3] = {gf * g[0], gf * g[1], gf * g[2]};
+                if (POS && !D.self_image) {
+                    sg[j][0] -= gi[0];
+                    sg[j][1] -= gi[1];
+                    sg[j][2] -= gi[2];
+                }
+                if (STRAIN) {
+#pragma unroll
+                    for (int x = 0; x < 3; x++) {
+                        const double vx = D.inv ? -D.v[x] : D.v[x];
+#pragma unroll
+                        for (int y = 0; y < 3; y++) st[j][x * 3 + y] += vx * gi[y];
+                    }
+                }
+                if (CELL) {
+#pragma unroll
+                    for (int x = 0; x < 3; x++) {
+                        const double sx = D.inv ? -D.sh[x] : D.sh[x];
+#pragma unroll
+                        for (int y = 0; y < 3; y++) ce[j][x * 3 + y] += sx * gi[y];
+                    }
+                }
+            }
+        }
+    }
+    if (!active) return;
+    const int64_t base = c * S + t;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        if (j == 1 && !has1) break;
+        const int n = n0 + j, k = lm * N + n;
+        const double self = (t == tc && l == 0) ? a.self_contribution[n] : 0.0;
+        a.coef[base * K + k] = self + acc[j];
+        if (POS) {
+            double* sgp = a.self_grad + base * 3 * K;
+            sgp[k] = sg[j][0];
+            sgp[K + k] = sg[j][1];
+            sgp[2 * K + k] = sg[j][2];
+        }
+        if (STRAIN) {
+            double* o = a.strain + base * 9 * K;
+#pragma unroll
+            for (int x = 0; x < 9; x++) o[x * K + k] = st[j][x];
+        }
+        if (CELL) {
+            double* o = a.cellg + base * 9 * K;
+#pragma unroll
+            for (int x = 0; x < 9; x++) o[x * K + k] = ce[j][x];
+        }
+    }
+}
+
 // spherical_expansion calculator output: values / strain / cell of one
 // (block, sample) row per CTA
 __global__ void se_output_rows_kernel(SeOutArgs a, int do_strain, int do_cell) {
@@ -307,6 +515,54 @@ void launch_se_accumulate(const SeArgs& args, cudaStream_t stream) {
     else if (!p && !st && ce) SE_LAUNCH(false, false, true);
     else SE_LAUNCH(false, true, true);
 #undef SE_LAUNCH
+    CUDA_CHECK(cudaGetLastError());
+}
+
+namespace {
+int fused_state = -1;  // -1: not read from the environment yet
+}
+
+bool se_fused_enabled() {
+    if (fused_state < 0) {
+        const char* env = std::getenv("FEATOMIC_B200_FUSED_SE");
+        fused_state = (env && env[0] == '0') ? 0 : 1;
+    }
+    return fused_state == 1;
+}
+
+void set_se_fused_enabled(bool enabled) { fused_state = enabled ? 1 : 0; }
+
+bool se_fused_supported(const FeatureLayout& layout, const DeviceRadial& radial) {
+    const size_t bytes = sizeof(double) * fused_shared_doubles(layout.lmax, layout.nmax, layout.with_grad);
+    const int items = layout.L2 * ((layout.nmax + 1) / 2);
+    return radial.splined && layout.lmax <= LMAX_SMALL && items <= 256 && bytes <= 160 * 1024;
+}
+
+void launch_se_fused(const SeArgs& args, const DevicePairs& pairs, const DeviceRadial& radial, const DeviceYlm& ylm,
+                     const CutoffParams& cut, cudaStream_t stream) {
+    if (args.n_centres == 0) return;
+    const FeatureLayout& L = args.layout;
+    const int items = L.L2 * ((L.nmax + 1) / 2);
+    const int threads = std::max(32, (items + 31) / 32 * 32);
+    const size_t smem = sizeof(double) * fused_shared_doubles(L.lmax, L.nmax, L.with_grad);
+    const bool grad = L.with_grad;
+    const bool p = grad && args.do_positions, st = grad && args.do_strain, ce = grad && args.do_cell;
+    const unsigned blocks = (unsigned)(args.n_centres * args.n_species);
+#define SE_FUSED(P, ST, CE)                                                                                           \
+    do {                                                                                                              \
+        CUDA_CHECK(cudaFuncSetAttribute(se_fused_kernel<P, ST, CE>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                        (int)smem));                                                                  \
+        se_fused_kernel<P, ST, CE><<<blocks, threads, smem, stream>>>(args, pairs, radial, ylm, cut);                 \
+    } while (0)
+    if (!p && !st && !ce) SE_FUSED(false, false, false);
+    else if (p && !st && !ce) SE_FUSED(true, false, false);
+    else if (p && st && !ce) SE_FUSED(true, true, false);
+    else if (p && st && ce) SE_FUSED(true, true, true);
+    else if (p && !st && ce) SE_FUSED(true, false, true);
+    else if (!p && st && !ce) SE_FUSED(false, true, false);
+    else if (!p && !st && ce) SE_FUSED(false, false, true);
+    else SE_FUSED(false, true, true);
+#undef SE_FUSED
     CUDA_CHECK(cudaGetLastError());
 }
 

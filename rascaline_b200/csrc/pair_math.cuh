@@ -231,24 +231,139 @@ __device__ __forceinline__ void ylm_rows(const DeviceYlmT<T>& tab, T ux, T uy, T
     }
 }
 
+// The same harmonics split by column m, for one thread per (direction, m).
+// The direction's angles, as ylm_compute derives them:
+template <typename T>
+struct YlmAngles {
+    T ct, st, cp, sp;
+};
+
+template <typename T>
+__device__ __forceinline__ YlmAngles<T> ylm_angles(T ux, T uy, T uz) {
+    YlmAngles<T> a;
+    const T sxy = hypot(ux, uy);
+    a.ct = uz;
+    a.st = sxy;
+    if (sxy > T(soap::DBL_EPS)) {
+        a.cp = ux / sxy;
+        a.sp = uy / sxy;
+    } else {
+        a.cp = T(1);
+        a.sp = T(0);
+    }
+    return a;
+}
+
+// Column m of the associated Legendre table, P(l, m) for l = m..lmax, written
+// to P[lidx(l, m)].  The recursions of ylm_compute restricted to one column
+// (every P(l, m) depends on P(l - 1, m), P(l - 2, m) and the diagonal chain
+// only), with the same operations in the same order.
+template <typename T>
+__device__ __forceinline__ void ylm_legendre_column(const DeviceYlmT<T>& tab, const YlmAngles<T>& a, int m,
+                                                    T* __restrict__ P) {
+    const int lmax = tab.lmax;
+    const T SQRT_1_OVER_2PI = T(0.3989422804014327);
+    const T SQRT_3 = T(1.7320508075688772);
+    const T SQRT_3_OVER_2 = T(1.224744871391589);
+    T value = SQRT_1_OVER_2PI;  // P(m, m) after m steps of the diagonal chain
+    if (m >= 1) value *= -SQRT_3_OVER_2 * a.st;
+    for (int l = 2; l <= m; l++) value *= -tab.sq_half[l] * a.st;
+    P[lidx(m, m)] = value;
+    if (m + 1 > lmax) return;
+    T pm2 = value;
+    T pm1 = m == 0 ? a.ct * SQRT_3 * value : a.ct * tab.sq_2l1[m + 1] * value;
+    P[lidx(m + 1, m)] = pm1;
+    for (int l = m + 2; l <= lmax; l++) {
+        const T p = tab.A[lidx(l, m)] * (a.ct * pm1 + tab.B[lidx(l, m)] * pm2);
+        P[lidx(l, m)] = p;
+        pm2 = pm1;
+        pm1 = p;
+    }
+}
+
+// Y_l^{+-m} (and gradients when GX != nullptr) of column m for l = m..lmax,
+// from the complete Legendre table P (all columns), indexed l^2 + l + m as in
+// ylm_compute; the same operations in the same order.
+template <typename T>
+__device__ __forceinline__ void ylm_column_outputs(const DeviceYlmT<T>& tab, const YlmAngles<T>& a, int m,
+                                                   const T* __restrict__ P, T* __restrict__ Y, T* __restrict__ GX,
+                                                   T* __restrict__ GY, T* __restrict__ GZ) {
+    const int lmax = tab.lmax;
+    const T SQRT_2 = T(1.4142135623730951);
+    const T ct = a.ct, st = a.st, cp = a.cp, sp = a.sp;
+    const bool grad = GX != nullptr;
+    if (m == 0) {
+        for (int l = 0; l <= lmax; l++) Y[l * l + l] = P[lidx(l, 0)] / SQRT_2;
+        if (grad) {
+            GX[0] = T(0);
+            GY[0] = T(0);
+            GZ[0] = T(0);
+            for (int l = 1; l <= lmax; l++) {
+                T lf = tab.sq_ll1[l] * P[lidx(l, 1)];
+                GX[l * l + l] = cp * ct * lf;
+                GY[l * l + l] = sp * ct * lf;
+                GZ[l * l + l] = -st * lf;
+            }
+        }
+        return;
+    }
+    T cos1 = T(1), sin1 = T(0), cos2 = -cp, sin2 = sp;
+    T m2c = T(-2) * cp;
+    T smp = T(0), cmp = T(0);
+    for (int k = 1; k <= m; k++) {
+        smp = m2c * sin1 - sin2;
+        cmp = m2c * cos1 - cos2;
+        sin2 = sin1;
+        sin1 = smp;
+        cos2 = cos1;
+        cos1 = cmp;
+    }
+    for (int l = m; l <= lmax; l++) {
+        T p = P[lidx(l, m)];
+        Y[l * l + l + m] = p * cmp;
+        Y[l * l + l - m] = p * smp;
+    }
+    if (!grad) return;
+    for (int l = m; l <= lmax; l++) {
+        // derivative factor (:256-298) and P / sin(theta) or its pole form
+        T dp;
+        if (m < l) dp = tab.sq_plus[lidx(l, m)] * P[lidx(l, m - 1)] - tab.sq_minus[lidx(l, m)] * P[lidx(l, m + 1)];
+        else dp = tab.sq_plus[lidx(l, l)] * P[lidx(l, l - 1)] - tab.sq_minus[lidx(l, l)] * T(0);
+        T pot = st > T(0.1) ? (T)m / st * P[lidx(l, m)] : T(-0.5) / ct * dp;
+        T sdp = smp * dp, cdp = cmp * dp;
+        GX[l * l + l + m] = sp * pot * smp - T(0.5) * ct * cp * cdp;
+        GX[l * l + l - m] = -sp * pot * cmp - T(0.5) * ct * cp * sdp;
+        GY[l * l + l + m] = -cp * pot * smp - T(0.5) * ct * sp * cdp;
+        GY[l * l + l - m] = cp * pot * cmp - T(0.5) * ct * sp * sdp;
+        GZ[l * l + l + m] = T(0.5) * st * cdp;
+        GZ[l * l + l - m] = T(0.5) * st * sdp;
+    }
+}
+
 // Radial integral of one angular channel in FP64: Hermite spline
 // (featomic/src/math/splines.rs:225-289) or the analytic GTO integral times
 // the orthonormalisation matrix (radial_integral/gto.rs:115-205).  Returns
 // false when the analytic integral did not converge.
+__device__ inline void radial_spline_compute(const DeviceRadial& R, int l, double r, double* __restrict__ val,
+                                             double* __restrict__ grad) {
+    const int N = R.nmax;
+    const double* pos = R.positions + R.knot_offset[l];
+    int count = R.knot_count[l];
+    int k = soap::spline_interval(pos, count, r);
+    soap::HermiteWeights w = soap::hermite_weights(pos[k], pos[k + 1], r);
+    const double* pv = R.values + ((size_t)R.knot_offset[l] + k) * N;
+    const double* pd = R.derivs + ((size_t)R.knot_offset[l] + k) * N;
+    for (int n = 0; n < N; n++) {
+        val[n] = soap::hermite_value(w, pv[n], pd[n], pv[N + n], pd[N + n]);
+        if (grad) grad[n] = soap::hermite_derivative(w, pv[n], pd[n], pv[N + n], pd[N + n]);
+    }
+}
+
 __device__ inline bool radial_compute(const DeviceRadial& R, int l, double r, double* __restrict__ val,
                                       double* __restrict__ grad) {
     const int N = R.nmax;
     if (R.splined) {
-        const double* pos = R.positions + R.knot_offset[l];
-        int count = R.knot_count[l];
-        int k = soap::spline_interval(pos, count, r);
-        soap::HermiteWeights w = soap::hermite_weights(pos[k], pos[k + 1], r);
-        const double* pv = R.values + ((size_t)R.knot_offset[l] + k) * N;
-        const double* pd = R.derivs + ((size_t)R.knot_offset[l] + k) * N;
-        for (int n = 0; n < N; n++) {
-            val[n] = soap::hermite_value(w, pv[n], pd[n], pv[N + n], pd[N + n]);
-            if (grad) grad[n] = soap::hermite_derivative(w, pv[n], pd[n], pv[N + n], pd[N + n]);
-        }
+        radial_spline_compute(R, l, r, val, grad);
         return true;
     }
     double raw[64], graw[64];

@@ -11,66 +11,100 @@
 // gradient sample labels are the only per-row work.
 #include "plan.hpp"
 
+#include <omp.h>
+
 #include <algorithm>
 
 namespace fb200 {
 
-Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_t n_pairs, const int32_t* first,
-                                  const int32_t* second) {
-    Neighborhoods nh;
+void build_neighborhoods(const std::vector<HostSystem>& systems, int64_t n_pairs, const int32_t* first,
+                         const int32_t* second, Neighborhoods& nh) {
+    // every vector is resized, not reallocated: a Neighborhoods kept by the
+    // caller between calls reuses its storage (no page faults on the host)
     int64_t n_atoms = 0;
     for (auto& s : systems) n_atoms += s.n_atoms;
     nh.n_atoms = n_atoms;
     nh.atom_offset.resize(systems.size() + 1);
     nh.atom_system.resize(n_atoms);
     nh.atom_local.resize(n_atoms);
-    std::vector<int32_t> types(n_atoms);
+    nh.atom_species.resize(n_atoms);
     {
         int64_t a = 0;
         nh.atom_offset[0] = 0;
         for (size_t s = 0; s < systems.size(); s++) {
             for (int64_t i = 0; i < systems[s].n_atoms; i++, a++) {
-                types[a] = systems[s].types[i];
                 nh.atom_system[a] = (int32_t)s;
                 nh.atom_local[a] = (int32_t)i;
             }
             nh.atom_offset[s + 1] = a;
         }
     }
-    nh.species_types = types;
+    nh.species_types.clear();
+    for (auto& s : systems) nh.species_types.insert(nh.species_types.end(), s.types.begin(), s.types.end());
     std::sort(nh.species_types.begin(), nh.species_types.end());
     nh.species_types.erase(std::unique(nh.species_types.begin(), nh.species_types.end()), nh.species_types.end());
     const int S = nh.n_species = (int)nh.species_types.size();
-    nh.atom_species.resize(n_atoms);
-    for (int64_t a = 0; a < n_atoms; a++)
-        nh.atom_species[a] = (int32_t)(std::lower_bound(nh.species_types.begin(), nh.species_types.end(), types[a]) -
-                                       nh.species_types.begin());
+    if (S > 64) throw invalid_parameter("more than 64 atomic types are not supported");
+    {
+        int64_t a = 0;
+        for (auto& s : systems)
+            for (int32_t t : s.types)
+                nh.atom_species[a++] = (int32_t)(std::lower_bound(nh.species_types.begin(), nh.species_types.end(), t) -
+                                                 nh.species_types.begin());
+    }
     const int32_t* sp = nh.atom_species.data();
 
-    // directions: counting sort on (centre, species of the other atom), stable in pair order
-    nh.seg_offset.assign((size_t)n_atoms * S + 1, 0);
-    int64_t* seg = nh.seg_offset.data();
-    for (int64_t p = 0; p < n_pairs; p++) {
-        seg[(size_t)first[p] * S + sp[second[p]] + 1]++;
-        seg[(size_t)second[p] * S + sp[first[p]] + 1]++;
-    }
-    for (size_t k = 1; k < nh.seg_offset.size(); k++) seg[k] += seg[k - 1];
-    std::vector<int64_t> fill(nh.seg_offset.begin(), nh.seg_offset.end() - 1);
+    // directions: counting sort on (centre, species of the other atom),
+    // stable in pair order.  Each thread counts a contiguous range of pairs;
+    // a thread's slice of every bin starts after the slices of the threads
+    // before it, so the parallel fill keeps pair order inside every bin.
+    const int64_t n_bins = n_atoms * S;
+    nh.seg_offset.assign((size_t)n_bins + 1, 0);
     nh.dir_code.resize(2 * (size_t)n_pairs);
+    int64_t* seg = nh.seg_offset.data();
     int32_t* dir = nh.dir_code.data();
-    for (int64_t p = 0; p < n_pairs; p++) {
-        dir[fill[(size_t)first[p] * S + sp[second[p]]]++] = (int32_t)(p << 1);
-        dir[fill[(size_t)second[p] * S + sp[first[p]]]++] = (int32_t)((p << 1) | 1);
+    const int n_threads = std::max(1, std::min(omp_get_max_threads(), (int)std::min<int64_t>(64, n_pairs / 2048 + 1)));
+    nh.bin_scratch.assign((size_t)n_threads * n_bins, 0);
+    int64_t* local = nh.bin_scratch.data();
+#pragma omp parallel num_threads(n_threads)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const int64_t p0 = n_pairs * t / nt, p1 = n_pairs * (t + 1) / nt;
+        int64_t* mine = local + (size_t)t * n_bins;
+        for (int64_t p = p0; p < p1; p++) {
+            mine[(size_t)first[p] * S + sp[second[p]]]++;
+            mine[(size_t)second[p] * S + sp[first[p]]]++;
+        }
+#pragma omp barrier
+        // bin totals and each thread's starting position, by bin ranges
+        const int64_t b0 = n_bins * t / nt, b1 = n_bins * (t + 1) / nt;
+        for (int64_t b = b0; b < b1; b++) {
+            int64_t total = 0;
+            for (int k = 0; k < nt; k++) {
+                const int64_t c = local[(size_t)k * n_bins + b];
+                local[(size_t)k * n_bins + b] = total;
+                total += c;
+            }
+            seg[b + 1] = total;
+        }
+#pragma omp barrier
+#pragma omp single
+        for (int64_t b = 1; b <= n_bins; b++) seg[b] += seg[b - 1];
+        for (int64_t p = p0; p < p1; p++) {
+            const size_t bf = (size_t)first[p] * S + sp[second[p]], bs = (size_t)second[p] * S + sp[first[p]];
+            dir[seg[bf] + mine[bf]++] = (int32_t)(p << 1);
+            dir[seg[bs] + mine[bs]++] = (int32_t)((p << 1) | 1);
+        }
     }
     // the other atom of every direction, in segment order: the merges below
     // then read one contiguous array per segment
-    std::vector<int32_t> other_atom(2 * (size_t)n_pairs);
+    nh.other_atom.resize(2 * (size_t)n_pairs);
+    int32_t* other = nh.other_atom.data();
 #pragma omp parallel for schedule(static)
     for (int64_t k = 0; k < 2 * n_pairs; k++) {
         const int32_t code = dir[k];
-        other_atom[k] = (code & 1) ? first[code >> 1] : second[code >> 1];
+        other[k] = (code & 1) ? first[code >> 1] : second[code >> 1];
     }
-    const int32_t* other = other_atom.data();
 
     // unique neighbours.  Inside a segment the other atoms are sorted (pairs
     // with the centre second come first, ordered by first; then the centre's
@@ -127,7 +161,6 @@ Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_
             for (int t = 0; t < S; t++) count_out[t] = cum[t];
         return n;
     };
-    if (S > 64) throw invalid_parameter("more than 64 atomic types are not supported");
 #pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < n_atoms; c++) {
         nh.entry_offset[c + 1] = merge(c, nullptr, nullptr, &nh.species_count[(size_t)c * S]);
@@ -140,6 +173,12 @@ Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_
 #pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < n_atoms; c++)
         merge(c, nh.entries.data() + nh.entry_offset[c], nh.entry_cum.data() + nh.entry_offset[c] * (S + 1), nullptr);
+}
+
+Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_t n_pairs, const int32_t* first,
+                                  const int32_t* second) {
+    Neighborhoods nh;
+    build_neighborhoods(systems, n_pairs, first, second, nh);
     return nh;
 }
 

@@ -34,10 +34,16 @@ struct Neighborhoods {
     std::vector<int32_t> species_count;  // [n_atoms * S]
     // species present around each centre (own species included)
     std::vector<uint8_t> species_mask;   // [n_atoms * S]
+    // working storage of the build, kept with the rest for reuse
+    std::vector<int32_t> other_atom;     // the other atom of every direction
+    std::vector<int64_t> bin_scratch;    // per-thread counting-sort bins
 };
 
 Neighborhoods build_neighborhoods(const std::vector<HostSystem>& systems, int64_t n_pairs, const int32_t* first,
                                   const int32_t* second);
+// the same into `nh`, reusing its storage
+void build_neighborhoods(const std::vector<HostSystem>& systems, int64_t n_pairs, const int32_t* first,
+                         const int32_t* second, Neighborhoods& nh);
 
 // Output plan: labels of every block and where the block lives in the
 // output buffer (offsets in doubles)

@@ -26,6 +26,8 @@
 // the slot's first row plus the rank of the neighbour among the rows of that
 // sample (prefix counts per species).
 
+#include <cub/cub.cuh>
+
 #include <map>
 #include <mutex>
 
@@ -592,7 +594,120 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
     CUDA_CHECK(cudaEventDestroy(join));
 }
 
+// One centre's S-way merge of its (centre, species) segments of directions,
+// by the other atom's index (plan.cpp build_neighborhoods): counts the unique
+// neighbours (FILL false) or writes them with their prefix counts (FILL true)
+constexpr int NB_MAX_SPECIES = 64;
+
+template <bool FILL>
+__global__ void neighborhoods_kernel(const int32_t* __restrict__ first, const int32_t* __restrict__ second,
+                                     const int32_t* __restrict__ atom_species, const int32_t* __restrict__ dir,
+                                     const int64_t* __restrict__ seg, int S, int64_t n_atoms,
+                                     int64_t* __restrict__ counts, const int64_t* __restrict__ offsets,
+                                     PsEntry* __restrict__ entries, int32_t* __restrict__ entry_cum,
+                                     int32_t* __restrict__ species_count, uint8_t* __restrict__ species_mask) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (!FILL && c == n_atoms) counts[n_atoms] = 0;  // the scan's last element
+    if (c >= n_atoms) return;
+    int64_t pos[NB_MAX_SPECIES], end[NB_MAX_SPECIES];
+    int32_t head[NB_MAX_SPECIES], cum[NB_MAX_SPECIES + 1];
+    const int sc = atom_species[c];
+    auto other = [&](int64_t d) -> int32_t {
+        const int32_t code = dir[d];
+        return (code & 1) ? first[code >> 1] : second[code >> 1];
+    };
+    // head[t]: the other atom at the front of segment t, INT32_MAX once it
+    // is exhausted (atoms of different species differ, so heads never tie)
+    for (int t = 0; t < S; t++) {
+        pos[t] = seg[c * S + t];
+        end[t] = seg[c * S + t + 1];
+        head[t] = pos[t] < end[t] ? other(pos[t]) : INT32_MAX;
+        cum[t] = 0;
+    }
+    cum[S] = 0;
+    const int64_t base = FILL ? offsets[c] : 0;
+    int64_t n = 0;
+    auto emit = [&](int32_t atom, int32_t species, int32_t d0, int32_t d1) {
+        if (FILL) {
+            entries[base + n] = PsEntry{atom, species, d0, d1};
+            int32_t* w = entry_cum + (base + n) * (S + 1);
+            for (int t = 0; t <= S; t++) w[t] = cum[t];
+        }
+        n++;
+    };
+    bool self_done = false;
+    while (true) {
+        int best = 0;
+        int32_t best_atom = head[0];
+        for (int t = 1; t < S; t++) {
+            if (head[t] < best_atom) {
+                best = t;
+                best_atom = head[t];
+            }
+        }
+        if (best_atom == INT32_MAX) best = -1;
+        if (!self_done && (best < 0 || best_atom >= (int32_t)c)) {
+            emit((int32_t)c, sc, -1, -1);
+            cum[S] = 1;
+            self_done = true;
+        }
+        if (best < 0) break;
+        const int64_t d0 = pos[best];
+        int64_t d = d0 + 1;
+        int32_t next = INT32_MAX;
+        while (d < end[best]) {
+            next = other(d);
+            if (next != best_atom) break;
+            next = INT32_MAX;
+            d++;
+        }
+        pos[best] = d;
+        head[best] = next;
+        if (best_atom == (int32_t)c) continue;  // periodic images of the centre itself
+        emit(best_atom, best, (int32_t)d0, (int32_t)d);
+        cum[best]++;
+    }
+    if (!FILL) {
+        counts[c] = n;
+        for (int t = 0; t < S; t++) {
+            species_count[c * S + t] = cum[t];
+            species_mask[c * S + t] = (end[t] > seg[c * S + t] || t == sc) ? 1 : 0;
+        }
+    }
+}
+
 }  // namespace
+
+DeviceNeighborhoods launch_neighborhoods(const DevicePairs& pairs, const int32_t* atom_species, const int32_t* dir_code,
+                                         const int64_t* seg_offset, int n_species, int64_t n_atoms, DeviceArena& arena,
+                                         cudaStream_t stream) {
+    if (n_species > NB_MAX_SPECIES) throw invalid_parameter("more than 64 atomic types are not supported");
+    if (2 * pairs.count + n_atoms >= (int64_t)INT32_MAX) throw invalid_parameter("too many pairs");
+    DeviceNeighborhoods nb;
+    const int S = n_species;
+    const int64_t capacity = 2 * pairs.count + n_atoms;  // every direction and every centre at most once
+    int64_t* counts = arena.alloc<int64_t>("nb.counts", n_atoms + 1);
+    nb.entry_offset = arena.alloc<int64_t>("nb.entry_offset", n_atoms + 1);
+    nb.entries = arena.alloc<PsEntry>("nb.entries", capacity);
+    nb.entry_cum = arena.alloc<int32_t>("nb.entry_cum", capacity * (S + 1));
+    nb.species_count = arena.alloc<int32_t>("nb.species_count", n_atoms * S);
+    nb.species_mask = arena.alloc<uint8_t>("nb.species_mask", n_atoms * S);
+    const int threads = 128;
+    const unsigned blocks = (unsigned)((n_atoms + 1 + threads - 1) / threads);
+    neighborhoods_kernel<false><<<blocks, threads, 0, stream>>>(pairs.first, pairs.second, atom_species, dir_code,
+                                                               seg_offset, S, n_atoms, counts, nullptr, nullptr,
+                                                               nullptr, nb.species_count, nb.species_mask);
+    CUDA_CHECK(cudaGetLastError());
+    size_t temp = 0;
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, temp, counts, nb.entry_offset, (int)(n_atoms + 1), stream));
+    void* scan_temp = arena.alloc_bytes("nb.scan_temp", temp);  // its own: this may run beside other scans
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(scan_temp, temp, counts, nb.entry_offset, (int)(n_atoms + 1), stream));
+    neighborhoods_kernel<true><<<blocks, threads, 0, stream>>>(pairs.first, pairs.second, atom_species, dir_code,
+                                                              seg_offset, S, n_atoms, nullptr, nb.entry_offset,
+                                                              nb.entries, nb.entry_cum, nullptr, nullptr);
+    CUDA_CHECK(cudaGetLastError());
+    return nb;
+}
 
 void launch_power_spectrum(const PsArgs& args, bool positions, bool strain, bool cell, cudaStream_t stream,
                            const PsEvents& events) {
