@@ -140,6 +140,16 @@ featomic_status_t featomic_profiling_get(const char* format, char* buffer, uintp
 
 /* mts_tensormap_free */
 mts_status_t mts_tensormap_free(mts_tensormap_t* tensor);
+/* A TensorMap holding labels only, the predefined samples / properties of a
+ * selection (featomic's LabelsSelection::Predefined, calculator.rs:38-44):
+ * block k has the key keys[k], the samples samples[k] and the properties
+ * properties[k] (a NULL array gives every block the single entry
+ * ("_" = 0)), no components, zero values.  Built with metatensor's own
+ * mts_block / mts_tensormap in featomic; this library keeps its TensorMaps
+ * opaque, so this stands in for those two calls.  Free with
+ * mts_tensormap_free. */
+featomic_status_t featomic_b200_labels_tensormap(const mts_labels_t* keys, const mts_labels_t* samples,
+                                                 const mts_labels_t* properties, mts_tensormap_t** tensor);
 /* mts_tensormap_keys: borrowed view */
 mts_status_t mts_tensormap_keys(const mts_tensormap_t* tensor, mts_labels_t* keys);
 /* mts_tensormap_block_by_id */

@@ -15,6 +15,7 @@ from .calculators import (  # noqa: F401
     System,
     TensorBlock,
     TensorMap,
+    labels_tensormap,
     neighbor_list,
     profiling_clear,
     profiling_enable,

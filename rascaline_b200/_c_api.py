@@ -165,6 +165,8 @@ SIGNATURES = {
                                                     ctypes.c_void_p, ctypes.c_void_p]),
     "featomic_b200_set_contraction_engine": (featomic_status_t, [ctypes.c_int32, ctypes.c_int32]),
     "featomic_b200_set_expansion_engine": (featomic_status_t, [ctypes.c_int32]),
+    "featomic_b200_labels_tensormap": (featomic_status_t, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                         ctypes.POINTER(ctypes.c_void_p)]),
     "featomic_b200_batch_create": (featomic_status_t, [ctypes.c_void_p, ctypes.c_size_t,
                                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int32),
                                                        ctypes.POINTER(ctypes.c_int32), ctypes.c_size_t,

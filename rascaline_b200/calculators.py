@@ -194,6 +194,32 @@ class TensorMap:
         return {"keys": self.keys.values, "blocks": blocks}
 
 
+def labels_tensormap(keys, samples=None, properties=None):
+    """TensorMap holding labels only, for predefined selections: one block
+    per key with ``samples[k]`` / ``properties[k]`` (``Labels`` or
+    ``(names, values)``; None gives a single placeholder entry), what
+    featomic users build with metatensor's ``TensorMap(keys, blocks)``."""
+    keep = []
+    keys = keys if isinstance(keys, Labels) else Labels(*keys)
+    n = len(keys.values)
+
+    def array(per_key):
+        if per_key is None:
+            return None
+        if len(per_key) != n:
+            raise ValueError("one Labels per key expected")
+        arr = (C.mts_labels_t * max(1, n))()
+        for k, labels in enumerate(per_key):
+            arr[k] = _c_labels(labels, keep).contents
+        keep.append(arr)
+        return arr
+
+    s, p = array(samples), array(properties)
+    out = ctypes.c_void_p()
+    C.check(C.lib().featomic_b200_labels_tensormap(_c_labels(keys, keep), s, p, ctypes.byref(out)))
+    return TensorMap(out)
+
+
 class System:
     """Atoms of one structure: atomic types, positions [n, 3] and the cell
     (3 x 3, rows are the cell vectors, all zero for a non-periodic system).
@@ -370,9 +396,11 @@ class CalculatorBase:
             return None
         return TensorMap(out)
 
-    def compute_device(self, positions, types, cells, system_sizes, gradients=None, stream=None):
+    def compute_device(self, positions, types, cells, system_sizes, gradients=None, stream=None,
+                       selected_samples=None, selected_properties=None, selected_keys=None):
         """Run on positions already on the GPU (torch CUDA float64 tensor of
-        shape [atoms, 3], all systems concatenated); the result stays on the GPU."""
+        shape [atoms, 3], all systems concatenated); the result stays on the
+        GPU.  Selections as in ``compute``, applied on the device."""
         import torch
         assert positions.is_cuda and positions.dtype == torch.float64 and positions.is_contiguous()
         types = np.ascontiguousarray(types, dtype=np.int32)
@@ -384,7 +412,7 @@ class CalculatorBase:
         dev.types = types.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
         dev.cells = cells.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         dev.positions = positions.data_ptr()
-        opts, keep = _options(gradients, True)
+        opts, keep = _options(gradients, True, selected_samples, selected_properties, selected_keys)
         if stream is None:
             stream = torch.cuda.current_stream().cuda_stream
         out = ctypes.c_void_p()

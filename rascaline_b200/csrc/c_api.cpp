@@ -160,14 +160,64 @@ Labels labels_from_c(const mts_labels_t* c, const char* what) {
     return out;
 }
 
+// The atoms within the cutoff of an atom, for the gradient samples of
+// predefined samples the full calculation does not produce: the systems' own
+// pairs, or the neighbour list kernel on positions from the host or (device
+// entry point) copied from the device; one list per system, built on first use
+struct NeighborCache {
+    const std::vector<HostSystem>* systems = nullptr;
+    double cutoff = 0.0;
+    const double* device_positions = nullptr;  // concatenated positions on the device
+    std::map<int64_t, std::vector<std::vector<int32_t>>> lists;
+
+    std::vector<int32_t> operator()(int64_t system, int64_t atom) {
+        auto it = lists.find(system);
+        if (it == lists.end()) {
+            const HostSystem& s = (*systems)[system];
+            std::vector<std::vector<int32_t>> around(s.n_atoms);
+            std::vector<Pair> pairs;
+            if (s.has_pairs) {
+                pairs = s.pairs;
+            } else if (device_positions) {
+                int64_t off = 0;
+                for (int64_t k = 0; k < system; k++) off += (*systems)[k].n_atoms;
+                std::vector<double> positions(3 * s.n_atoms);
+                if (s.n_atoms &&
+                    cudaMemcpy(positions.data(), device_positions + 3 * off, sizeof(double) * 3 * s.n_atoms,
+                               cudaMemcpyDeviceToHost) != cudaSuccess) {
+                    cudaGetLastError();
+                    throw internal_error("could not read the positions back from the device");
+                }
+                pairs = neighbor_list(positions.data(), s.n_atoms, s.cell, cutoff);
+            } else {
+                pairs = neighbor_list(s.positions.data(), s.n_atoms, s.cell, cutoff);
+            }
+            for (auto& p : pairs) {
+                around[p.first].push_back((int32_t)p.second);
+                around[p.second].push_back((int32_t)p.first);
+            }
+            it = lists.emplace(system, std::move(around)).first;
+        }
+        return it->second[atom];
+    }
+};
+
 // featomic's selections in C form (featomic.h:245-277) -> owned labels
 struct SelectionStorage {
     Labels keys, samples, properties;
     Selection selection;
+    std::shared_ptr<NeighborCache> neighbors = std::make_shared<NeighborCache>();
 };
 
-void parse_selections(const featomic_calculation_options_t& options, int max_angular, SelectionStorage& st) {
+void parse_selections(const featomic_calculation_options_t& options, int max_angular, SelectionStorage& st,
+                      const std::vector<HostSystem>& systems, double cutoff, const double* device_positions = nullptr) {
     st.selection.max_angular = max_angular;
+    st.neighbors->systems = &systems;
+    st.neighbors->cutoff = cutoff;
+    st.neighbors->device_positions = device_positions;
+    st.selection.systems = &systems;
+    auto cache = st.neighbors;
+    st.selection.neighbors = [cache](int64_t system, int64_t atom) { return (*cache)(system, atom); };
     if (options.selected_keys) {
         st.keys = labels_from_c(options.selected_keys, "keys");
         st.selection.keys = &st.keys;
@@ -336,7 +386,8 @@ featomic_status_t featomic_calculator_compute(featomic_calculator_t* calculator,
             }
         }
         SelectionStorage selection;
-        parse_selections(options, calculator->impl->hypers.max_angular, selection);
+        parse_selections(options, calculator->impl->hypers.max_angular, selection, host,
+                         calculator->impl->hypers.cutoff);
         warn_close_pairs(host);
         auto tm = compute(*calculator->impl, host, g, false, nullptr, nullptr);
         record_profile(calculator->impl->engine->last_times());
@@ -376,12 +427,13 @@ featomic_status_t featomic_b200_calculator_compute_device(featomic_calculator_t*
                 throw invalid_parameter("featomic_b200_calculator_compute_device expects device positions");
             }
         }
-        if (options.selected_samples.subset || options.selected_samples.predefined ||
-            options.selected_properties.subset || options.selected_properties.predefined || options.selected_keys)
-            throw invalid_parameter("selections are supported by featomic_calculator_compute (host output) only");
+        SelectionStorage selection;
+        parse_selections(options, calculator->impl->hypers.max_angular, selection, host,
+                         calculator->impl->hypers.cutoff, systems->positions);
         auto tm = compute(*calculator->impl, host, g, true, systems->positions, (cudaStream_t)stream);
         record_profile(calculator->impl->engine->last_times());
-        *descriptor = wrap(std::move(tm));
+        if (selection.selection.any()) CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
+        *descriptor = wrap(apply_selection(std::move(tm), selection.selection));
     });
 }
 
@@ -548,6 +600,40 @@ featomic_status_t featomic_b200_set_contraction_engine(int32_t tensor_cores, int
             throw fb200::invalid_parameter("channels_per_round must be between 1 and 4 (0 keeps the current value)");
         fb200::set_dense_mma_enabled(tensor_cores == 1);
         if (channels_per_round > 0) fb200::dense_mma_channels_per_round = channels_per_round;
+    });
+}
+
+featomic_status_t featomic_b200_labels_tensormap(const mts_labels_t* keys, const mts_labels_t* samples,
+                                                 const mts_labels_t* properties, mts_tensormap_t** tensor) {
+    return guarded([&] {
+        CHECK_POINTER(keys);
+        CHECK_POINTER(tensor);
+        auto tm = std::make_unique<TensorMap>();
+        tm->keys = labels_from_c(keys, "keys");
+        const size_t n = tm->keys.count();
+        Labels single;
+        single.names = {"_"};
+        single.values = {0};
+        std::vector<Block*> blocks;
+        size_t total = 0;
+        for (size_t k = 0; k < n; k++) {
+            auto b = std::make_unique<Block>();
+            b->samples = samples ? labels_from_c(samples + k, "samples") : single;
+            b->properties = properties ? labels_from_c(properties + k, "properties") : single;
+            b->shape = {b->samples.count(), b->properties.count()};
+            total += b->size();
+            blocks.push_back(b.get());
+            tm->blocks.push_back(std::move(b));
+        }
+        auto* zeros = static_cast<double*>(std::calloc(std::max<size_t>(1, total), sizeof(double)));
+        if (!zeros) throw std::bad_alloc();
+        tm->storage = std::shared_ptr<void>(zeros, std::free);
+        size_t off = 0;
+        for (Block* b : blocks) {
+            b->data = zeros + off;
+            off += b->size();
+        }
+        *tensor = wrap(std::move(tm));
     });
 }
 

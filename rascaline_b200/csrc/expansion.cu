@@ -21,6 +21,7 @@
 //   first->second orientation, the self (centre) gradient, and the strain and
 //   cell gradients, with the (-1)^l / -(-1)^l factors of the reversed pair
 //   (spherical_expansion_pair.rs:130-163).
+#include <algorithm>
 #include <cstdlib>
 
 #include "engine.hpp"
@@ -697,6 +698,27 @@ void launch_se_output(const SeOutArgs& args, bool positions, bool strain, bool c
         se_output_gradients_kernel<<<(unsigned)args.n_grad_rows, 128, 0, stream>>>(args);
         CUDA_CHECK(cudaGetLastError());
     }
+}
+
+// rows and property columns of one output array for a selection
+__global__ void gather_rows_kernel(const double* __restrict__ src, const int64_t* __restrict__ rows, int64_t n_rows,
+                                   int64_t inner, int64_t src_props, const int64_t* __restrict__ props,
+                                   int64_t n_props, double* __restrict__ dst) {
+    const int64_t total = n_rows * inner * n_props;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = i % n_props, rm = i / n_props;
+        const int64_t m = rm % inner, r = rows[rm / inner];
+        dst[i] = r < 0 ? 0.0 : src[(r * inner + m) * src_props + props[p]];
+    }
+}
+
+void launch_gather_rows(const double* src, const int64_t* rows, int64_t n_rows, int64_t inner, int64_t src_props,
+                        const int64_t* props, int64_t n_props, double* dst) {
+    const int64_t total = n_rows * inner * n_props;
+    if (total == 0) return;
+    const int threads = 256;
+    const unsigned blocks = (unsigned)std::min<int64_t>((total + threads - 1) / threads, 148 * 16);
+    gather_rows_kernel<<<blocks, threads>>>(src, rows, n_rows, inner, src_props, props, n_props, dst);
 }
 
 }  // namespace fb200

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -201,7 +202,8 @@ std::unique_ptr<TensorMap> compute(CalculatorImpl& calc, std::vector<HostSystem>
                                    const double* positions_device, void* stream);
 
 // Samples / properties / keys selections (featomic's CalculationOptions,
-// calculator.rs:20-158), applied to the host output of a full calculation
+// calculator.rs:20-158), applied to the output of a full calculation (on the
+// host, or on the device with a gather kernel)
 struct Selection {
     const Labels* keys = nullptr;
     const Labels* samples = nullptr;
@@ -209,10 +211,21 @@ struct Selection {
     const TensorMap* samples_predefined = nullptr;
     const TensorMap* properties_predefined = nullptr;
     int max_angular = 0;  // for the components of keys the systems do not produce
+    // predefined samples the full calculation does not produce (a centre of
+    // the key's center_type without neighbours of a key's neighbour type)
+    // get zero rows; their positions gradient samples need the atomic types
+    // and the atoms within the cutoff of an atom (any order, repeats allowed)
+    const std::vector<HostSystem>* systems = nullptr;
+    std::function<std::vector<int32_t>(int64_t system, int64_t atom)> neighbors;
     bool any() const { return keys || samples || properties || samples_predefined || properties_predefined; }
 };
 
 std::unique_ptr<TensorMap> apply_selection(std::unique_ptr<TensorMap> full, const Selection& selection);
+
+// dst[r][m][p] = src[rows[r]][m][props[p]] on the device (rows[r] < 0: zero
+// row), src rows of `inner` x `src_props` doubles; index arrays on the device
+void launch_gather_rows(const double* src, const int64_t* rows, int64_t n_rows, int64_t inner, int64_t src_props,
+                        const int64_t* props, int64_t n_props, double* dst);
 
 // run kernel (a) on one system given on the host, return the pairs
 std::vector<Pair> neighbor_list(const double* positions, int64_t n_atoms, const double* cell, double cutoff);

@@ -1,6 +1,7 @@
 // Samples / properties / keys selections of a compute call
 // (featomic/src/calculator.rs:20-158 LabelsSelection::select, :287-310 keys),
-// applied to the host TensorMap of the full calculation.
+// applied to the output of the full calculation, on the host or, for device
+// output, by a gather kernel on the device.
 //
 // featomic computes only the selected entries; their values do not depend on
 // what else is computed, so selecting rows and columns of the full output
@@ -11,10 +12,20 @@
 //   Subset     per block, the default entries matching any row of the
 //              selection on the selection's names, in default order
 //   Predefined per block, the labels of the predefined TensorMap's block
-//              with the same key, in that order
+//              with the same key, in that order.  A predefined sample the
+//              full calculation does not have (a centre of the key's
+//              center_type without neighbours of one of the key's neighbour
+//              types) is a zero row, as featomic computes it, with zero
+//              gradient rows for the atoms featomic lists
+//              (atom_centered.rs:103-147); predefined properties must be
+//              properties of the calculator
 // Gradient rows follow their samples (positions rows keep their order within
 // a sample, their "sample" column is renumbered); properties are selected on
 // the last axis of every array.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -61,8 +72,10 @@ std::vector<int64_t> select_subset(const Labels& labels, const Labels& selection
     return out;
 }
 
-// indices of the predefined entries inside `labels` (same names required)
-std::vector<int64_t> select_predefined(const Labels& labels, const Labels& predefined, const char* kind) {
+// indices of the predefined entries inside `labels` (same names required);
+// an entry the full calculation does not have is -1 when `allow_absent`
+std::vector<int64_t> select_predefined(const Labels& labels, const Labels& predefined, const char* kind,
+                                       bool allow_absent) {
     if (predefined.names != labels.names)
         throw invalid_parameter(std::string("invalid predefined ") + kind + " names: expected [" + join(labels.names) +
                                 "], but got [" + join(predefined.names) + "]");
@@ -74,13 +87,63 @@ std::vector<int64_t> select_predefined(const Labels& labels, const Labels& prede
     for (size_t r = 0; r < predefined.count(); r++) {
         auto it = index.find(std::vector<int32_t>(predefined.values.begin() + r * w,
                                                   predefined.values.begin() + (r + 1) * w));
-        if (it == index.end())
+        if (it == index.end() && !allow_absent)
             throw invalid_parameter(std::string("predefined ") + kind +
-                                    " selection contains an entry that the systems do not produce; featomic-b200 only "
-                                    "selects among the computed entries");
-        out.push_back(it->second);
+                                    " selection contains an entry outside of this calculator's " + kind);
+        out.push_back(it == index.end() ? -1 : it->second);
     }
     return out;
+}
+
+// value of the key column `name` of key k, or INT32_MIN without that column
+int32_t key_value(const Labels& keys, size_t k, const std::string& name) {
+    const size_t w = keys.names.size();
+    for (size_t c = 0; c < w; c++)
+        if (keys.names[c] == name) return keys.values[k * w + c];
+    return INT32_MIN;
+}
+
+// A predefined sample (system, atom) of key k that the full calculation did
+// not produce: a centre of the key's center_type lacking neighbours of one
+// of the key's neighbour types, whose values and gradients are all zero
+// (its coefficients for that neighbour type vanish).  Returns its positions
+// gradient samples: featomic's AtomCenteredSamples::gradients_for
+// (labels/samples/atom_centered.rs:103-147) with self pairs, the atoms of
+// the key's neighbour types within the cutoff plus the centre itself when
+// one matched or its own type is one of them, by atom index.
+std::vector<int32_t> absent_sample(const Selection& sel, const Labels& keys, size_t k, int32_t system, int32_t atom,
+                                   bool positions) {
+    const int32_t center_type = key_value(keys, k, "center_type");
+    std::vector<int32_t> wanted;
+    for (const char* name : {"neighbor_type", "neighbor_1_type", "neighbor_2_type"}) {
+        const int32_t t = key_value(keys, k, name);
+        if (t != INT32_MIN) wanted.push_back(t);
+    }
+    if (center_type == INT32_MIN || wanted.empty() || !sel.systems)
+        throw invalid_parameter("predefined samples selection contains a sample this calculator does not produce");
+    if (system < 0 || (size_t)system >= sel.systems->size() || atom < 0 ||
+        atom >= (int32_t)(*sel.systems)[system].n_atoms)
+        throw invalid_parameter("predefined samples selection contains (system=" + std::to_string(system) +
+                                ", atom=" + std::to_string(atom) + "), which is not an atom of the systems");
+    const std::vector<int32_t>& types = (*sel.systems)[system].types;
+    if (types[atom] != center_type)
+        throw invalid_parameter("predefined samples selection contains (system=" + std::to_string(system) +
+                                ", atom=" + std::to_string(atom) + ") of atomic type " + std::to_string(types[atom]) +
+                                " in a block with center_type=" + std::to_string(center_type) +
+                                "; featomic-b200 computes the atoms of the block's center_type only");
+    std::vector<int32_t> atoms;
+    if (!positions) return atoms;
+    auto matches = [&](int32_t t) { return std::find(wanted.begin(), wanted.end(), t) != wanted.end(); };
+    bool with_centre = matches(types[atom]);
+    for (int32_t j : sel.neighbors(system, atom)) {
+        if (!matches(types[j])) continue;
+        atoms.push_back(j);
+        with_centre = true;
+    }
+    if (with_centre) atoms.push_back(atom);
+    std::sort(atoms.begin(), atoms.end());
+    atoms.erase(std::unique(atoms.begin(), atoms.end()), atoms.end());
+    return atoms;
 }
 
 Labels rows_of(const Labels& labels, const std::vector<int64_t>& rows) {
@@ -105,24 +168,70 @@ const Block* predefined_block(const TensorMap& tm, const Labels& keys, size_t k,
     throw invalid_parameter("expected a block for (" + print + ") in predefined " + kind + " selection");
 }
 
-// copy of `src` restricted to `rows` of axis 0 and `props` of the last axis
-void copy_rows(const Block& src, const std::vector<int64_t>& rows, const std::vector<int64_t>& props, double* dst) {
-    const size_t n_props = src.shape.back();
-    size_t inner = 1;  // product of the middle axes
-    for (size_t a = 1; a + 1 < src.shape.size(); a++) inner *= src.shape[a];
+// one array of the output: rows of `src` (-1: a zero row), every middle
+// axis, the block's selected properties
+struct Gather {
+    const double* src;  // null: all rows zero
+    std::vector<int64_t> rows;
+    int64_t inner, src_props;
+    const std::vector<int64_t>* props;
+    double* dst;
+};
+
+void gather_host(const Gather& g) {
+    const std::vector<int64_t>& props = *g.props;
     size_t o = 0;
-    for (int64_t r : rows)
-        for (size_t m = 0; m < inner; m++) {
-            const double* s = src.data + ((size_t)r * inner + m) * n_props;
-            for (int64_t p : props) dst[o++] = s[p];
+    for (int64_t r : g.rows)
+        for (int64_t m = 0; m < g.inner; m++) {
+            if (r < 0 || !g.src) {
+                for (size_t p = 0; p < props.size(); p++) g.dst[o++] = 0.0;
+                continue;
+            }
+            const double* s = g.src + ((size_t)r * g.inner + m) * g.src_props;
+            for (int64_t p : props) g.dst[o++] = s[p];
         }
+}
+
+void check_cuda(cudaError_t status) {
+    if (status != cudaSuccess) {
+        cudaGetLastError();
+        throw internal_error(std::string("CUDA error in a device selection: ") + cudaGetErrorString(status));
+    }
+}
+
+void gather_device(const std::vector<Gather>& gathers) {
+    // every index array in one upload
+    std::vector<int64_t> index;
+    std::vector<size_t> at;
+    std::map<const std::vector<int64_t>*, size_t> props_at;
+    for (auto& g : gathers) {
+        at.push_back(index.size());
+        for (int64_t r : g.rows) index.push_back(g.src ? r : -1);
+        if (!props_at.count(g.props)) {
+            props_at[g.props] = index.size();
+            index.insert(index.end(), g.props->begin(), g.props->end());
+        }
+    }
+    int64_t* d_index = nullptr;
+    check_cuda(cudaMalloc(&d_index, sizeof(int64_t) * std::max<size_t>(1, index.size())));
+    std::shared_ptr<void> keep(d_index, [](void* q) { cudaFree(q); });
+    if (!index.empty())
+        check_cuda(cudaMemcpy(d_index, index.data(), sizeof(int64_t) * index.size(), cudaMemcpyHostToDevice));
+    for (size_t k = 0; k < gathers.size(); k++) {
+        const Gather& g = gathers[k];
+        if (g.rows.empty() || g.props->empty()) continue;
+        launch_gather_rows(g.src, d_index + at[k], (int64_t)g.rows.size(), g.inner, g.src_props,
+                           d_index + props_at[g.props], (int64_t)g.props->size(), g.dst);
+        check_cuda(cudaGetLastError());
+    }
+    // the source TensorMap and the index arrays are released after return
+    check_cuda(cudaDeviceSynchronize());
 }
 
 }  // namespace
 
 std::unique_ptr<TensorMap> apply_selection(std::unique_ptr<TensorMap> full, const Selection& sel) {
     if (!sel.any()) return full;
-    if (full->on_device) throw invalid_parameter("selections are only supported with host output");
     const TensorMap& tm = *full;
 
     // keys
@@ -148,13 +257,17 @@ std::unique_ptr<TensorMap> apply_selection(std::unique_ptr<TensorMap> full, cons
     }
     if (tm.blocks.empty()) throw invalid_parameter("selections need at least one computed block");
     const Block& any = *tm.blocks[0];
+    bool any_positions = false;
+    for (auto& g : any.gradients) any_positions |= g.first == "positions";
 
-    // per output block: selected sample rows and property columns
+    // per output block: selected sample rows (-1: a predefined sample the
+    // full calculation does not have) and property columns
     struct Plan {
         const Block* src;
         std::vector<int64_t> rows, props;
         std::vector<Labels> components;
         Labels samples, properties;
+        std::map<size_t, std::vector<int32_t>> absent_atoms;  // output row -> positions gradient atoms
     };
     std::vector<Plan> plans(keys.count());
     size_t total = 0;
@@ -186,35 +299,70 @@ std::unique_ptr<TensorMap> apply_selection(std::unique_ptr<TensorMap> full, cons
         }
         for (size_t r = 0; r < p.samples.count(); r++) p.rows.push_back((int64_t)r);
         for (size_t c = 0; c < p.properties.count(); c++) p.props.push_back((int64_t)c);
-        if (sel.samples) p.rows = select_subset(p.samples, *sel.samples, "samples");
-        if (sel.samples_predefined)
-            p.rows = select_predefined(p.samples, predefined_block(*sel.samples_predefined, keys, k, "samples")->samples,
-                                       "samples");
+        if (sel.samples) {
+            p.rows = select_subset(p.samples, *sel.samples, "samples");
+            p.samples = rows_of(p.samples, p.rows);
+        }
+        if (sel.samples_predefined) {
+            const Labels& wanted = predefined_block(*sel.samples_predefined, keys, k, "samples")->samples;
+            p.rows = select_predefined(p.samples, wanted, "samples", true);
+            p.samples = wanted;
+            const size_t sw = wanted.names.size();
+            for (size_t r = 0; r < p.rows.size(); r++) {
+                if (p.rows[r] >= 0) continue;
+                if (sw != 2 || wanted.names[0] != "system" || wanted.names[1] != "atom")
+                    throw invalid_parameter("predefined samples selection contains a sample this calculator does not "
+                                            "produce");
+                p.absent_atoms[r] = absent_sample(sel, keys, k, wanted.values[r * sw], wanted.values[r * sw + 1],
+                                                  any_positions);
+            }
+        }
         if (sel.properties) p.props = select_subset(p.properties, *sel.properties, "properties");
         if (sel.properties_predefined)
             p.props = select_predefined(
                 p.properties, predefined_block(*sel.properties_predefined, keys, k, "properties")->properties,
-                "properties");
-        p.samples = rows_of(p.samples, p.rows);
+                "properties", false);
         p.properties = rows_of(p.properties, p.props);
         size_t comp = 1;
         for (auto& c : p.components) comp *= c.count();
         total += p.rows.size() * comp * p.props.size();
-        if (p.src)
-            for (auto& g : p.src->gradients) {
-                size_t inner = 1;
-                for (size_t a = 1; a + 1 < g.second->shape.size(); a++) inner *= g.second->shape[a];
-                total += g.second->shape[0] * inner * p.props.size();  // upper bound for positions rows
+        for (auto& named : any.gradients) {
+            size_t inner = 1;
+            const Block& g = *named.second;
+            for (size_t a = 1; a + 1 < g.shape.size(); a++) inner *= g.shape[a];
+            inner = inner / std::max<size_t>(1, [&] {
+                size_t c = 1;
+                for (auto& l : any.components) c *= l.count();
+                return c;
+            }()) * comp;
+            size_t rows = 0;
+            if (named.first == "positions") {
+                if (p.src)
+                    for (auto& sg : p.src->gradients)
+                        if (sg.first == "positions") rows += sg.second->shape[0];  // upper bound
+                for (auto& a : p.absent_atoms) rows += a.second.size();
+            } else {
+                rows = p.rows.size();
             }
+            total += rows * inner * p.props.size();
+        }
     }
 
     auto out = std::make_unique<TensorMap>();
     out->keys = keys;
-    out->on_device = false;
+    out->on_device = tm.on_device;
     out->device = tm.device;
-    double* buffer = static_cast<double*>(std::malloc(std::max<size_t>(8, sizeof(double) * total)));
-    if (!buffer) throw std::bad_alloc();
-    out->storage = std::shared_ptr<void>(buffer, std::free);
+    double* buffer = nullptr;
+    const size_t bytes = std::max<size_t>(8, sizeof(double) * total);
+    if (tm.on_device) {
+        check_cuda(cudaMalloc(&buffer, bytes));
+        out->storage = std::shared_ptr<void>(buffer, [](void* q) { cudaFree(q); });
+    } else {
+        buffer = static_cast<double*>(std::malloc(bytes));
+        if (!buffer) throw std::bad_alloc();
+        out->storage = std::shared_ptr<void>(buffer, std::free);
+    }
+    std::vector<Gather> gathers;
     size_t off = 0;
     for (size_t k = 0; k < keys.count(); k++) {
         Plan& p = plans[k];
@@ -226,7 +374,12 @@ std::unique_ptr<TensorMap> apply_selection(std::unique_ptr<TensorMap> full, cons
         for (auto& c : p.components) blk->shape.push_back(c.count());
         blk->shape.push_back(p.props.size());
         blk->data = buffer + off;
-        if (p.src) copy_rows(*p.src, p.rows, p.props, blk->data);
+        {
+            size_t comp = 1;
+            for (auto& c : p.components) comp *= c.count();
+            gathers.push_back(Gather{p.src ? p.src->data : nullptr, p.rows, (int64_t)comp,
+                                     p.src ? (int64_t)p.src->shape.back() : 0, &p.props, blk->data});
+        }
         off += blk->size();
         // gradients present in the full output (all blocks carry the same set)
         for (auto& named : any.gradients) {
@@ -246,23 +399,34 @@ std::unique_ptr<TensorMap> apply_selection(std::unique_ptr<TensorMap> full, cons
             gb->properties = p.properties;
             gb->samples.names = named.second->samples.names;
             std::vector<int64_t> grows;
-            if (gsrc && name == "positions") {
-                // rows of each kept sample, in their order, renumbered
-                std::vector<std::vector<int64_t>> by_sample(p.src->samples.count());
-                const size_t gw = gsrc->samples.names.size();
-                for (size_t r = 0; r < gsrc->samples.count(); r++)
-                    by_sample[gsrc->samples.values[r * gw]].push_back((int64_t)r);
-                for (size_t s = 0; s < p.rows.size(); s++)
+            if (name == "positions") {
+                // rows of each kept sample, in their order, renumbered; zero
+                // rows for the samples the full calculation does not have
+                std::vector<std::vector<int64_t>> by_sample(gsrc ? p.src->samples.count() : 0);
+                const size_t gw = named.second->samples.names.size();
+                if (gsrc)
+                    for (size_t r = 0; r < gsrc->samples.count(); r++)
+                        by_sample[gsrc->samples.values[r * gw]].push_back((int64_t)r);
+                for (size_t s = 0; s < p.rows.size(); s++) {
+                    if (p.rows[s] < 0) {
+                        const int32_t system = p.samples.values[2 * s];
+                        for (int32_t a : p.absent_atoms[s]) {
+                            grows.push_back(-1);
+                            gb->samples.values.insert(gb->samples.values.end(), {(int32_t)s, system, a});
+                        }
+                        continue;
+                    }
                     for (int64_t r : by_sample[p.rows[s]]) {
                         grows.push_back(r);
                         gb->samples.values.push_back((int32_t)s);
                         gb->samples.values.insert(gb->samples.values.end(), gsrc->samples.values.begin() + r * gw + 1,
                                                   gsrc->samples.values.begin() + (r + 1) * gw);
                     }
-            } else if (gsrc) {
+                }
+            } else {
                 // strain / cell: one row per sample
                 for (size_t s = 0; s < p.rows.size(); s++) {
-                    grows.push_back(p.rows[s]);
+                    grows.push_back(gsrc ? p.rows[s] : -1);
                     gb->samples.values.push_back((int32_t)s);
                 }
             }
@@ -270,13 +434,21 @@ std::unique_ptr<TensorMap> apply_selection(std::unique_ptr<TensorMap> full, cons
             for (auto& c : gb->components) gb->shape.push_back(c.count());
             gb->shape.push_back(p.props.size());
             gb->data = buffer + off;
-            if (gsrc) copy_rows(*gsrc, grows, p.props, gb->data);
+            size_t inner = 1;
+            for (size_t a = 1; a + 1 < gb->shape.size(); a++) inner *= gb->shape[a];
+            gathers.push_back(Gather{gsrc ? gsrc->data : nullptr, grows, (int64_t)inner,
+                                     gsrc ? (int64_t)gsrc->shape.back() : 0, &p.props, gb->data});
             off += gb->size();
             blk->gradients.emplace_back(name, std::move(gb));
         }
         out->blocks.push_back(std::move(blk));
     }
     if (off > std::max<size_t>(total, 1)) throw internal_error("selection: output buffer overflow");
+    if (tm.on_device) {
+        gather_device(gathers);
+    } else {
+        for (auto& g : gathers) gather_host(g);
+    }
     return out;
 }
 

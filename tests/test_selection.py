@@ -1,123 +1,232 @@
 """Samples / properties / keys selections (featomic/src/calculator.rs:20-158,
-:287-310): the selected output equals the matching rows and columns of the
-full output, gradients follow their samples, and the errors name what is
-wrong.  The test recipe follows featomic's compute_partial
-(featomic/src/calculators/tests_utils.rs)."""
+:287-310) against the oracle's restatement of featomic's selection rules
+(oracle/selection.py) applied to the oracle's full calculation.
+
+Every case runs through featomic_calculator_compute (host output) and
+featomic_b200_calculator_compute_device (device output, the selection applied
+by a gather kernel on the device).  Labels (keys, samples, properties,
+gradient samples) must be identical; values and gradients within the parity
+bound |x - ref| <= 1e-10 |ref| + 1e-12 max|ref|.  Cases: subsets of samples
+and properties (fewer names than the calculator's), keys with fewer names and
+with all names (a key the systems do not produce gets an empty block),
+predefined samples and properties, predefined samples the full calculation
+does not produce (centres without neighbours of one of the key's types: zero
+rows, with featomic's gradient samples), and the error messages."""
 import numpy as np
 import pytest
 
 import rascaline_b200 as rb
 from rascaline_b200 import workloads
+from oracle import oracle
+from oracle import selection as oracle_selection
 
 pytestmark = pytest.mark.gpu
 
-GRADS = ["positions", "strain"]
+GRADS = ["positions", "strain", "cell"]
+CUTOFF = 4.5
 
 
-def _system():
-    return workloads.random_box(60, density=0.1, species=(1, 6, 8), seed=17, strain=0.01)
+def _hypers(calculator):
+    if calculator == "soap_radial_spectrum":
+        return {"cutoff": {"radius": CUTOFF, "smoothing": {"type": "ShiftedCosine", "width": 0.5}},
+                "density": {"type": "Gaussian", "width": 0.3},
+                "basis": {"radial": {"type": "Gto", "max_radial": 4}}}
+    return workloads.hypers(CUTOFF, 4, 3)
 
 
-def _by_key(tm):
-    return {tuple(k): b for k, b in zip(tm.keys.values, tm.blocks())}
+CLASSES = {"soap_power_spectrum": rb.SoapPowerSpectrum, "spherical_expansion": rb.SphericalExpansion,
+           "soap_radial_spectrum": rb.SoapRadialSpectrum}
 
 
-def _check_block(full, part, rows, cols):
-    np.testing.assert_array_equal(part.samples.values, full.samples.values[rows])
-    np.testing.assert_array_equal(part.properties.values, full.properties.values[cols])
-    np.testing.assert_array_equal(part.values, full.values[rows][..., cols])
-    # positions rows of the kept samples, renumbered
-    fg, pg = full.gradient("positions"), part.gradient("positions")
-    expected, samples = [], []
-    for new, old in enumerate(rows):
-        for r in np.nonzero(fg.samples.values[:, 0] == old)[0]:
-            expected.append(fg.values[r][..., cols])
-            samples.append([new] + list(fg.samples.values[r, 1:]))
-    np.testing.assert_array_equal(pg.samples.values.reshape(-1, 3), np.array(samples, dtype=np.int32).reshape(-1, 3))
-    if expected:
-        np.testing.assert_array_equal(pg.values, np.array(expected))
-    sg = part.gradient("strain")
-    np.testing.assert_array_equal(sg.values, full.gradient("strain").values[rows][..., cols])
+def _one_oxygen():
+    # 59 H / C atoms and one O: most centres have no O neighbour, so the
+    # blocks with an O neighbour type miss many centres
+    box = workloads.random_box(60, density=0.1, species=(1, 6), seed=17, strain=0.01)
+    box["types"] = np.array(box["types"], dtype=np.int32)
+    box["types"][23] = 8
+    return box
 
 
-@pytest.mark.parametrize("calculator", ["soap_power_spectrum", "spherical_expansion"])
-def test_samples_and_properties_subsets(calculator):
-    cls = {"soap_power_spectrum": rb.SoapPowerSpectrum, "spherical_expansion": rb.SphericalExpansion}[calculator]
-    calc = cls(**workloads.hypers(4.5, 4, 3))
-    system = rb.System.from_dict(_system())
-    full = calc.compute(system, gradients=GRADS)
-    samples = rb.Labels(["atom"], [[3], [0], [41], [17]])
-    if calculator == "soap_power_spectrum":
-        properties = rb.Labels(["l", "n_2"], [[0, 1], [2, 4], [3, 0]])
+@pytest.fixture(scope="module")
+def system():
+    return _one_oxygen()
+
+
+@pytest.fixture(scope="module")
+def full_oracle(system):
+    return {c: oracle.compute(c, _hypers(c), [system], GRADS, threads=4) for c in CLASSES}
+
+
+def _ours(calculator, system, device, **selection):
+    calc = CLASSES[calculator](**_hypers(calculator))
+    if not device:
+        tm = calc.compute(rb.System.from_dict(system), gradients=GRADS, **selection)
     else:
-        properties = rb.Labels(["n"], [[4], [1]])
-    part = calc.compute(system, gradients=GRADS, selected_samples=samples, selected_properties=properties)
-    np.testing.assert_array_equal(part.keys.values, full.keys.values)
-    for key, fb in _by_key(full).items():
-        pb = _by_key(part)[key]
-        rows = [r for r, s in enumerate(fb.samples.values) if s[1] in (3, 0, 41, 17)]
-        sel = {tuple(v) for v in properties.values}
-        names = properties.names
-        cols = [c for c, p in enumerate(fb.properties.values)
-                if tuple(p[fb.properties.names.index(n)] for n in names) in sel]
-        _check_block(fb, pb, rows, cols)
+        import torch
+        pos = torch.tensor(system["positions"], device="cuda")
+        tm = calc.compute_device(pos, system["types"], np.asarray(system["cell"]).reshape(1, 9),
+                                 [len(system["types"])], gradients=GRADS, **selection)
+        torch.cuda.synchronize()
+    return tm
 
 
-def test_selected_keys():
-    calc = rb.SoapPowerSpectrum(**workloads.hypers(4.5, 4, 3))
-    system = rb.System.from_dict(_system())
-    full = calc.compute(system, gradients=GRADS)
+def _close(a, b, what):
+    a, b = np.asarray(a), np.asarray(b)
+    assert a.shape == b.shape, (what, a.shape, b.shape)
+    if b.size == 0:
+        return
+    bound = 1e-10 * np.abs(b) + 1e-12 * np.max(np.abs(b))
+    assert np.all(np.abs(a - b) <= bound), (what, np.max(np.abs(a - b)))
+
+
+def _compare(ours, ref):
+    np.testing.assert_array_equal(ours.keys.values, ref["keys"])
+    assert ours.keys.names == ref["key_names"]
+    blocks = ours.blocks()
+    assert len(blocks) == len(ref["blocks"])
+    for block, rb_ in zip(blocks, ref["blocks"]):
+        assert block.samples.names == rb_["sample_names"]
+        assert block.properties.names == rb_["property_names"]
+        np.testing.assert_array_equal(block.samples.values.reshape(-1, 2), rb_["samples"])
+        np.testing.assert_array_equal(block.properties.values.reshape(rb_["properties"].shape), rb_["properties"])
+        values = block.values
+        values = values if isinstance(values, np.ndarray) else values.cpu().numpy()
+        _close(values, rb_["values"], "values")
+        for name in GRADS:
+            g = block.gradient(name)
+            gv = g.values if isinstance(g.values, np.ndarray) else g.values.cpu().numpy()
+            width = rb_["gradients"][name]["samples"].shape[1]
+            np.testing.assert_array_equal(g.samples.values.reshape(-1, width), rb_["gradients"][name]["samples"])
+            _close(gv, rb_["gradients"][name]["values"], f"{name} gradients")
+
+
+def _run(calculator, system, full_oracle, device, selection, oracle_args):
+    ours = _ours(calculator, system, device, **selection)
+    ref = oracle_selection.select(calculator, full_oracle[calculator], [system], CUTOFF, GRADS, **oracle_args)
+    _compare(ours, ref)
+
+
+DEVICE = [False, True]
+
+
+@pytest.mark.parametrize("device", DEVICE, ids=["host", "device"])
+@pytest.mark.parametrize("calculator", list(CLASSES))
+def test_subsets(calculator, device, system, full_oracle):
+    samples = (["atom"], [[3], [0], [41], [17], [23]])
+    props = (["l", "n_2"], [[0, 1], [2, 4], [3, 0]]) if calculator == "soap_power_spectrum" else (["n"], [[4], [1]])
+    _run(calculator, system, full_oracle, device,
+         dict(selected_samples=rb.Labels(*samples), selected_properties=rb.Labels(*props)),
+         dict(samples=("subset",) + samples, properties=("subset",) + props))
+
+
+@pytest.mark.parametrize("device", DEVICE, ids=["host", "device"])
+def test_keys(device, system, full_oracle):
     # fewer names: the default keys with center_type 6
-    part = calc.compute(system, gradients=GRADS, selected_keys=rb.Labels(["center_type"], [[6]]))
-    assert all(k[0] == 6 for k in part.keys.values)
-    assert len(part.keys) == sum(1 for k in full.keys.values if k[0] == 6)
+    keys = (["center_type"], [[6]])
+    _run("soap_power_spectrum", system, full_oracle, device, dict(selected_keys=rb.Labels(*keys)),
+         dict(keys=keys))
     # all names: exactly these keys, in this order; (9, 1, 1) is not produced
-    keys = rb.Labels(["center_type", "neighbor_1_type", "neighbor_2_type"], [[8, 1, 6], [9, 1, 1], [1, 1, 1]])
-    part = calc.compute(system, gradients=GRADS, selected_keys=keys)
-    np.testing.assert_array_equal(part.keys.values, keys.values)
-    fb = _by_key(full)
-    for key, pb in _by_key(part).items():
-        if key == (9, 1, 1):
-            assert pb.values.shape == (0, fb[(1, 1, 1)].values.shape[1])
-            assert pb.gradient("positions").values.shape[0] == 0
+    keys = (["center_type", "neighbor_1_type", "neighbor_2_type"], [[8, 1, 6], [9, 1, 1], [1, 1, 1]])
+    _run("soap_power_spectrum", system, full_oracle, device, dict(selected_keys=rb.Labels(*keys)),
+         dict(keys=keys))
+    keys = (["o3_lambda", "o3_sigma", "center_type", "neighbor_type"], [[2, 1, 9, 1], [1, 1, 1, 6], [3, 1, 8, 8]])
+    _run("spherical_expansion", system, full_oracle, device, dict(selected_keys=rb.Labels(*keys)),
+         dict(keys=keys))
+
+
+def _predefined_samples(calculator, full, key_rows, extra):
+    """Per key: a few default samples in reverse order, plus `extra` samples
+    (which the full calculation may not have) for the keys that accept them."""
+    key_names = oracle_selection.KEY_NAMES[calculator]
+    blocks = {}
+    for key, block in zip(full["keys"], full["blocks"]):
+        key = tuple(int(x) for x in key)
+        rows = [tuple(int(x) for x in s) for s in block["samples"][::-7]]
+        for s in extra.get(key, []):
+            if s not in rows:
+                rows.append(s)
+        blocks[key] = (["system", "atom"], np.array(rows, dtype=np.int32).reshape(-1, 2))
+    keys = [tuple(int(x) for x in k) for k in full["keys"]]
+    tensor = rb.labels_tensormap(rb.Labels(key_names, keys), samples=[rb.Labels(*blocks[k]) for k in keys])
+    return tensor, ("predefined", blocks, key_names)
+
+
+def _centres_without(system, centre_type, neighbour_type):
+    nl = oracle.neighbors(system["positions"], system["cell"], CUTOFF)
+    types = system["types"]
+    has = set()
+    for i, j in zip(nl["first"], nl["second"]):
+        if types[j] == neighbour_type:
+            has.add(int(i))
+        if types[i] == neighbour_type:
+            has.add(int(j))
+    return [a for a in range(len(types)) if types[a] == centre_type and a not in has]
+
+
+@pytest.mark.parametrize("device", DEVICE, ids=["host", "device"])
+@pytest.mark.parametrize("calculator", list(CLASSES))
+def test_predefined_samples_with_absent_centres(calculator, device, system, full_oracle):
+    full = full_oracle[calculator]
+    lonely_h = _centres_without(system, 1, 8)[:4]
+    lonely_c = _centres_without(system, 6, 8)[:3]
+    assert len(lonely_h) == 4 and len(lonely_c) == 3
+    extra = {}
+    for key in full["keys"]:
+        key = tuple(int(x) for x in key)
+        if calculator == "soap_power_spectrum":
+            centre, types = key[0], key[1:]
         else:
-            np.testing.assert_array_equal(pb.values, fb[key].values)
+            centre, types = key[-2], key[-1:]
+        if 8 in types:
+            extra[key] = [(0, a) for a in (lonely_h if centre == 1 else lonely_c if centre == 6 else [])]
+    assert any(extra.values())
+    tensor, oracle_spec = _predefined_samples(calculator, full, None, extra)
+    _run(calculator, system, full_oracle, device, dict(selected_samples=tensor), dict(samples=oracle_spec))
 
 
-def test_missing_key_of_the_spherical_expansion_has_its_components():
-    calc = rb.SphericalExpansion(**workloads.hypers(4.5, 4, 3))
-    system = rb.System.from_dict(_system())
-    keys = rb.Labels(["o3_lambda", "o3_sigma", "center_type", "neighbor_type"], [[2, 1, 9, 1], [1, 1, 1, 6]])
-    part = calc.compute(system, gradients=GRADS, selected_keys=keys)
-    block = part.block_by_id(0)
-    assert block.values.shape == (0, 5, 5)
-    assert block.gradient("positions").values.shape == (0, 3, 5, 5)
-    with pytest.raises(rb.FeatomicError, match="max_angular"):
-        calc.compute(system, selected_keys=rb.Labels(keys.names, [[7, 1, 1, 1]]))
+@pytest.mark.parametrize("device", DEVICE, ids=["host", "device"])
+def test_predefined_properties(device, system, full_oracle):
+    full = full_oracle["soap_power_spectrum"]
+    key_names = oracle_selection.KEY_NAMES["soap_power_spectrum"]
+    keys = [tuple(int(x) for x in k) for k in full["keys"]]
+    blocks = {}
+    for k, key in enumerate(keys):
+        props = full["blocks"][k]["properties"][(k % 5)::9][::-1]
+        blocks[key] = (["l", "n_1", "n_2"], props)
+    tensor = rb.labels_tensormap(rb.Labels(key_names, keys), properties=[rb.Labels(*blocks[k]) for k in keys])
+    _run("soap_power_spectrum", system, full_oracle, device, dict(selected_properties=tensor),
+         dict(properties=("predefined", blocks, key_names)))
 
 
-def test_predefined_selection():
-    calc = rb.SoapPowerSpectrum(**workloads.hypers(4.5, 4, 3))
-    system = rb.System.from_dict(_system())
-    full = calc.compute(system, gradients=GRADS)
-    template = calc.compute(system, selected_samples=rb.Labels(["atom"], [[5], [2], [30]]),
-                            selected_properties=rb.Labels(["l"], [[1]]))
-    part = calc.compute(system, gradients=GRADS, selected_samples=template, selected_properties=template)
-    for key, pb in _by_key(part).items():
-        tb, fb = _by_key(template)[key], _by_key(full)[key]
-        np.testing.assert_array_equal(pb.samples.values, tb.samples.values)
-        np.testing.assert_array_equal(pb.properties.values, tb.properties.values)
-        rows = [[tuple(s) for s in fb.samples.values].index(tuple(s)) for s in tb.samples.values]
-        cols = [[tuple(p) for p in fb.properties.values].index(tuple(p)) for p in tb.properties.values]
-        _check_block(fb, pb, rows, cols)
-
-
-def test_selection_errors():
-    calc = rb.SoapPowerSpectrum(**workloads.hypers(4.5, 4, 3))
-    system = rb.System.from_dict(_system())
+def test_errors(system, full_oracle):
+    calc = rb.SoapPowerSpectrum(**_hypers("soap_power_spectrum"))
+    s = rb.System.from_dict(system)
     with pytest.raises(rb.FeatomicError, match="'foo' in samples selection is not part of the samples"):
-        calc.compute(system, selected_samples=rb.Labels(["foo"], [[0]]))
+        calc.compute(s, selected_samples=rb.Labels(["foo"], [[0]]))
     with pytest.raises(rb.FeatomicError, match="'n' in properties selection is not part of the properties"):
-        calc.compute(system, selected_properties=rb.Labels(["n"], [[0]]))
+        calc.compute(s, selected_properties=rb.Labels(["n"], [[0]]))
     with pytest.raises(rb.FeatomicError, match="selected keys can not be empty"):
-        calc.compute(system, selected_keys=rb.Labels(["center_type"], np.zeros((0, 1))))
+        calc.compute(s, selected_keys=rb.Labels(["center_type"], np.zeros((0, 1))))
+    # the oracle raises the same errors
+    with pytest.raises(oracle_selection.SelectionError, match="'foo' in samples selection is not part of the samples"):
+        oracle_selection.select("soap_power_spectrum", full_oracle["soap_power_spectrum"], [system], CUTOFF,
+                                samples=("subset", ["foo"], [[0]]))
+    full = full_oracle["soap_power_spectrum"]
+    keys = [tuple(int(x) for x in k) for k in full["keys"]]
+    key_names = oracle_selection.KEY_NAMES["soap_power_spectrum"]
+    # a block missing from the predefined TensorMap
+    tensor = rb.labels_tensormap(rb.Labels(key_names, keys[1:]),
+                                 samples=[rb.Labels(["system", "atom"], [[0, 0]]) for _ in keys[1:]])
+    printed = ", ".join(f"{n}={v}" for n, v in zip(key_names, keys[0]))
+    with pytest.raises(rb.FeatomicError, match=rf"expected a block for \({printed}\) in predefined samples"):
+        calc.compute(s, selected_samples=tensor)
+    # wrong label names
+    tensor = rb.labels_tensormap(rb.Labels(key_names, keys), samples=[rb.Labels(["atom"], [[0]]) for _ in keys])
+    with pytest.raises(rb.FeatomicError, match=r"invalid predefined samples names: expected \[system, atom\]"):
+        calc.compute(s, selected_samples=tensor)
+    # a centre of another type than the key's center_type
+    first_h = int(np.nonzero(system["types"] == 1)[0][0])
+    tensor = rb.labels_tensormap(rb.Labels(key_names, keys),
+                                 samples=[rb.Labels(["system", "atom"], [[0, first_h]]) for _ in keys])
+    with pytest.raises(rb.FeatomicError, match="computes the atoms of the block's center_type only"):
+        calc.compute(s, selected_samples=tensor)
