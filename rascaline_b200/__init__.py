@@ -8,6 +8,7 @@ CPU fallback: without the library or a CUDA device the calls fail.
 from .calculators import (  # noqa: F401
     CalculatorBase,
     Labels,
+    LodeSphericalExpansion,
     SoapPowerSpectrum,
     SoapRadialSpectrum,
     SphericalExpansion,

@@ -449,6 +449,20 @@ class SphericalExpansion(CalculatorBase):
         super().__init__("spherical_expansion", {"cutoff": cutoff, "density": density, "basis": basis})
 
 
+class LodeSphericalExpansion(CalculatorBase):
+    """featomic's ``lode_spherical_expansion``: long-range expansion of a
+    smeared power-law density in periodic systems, computed in reciprocal
+    space (featomic/src/calculators/lode/spherical_expansion.rs).  Keys
+    (o3_lambda, o3_sigma, center_type, neighbor_type), samples (system,
+    atom), positions gradients only."""
+
+    def __init__(self, density, basis, k_cutoff=None):
+        parameters = {"density": density, "basis": basis}
+        if k_cutoff is not None:
+            parameters["k_cutoff"] = k_cutoff
+        super().__init__("lode_spherical_expansion", parameters)
+
+
 class SphericalExpansionByPair(CalculatorBase):
     """featomic's ``spherical_expansion_by_pair``: one row per pair and
     direction, keys (o3_lambda, o3_sigma, first_atom_type, second_atom_type),

@@ -20,6 +20,7 @@
 #include "dense.hpp"
 #include "engine.hpp"
 #include "host.hpp"
+#include "lode.hpp"
 #include "surrogate.hpp"
 
 using namespace fb200;
@@ -215,7 +216,7 @@ void parse_selections(const featomic_calculation_options_t& options, int max_ang
     st.neighbors->systems = &systems;
     st.neighbors->cutoff = cutoff;
     st.neighbors->device_positions = device_positions;
-    st.selection.systems = &systems;
+    st.selection.systems = cutoff > 0.0 ? &systems : nullptr;  // no neighbour rule without a cutoff
     auto cache = st.neighbors;
     st.selection.neighbors = [cache](int64_t system, int64_t atom) { return (*cache)(system, atom); };
     if (options.selected_keys) {
@@ -235,6 +236,18 @@ void parse_selections(const featomic_calculation_options_t& options, int max_ang
         }
         if (s.predefined) (k == 0 ? st.selection.samples_predefined : st.selection.properties_predefined) = s.predefined->tm.get();
     }
+}
+
+const PhaseTimes& last_times(const CalculatorImpl& c) {
+    return c.lode ? c.lode->last_times() : c.engine->last_times();
+}
+
+// the SOAP engine behind an entry point that only SOAP calculators have
+Engine& soap_engine(const featomic_calculator_t* calculator) {
+    if (!calculator->impl->engine)
+        throw invalid_parameter("this function needs a SOAP calculator (spherical expansion, power spectrum or "
+                                "radial spectrum), not " + calculator->impl->name);
+    return *calculator->impl->engine;
 }
 
 mts_tensormap_t* wrap(std::unique_ptr<TensorMap> tm) {
@@ -364,8 +377,9 @@ featomic_status_t featomic_calculator_compute(featomic_calculator_t* calculator,
             h.positions.assign(positions, positions + 3 * n);
             for (double x : h.positions)
                 if (!std::isfinite(x)) throw invalid_parameter("atomic positions must be finite");
-            if (!options.use_native_system) {
-                // the caller's own neighbour list (featomic/src/c_api/system.rs:248-320)
+            if (!options.use_native_system && !calculator->impl->lode) {
+                // the caller's own neighbour list (featomic/src/c_api/system.rs:248-320);
+                // the LODE calculator has no cutoff and asks for none
                 if (!sys.compute_neighbors || !sys.pairs)
                     throw invalid_parameter("system callbacks `compute_neighbors` and `pairs` are required when use_native_system is false");
                 check_system_status(sys.compute_neighbors(sys.user_data, cutoff), "compute_neighbors");
@@ -390,7 +404,7 @@ featomic_status_t featomic_calculator_compute(featomic_calculator_t* calculator,
                          calculator->impl->hypers.cutoff);
         warn_close_pairs(host);
         auto tm = compute(*calculator->impl, host, g, false, nullptr, nullptr);
-        record_profile(calculator->impl->engine->last_times());
+        record_profile(last_times(*calculator->impl));
         *descriptor = wrap(apply_selection(std::move(tm), selection.selection));
     });
 }
@@ -431,7 +445,7 @@ featomic_status_t featomic_b200_calculator_compute_device(featomic_calculator_t*
         parse_selections(options, calculator->impl->hypers.max_angular, selection, host,
                          calculator->impl->hypers.cutoff, systems->positions);
         auto tm = compute(*calculator->impl, host, g, true, systems->positions, (cudaStream_t)stream);
-        record_profile(calculator->impl->engine->last_times());
+        record_profile(last_times(*calculator->impl));
         if (selection.selection.any()) CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
         *descriptor = wrap(apply_selection(std::move(tm), selection.selection));
     });
@@ -490,7 +504,7 @@ featomic_status_t featomic_b200_power_spectrum_dense(featomic_calculator_t* calc
             sp.assign(species, species + n_species);
         }
         auto result = std::make_unique<featomic_b200_dense_t>();
-        result->state = calculator->impl->engine->forward_dense(precision, host, systems->positions, sp, values,
+        result->state = soap_engine(calculator).forward_dense(precision, host, systems->positions, sp, values,
                                                                 (int64_t)values_count, (cudaStream_t)stream);
         *state = result.release();
     });
@@ -671,7 +685,7 @@ featomic_status_t featomic_b200_batch_create(featomic_calculator_t* calculator, 
             sp.assign(species, species + n_species);
         }
         auto result = std::make_unique<featomic_b200_batch_t>();
-        result->plan = std::make_unique<BatchPlan>(*calculator->impl->engine, sizes, t, sp);
+        result->plan = std::make_unique<BatchPlan>(soap_engine(calculator), sizes, t, sp);
         *batch = result.release();
     });
 }
@@ -762,7 +776,7 @@ featomic_status_t featomic_b200_surrogate_create(featomic_calculator_t* calculat
         auto result = std::make_unique<featomic_b200_surrogate_t>();
         if (calculator->impl->hypers.explicit_basis() || calculator->impl->hypers.tabulated_basis())
             throw invalid_parameter("the learned radial surrogate needs a GTO TensorProduct basis");
-        result->impl = std::make_shared<RadialSurrogate>(*calculator->impl->engine, hidden, seed);
+        result->impl = std::make_shared<RadialSurrogate>(soap_engine(calculator), hidden, seed);
         *surrogate = result.release();
     });
 }
@@ -886,9 +900,9 @@ featomic_status_t featomic_b200_calculator_set_surrogate(featomic_calculator_t* 
                                                          featomic_b200_surrogate_t* surrogate) {
     return guarded([&] {
         CHECK_POINTER(calculator);
-        if (surrogate && surrogate->impl->engine() != calculator->impl->engine.get())
+        if (surrogate && surrogate->impl->engine() != &soap_engine(calculator))
             throw invalid_parameter("the surrogate was trained for another calculator");
-        calculator->impl->engine->set_surrogate(surrogate ? surrogate->impl : nullptr);
+        soap_engine(calculator).set_surrogate(surrogate ? surrogate->impl : nullptr);
     });
 }
 
@@ -941,7 +955,7 @@ featomic_status_t featomic_b200_radial_integral(const featomic_calculator_t* cal
                                                 uintptr_t n_r, double* values, double* gradients, int32_t* knots) {
     return guarded([&] {
         CHECK_POINTER(calculator);
-        const RadialTables& t = calculator->impl->engine->radial();
+        const RadialTables& t = soap_engine(calculator).radial();
         if (n_r > 0) {
             CHECK_POINTER(r);
             CHECK_POINTER(values);
@@ -964,7 +978,7 @@ featomic_status_t featomic_b200_dense_timings(const featomic_calculator_t* calcu
     return guarded([&] {
         CHECK_POINTER(calculator);
         CHECK_POINTER(times);
-        const std::vector<double> t = calculator->impl->engine->dense_times();
+        const std::vector<double> t = soap_engine(calculator).dense_times();
         for (uintptr_t k = 0; k < count && k < t.size(); k++) times[k] = t[k];
     });
 }
@@ -974,7 +988,7 @@ featomic_status_t featomic_b200_calculator_timings(const featomic_calculator_t* 
     return guarded([&] {
         CHECK_POINTER(calculator);
         CHECK_POINTER(times);
-        const PhaseTimes& t = calculator->impl->engine->last_times();
+        const PhaseTimes& t = last_times(*calculator->impl);
         double all[12] = {t.neighbors,    t.metadata,       t.features,
                           t.expansion,    t.contraction,    t.transfer,
                           t.total,        t.ps_values,      t.ps_positions,

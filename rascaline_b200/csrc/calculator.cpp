@@ -1,9 +1,10 @@
 // Calculator facade: registry, construction from JSON and dispatch to the
 // engine (featomic/src/calculator.rs:243-526, registry :574-588): spherical
-// expansion, spherical expansion by pair, SOAP power spectrum and SOAP radial
-// spectrum.
+// expansion, spherical expansion by pair, SOAP power spectrum, SOAP radial
+// spectrum and the LODE spherical expansion.
 #include "engine.hpp"
 #include "host.hpp"
+#include "lode.hpp"
 
 namespace fb200 {
 
@@ -31,8 +32,16 @@ std::unique_ptr<CalculatorImpl> create_calculator(const std::string& name, const
         c->hypers = parse_hypers(json, /*deny_unknown_top=*/true);
         c->power_spectrum = false;
         c->by_pair = true;
-    } else if (name == "lode_spherical_expansion" || name == "atomic_composition" || name == "dummy_calculator" ||
-               name == "neighbor_list" || name == "sorted_distances") {
+    } else if (name == "lode_spherical_expansion") {
+        // no cutoff: every atom of the periodic system is a neighbour
+        c->pretty_name = "lode spherical expansion";
+        LodeHypers lh = parse_lode_hypers(json);
+        c->hypers.max_angular = lh.max_angular;
+        c->hypers.max_radial = lh.max_radial;
+        c->lode = std::make_unique<LodeEngine>(lh);
+        return c;
+    } else if (name == "atomic_composition" || name == "dummy_calculator" || name == "neighbor_list" ||
+               name == "sorted_distances") {
         throw invalid_parameter("calculator '" + name + "' is not implemented by featomic-b200");
     } else {
         throw invalid_parameter("unknown calculator with name '" + name + "'");
@@ -121,6 +130,7 @@ std::unique_ptr<TensorMap> explicit_basis_output(std::unique_ptr<TensorMap> tm, 
 
 std::unique_ptr<TensorMap> compute(CalculatorImpl& calc, std::vector<HostSystem>& systems, const GradientOptions& grads,
                                    bool device_output, const double* positions_device, void* stream) {
+    if (calc.lode) return calc.lode->compute(systems, grads, device_output, positions_device, (cudaStream_t)stream);
     if (calc.hypers.explicit_basis() && device_output)
         throw invalid_parameter("the Explicit basis is supported with host output (featomic_calculator_compute) only");
     const int kind = calc.power_spectrum ? Engine::OUTPUT_POWER_SPECTRUM

@@ -81,6 +81,39 @@ struct Hypers {
 // instead of a SphericalExpansionBasis, with max_angular = 0.
 Hypers parse_hypers(const std::string& json, bool deny_unknown_top, bool radial_spectrum_basis = false);
 
+// LODE spherical expansion (featomic/src/calculators/lode/
+// spherical_expansion.rs:30-58): smeared power-law density, GTO radial basis
+// of an explicit radius, k-space cutoff (default 1.2 pi / smearing)
+struct LodeHypers {
+    double smearing = 0.0;
+    int exponent = 0;
+    double center_atom_weight = 1.0;
+    double k_cutoff = 0.0;
+    int max_angular = 0;
+    int max_radial = 0;
+    double radius = 0.0;
+    bool splined = true;
+    double spline_accuracy = 1e-8;
+    int nmax() const { return max_radial + 1; }
+};
+
+LodeHypers parse_lode_hypers(const std::string& json);
+
+// GTO radial basis (shared/basis/radial/gto.rs:44-80): Gaussian widths
+// radius max(sqrt(n), 1) / size and the orthonormalisation matrix O,
+// row-major, orthonormal functions R_k = sum_n O[k][n] raw_n
+std::vector<double> gto_basis_widths(int size, double radius);
+std::vector<double> gto_basis_orthonormalization(int size, double radius);
+
+// Adaptive Hermite spline knots of a function R -> R^n on [0, stop]: 11
+// uniform points, then every interval midpoint until the mean absolute or the
+// mean relative interpolation error over the first `checked` outputs at the
+// midpoints drops below `accuracy` (featomic/src/math/splines.rs:79-193, at
+// most 10 000 points).  `eval(x, values, derivatives)` fills n outputs.
+void build_spline_knots(const std::function<void(double, double*, double*)>& eval, double stop, int n, int checked,
+                        double accuracy, std::vector<double>& positions, std::vector<double>& values,
+                        std::vector<double>& derivatives);
+
 // ---------------------------------------------------------------------------
 // Radial integral tables (one Hermite spline per angular channel, knots chosen
 // adaptively like featomic/src/math/splines.rs:79-193)
@@ -177,6 +210,7 @@ struct GradientOptions {
 };
 
 class Engine;
+class LodeEngine;
 
 struct CalculatorImpl {
     std::string name;        // registry name
@@ -184,7 +218,8 @@ struct CalculatorImpl {
     std::string parameters;  // JSON as given
     Hypers hypers;
     std::vector<double> cutoffs;
-    std::unique_ptr<Engine> engine;
+    std::unique_ptr<Engine> engine;      // SOAP calculators
+    std::unique_ptr<LodeEngine> lode;    // lode_spherical_expansion
     bool power_spectrum = false;
     bool radial_spectrum = false;  // spherical expansion l = 0, keys (center_type, neighbor_type)
     bool by_pair = false;          // spherical_expansion_by_pair

@@ -521,6 +521,9 @@ std::vector<double> gto_orthonormalization(int size, double radius) {
 
 }  // namespace
 
+std::vector<double> gto_basis_widths(int size, double radius) { return gto_widths(size, radius); }
+std::vector<double> gto_basis_orthonormalization(int size, double radius) { return gto_orthonormalization(size, radius); }
+
 void radial_integral_host(const RadialTables& t, int l, double r, double* values, double* grads) {
     int N = t.nmax;
     if (t.splined) {
@@ -549,6 +552,130 @@ void radial_integral_host(const RadialTables& t, int l, double r, double* values
         }
         values[k] = s;
         if (grads) grads[k] = sg;
+    }
+}
+
+// featomic/src/calculators/lode/spherical_expansion.rs:30-58 and :180-224
+// (validation); LodeRadialBasis::Gto of shared/basis/radial/mod.rs:55-68
+LodeHypers parse_lode_hypers(const std::string& text) {
+    Value root;
+    try {
+        root = json::parse(text);
+    } catch (json::ParseError& e) {
+        throw json_error(e.what());
+    }
+    object(root, "struct LodeSphericalExpansionParameters");
+    LodeHypers h;
+    const Value& density = object(field(root, "density", "parameters"), "struct Density");
+    std::string dt = tag(density, "Density");
+    if (dt != "SmearedPowerLaw") {
+        if (dt != "Gaussian" && dt != "DiracDelta")
+            throw json_error("unknown variant `" + dt + "`, expected one of `DiracDelta`, `Gaussian`, `SmearedPowerLaw`");
+        throw invalid_parameter("only SmearedPowerLaw density can be used with LODE");
+    }
+    h.smearing = as_f64(field(density, "smearing", "SmearedPowerLaw"), "smearing");
+    h.exponent = (int)as_usize(field(density, "exponent", "SmearedPowerLaw"), "exponent");
+    if (const Value* cw = density.get("center_atom_weight")) h.center_atom_weight = as_f64(*cw, "center_atom_weight");
+    if (const Value* sc = density.get("scaling"))
+        if (sc->kind != Value::Null) throw invalid_parameter("LODE does not support custom density scaling");
+    if (h.exponent >= 10) throw invalid_parameter("LODE is only implemented for potential_exponent < 10");
+    h.k_cutoff = 1.2 * M_PI / h.smearing;
+    if (const Value* kc = root.get("k_cutoff"))
+        if (kc->kind != Value::Null) h.k_cutoff = as_f64(*kc, "k_cutoff");
+
+    const Value& basis = object(field(root, "basis", "parameters"), "internally tagged enum SphericalExpansionBasis");
+    std::string bt = tag(basis, "SphericalExpansionBasis");
+    if (bt == "Explicit") throw invalid_parameter("the Explicit basis is not supported by featomic-b200's LODE");
+    if (bt != "TensorProduct") throw json_error("unknown variant `" + bt + "`, expected `TensorProduct` or `Explicit`");
+    deny_unknown(basis, {"type", "max_angular", "radial", "spline_accuracy"}, "TensorProduct");
+    h.max_angular = (int)as_usize(field(basis, "max_angular", "TensorProduct"), "max_angular");
+    const Value& radial = object(field(basis, "radial", "TensorProduct"), "internally tagged enum LodeRadialBasis");
+    std::string rt = tag(radial, "LodeRadialBasis");
+    if (rt == "Tabulated") throw invalid_parameter("the Tabulated radial basis is not supported by featomic-b200's LODE");
+    if (rt != "Gto") throw json_error("unknown variant `" + rt + "`, expected `Gto` or `Tabulated`");
+    deny_unknown(radial, {"type", "max_radial", "radius"}, "Gto");
+    h.max_radial = (int)as_usize(field(radial, "max_radial", "Gto"), "max_radial");
+    h.radius = as_f64(field(radial, "radius", "Gto"), "radius");
+    if (const Value* sa = basis.get("spline_accuracy")) {
+        if (sa->kind == Value::Null) h.splined = false;
+        else h.spline_accuracy = as_f64(*sa, "spline_accuracy");
+    }
+    // gto.rs:27-57 (LODE)
+    if (h.radius < 1e-16) throw invalid_parameter("radius of GTO radial basis can not be negative");
+    if (!std::isfinite(h.radius)) throw invalid_parameter("radius of GTO radial basis can not be infinite/NaN");
+    if (h.splined && h.spline_accuracy < 0.0) {
+        std::ostringstream m;
+        m << "got invalid accuracy in spline (" << h.spline_accuracy << "), it must be positive";
+        throw invalid_parameter(m.str());
+    }
+    if (h.max_angular > 16) throw invalid_parameter("featomic-b200's LODE supports max_angular <= 16");
+    if (h.nmax() > 64) throw invalid_parameter("featomic-b200's LODE supports max_radial < 64");
+    return h;
+}
+
+void build_spline_knots(const std::function<void(double, double*, double*)>& eval, double stop, int N, int NL,
+                        double accuracy, std::vector<double>& pos, std::vector<double>& val, std::vector<double>& der) {
+    pos.clear();
+    val.clear();
+    der.clear();
+    std::vector<double> v(N), d(N);
+    const int initial = 11;
+    double step = (stop - 0.0) / (double)(initial - 1);
+    for (int k = 0; k < initial - 1; k++) {
+        double x = 0.0 + (double)k * step;
+        eval(x, v.data(), d.data());
+        pos.push_back(x);
+        val.insert(val.end(), v.begin(), v.end());
+        der.insert(der.end(), d.begin(), d.end());
+    }
+    eval(stop, v.data(), d.data());
+    pos.push_back(stop);
+    val.insert(val.end(), v.begin(), v.end());
+    der.insert(der.end(), d.begin(), d.end());
+
+    while (true) {
+        double mean_abs = 0.0, mean_rel = 0.0;
+        size_t count = 0;
+        std::vector<double> mid_pos, mid_val, mid_der;
+        for (size_t k = 0; k + 1 < pos.size(); k++) {
+            double x = (pos[k] + pos[k + 1]) / 2.0;
+            eval(x, v.data(), d.data());
+            auto w = soap::hermite_weights(pos[k], pos[k + 1], x);
+            for (int n = 0; n < NL; n++) {
+                double s = soap::hermite_value(w, val[k * N + n], der[k * N + n], val[(k + 1) * N + n], der[(k + 1) * N + n]);
+                mean_abs += std::fabs(s - v[n]);
+                mean_rel += std::fabs((s - v[n]) / v[n]);
+                count++;
+            }
+            mid_pos.push_back(x);
+            mid_val.insert(mid_val.end(), v.begin(), v.end());
+            mid_der.insert(mid_der.end(), d.begin(), d.end());
+        }
+        if (count == 0) break;  // an angular channel absent from an Explicit basis
+        mean_abs /= (double)count;
+        mean_rel /= (double)count;
+        if (mean_abs < accuracy || mean_rel < accuracy) break;
+        if (pos.size() + mid_pos.size() > 10000) {
+            std::ostringstream m;
+            m << "failed to reach requested accuracy (" << accuracy
+              << ") in spline interpolation, mean absolute error is " << mean_abs
+              << " and mean relative error is " << mean_rel;
+            throw internal_error(m.str());
+        }
+        std::vector<double> p2, v2, d2;
+        for (size_t k = 0; k < pos.size(); k++) {
+            p2.push_back(pos[k]);
+            v2.insert(v2.end(), val.begin() + k * N, val.begin() + (k + 1) * N);
+            d2.insert(d2.end(), der.begin() + k * N, der.begin() + (k + 1) * N);
+            if (k < mid_pos.size()) {
+                p2.push_back(mid_pos[k]);
+                v2.insert(v2.end(), mid_val.begin() + k * N, mid_val.begin() + (k + 1) * N);
+                d2.insert(d2.end(), mid_der.begin() + k * N, mid_der.begin() + (k + 1) * N);
+            }
+        }
+        pos.swap(p2);
+        val.swap(v2);
+        der.swap(d2);
     }
 }
 
@@ -623,66 +750,12 @@ RadialTables build_radial_tables(const Hypers& h) {
                     radial_integral_host(tl, l, x, v.data(), d.data());
                 }
             };
-            const int initial = 11;
-            double step = (h.cutoff - 0.0) / (double)(initial - 1);
             std::vector<double> v, d;
-            for (int k = 0; k < initial - 1; k++) {
-                double x = 0.0 + (double)k * step;
+            build_spline_knots([&](double x, double* vv, double* dd) {
                 eval(x, v, d);
-                pos.push_back(x);
-                val.insert(val.end(), v.begin(), v.end());
-                der.insert(der.end(), d.begin(), d.end());
-            }
-            eval(h.cutoff, v, d);
-            pos.push_back(h.cutoff);
-            val.insert(val.end(), v.begin(), v.end());
-            der.insert(der.end(), d.begin(), d.end());
-
-            std::vector<double> interp(N);
-            while (true) {
-                double mean_abs = 0.0, mean_rel = 0.0;
-                size_t count = 0;
-                std::vector<double> mid_pos, mid_val, mid_der;
-                for (size_t k = 0; k + 1 < pos.size(); k++) {
-                    double x = (pos[k] + pos[k + 1]) / 2.0;
-                    eval(x, v, d);
-                    auto w = soap::hermite_weights(pos[k], pos[k + 1], x);
-                    for (int n = 0; n < NL; n++) {
-                        double s = soap::hermite_value(w, val[k * N + n], der[k * N + n], val[(k + 1) * N + n], der[(k + 1) * N + n]);
-                        mean_abs += std::fabs(s - v[n]);
-                        mean_rel += std::fabs((s - v[n]) / v[n]);
-                        count++;
-                    }
-                    mid_pos.push_back(x);
-                    mid_val.insert(mid_val.end(), v.begin(), v.end());
-                    mid_der.insert(mid_der.end(), d.begin(), d.end());
-                }
-                if (count == 0) break;  // an angular channel absent from an Explicit basis
-                mean_abs /= (double)count;
-                mean_rel /= (double)count;
-                if (mean_abs < h.spline_accuracy || mean_rel < h.spline_accuracy) break;
-                if (pos.size() + mid_pos.size() > 10000) {
-                    std::ostringstream m;
-                    m << "failed to reach requested accuracy (" << h.spline_accuracy
-                      << ") in spline interpolation, mean absolute error is " << mean_abs
-                      << " and mean relative error is " << mean_rel;
-                    throw internal_error(m.str());
-                }
-                std::vector<double> p2, v2, d2;
-                for (size_t k = 0; k < pos.size(); k++) {
-                    p2.push_back(pos[k]);
-                    v2.insert(v2.end(), val.begin() + k * N, val.begin() + (k + 1) * N);
-                    d2.insert(d2.end(), der.begin() + k * N, der.begin() + (k + 1) * N);
-                    if (k < mid_pos.size()) {
-                        p2.push_back(mid_pos[k]);
-                        v2.insert(v2.end(), mid_val.begin() + k * N, mid_val.begin() + (k + 1) * N);
-                        d2.insert(d2.end(), mid_der.begin() + k * N, mid_der.begin() + (k + 1) * N);
-                    }
-                }
-                pos.swap(p2);
-                val.swap(v2);
-                der.swap(d2);
-            }
+                std::copy(v.begin(), v.end(), vv);
+                std::copy(d.begin(), d.end(), dd);
+            }, h.cutoff, N, NL, h.spline_accuracy, pos, val, der);
             offsets.push_back((int32_t)all_pos.size());
             counts.push_back((int32_t)pos.size());
             all_pos.insert(all_pos.end(), pos.begin(), pos.end());

@@ -16,10 +16,14 @@ Outputs (all committed):
 
 * ``<name>-input.json``          the calculator inputs, copied verbatim
 * ``<name>.npz``                 the expected arrays (key ``values``)
+* ``lode-exponent-<p>-<name>``   the LODE spherical expansion fixtures of
+  ``generated/lode-spherical-expansion/exponent-<p>/`` (p = 1..6)
 * ``known_answers.json``         inline known answers, extracted by regex from
   ``math/hyp1f1.rs`` (mpmath table), ``calculators/soap/cutoff.rs`` (shifted
-  cosine values), ``systems/neighbors.rs`` (ASE neighbour distances) and
-  ``math/gamma.rs`` (gamma / ln_gamma spot values).
+  cosine values), ``systems/neighbors.rs`` (ASE neighbour distances),
+  ``math/gamma.rs`` (gamma / ln_gamma spot values), ``math/exp.rs`` (scipy
+  exp1 / expi values) and ``calculators/lode/radial_integral/gto.rs``
+  (pyLODE central-atom contributions).
 """
 import gzip
 import io
@@ -122,6 +126,33 @@ def extract_gamma(src):
     return out
 
 
+def extract_exp(src):
+    """scipy reference values of `math/exp.rs` tests: [x, expected] pairs for
+    exp1 and expi (finite expected values only)."""
+    out = {}
+    for fn in ("exp1", "expi"):
+        pat = r"assert_relative_eq!\(" + fn + r"\((" + _FLOAT + r")\), (" + _FLOAT + r")"
+        out[fn] = [[float(a), float(b)] for a, b in re.findall(pat, src)]
+    return out
+
+
+def extract_lode_center(src):
+    """`central_atom_contribution` test of `lode/radial_integral/gto.rs`:
+    exponents, GTO (max_radial, radius), smearing and the pyLODE values."""
+    body = src[src.index("fn central_atom_contribution"):]
+    exponents = [int(v) for v in re.search(r"potential_exponents = \[(.*?)\]", body).group(1).split(",")]
+    start = body.index("let reference_vals")
+    block = body[start:body.index("]];", start) + 1]
+    rows = [[float(v) for v in re.findall(_FLOAT, row)] for row in re.findall(r"\[([^\[\]]+)\]", block)]
+    m = re.search(r"max_radial: (\d+), radius: (" + _FLOAT + r")", body)
+    smearing = float(re.search(r"smearing: (" + _FLOAT + r")", body).group(1))
+    return {"exponents": exponents, "values": rows, "max_radial": int(m.group(1)), "radius": float(m.group(2)),
+            "smearing": smearing}
+
+
+LODE = ["values-input.json", "values.npy.gz", "gradients-input.json", "positions-gradient.npy.gz"]
+
+
 def main(root):
     generated = os.path.join(root, "featomic", "tests", "data", "generated")
     for name in INPUTS:
@@ -131,17 +162,32 @@ def main(root):
             array = np.load(io.BytesIO(fd.read()))
         np.savez_compressed(os.path.join(HERE, name + ".npz"), values=array)
 
+    for p in range(1, 7):
+        folder = os.path.join(generated, "lode-spherical-expansion", f"exponent-{p}")
+        for name in LODE:
+            target = os.path.join(HERE, f"lode-exponent-{p}-{name}")
+            if name.endswith(".json"):
+                shutil.copyfile(os.path.join(folder, name), target)
+            else:
+                with gzip.open(os.path.join(folder, name), "rb") as fd:
+                    array = np.load(io.BytesIO(fd.read()))
+                np.savez_compressed(target.replace(".npy.gz", ".npz"), values=array)
+
     src = os.path.join(root, "featomic", "src")
     known = {
         "hyp1f1": extract_hyp1f1(_read(src, "math/hyp1f1.rs")),
         "cutoff": extract_cutoff(_read(src, "calculators/soap/cutoff.rs")),
         "neighbors_non_periodic": extract_neighbors(_read(src, "systems/neighbors.rs")),
         "gamma": extract_gamma(_read(src, "math/gamma.rs")),
+        "exp": extract_exp(_read(src, "math/exp.rs")),
+        "lode_center": extract_lode_center(_read(src, "calculators/lode/radial_integral/gto.rs")),
         "sources": {
             "hyp1f1": "featomic/src/math/hyp1f1.rs:263-288",
             "cutoff": "featomic/src/calculators/soap/cutoff.rs:97-112",
             "neighbors_non_periodic": "featomic/src/systems/neighbors.rs:413-444",
             "gamma": "featomic/src/math/gamma.rs:330-390",
+            "exp": "featomic/src/math/exp.rs:69-95",
+            "lode_center": "featomic/src/calculators/lode/radial_integral/gto.rs:261-286",
         },
     }
     with open(os.path.join(HERE, "known_answers.json"), "w") as fd:
