@@ -807,6 +807,85 @@ def cg_form(steps, warmup):
     }
 
 
+def lode_form(steps, warmup):
+    """LODE spherical expansion of the 1000-atom benchmark box (potential
+    exponent 1, smearing 1 A, k_cutoff 1.2 pi / smearing, GTO radius 5.5 A,
+    max_radial 7, max_angular 6, 4 species): values, positions in HBM, output
+    left in HBM, CUDA events around each compute.  Beside it: positions
+    gradients of a 64-atom box (their rows grow as atoms^2), and the oracle's
+    numpy restatement on the 1000-atom box (one run)."""
+    import torch
+    import rascaline_b200 as rb
+    from oracle import lode as oracle_lode
+    from rascaline_b200 import workloads
+
+    system, _ = workload()
+    n = len(system["types"])
+    hypers = {"density": {"type": "SmearedPowerLaw", "smearing": 1.0, "exponent": 1},
+              "basis": {"type": "TensorProduct", "max_angular": 6,
+                        "radial": {"type": "Gto", "max_radial": 7, "radius": 5.5}}}
+    calc = rb.LodeSphericalExpansion(**hypers)
+    pos = torch.tensor(system["positions"], device="cuda")
+    cell = np.asarray(system["cell"]).reshape(1, 9)
+
+    def run(p, types, c, sizes, gradients=()):
+        return calc.compute_device(p, types, c, sizes, gradients=list(gradients))
+
+    for _ in range(max(3, warmup)):
+        tm = run(pos, system["types"], cell, [n])
+    torch.cuda.synchronize()
+    del tm
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    kernel_ms = []
+    for k in range(steps):
+        starts[k].record()
+        tm = run(pos, system["types"], cell, [n])
+        ends[k].record()
+        kernel_ms.append(calc.timings()["expansion"])
+        del tm
+    torch.cuda.synchronize()
+    ms = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)]))
+    k_vectors = len(oracle_lode.k_vectors(system["cell"], 1.2 * np.pi)[0])
+    flops = 2.0 * n * 4 * k_vectors * 49 * 8  # the values contraction over k
+    # positions gradients of a small box
+    small = workloads.random_box(64, density=0.1, min_distance=0.9, seed=9)
+    spos = torch.tensor(small["positions"], device="cuda")
+    scell = np.asarray(small["cell"]).reshape(1, 9)
+    for _ in range(2):
+        tm = run(spos, small["types"], scell, [64], ["positions"])
+    torch.cuda.synchronize()
+    del tm
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        tm = run(spos, small["types"], scell, [64], ["positions"])
+        del tm
+    t1.record()
+    torch.cuda.synchronize()
+    grad_ms = t0.elapsed_time(t1) / steps
+    # the oracle on the 1000-atom box
+    start = time.perf_counter()
+    oracle_lode.compute(dict(hypers, basis=dict(hypers["basis"], spline_accuracy=None)), [system])
+    cpu_s = time.perf_counter() - start
+    return {
+        "workload": "random_box_1000_rho0.1_lode_p1_smearing1_nmax7_lmax6_values_fp64",
+        "metric": "atom-envs/s (LODE spherical expansion values)",
+        "value": n / (ms / 1000.0),
+        "ms_per_step": ms,
+        "kernel_ms": float(np.mean(kernel_ms)),
+        "k_vectors": k_vectors,
+        "fp64_tflops_values_contraction": flops / (float(np.mean(kernel_ms)) / 1000.0) / 1e12,
+        "gradients_64_atoms_ms": grad_ms,
+        "dtype": "f64",
+        "cpu_baseline": {"value": n / cpu_s, "unit": "atom-envs/s", "cores": 1, "kind": "port",
+                         "sample": "one oracle (numpy) run on the 1000-atom box, analytic radial integral"},
+        "gpu_launches_per_step": 5,
+        "steps": steps,
+    }
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -818,7 +897,7 @@ def main():
                         help="skip the FP32 adjoint form measured beside the drop-in")
     parser.add_argument("--atoms", type=int, default=1000,
                         help="atoms in the box (1000 is the benchmark; smaller boxes are for profiling)")
-    parser.add_argument("--only", choices=["adjoint", "batched", "surrogate", "combined", "cg"],
+    parser.add_argument("--only", choices=["adjoint", "batched", "surrogate", "combined", "cg", "lode"],
                         help="run one chosen form alone and print its object (profiling)")
     parser.add_argument("--adjoint-atoms", type=int, default=20000,
                         help="atoms of the adjoint form's box with --only adjoint (20000 is the benchmark)")
@@ -829,6 +908,7 @@ def main():
         import torch
         torch.cuda.set_device(0)
         form = {"adjoint": lambda k, w: adjoint_form(k, w, args.adjoint_atoms), "batched": batched_form, "cg": cg_form,
+                "lode": lode_form,
                 "surrogate": lambda k, w: surrogate_form(k, w, args.train_steps),
                 "combined": lambda k, w: combined_form(k, w, args.train_steps)}[args.only]
         print(json.dumps({args.only + "_form": form(args.steps, args.warmup)}), flush=True)
@@ -946,9 +1026,11 @@ def main():
             "traffic": profile_traffic("ps_positions_random_box_1000"),
         },
         "clocks": clocks,
-        # per step: neighbour list 4 + its 4 CUB scan kernels, pair features,
-        # spherical expansion, power spectrum values / positions / strain
-        "gpu_launches": 13 * args.steps,
+        # per step, this library's own kernels: neighbour list (assign, fill,
+        # count, write), direction keys and segments, neighbourhood tables
+        # (count, fill), fused spherical expansion, power spectrum values /
+        # positions / strain; beside them 11 CUB sort / scan kernels
+        "gpu_launches": 12 * args.steps,
     }
     if not args.no_chosen_forms:
         line["adjoint_form"] = adjoint_form(args.steps, args.warmup)
@@ -958,6 +1040,7 @@ def main():
         line["surrogate_form"] = surrogate_form(min(args.steps, 5), args.warmup, args.train_steps)
         line["combined_form"] = combined_form(args.steps, args.warmup, args.train_steps, line["value"])
         line["cg_form"] = cg_form(min(args.steps, 10), args.warmup)
+        line["lode_form"] = lode_form(min(args.steps, 10), args.warmup)
         # a compact summary of the chosen forms placed before the long objects
         forms = {}
         for name in ("adjoint_form", "batched_form", "combined_form"):

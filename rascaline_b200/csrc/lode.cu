@@ -465,11 +465,22 @@ __global__ void __launch_bounds__(LODE_THREADS) lode_values_kernel(LodeArgs a, c
             const int o = o0 + q * LODE_THREADS + threadIdx.x;
             if (o >= outs) continue;
             const double* Tk = a.T + (size_t)k0 * outs + o;
-            const bool odd = parity[q];
-            for (int kk = 0; kk < nk; kk++) {
+            const double(*w)[LODE_CHUNK] = parity[q] ? wi : wr;
+            int kk = 0;
+            // four k-vectors per step: the loads first, then each sum in k order
+            for (; kk + 4 <= nk; kk += 4) {
+                double tv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) tv[u] = Tk[(size_t)(kk + u) * outs];
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int c = 0; c < LODE_GROUP; c++) acc[c][q] += w[c][kk + u] * tv[u];
+            }
+            for (; kk < nk; kk++) {
                 const double tv = Tk[(size_t)kk * outs];
 #pragma unroll
-                for (int c = 0; c < LODE_GROUP; c++) acc[c][q] += (odd ? wi[c][kk] : wr[c][kk]) * tv;
+                for (int c = 0; c < LODE_GROUP; c++) acc[c][q] += w[c][kk] * tv;
             }
         }
     }
@@ -553,7 +564,20 @@ __global__ void __launch_bounds__(LODE_THREADS) lode_gradients_kernel(LodeArgs a
             const bool oddl = l_of(o / a.N) & 1;
             const double* p = oddl ? po : pe;
             const double* Tk = a.T + (size_t)k0 * outs + o;
-            for (int kk = 0; kk < nk; kk++) {
+            int kk = 0;
+            for (; kk + 4 <= nk; kk += 4) {
+                double tv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) tv[u] = Tk[(size_t)(kk + u) * outs];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const double s = p[kk + u] * tv[u] * kn[kk + u];
+                    acc[q][0] += s * kd[kk + u][0];
+                    acc[q][1] += s * kd[kk + u][1];
+                    acc[q][2] += s * kd[kk + u][2];
+                }
+            }
+            for (; kk < nk; kk++) {
                 const double s = p[kk] * Tk[(size_t)kk * outs] * kn[kk];
                 acc[q][0] += s * kd[kk][0];
                 acc[q][1] += s * kd[kk][1];
