@@ -32,7 +32,7 @@ from . import _c_api as C
 from .calculators import CalculatorBase, Labels
 
 __all__ = ["System", "Calculator", "SoapPowerSpectrum", "SphericalExpansion", "TorchTensorMap", "TorchBlock", "Batch",
-           "dense_power_spectrum", "dense_spherical_expansion", "dense_jvp"]
+           "dense_power_spectrum", "dense_spherical_expansion", "dense_jvp", "register_autograd"]
 
 
 class System:
@@ -53,8 +53,11 @@ class System:
 class DenseState:
     """A forward pass kept for its backward pass (featomic_b200_dense_t)."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, calculator):
         self._handle = handle
+        # the state refers to its calculator's device tables and must be
+        # freed before it (featomic_b200_dense_free): keep the calculator alive
+        self._calculator = calculator
         n = [ctypes.c_size_t() for _ in range(5)]
         C.check(C.lib().featomic_b200_dense_shape(handle, *[ctypes.byref(x) for x in n]))
         self.n_atoms, self.n_species, self.n_keys, self.n_properties, self.n_pairs = [x.value for x in n]
@@ -118,7 +121,7 @@ def dense_power_spectrum(calculator, positions, types, cells, sizes, precision=6
     C.check(C.lib().featomic_b200_power_spectrum_dense(
         calculator._handle, ctypes.byref(dev), sp.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), S, precision,
         values.data_ptr(), values.numel(), ctypes.byref(handle), ctypes.c_void_p(stream)))
-    return values, DenseState(handle)
+    return values, DenseState(handle, calculator)
 
 
 def dense_backward(state, grad_values, n_systems, strain=False, cell=True):
@@ -162,7 +165,7 @@ def dense_spherical_expansion(calculator, positions, types, cells, sizes, precis
     C.check(C.lib().featomic_b200_spherical_expansion_dense(
         calculator._handle, ctypes.byref(dev), sp.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(sp), precision,
         values.data_ptr(), values.numel(), ctypes.byref(handle), ctypes.c_void_p(stream)))
-    return values, DenseState(handle)
+    return values, DenseState(handle, calculator)
 
 
 def expansion_backward(state, grad_coefficients, n_systems, strain=False, cell=True):
@@ -272,11 +275,105 @@ class _DenseForward(torch.autograd.Function):
 
 
 class TorchBlock:
-    def __init__(self, values, samples, properties, components=None):
+    def __init__(self, values, samples, properties, components=None, gradients=None):
         self.values = values
         self.samples = samples
         self.properties = properties
         self.components = components or []
+        self._gradients = dict(gradients or {})
+
+    def gradient(self, parameter):
+        return self._gradients[parameter]
+
+    def gradients_list(self):
+        return list(self._gradients)
+
+
+class _ExplicitGradients(torch.autograd.Function):
+    """featomic-torch's FeatomicAutograd (autograd.cpp:99-233) with the
+    contractions of PositionsGrad (:237-317) and CellGrad (:429-503): the
+    block's values, whose backward contracts dA/dX with the precomputed
+    explicit gradient blocks, on the device.  The backward is written with
+    differentiable torch operations, so it is itself differentiable with
+    respect to dA/dX (double backward, :318-426); second derivatives with
+    respect to positions and cells are zero here, with featomic-torch's
+    warning."""
+
+    @staticmethod
+    def forward(ctx, positions, cells, values, grad_samples, grad_values, atom_start, cell_values, sample_systems):
+        ctx.save_for_backward(grad_samples, grad_values, atom_start, cell_values, sample_systems)
+        ctx.shapes = (positions.shape, cells.shape)
+        return values.detach().clone()
+
+    @staticmethod
+    def backward(ctx, dA_dX):
+        grad_samples, grad_values, atom_start, cell_values, sample_systems = ctx.saved_tensors
+        pos_shape, cell_shape = ctx.shapes
+        dA_dr = dA_dH = None
+        flat = dA_dX.reshape(dA_dX.shape[0], -1)
+        if ctx.needs_input_grad[0]:
+            if torch.is_grad_enabled():
+                warnings.warn("second derivatives with respect to positions are not implemented and will not be "
+                              "accumulated during backward() calls", stacklevel=2)
+            rows = grad_values.reshape(grad_values.shape[0], 3, -1)
+            sample = grad_samples[:, 0].long()
+            atom = atom_start[grad_samples[:, 1].long()] + grad_samples[:, 2].long()
+            contrib = torch.einsum("rxf,rf->rx", rows.to(flat.dtype), flat[sample])
+            dA_dr = torch.zeros(pos_shape, dtype=flat.dtype, device=flat.device).index_add(0, atom, contrib)
+        if ctx.needs_input_grad[1]:
+            if torch.is_grad_enabled():
+                warnings.warn("second derivatives with respect to cell matrix are not implemented and will not be "
+                              "accumulated during backward() calls", stacklevel=2)
+            rows = cell_values.reshape(cell_values.shape[0], 3, 3, -1)
+            contrib = torch.einsum("sabf,sf->sab", rows.to(flat.dtype), flat)
+            dA_dH = torch.zeros(cell_shape, dtype=flat.dtype, device=flat.device).index_add(
+                0, sample_systems.long(), contrib)
+        return dA_dr, dA_dH, None, None, None, None, None, None
+
+
+def register_autograd(systems, precomputed, forward_gradients=None):
+    """featomic-torch's ``register_autograd(systems, precomputed,
+    forward_gradients)`` (featomic-torch/src/calculator.cpp:314-383): connect
+    the blocks of a TensorMap computed with explicit gradients (``compute`` /
+    ``compute_device`` with ``gradients=["positions", "cell"]``) to the
+    systems' positions and cells in torch's autograd graph.  Returns a
+    TorchTensorMap whose block values carry autograd and which keeps the
+    gradients listed in ``forward_gradients`` (all of the precomputed ones
+    when None)."""
+    if isinstance(systems, System):
+        systems = [systems]
+    blocks = precomputed.blocks()
+    if len(blocks) == 0:
+        return precomputed
+    positions = torch.cat([s.positions.reshape(-1, 3) for s in systems])
+    cells = torch.stack([s.cell.reshape(3, 3) for s in systems])
+    available = blocks[0].gradients_list()
+    if positions.requires_grad and "positions" not in available:
+        raise ValueError("expected the precomputed TensorMap to contain gradients with respect to 'positions' "
+                         "since one of the system `requires_grad` for its positions")
+    if cells.requires_grad and "cell" not in available:
+        raise ValueError("expected the precomputed TensorMap to contain gradients with respect to 'cell' since "
+                         "one of the system `requires_grad` for its cell")
+    keep = available if forward_gradients is None else list(forward_gradients)
+    starts = torch.tensor(np.concatenate([[0], np.cumsum([len(s) for s in systems])[:-1]]), dtype=torch.long,
+                          device=positions.device)
+    empty = torch.zeros(0, device=positions.device)
+    out = []
+    for block in blocks:
+        values = torch.as_tensor(block.values, device=positions.device)
+        samples = torch.as_tensor(np.asarray(block.samples.values), device=positions.device)
+        gs = gv = cv = empty
+        if positions.requires_grad:
+            g = block.gradient("positions")
+            gs = torch.as_tensor(np.asarray(g.samples.values), device=positions.device)
+            gv = torch.as_tensor(g.values, device=positions.device)
+        if cells.requires_grad:
+            cv = torch.as_tensor(block.gradient("cell").values, device=positions.device)
+        attached = _ExplicitGradients.apply(positions, cells, values, gs, gv, starts, cv,
+                                            samples[:, 0] if len(samples) else empty)
+        grads = {name: block.gradient(name) for name in keep if name in available}
+        out.append(TorchBlock(attached, block.samples, block.properties, list(block.components), grads))
+    return TorchTensorMap(precomputed.keys, out)
 
 
 class TorchTensorMap:
