@@ -220,7 +220,9 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
 
 // Fused form of pair_features + se_accumulate (lmax <= 8): one CTA per
 // (centre, neighbour species) segment.  For each chunk of FUSED_CHUNK
-// directions the pair terms are built in shared memory instead of being read
+// directions (32: nearly every segment is one chunk, and 86 KB of shared
+// memory still fits the two CTAs per SM the registers allow) the pair terms
+// are built in shared memory instead of being read
 // back from per-pair records in HBM: one thread per (direction, m) evaluates
 // column m of the Legendre table and then Y_l^{+-m} (+ gradients), one thread
 // per (direction, l) the radial integral R_nl (+ dR/dr), one thread per
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
 // radial functions of one (l, m) over the chunk's directions in pair order.
 // The same functions in the same order as the two-kernel path, so the results
 // are bit-identical to it; no atomics.
-constexpr int FUSED_CHUNK = 16;
+constexpr int FUSED_CHUNK = 32;
 
 struct FusedDir {
     double f, fg, r, u[3], v[3], sh[3];
