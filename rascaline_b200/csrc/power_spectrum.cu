@@ -492,6 +492,296 @@ __global__ void __launch_bounds__(POS_WARPS * 32, POS_MIN_BLOCKS) ps_positions_k
     }
 }
 
+// ---------------------------------------------------------------------------
+// Positions-gradient rows, staged form (nmax <= 8, at most 10 species).
+//
+// A CTA owns a contiguous range of one centre's neighbour entries (the rows
+// of consecutive entries in a slot are consecutive in memory).  Its four
+// warps share, in shared memory:
+//   * the centre's coefficients of every species in DMMA fragment order,
+//     zero-padded to 4 m and 8 n per l (so that padding contributes nothing);
+//   * a ring of three pair-gradient buffers [3][(l m)][n], filled by cp.async
+//     two entries ahead of the one being computed (for nmax = 8 the 16-byte
+//     chunks of each 64-byte row are swizzled so that the fragment loads of
+//     four consecutive rows hit 32 distinct banks);
+//   * the slot tables, the slots of each neighbour species, and the entry
+//     metadata of up to STG_CHUNK entries.
+// Every (entry, slot) is one item: a warp computes the whole gradient row
+// (3 x (lmax + 1) tiles of 8 x 8, written front to back with 512-byte
+// streaming stores) on the FP64 tensor cores, so each row leaves the SM in
+// one short burst.  The per-l products and their order equal the per-warp
+// DMMA form above; the centre's own row and entries with several periodic
+// images of one neighbour take the CUDA-core rows with global operands.
+constexpr int STG_WARPS = 4;
+constexpr int STG_RING = 3;
+constexpr int STG_CHUNK = 64;
+constexpr int STG_SPLIT = 2;
+constexpr int STG_MAX_SPECIES = 10;
+constexpr int STG_MAX_SLOTS = STG_MAX_SPECIES * (STG_MAX_SPECIES + 1) / 2;
+constexpr int STG_G_PAD = 32;  // doubles after each gradient buffer, read by the padded last m step
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// DMMA steps of 4 m values over l = 0..lmax
+__host__ __device__ __forceinline__ int stg_steps(int lmax) {
+    int n = 0;
+    for (int l = 0; l <= lmax; l++) n += (2 * l + 1 + 3) / 4;
+    return n;
+}
+
+// position of element n of row r (64-byte rows of 4 chunks of 16 bytes) in
+// the swizzled nmax = 8 gradient buffer: chunk c of row r sits at c ^ 2 when
+// bit 1 of r is set
+__device__ __forceinline__ int stg_swizzle8(int r, int n) {
+    return r * 8 + ((((n >> 1) ^ (((r >> 1) & 1) << 1))) << 1) + (n & 1);
+}
+
+struct StgLayout {
+    int P;        // doubles per species of the fragment-ordered coefficients (32 per step)
+    int GB;       // doubles per gradient buffer (3 K + padding, even)
+    size_t cf, scale, ring, slot_base, slot_ab, sp_count, sp_slot, meta_entry, meta_code, meta_cum, bytes;
+};
+
+__host__ __device__ inline StgLayout stg_layout(int S, int lmax, int nmax) {
+    StgLayout L{};
+    const int K = (lmax + 1) * (lmax + 1) * nmax;
+    L.P = 32 * stg_steps(lmax);
+    L.GB = (3 * K + STG_G_PAD + 1) & ~1;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = off;
+        off += (bytes + 15) & ~(size_t)15;
+        return at;
+    };
+    L.cf = take(sizeof(double) * S * L.P);
+    L.scale = take(sizeof(double) * 2 * (lmax + 1));
+    L.ring = take(sizeof(double) * STG_RING * L.GB);
+    L.slot_base = take(sizeof(int64_t) * STG_MAX_SLOTS);
+    L.slot_ab = take(sizeof(int32_t) * 2 * STG_MAX_SLOTS);
+    L.sp_count = take(sizeof(int32_t) * STG_MAX_SPECIES);
+    L.sp_slot = take(sizeof(int32_t) * STG_MAX_SPECIES * STG_MAX_SPECIES);
+    L.meta_entry = take(sizeof(PsEntry) * STG_CHUNK);
+    L.meta_code = take(sizeof(int32_t) * STG_CHUNK);
+    L.meta_cum = take(sizeof(int32_t) * STG_CHUNK * (S + 1));
+    L.bytes = off;
+    return L;
+}
+
+// one (entry, slot) row from a staged pair gradient: per l, the three 8 x 8
+// tiles G^T C_b (entry species == a) and C_a^T G (entry species == b)
+template <bool N8>
+__device__ __forceinline__ void stg_row(int lane, int lmax, int nmax, int64_t n_props, const double* __restrict__ gs,
+                                        const double* __restrict__ cf, int P, const double* __restrict__ scale_s,
+                                        int a, int b, int s, bool flip, double* __restrict__ out) {
+    const int tm = lane & 3, tn = lane >> 2;
+    const bool t1 = s == a, t2 = s == b;
+    const double* ca = cf + a * P + lane;
+    const double* cb = cf + b * P + lane;
+    const int RB = (lmax + 1) * (lmax + 1);  // rows of one component
+    const int N = N8 ? 8 : nmax;
+    const bool vec = N8 && ((((uintptr_t)out) & 15) == 0);
+    const double* scales = scale_s + (a != b ? lmax + 1 : 0);
+    int step = 0;
+    for (int l = 0; l <= lmax; l++) {
+        const int steps = (2 * l + 1 + 3) >> 2;
+        double acc[3][2];
+#pragma unroll
+        for (int x = 0; x < 3; x++) acc[x][0] = acc[x][1] = 0.0;
+        for (int st = 0; st < steps; st++) {
+            const int r = l * l + 4 * st + tm;
+            double g[3];
+#pragma unroll
+            for (int x = 0; x < 3; x++) g[x] = N8 ? gs[stg_swizzle8(x * RB + r, tn)] : gs[(x * RB + r) * N + tn];
+            if (t1) {
+                const double c = cb[(step + st) * 32];
+#pragma unroll
+                for (int x = 0; x < 3; x++) dmma_8x8x4(acc[x], g[x], c);
+            }
+            if (t2) {
+                const double c = ca[(step + st) * 32];
+#pragma unroll
+                for (int x = 0; x < 3; x++) dmma_8x8x4(acc[x], c, g[x]);
+            }
+        }
+        step += steps;
+        // -(-1)^l of a reversed pair, exact, folded into the scale
+        const double scale = (flip && (l & 1) == 0) ? -scales[l] : scales[l];
+        const int n2 = 2 * tm;
+        if (vec) {
+            double* o = out + (int64_t)l * 64 + tn * 8 + n2;
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                double2 w;
+                w.x = acc[x][0] * scale;
+                w.y = acc[x][1] * scale;
+                __stcs(reinterpret_cast<double2*>(o + x * n_props), w);
+            }
+        } else if (tn < N) {
+            double* o = out + (int64_t)l * N * N + tn * N + n2;
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                if (n2 < N) __stcs(o + x * n_props, acc[x][0] * scale);
+                if (n2 + 1 < N) __stcs(o + x * n_props + 1, acc[x][1] * scale);
+            }
+        }
+    }
+}
+
+template <bool N8>
+__global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(PsArgs a) {
+    extern __shared__ __align__(16) unsigned char stg_smem[];
+    const int64_t c = blockIdx.x / STG_SPLIT;
+    const int part = (int)(blockIdx.x - c * STG_SPLIT);
+    const int S = a.n_species, L = a.lmax, N = a.nmax;
+    const int K = (L + 1) * (L + 1) * N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t e_first = a.entry_offset[c], n_entries = a.entry_offset[c + 1] - e_first;
+    const int64_t eb = e_first + n_entries * part / STG_SPLIT;
+    const int64_t ee = e_first + n_entries * (part + 1) / STG_SPLIT;
+    if (eb >= ee) return;
+
+    const StgLayout lay = stg_layout(S, L, N);
+    double* cf = reinterpret_cast<double*>(stg_smem + lay.cf);
+    double* scale_s = reinterpret_cast<double*>(stg_smem + lay.scale);
+    double* ring = reinterpret_cast<double*>(stg_smem + lay.ring);
+    int64_t* slot_base = reinterpret_cast<int64_t*>(stg_smem + lay.slot_base);
+    int32_t* slot_ab = reinterpret_cast<int32_t*>(stg_smem + lay.slot_ab);
+    int32_t* sp_count = reinterpret_cast<int32_t*>(stg_smem + lay.sp_count);
+    int32_t* sp_slot = reinterpret_cast<int32_t*>(stg_smem + lay.sp_slot);
+    PsEntry* meta_entry = reinterpret_cast<PsEntry*>(stg_smem + lay.meta_entry);
+    int32_t* meta_code = reinterpret_cast<int32_t*>(stg_smem + lay.meta_code);
+    int32_t* meta_cum = reinterpret_cast<int32_t*>(stg_smem + lay.meta_cum);
+
+    // coefficients in fragment order: element (step, lane) of species sp is
+    // c[l, m = 4 st + lane % 4, n = lane / 4], zero outside m < 2l+1, n < nmax
+    const double* coef = a.coef + c * S * K;
+    for (int i = threadIdx.x; i < S * lay.P; i += blockDim.x) {
+        const int sp = i / lay.P, rem = i - sp * lay.P;
+        int g = rem >> 5;
+        const int t = rem & 31;
+        int l = 0;
+        while (g >= ((2 * l + 1 + 3) >> 2)) {
+            g -= (2 * l + 1 + 3) >> 2;
+            l++;
+        }
+        const int m = 4 * g + (t & 3), n = t >> 2;
+        cf[i] = (m < 2 * l + 1 && n < N) ? coef[sp * K + (l * l + m) * N + n] : 0.0;
+    }
+    load_scales(L, scale_s);
+    // the padded last m steps read past the gradient: keep that tail finite
+    for (int i = threadIdx.x; i < STG_RING * (lay.GB - 3 * K); i += blockDim.x) {
+        const int buf = i / (lay.GB - 3 * K), j = i - buf * (lay.GB - 3 * K);
+        ring[buf * lay.GB + 3 * K + j] = 0.0;
+    }
+    const int64_t s0 = a.slot_offset[c];
+    // one slot per species pair a <= b of the centre's keys: at most
+    // STG_MAX_SLOTS for the species counts this kernel is launched with
+    const int ns = (int)(a.slot_offset[c + 1] - s0);
+    if (ns > STG_MAX_SLOTS) return;
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+        const PsKeySlot slot = a.slots[s0 + i];
+        slot_base[i] = a.off_positions[slot.block] + a.slot_row[s0 + i] * 3 * a.n_props;
+        slot_ab[2 * i] = slot.a;
+        slot_ab[2 * i + 1] = slot.b;
+    }
+    __syncthreads();
+    if (threadIdx.x < S) {
+        const int sp = threadIdx.x;
+        int n = 0;
+        for (int i = 0; i < ns; i++)
+            if (slot_ab[2 * i] == sp || slot_ab[2 * i + 1] == sp) sp_slot[sp * STG_MAX_SPECIES + n++] = i;
+        sp_count[sp] = n;
+    }
+
+    const bool aligned16 = ((3 * K) & 1) == 0;
+    for (int64_t chunk = eb; chunk < ee; chunk += STG_CHUNK) {
+        const int nc = (int)min((int64_t)STG_CHUNK, ee - chunk);
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+            const PsEntry entry = a.entries[chunk + i];
+            meta_entry[i] = entry;
+            meta_code[i] = (entry.d1 - entry.d0 == 1) ? a.dir_code[entry.d0] : 0;
+        }
+        for (int i = threadIdx.x; i < nc * (S + 1); i += blockDim.x) meta_cum[i] = a.entry_cum[chunk * (S + 1) + i];
+        __syncthreads();
+
+        // pair gradient of entry k into ring buffer k % STG_RING (regular
+        // entries only: one pair, not the centre)
+        auto issue = [&](int k) {
+            if (k < nc) {
+                const PsEntry entry = meta_entry[k];
+                if (entry.atom != (int32_t)c && entry.d1 - entry.d0 == 1) {
+                    const double* src = a.pair_grad + (int64_t)(meta_code[k] >> 1) * 3 * K;
+                    double* dst = ring + (k % STG_RING) * lay.GB;
+                    if (N8) {
+                        for (int q = threadIdx.x; q < 3 * K / 2; q += blockDim.x) {
+                            const int r = q >> 2, ch = q & 3;
+                            cp_async16(dst + r * 8 + ((ch ^ (((r >> 1) & 1) << 1)) << 1), src + 2 * q);
+                        }
+                    } else if (aligned16) {
+                        for (int q = threadIdx.x; q < 3 * K / 2; q += blockDim.x) cp_async16(dst + 2 * q, src + 2 * q);
+                    } else {
+                        for (int q = threadIdx.x; q < 3 * K; q += blockDim.x) cp_async8(dst + q, src + q);
+                    }
+                }
+            }
+            cp_async_commit();
+        };
+        issue(0);
+        issue(1);
+        for (int k = 0; k < nc; k++) {
+            cp_async_wait<1>();
+            // entry k's gradient is visible to every warp, and every warp is
+            // done with entry k - 1, whose buffer the next issue reuses
+            __syncthreads();
+            issue(k + 2);
+            const PsEntry entry = meta_entry[k];
+            const int32_t* cum = meta_cum + k * (S + 1);
+            const bool self = entry.atom == (int32_t)c;
+            const bool regular = !self && entry.d1 - entry.d0 == 1;
+            const int n_items = self ? ns : sp_count[entry.species];
+            for (int it = warp; it < n_items; it += STG_WARPS) {
+                const int si = self ? it : sp_slot[entry.species * STG_MAX_SPECIES + it];
+                const int sa = slot_ab[2 * si], sb = slot_ab[2 * si + 1];
+                const int64_t rank = cum[sa] + (sa != sb ? cum[sb] : 0) + cum[S];
+                double* out = a.out + slot_base[si] + rank * 3 * a.n_props;
+                if (regular) {
+                    stg_row<N8>(lane, L, N, a.n_props, ring + (k % STG_RING) * lay.GB, cf, lay.P, scale_s, sa, sb,
+                                entry.species, meta_code[k] & 1, out);
+                } else {
+                    const PsKeySlot slot{0, 0, sa, sb};
+                    const double* self_a = a.self_grad + ((int64_t)c * S + sa) * 3 * K;
+                    const double* self_b = a.self_grad + ((int64_t)c * S + sb) * 3 * K;
+                    if (self) {
+                        DirectSource none{nullptr, false};
+                        positions_row(a, lane, K, coef, scale_s, slot, true, entry.species, none, self_a, self_b, out);
+                    } else {
+                        ImagesSource images{a.dir_code + entry.d0, entry.d1 - entry.d0, a.pair_grad, 3 * (int64_t)K};
+                        positions_row(a, lane, K, coef, scale_s, slot, false, entry.species, images, self_a, self_b,
+                                      out);
+                    }
+                }
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();  // metadata and ring are reused by the next chunk
+    }
+}
+
 // strain (which = 0) or cell (which = 1) rows: 9 components, done as three
 // passes of 3 to bound the register tile
 template <int MAXN>
@@ -550,6 +840,8 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
         CUDA_CHECK(cudaFuncSetAttribute(ps_values_kernel<MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         CUDA_CHECK(cudaFuncSetAttribute(ps_positions_kernel<MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         CUDA_CHECK(cudaFuncSetAttribute(ps_strain_cell_kernel<MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(ps_positions_staged_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(ps_positions_staged_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         configured = true;
     }
     if (coef_bytes > 200 * 1024) throw invalid_parameter("too many species / radial / angular functions for the power spectrum kernels");
@@ -584,7 +876,14 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
     // caller's stream: positions
     if (events.before_positions) CUDA_CHECK(cudaEventRecord(events.before_positions, stream));
     if (positions) {
-        ps_positions_kernel<MAXN><<<(unsigned)(args.n_centres * POS_SPLIT), POS_WARPS * 32, pos_bytes, stream>>>(args);
+        const StgLayout stg = stg_layout(args.n_species, args.lmax, args.nmax);
+        if (args.nmax <= 8 && args.n_species <= STG_MAX_SPECIES && stg.bytes <= 200 * 1024) {
+            const unsigned grid = (unsigned)(args.n_centres * STG_SPLIT);
+            if (args.nmax == 8) ps_positions_staged_kernel<true><<<grid, STG_WARPS * 32, stg.bytes, stream>>>(args);
+            else ps_positions_staged_kernel<false><<<grid, STG_WARPS * 32, stg.bytes, stream>>>(args);
+        } else {
+            ps_positions_kernel<MAXN><<<(unsigned)(args.n_centres * POS_SPLIT), POS_WARPS * 32, pos_bytes, stream>>>(args);
+        }
         CUDA_CHECK(cudaGetLastError());
     }
     if (events.after_positions) CUDA_CHECK(cudaEventRecord(events.after_positions, stream));

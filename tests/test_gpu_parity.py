@@ -200,6 +200,12 @@ def test_mixed_systems(oracle):
                          ("positions", "strain"))
 
 
+def test_power_spectrum_many_radial_functions(oracle):
+    # more than 8 radial functions: the positions rows take the per-warp kernel
+    systems = [workloads.random_box(80, seed=21)]
+    check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(4.0, 9, 2), systems, ("positions", "strain"))
+
+
 def test_user_neighbor_list(oracle):
     # use_native_system = False: pairs come from the caller (here, the oracle's list)
     systems = [workloads.random_box(250, seed=12)]
