@@ -500,25 +500,29 @@ __global__ void __launch_bounds__(POS_WARPS * 32, POS_MIN_BLOCKS) ps_positions_k
 // warps share, in shared memory:
 //   * the centre's coefficients of every species in DMMA fragment order,
 //     zero-padded to 4 m and 8 n per l (so that padding contributes nothing);
-//   * a ring of three pair-gradient buffers [3][(l m)][n], filled by cp.async
-//     two entries ahead of the one being computed (for nmax = 8 the 16-byte
-//     chunks of each 64-byte row are swizzled so that the fragment loads of
-//     four consecutive rows hit 32 distinct banks);
+//   * a ring of three pair-gradient buffers filled by cp.async two entries
+//     ahead of the one being computed.  For nmax = 8 a buffer holds
+//     [3][step][4 m][8 n] (m padded to 4 per l like the coefficients, the
+//     padding kept at zero), with the 16-byte chunks of the rows m = 2, 3 of
+//     each step swapped pairwise, so that a fragment load is one offset per
+//     lane plus a warp-uniform step offset and its 32 lanes hit 32 distinct
+//     banks in each half warp; other nmax keep featomic's [3][(l m)][n];
 //   * the slot tables, the slots of each neighbour species, and the entry
 //     metadata of up to STG_CHUNK entries.
 // Every (entry, slot) is one item: a warp computes the whole gradient row
 // (3 x (lmax + 1) tiles of 8 x 8, written front to back with 512-byte
 // streaming stores) on the FP64 tensor cores, so each row leaves the SM in
 // one short burst.  The per-l products and their order equal the per-warp
-// DMMA form above; the centre's own row and entries with several periodic
-// images of one neighbour take the CUDA-core rows with global operands.
+// DMMA form above.  Entries with several periodic images of one neighbour
+// take the CUDA-core rows with global operands; the centre's own rows are
+// written by ps_centre_rows_kernel on the side stream.
 constexpr int STG_WARPS = 4;
 constexpr int STG_RING = 3;
 constexpr int STG_CHUNK = 64;
 constexpr int STG_SPLIT = 2;
 constexpr int STG_MAX_SPECIES = 10;
 constexpr int STG_MAX_SLOTS = STG_MAX_SPECIES * (STG_MAX_SPECIES + 1) / 2;
-constexpr int STG_G_PAD = 32;  // doubles after each gradient buffer, read by the padded last m step
+constexpr int STG_G_PAD = 32;  // doubles after an unpadded gradient buffer, read by the padded last m step
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
@@ -544,24 +548,26 @@ __host__ __device__ __forceinline__ int stg_steps(int lmax) {
     return n;
 }
 
-// position of element n of row r (64-byte rows of 4 chunks of 16 bytes) in
-// the swizzled nmax = 8 gradient buffer: chunk c of row r sits at c ^ 2 when
-// bit 1 of r is set
-__device__ __forceinline__ int stg_swizzle8(int r, int n) {
-    return r * 8 + ((((n >> 1) ^ (((r >> 1) & 1) << 1))) << 1) + (n & 1);
+// offset of lane (m = lane % 4, n = lane / 4) inside a 32-double step block
+// of the swizzled nmax = 8 buffer: chunk n / 2 of rows m = 2, 3 is stored at
+// (n / 2) ^ 2
+__device__ __forceinline__ int stg_lane_offset8(int lane) {
+    const int tm = lane & 3, tn = lane >> 2;
+    return tm * 8 + ((((tn >> 1) ^ (((tm >> 1) & 1) << 1))) << 1) + (tn & 1);
 }
 
 struct StgLayout {
     int P;        // doubles per species of the fragment-ordered coefficients (32 per step)
-    int GB;       // doubles per gradient buffer (3 K + padding, even)
-    size_t cf, scale, ring, slot_base, slot_ab, sp_count, sp_slot, meta_entry, meta_code, meta_cum, bytes;
+    int GB;       // doubles per gradient buffer (even)
+    size_t cf, scale, ring, rows, slot_base, slot_ab, sp_count, sp_slot, meta_entry, meta_code, meta_cum, bytes;
 };
 
 __host__ __device__ inline StgLayout stg_layout(int S, int lmax, int nmax) {
     StgLayout L{};
-    const int K = (lmax + 1) * (lmax + 1) * nmax;
+    const int RB = (lmax + 1) * (lmax + 1);
+    const int K = RB * nmax;
     L.P = 32 * stg_steps(lmax);
-    L.GB = (3 * K + STG_G_PAD + 1) & ~1;
+    L.GB = nmax == 8 ? 3 * L.P : (3 * K + STG_G_PAD + 1) & ~1;
     size_t off = 0;
     auto take = [&](size_t bytes) {
         const size_t at = off;
@@ -571,6 +577,7 @@ __host__ __device__ inline StgLayout stg_layout(int S, int lmax, int nmax) {
     L.cf = take(sizeof(double) * S * L.P);
     L.scale = take(sizeof(double) * 2 * (lmax + 1));
     L.ring = take(sizeof(double) * STG_RING * L.GB);
+    L.rows = take(sizeof(int32_t) * 3 * RB);
     L.slot_base = take(sizeof(int64_t) * STG_MAX_SLOTS);
     L.slot_ab = take(sizeof(int32_t) * 2 * STG_MAX_SLOTS);
     L.sp_count = take(sizeof(int32_t) * STG_MAX_SPECIES);
@@ -592,10 +599,12 @@ __device__ __forceinline__ void stg_row(int lane, int lmax, int nmax, int64_t n_
     const bool t1 = s == a, t2 = s == b;
     const double* ca = cf + a * P + lane;
     const double* cb = cf + b * P + lane;
-    const int RB = (lmax + 1) * (lmax + 1);  // rows of one component
+    const int RB = (lmax + 1) * (lmax + 1);  // rows (l, m) of one component
     const int N = N8 ? 8 : nmax;
     const bool vec = N8 && ((((uintptr_t)out) & 15) == 0);
     const double* scales = scale_s + (a != b ? lmax + 1 : 0);
+    // N8: component x of step st starts at (x P + 32 st) + the lane's offset
+    const double* g0 = gs + (N8 ? stg_lane_offset8(lane) : 0);
     int step = 0;
     for (int l = 0; l <= lmax; l++) {
         const int steps = (2 * l + 1 + 3) >> 2;
@@ -603,10 +612,16 @@ __device__ __forceinline__ void stg_row(int lane, int lmax, int nmax, int64_t n_
 #pragma unroll
         for (int x = 0; x < 3; x++) acc[x][0] = acc[x][1] = 0.0;
         for (int st = 0; st < steps; st++) {
-            const int r = l * l + 4 * st + tm;
             double g[3];
+            if (N8) {
+                const double* gp = g0 + (step + st) * 32;
 #pragma unroll
-            for (int x = 0; x < 3; x++) g[x] = N8 ? gs[stg_swizzle8(x * RB + r, tn)] : gs[(x * RB + r) * N + tn];
+                for (int x = 0; x < 3; x++) g[x] = gp[x * P];
+            } else {
+                const int r = l * l + 4 * st + tm;
+#pragma unroll
+                for (int x = 0; x < 3; x++) g[x] = gs[(x * RB + r) * N + tn];
+            }
             if (t1) {
                 const double c = cb[(step + st) * 32];
 #pragma unroll
@@ -642,13 +657,25 @@ __device__ __forceinline__ void stg_row(int lane, int lmax, int nmax, int64_t n_
     }
 }
 
+// (l, step offset) of row lm = l^2 + m
+__device__ __forceinline__ void stg_row_position(int lm, int& l, int& m, int& step) {
+    l = 0;
+    step = 0;
+    while ((l + 1) * (l + 1) <= lm) {
+        step += (2 * l + 1 + 3) >> 2;
+        l++;
+    }
+    m = lm - l * l;
+}
+
 template <bool N8>
 __global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(PsArgs a) {
     extern __shared__ __align__(16) unsigned char stg_smem[];
     const int64_t c = blockIdx.x / STG_SPLIT;
     const int part = (int)(blockIdx.x - c * STG_SPLIT);
     const int S = a.n_species, L = a.lmax, N = a.nmax;
-    const int K = (L + 1) * (L + 1) * N;
+    const int RB = (L + 1) * (L + 1);
+    const int K = RB * N;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t e_first = a.entry_offset[c], n_entries = a.entry_offset[c + 1] - e_first;
     const int64_t eb = e_first + n_entries * part / STG_SPLIT;
@@ -659,6 +686,7 @@ __global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(
     double* cf = reinterpret_cast<double*>(stg_smem + lay.cf);
     double* scale_s = reinterpret_cast<double*>(stg_smem + lay.scale);
     double* ring = reinterpret_cast<double*>(stg_smem + lay.ring);
+    int32_t* rows = reinterpret_cast<int32_t*>(stg_smem + lay.rows);
     int64_t* slot_base = reinterpret_cast<int64_t*>(stg_smem + lay.slot_base);
     int32_t* slot_ab = reinterpret_cast<int32_t*>(stg_smem + lay.slot_ab);
     int32_t* sp_count = reinterpret_cast<int32_t*>(stg_smem + lay.sp_count);
@@ -683,10 +711,23 @@ __global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(
         cf[i] = (m < 2 * l + 1 && n < N) ? coef[sp * K + (l * l + m) * N + n] : 0.0;
     }
     load_scales(L, scale_s);
-    // the padded last m steps read past the gradient: keep that tail finite
-    for (int i = threadIdx.x; i < STG_RING * (lay.GB - 3 * K); i += blockDim.x) {
-        const int buf = i / (lay.GB - 3 * K), j = i - buf * (lay.GB - 3 * K);
-        ring[buf * lay.GB + 3 * K + j] = 0.0;
+    if (N8) {
+        // padded rows stay zero; rows[r]: first double of source row r
+        // (x, l, m) in the buffer, times 2, plus the row's chunk swap bit
+        for (int i = threadIdx.x; i < STG_RING * lay.GB; i += blockDim.x) ring[i] = 0.0;
+        for (int r = threadIdx.x; r < 3 * RB; r += blockDim.x) {
+            const int x = r / RB;
+            int l, m, step;
+            stg_row_position(r - x * RB, l, m, step);
+            const int dest = x * lay.P + (step + (m >> 2)) * 32 + (m & 3) * 8;
+            rows[r] = 2 * dest + ((m >> 1) & 1);
+        }
+    } else {
+        // the padded last m step reads past the gradient: keep that tail finite
+        for (int i = threadIdx.x; i < STG_RING * (lay.GB - 3 * K); i += blockDim.x) {
+            const int buf = i / (lay.GB - 3 * K), j = i - buf * (lay.GB - 3 * K);
+            ring[buf * lay.GB + 3 * K + j] = 0.0;
+        }
     }
     const int64_t s0 = a.slot_offset[c];
     // one slot per species pair a <= b of the centre's keys: at most
@@ -729,8 +770,8 @@ __global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(
                     double* dst = ring + (k % STG_RING) * lay.GB;
                     if (N8) {
                         for (int q = threadIdx.x; q < 3 * K / 2; q += blockDim.x) {
-                            const int r = q >> 2, ch = q & 3;
-                            cp_async16(dst + r * 8 + ((ch ^ (((r >> 1) & 1) << 1)) << 1), src + 2 * q);
+                            const int e = rows[q >> 2], ch = q & 3;
+                            cp_async16(dst + (e >> 1) + ((ch ^ ((e & 1) << 1)) << 1), src + 2 * q);
                         }
                     } else if (aligned16) {
                         for (int q = threadIdx.x; q < 3 * K / 2; q += blockDim.x) cp_async16(dst + 2 * q, src + 2 * q);
@@ -750,12 +791,12 @@ __global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(
             __syncthreads();
             issue(k + 2);
             const PsEntry entry = meta_entry[k];
+            if (entry.atom == (int32_t)c) continue;  // the centre's own rows: ps_centre_rows_kernel
             const int32_t* cum = meta_cum + k * (S + 1);
-            const bool self = entry.atom == (int32_t)c;
-            const bool regular = !self && entry.d1 - entry.d0 == 1;
-            const int n_items = self ? ns : sp_count[entry.species];
+            const bool regular = entry.d1 - entry.d0 == 1;
+            const int n_items = sp_count[entry.species];
             for (int it = warp; it < n_items; it += STG_WARPS) {
-                const int si = self ? it : sp_slot[entry.species * STG_MAX_SPECIES + it];
+                const int si = sp_slot[entry.species * STG_MAX_SPECIES + it];
                 const int sa = slot_ab[2 * si], sb = slot_ab[2 * si + 1];
                 const int64_t rank = cum[sa] + (sa != sb ? cum[sb] : 0) + cum[S];
                 double* out = a.out + slot_base[si] + rank * 3 * a.n_props;
@@ -764,21 +805,165 @@ __global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(
                                 entry.species, meta_code[k] & 1, out);
                 } else {
                     const PsKeySlot slot{0, 0, sa, sb};
-                    const double* self_a = a.self_grad + ((int64_t)c * S + sa) * 3 * K;
-                    const double* self_b = a.self_grad + ((int64_t)c * S + sb) * 3 * K;
-                    if (self) {
-                        DirectSource none{nullptr, false};
-                        positions_row(a, lane, K, coef, scale_s, slot, true, entry.species, none, self_a, self_b, out);
-                    } else {
-                        ImagesSource images{a.dir_code + entry.d0, entry.d1 - entry.d0, a.pair_grad, 3 * (int64_t)K};
-                        positions_row(a, lane, K, coef, scale_s, slot, false, entry.species, images, self_a, self_b,
-                                      out);
-                    }
+                    ImagesSource images{a.dir_code + entry.d0, entry.d1 - entry.d0, a.pair_grad, 3 * (int64_t)K};
+                    positions_row(a, lane, K, coef, scale_s, slot, false, entry.species, images, nullptr, nullptr, out);
                 }
             }
         }
         cp_async_wait<0>();
         __syncthreads();  // metadata and ring are reused by the next chunk
+    }
+}
+
+// Rows of one centre and one slot (a, b) built from two operands of three
+// components each, D_a and D_b ([3][(l m)][n] in global memory):
+//   tile[x] = sum_m D_a[x][l m][n1] c_b[l m][n2] + c_a[l m][n1] D_b[x][l m][n2]
+// on the FP64 tensor cores, per l all fragment loads issued together (at most
+// CR_MAX_STEPS steps of 4 m, lmax <= 8).  The centre's own positions rows use
+// the self gradients, the strain / cell rows three components of the 3 x 3
+// gradients at a time.
+constexpr int CR_MAX_STEPS = 5;
+
+__device__ __forceinline__ void centre_row(int lane, int lmax, int nmax, int K, int64_t n_props,
+                                           const double* __restrict__ da, const double* __restrict__ db,
+                                           const double* __restrict__ cf, int P, const double* __restrict__ scales,
+                                           int a, int b, double* __restrict__ out) {
+    const int tm = lane & 3, tn = lane >> 2;
+    const double* ca = cf + a * P + lane;
+    const double* cb = cf + b * P + lane;
+    const int N = nmax;
+    const bool vec = N == 8 && ((((uintptr_t)out) & 15) == 0);
+    int step = 0;
+    for (int l = 0; l <= lmax; l++) {
+        const int M = 2 * l + 1, steps = (M + 3) >> 2;
+        double ga[CR_MAX_STEPS][3], gb[CR_MAX_STEPS][3], va[CR_MAX_STEPS], vb[CR_MAX_STEPS];
+#pragma unroll
+        for (int st = 0; st < CR_MAX_STEPS; st++) {
+            if (st < steps) {
+                const int m = 4 * st + tm;
+                const bool ok = m < M && tn < N;
+                const int idx = (l * l + m) * N + tn;
+#pragma unroll
+                for (int x = 0; x < 3; x++) {
+                    ga[st][x] = ok ? da[x * K + idx] : 0.0;
+                    gb[st][x] = ok ? db[x * K + idx] : 0.0;
+                }
+                va[st] = ca[(step + st) * 32];
+                vb[st] = cb[(step + st) * 32];
+            }
+        }
+        double acc[3][2];
+#pragma unroll
+        for (int x = 0; x < 3; x++) acc[x][0] = acc[x][1] = 0.0;
+#pragma unroll
+        for (int st = 0; st < CR_MAX_STEPS; st++) {
+            if (st < steps) {
+#pragma unroll
+                for (int x = 0; x < 3; x++) dmma_8x8x4(acc[x], ga[st][x], vb[st]);
+#pragma unroll
+                for (int x = 0; x < 3; x++) dmma_8x8x4(acc[x], va[st], gb[st][x]);
+            }
+        }
+        step += steps;
+        const double scale = scales[l];
+        const int n2 = 2 * tm;
+        if (vec) {
+            double* o = out + (int64_t)l * 64 + tn * 8 + n2;
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                double2 w;
+                w.x = acc[x][0] * scale;
+                w.y = acc[x][1] * scale;
+                __stcs(reinterpret_cast<double2*>(o + x * n_props), w);
+            }
+        } else if (tn < N) {
+            double* o = out + (int64_t)l * N * N + tn * N + n2;
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                if (n2 < N) __stcs(o + x * n_props, acc[x][0] * scale);
+                if (n2 + 1 < N) __stcs(o + x * n_props + 1, acc[x][1] * scale);
+            }
+        }
+    }
+}
+
+// The centre's rows, on the side stream beside the staged positions kernel:
+// its own positions-gradient rows (CR_SELF; featomic's
+// sum_m c_b dself_a + c_a dself_b) and its strain / cell rows (CR_STRAIN,
+// CR_CELL; three passes of three components).  One CTA per centre with the
+// coefficients in fragment order in shared memory; items (slot, kind, pass)
+// are spread over the warps.
+constexpr int CR_SELF = 1, CR_STRAIN = 2, CR_CELL = 4;
+
+__global__ void __launch_bounds__(128) ps_centre_rows_kernel(PsArgs a, int kinds) {
+    extern __shared__ __align__(16) double cr_smem[];
+    __shared__ int64_t self_entry;
+    const int64_t c = blockIdx.x;
+    const int S = a.n_species, L = a.lmax, N = a.nmax;
+    const int K = (L + 1) * (L + 1) * N;
+    const int P = 32 * stg_steps(L);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    double* cf = cr_smem;
+    double* scale_s = cr_smem + S * P;
+    const double* coef = a.coef + c * S * K;
+    for (int i = threadIdx.x; i < S * P; i += blockDim.x) {
+        const int sp = i / P, rem = i - sp * P;
+        int g = rem >> 5;
+        const int t = rem & 31;
+        int l = 0;
+        while (g >= ((2 * l + 1 + 3) >> 2)) {
+            g -= (2 * l + 1 + 3) >> 2;
+            l++;
+        }
+        const int m = 4 * g + (t & 3), n = t >> 2;
+        cf[i] = (m < 2 * l + 1 && n < N) ? coef[sp * K + (l * l + m) * N + n] : 0.0;
+    }
+    load_scales(L, scale_s);
+    // the centre's entry among its neighbour entries (sorted by atom index)
+    const int64_t e0 = a.entry_offset[c], ne = a.entry_offset[c + 1] - e0;
+    if (warp == 0) {
+        int64_t found = -1;
+        if (kinds & CR_SELF) {
+            for (int64_t base = 0; base < ne && found < 0; base += 32) {
+                const bool hit = base + lane < ne && a.entries[e0 + base + lane].atom == (int32_t)c;
+                const unsigned mask = __ballot_sync(0xffffffffu, hit);
+                if (mask) found = e0 + base + __ffs(mask) - 1;
+            }
+        }
+        if (lane == 0) self_entry = found;
+    }
+    __syncthreads();
+    const int64_t s0 = a.slot_offset[c];
+    const int ns = (int)(a.slot_offset[c + 1] - s0);
+    // per slot: the self row (if requested and the centre's entry exists),
+    // then 3 strain passes, then 3 cell passes
+    const int n_self = (kinds & CR_SELF) && self_entry >= 0 ? 1 : 0;
+    const int n_strain = (kinds & CR_STRAIN) ? 3 : 0, n_cell = (kinds & CR_CELL) ? 3 : 0;
+    const int per_slot = n_self + n_strain + n_cell;
+    for (int it = warp; it < ns * per_slot; it += nwarps) {
+        const int si = it / per_slot;
+        int kind = it - si * per_slot;
+        const PsKeySlot slot = a.slots[s0 + si];
+        const double* scales = scale_s + (slot.a != slot.b ? L + 1 : 0);
+        const double *da, *db;
+        double* out;
+        if (kind < n_self) {
+            const int32_t* cum = a.entry_cum + self_entry * (S + 1);
+            const int64_t rank = cum[slot.a] + (slot.a != slot.b ? cum[slot.b] : 0) + cum[S];
+            out = a.out + a.off_positions[slot.block] + (a.slot_row[s0 + si] + rank) * 3 * a.n_props;
+            da = a.self_grad + ((int64_t)c * S + slot.a) * 3 * K;
+            db = a.self_grad + ((int64_t)c * S + slot.b) * 3 * K;
+        } else {
+            kind -= n_self;
+            const bool strain = kind < n_strain;
+            const int xr = strain ? kind : kind - n_strain;
+            const double* src = strain ? a.strain : a.cellg;
+            const int64_t* offs = strain ? a.off_strain : a.off_cell;
+            out = a.out + offs[slot.block] + ((int64_t)slot.sample * 9 + 3 * xr) * a.n_props;
+            da = src + (((int64_t)c * S + slot.a) * 9 + 3 * xr) * K;
+            db = src + (((int64_t)c * S + slot.b) * 9 + 3 * xr) * K;
+        }
+        centre_row(lane, L, N, K, a.n_props, da, db, cf, P, scales, slot.a, slot.b, out);
     }
 }
 
@@ -823,8 +1008,12 @@ cudaStream_t side_stream() {
     std::lock_guard<std::mutex> lock(mutex);
     auto it = streams.find(device);
     if (it != streams.end()) return it->second;
+    // the highest priority: its short kernels take the SMs the positions
+    // kernel frees first, instead of queueing behind that kernel's waves
+    int least = 0, greatest = 0;
+    CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     cudaStream_t s = nullptr;
-    CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CUDA_CHECK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest));
     streams[device] = s;
     return s;
 }
@@ -842,6 +1031,7 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
         CUDA_CHECK(cudaFuncSetAttribute(ps_strain_cell_kernel<MAXN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         CUDA_CHECK(cudaFuncSetAttribute(ps_positions_staged_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         CUDA_CHECK(cudaFuncSetAttribute(ps_positions_staged_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CUDA_CHECK(cudaFuncSetAttribute(ps_centre_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         configured = true;
     }
     if (coef_bytes > 200 * 1024) throw invalid_parameter("too many species / radial / angular functions for the power spectrum kernels");
@@ -862,13 +1052,26 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
         CUDA_CHECK(cudaGetLastError());
     }
     if (events.after_values) CUDA_CHECK(cudaEventRecord(events.after_values, side));
-    if (strain) {
-        ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args, 0);
+    // nmax <= 8, lmax <= 8: the staged positions kernel, and the centres'
+    // own positions rows with the strain / cell rows in ps_centre_rows_kernel
+    const StgLayout stg = stg_layout(args.n_species, args.lmax, args.nmax);
+    const bool dmma_rows = args.nmax <= 8 && (2 * args.lmax + 1 + 3) / 4 <= CR_MAX_STEPS;
+    const bool staged = positions && dmma_rows && args.n_species <= STG_MAX_SPECIES && stg.bytes <= 200 * 1024;
+    const size_t cr_bytes = sizeof(double) * ((size_t)args.n_species * 32 * stg_steps(args.lmax) + 2 * (args.lmax + 1));
+    const int kinds = (staged ? CR_SELF : 0) | (strain ? CR_STRAIN : 0) | (cell ? CR_CELL : 0);
+    if (dmma_rows && cr_bytes <= 200 * 1024 && kinds != 0 && (staged || !positions)) {
+        ps_centre_rows_kernel<<<(unsigned)args.n_centres, 128, cr_bytes, side>>>(args, kinds);
         CUDA_CHECK(cudaGetLastError());
-    }
-    if (cell) {
-        ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args, 1);
-        CUDA_CHECK(cudaGetLastError());
+    } else {
+        if (staged) throw std::logic_error("the centres' own rows need ps_centre_rows_kernel");
+        if (strain) {
+            ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args, 0);
+            CUDA_CHECK(cudaGetLastError());
+        }
+        if (cell) {
+            ps_strain_cell_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args, 1);
+            CUDA_CHECK(cudaGetLastError());
+        }
     }
     if (events.after_strain_cell) CUDA_CHECK(cudaEventRecord(events.after_strain_cell, side));
     CUDA_CHECK(cudaEventRecord(join, side));
@@ -876,8 +1079,7 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
     // caller's stream: positions
     if (events.before_positions) CUDA_CHECK(cudaEventRecord(events.before_positions, stream));
     if (positions) {
-        const StgLayout stg = stg_layout(args.n_species, args.lmax, args.nmax);
-        if (args.nmax <= 8 && args.n_species <= STG_MAX_SPECIES && stg.bytes <= 200 * 1024) {
+        if (staged) {
             const unsigned grid = (unsigned)(args.n_centres * STG_SPLIT);
             if (args.nmax == 8) ps_positions_staged_kernel<true><<<grid, STG_WARPS * 32, stg.bytes, stream>>>(args);
             else ps_positions_staged_kernel<false><<<grid, STG_WARPS * 32, stg.bytes, stream>>>(args);

@@ -206,6 +206,12 @@ def test_power_spectrum_many_radial_functions(oracle):
     check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(4.0, 9, 2), systems, ("positions", "strain"))
 
 
+def test_strain_and_cell_without_positions(oracle):
+    systems = [workloads.random_box(90, seed=22)]
+    check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(4.5, 7, 5), systems, ("strain", "cell"))
+    check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(4.0, 5, 3), systems, ("cell",))
+
+
 def test_user_neighbor_list(oracle):
     # use_native_system = False: pairs come from the caller (here, the oracle's list)
     systems = [workloads.random_box(250, seed=12)]
