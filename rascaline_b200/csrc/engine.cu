@@ -252,6 +252,22 @@ cudaStream_t copy_stream() {
     return s;
 }
 
+// a stream per device for device-to-host copies that nothing on the device
+// waits for
+cudaStream_t readback_stream() {
+    static std::mutex mutex;
+    static std::map<int, cudaStream_t> streams;
+    int device = 0;
+    CUDA_CHECK(cudaGetDevice(&device));
+    std::lock_guard<std::mutex> lock(mutex);
+    auto it = streams.find(device);
+    if (it != streams.end()) return it->second;
+    cudaStream_t s = nullptr;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    streams[device] = s;
+    return s;
+}
+
 // makes `stream` wait for the uploads issued on the copy stream so far
 void join_uploads(cudaStream_t stream) {
     cudaEvent_t done = nullptr;
@@ -390,12 +406,12 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
     auto t_start = std::chrono::steady_clock::now();
     const bool ps = kind == OUTPUT_POWER_SPECTRUM, by_pair = kind == OUTPUT_BY_PAIR;
     upload_tables();
-    cudaEvent_t ev[15];
+    cudaEvent_t ev[16];
     for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
     struct EventGuard {
         cudaEvent_t* e;
         ~EventGuard() {
-            for (int k = 0; k < 15; k++) cudaEventDestroy(e[k]);
+            for (int k = 0; k < 16; k++) cudaEventDestroy(e[k]);
         }
     } guard{ev};
     CUDA_CHECK(cudaEventRecord(ev[0], stream));
@@ -543,7 +559,6 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
             cudaStream_t up = copy_stream();
             CUDA_CHECK(cudaEventRecord(ev[14], stream));
             CUDA_CHECK(cudaStreamWaitEvent(up, ev[14], 0));
-            nb = launch_neighborhoods(pairs, d_species, d_dir, d_seg, S, n_atoms, arena_, up);
             // pinned staging: [entry offsets][entries][species counts][species mask]
             nb_capacity = 2 * pairs.count + n_atoms;
             const size_t b_offset = sizeof(int64_t) * (n_atoms + 1), b_entries = sizeof(PsEntry) * nb_capacity;
@@ -553,14 +568,21 @@ std::unique_ptr<TensorMap> Engine::compute(int kind, std::vector<HostSystem>& sy
             nb_host_entries = (PsEntry*)(host + b_offset);
             nb_host_count = (int32_t*)(host + b_offset + b_entries);
             nb_host_mask = (uint8_t*)(host + b_offset + b_entries + b_count);
-            CUDA_CHECK(cudaMemcpyAsync(nb_host_count, nb.species_count, b_count, cudaMemcpyDeviceToHost, up));
-            CUDA_CHECK(cudaMemcpyAsync(nb_host_mask, nb.species_mask, n_atoms * S, cudaMemcpyDeviceToHost, up));
-            CUDA_CHECK(cudaEventRecord(ev[12], up));
+            // the species counts come back as soon as they are counted (ev[12]),
+            // before the scan and the fill of the entries
+            nb = launch_neighborhoods(pairs, d_species, d_dir, d_seg, S, n_atoms, arena_, up, nb_host_count,
+                                      nb_host_mask, ev[12]);
+            // the entries go back to the host (for the labels) on a stream of
+            // their own, so that the contraction kernels, which join the copy
+            // stream, do not wait for this copy
+            cudaStream_t back = readback_stream();
+            CUDA_CHECK(cudaEventRecord(ev[15], up));
+            CUDA_CHECK(cudaStreamWaitEvent(back, ev[15], 0));
             CUDA_CHECK(cudaMemcpyAsync(nb_host_offset, nb.entry_offset, sizeof(int64_t) * (n_atoms + 1),
-                                       cudaMemcpyDeviceToHost, up));
+                                       cudaMemcpyDeviceToHost, back));
             CUDA_CHECK(cudaMemcpyAsync(nb_host_entries, nb.entries, sizeof(PsEntry) * nb_capacity,
-                                       cudaMemcpyDeviceToHost, up));
-            CUDA_CHECK(cudaEventRecord(ev[13], up));
+                                       cudaMemcpyDeviceToHost, back));
+            CUDA_CHECK(cudaEventRecord(ev[13], back));
         }
         se.centre_species = d_species;
         se.seg_offset = d_seg;

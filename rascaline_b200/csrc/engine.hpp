@@ -252,9 +252,13 @@ struct DeviceNeighborhoods {
     int32_t* species_count = nullptr;  // [n_atoms * S]
     uint8_t* species_mask = nullptr;   // [n_atoms * S]
 };
+// When `host_count` / `host_mask` are given, the species counts and masks are
+// copied to them right after the counting kernel and `counted` is recorded
+// there, before the scan and the fill.
 DeviceNeighborhoods launch_neighborhoods(const DevicePairs& pairs, const int32_t* atom_species, const int32_t* dir_code,
                                          const int64_t* seg_offset, int n_species, int64_t n_atoms, DeviceArena& arena,
-                                         cudaStream_t stream);
+                                         cudaStream_t stream, int32_t* host_count = nullptr,
+                                         uint8_t* host_mask = nullptr, cudaEvent_t counted = nullptr);
 
 // Spherical expansion output scatter (spherical_expansion calculator)
 struct SeOutArgs {

@@ -82,7 +82,7 @@ __global__ void pair_features_kernel(DevicePairs pairs, DeviceRadial radial, Dev
 
 // Per-direction scalars staged in shared memory for a chunk of directions
 struct DirScalars {
-    double f, fg, r, u[3], v[3], sh[3];
+    double f, fg, r, rinv, u[3], v[3], sh[3];
     int64_t feature;  // offset of the pair's feature record
     int inv, self_image;
 };
@@ -137,6 +137,7 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
                     if (GRAD) {
                         D.fg = F[1];
                         D.r = F[2];
+                        D.rinv = 1.0 / D.r;
                         for (int x = 0; x < 3; x++) {
                             D.u[x] = F[3 + x];
                             D.v[x] = F[6 + x];
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
 #pragma unroll
                     for (int x = 0; x < 3; x++) {
                         const double dY = __ldg(F + L.off_dy + x * L.L2 + lm);
-                        g[x] = D.fg * D.u[x] * Rv * Yv + D.f * dR * D.u[x] * Yv + D.f * Rv * dY / D.r;
+                        g[x] = D.fg * D.u[x] * Rv * Yv + D.f * dR * D.u[x] * Yv + D.f * Rv * dY * D.rinv;
                     }
                     if (POS && !D.inv) {
                         double* pg = a.pair_grad + (D.feature / L.stride) * 3 * K;
@@ -233,7 +234,11 @@ __global__ void __launch_bounds__(256) se_accumulate_kernel(SeArgs a) {
 constexpr int FUSED_CHUNK = 32;
 
 struct FusedDir {
-    double f, fg, r, u[3], v[3], sh[3];
+    // rinv = 1 / r, computed once per direction: the angular gradient term
+    // f R dY / r is evaluated as f R dY * rinv (one extra rounding against
+    // featomic's division, far inside the 1e-10 parity bound; an FP64 divide
+    // per coefficient was most of this kernel's instruction stream)
+    double f, fg, r, rinv, u[3], v[3], sh[3];
     int64_t pair;
     int inv, self_image;
 };
@@ -322,6 +327,7 @@ __global__ void __launch_bounds__(256, 2) se_fused_kernel(SeArgs a, DevicePairs 
             D.f = sc * fc;
             D.fg = dfc * sc + fc * dsc;
             D.r = r;
+            D.rinv = 1.0 / r;
             D.u[0] = u0;
             D.u[1] = u1;
             D.u[2] = u2;
@@ -363,7 +369,7 @@ __global__ void __launch_bounds__(256, 2) se_fused_kernel(SeArgs a, DevicePairs 
                 const double dR = dRs[q * LR + ri + j];
                 double g[3];
 #pragma unroll
-                for (int x = 0; x < 3; x++) g[x] = D.fg * D.u[x] * Rv * Yv + D.f * dR * D.u[x] * Yv + D.f * Rv * dY[x] / D.r;
+                for (int x = 0; x < 3; x++) g[x] = D.fg * D.u[x] * Rv * Yv + D.f * dR * D.u[x] * Yv + D.f * Rv * dY[x] * D.rinv;
                 const int k = lm * N + n0 + j;
                 if (POS && !D.inv) {
                     double* pg = a.pair_grad + D.pair * 3 * K;

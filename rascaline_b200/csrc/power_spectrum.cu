@@ -1177,11 +1177,54 @@ __global__ void neighborhoods_kernel(const int32_t* __restrict__ first, const in
     }
 }
 
+// The counting half of neighborhoods_kernel, a warp per centre: within a
+// (centre, species) segment the other atoms come in increasing order with the
+// periodic images of one atom adjacent, so the unique neighbours of that
+// species are the directions whose other atom differs from the previous
+// direction's and is not the centre.  Writes the same counts, species counts
+// and species masks as neighborhoods_kernel<false>.
+__global__ void neighborhoods_count_kernel(const int32_t* __restrict__ first, const int32_t* __restrict__ second,
+                                           const int32_t* __restrict__ atom_species, const int32_t* __restrict__ dir,
+                                           const int64_t* __restrict__ seg, int S, int64_t n_atoms,
+                                           int64_t* __restrict__ counts, int32_t* __restrict__ species_count,
+                                           uint8_t* __restrict__ species_mask) {
+    const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c == n_atoms && lane == 0) counts[n_atoms] = 0;  // the scan's last element
+    if (c >= n_atoms) return;
+    auto other = [&](int64_t d) -> int32_t {
+        const int32_t code = dir[d];
+        return (code & 1) ? first[code >> 1] : second[code >> 1];
+    };
+    const int sc = atom_species[c];
+    int64_t total = 1;  // the centre itself
+    for (int t = 0; t < S; t++) {
+        const int64_t b = seg[c * S + t], e = seg[c * S + t + 1];
+        int32_t n = 0;
+        for (int64_t base = b; base < e; base += 32) {
+            const int64_t d = base + lane;
+            bool unique = false;
+            if (d < e) {
+                const int32_t o = other(d);
+                unique = o != (int32_t)c && (d == b || other(d - 1) != o);
+            }
+            n += __popc(__ballot_sync(0xffffffffu, unique));
+        }
+        if (lane == 0) {
+            species_count[c * S + t] = n;
+            species_mask[c * S + t] = (e > b || t == sc) ? 1 : 0;
+        }
+        total += n;
+    }
+    if (lane == 0) counts[c] = total;
+}
+
 }  // namespace
 
 DeviceNeighborhoods launch_neighborhoods(const DevicePairs& pairs, const int32_t* atom_species, const int32_t* dir_code,
                                          const int64_t* seg_offset, int n_species, int64_t n_atoms, DeviceArena& arena,
-                                         cudaStream_t stream) {
+                                         cudaStream_t stream, int32_t* host_count, uint8_t* host_mask,
+                                         cudaEvent_t counted) {
     if (n_species > NB_MAX_SPECIES) throw invalid_parameter("more than 64 atomic types are not supported");
     if (2 * pairs.count + n_atoms >= (int64_t)INT32_MAX) throw invalid_parameter("too many pairs");
     DeviceNeighborhoods nb;
@@ -1195,10 +1238,17 @@ DeviceNeighborhoods launch_neighborhoods(const DevicePairs& pairs, const int32_t
     nb.species_mask = arena.alloc<uint8_t>("nb.species_mask", n_atoms * S);
     const int threads = 128;
     const unsigned blocks = (unsigned)((n_atoms + 1 + threads - 1) / threads);
-    neighborhoods_kernel<false><<<blocks, threads, 0, stream>>>(pairs.first, pairs.second, atom_species, dir_code,
-                                                               seg_offset, S, n_atoms, counts, nullptr, nullptr,
-                                                               nullptr, nb.species_count, nb.species_mask);
+    const unsigned count_blocks = (unsigned)(((n_atoms + 1) * 32 + 255) / 256);
+    neighborhoods_count_kernel<<<count_blocks, 256, 0, stream>>>(pairs.first, pairs.second, atom_species, dir_code,
+                                                                seg_offset, S, n_atoms, counts, nb.species_count,
+                                                                nb.species_mask);
     CUDA_CHECK(cudaGetLastError());
+    if (host_count && host_mask) {
+        CUDA_CHECK(cudaMemcpyAsync(host_count, nb.species_count, sizeof(int32_t) * n_atoms * S, cudaMemcpyDeviceToHost,
+                                   stream));
+        CUDA_CHECK(cudaMemcpyAsync(host_mask, nb.species_mask, n_atoms * S, cudaMemcpyDeviceToHost, stream));
+        if (counted) CUDA_CHECK(cudaEventRecord(counted, stream));
+    }
     size_t temp = 0;
     CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, temp, counts, nb.entry_offset, (int)(n_atoms + 1), stream));
     void* scan_temp = arena.alloc_bytes("nb.scan_temp", temp);  // its own: this may run beside other scans
