@@ -951,7 +951,10 @@ def main():
     K = 49 * 8
     S = 4
     out_bytes = 8 * (samples * n_props + grad_rows * 3 * n_props + samples * 9 * n_props)
-    pos_kernel_bytes = 8 * (grad_rows * 3 * n_props + N_ATOMS * S * K + n_pairs * 3 * K + N_ATOMS * S * 3 * K)
+    # ps_positions_staged_kernel: every gradient row but the centres' own
+    # (one per sample, written by ps_centre_rows_kernel), the coefficients and
+    # the pair gradients read once
+    pos_kernel_bytes = 8 * ((grad_rows - samples) * 3 * n_props + N_ATOMS * S * K + n_pairs * 3 * K)
 
     sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
                            if os.environ.get("CUDA_VISIBLE_DEVICES", "").isdigit() else local)
@@ -1015,7 +1018,7 @@ def main():
             "d2h_bytes_per_step": out_bytes + n_pairs * 8,
         },
         "roofline": {
-            "kernel": "ps_positions_kernel",
+            "kernel": "ps_positions_staged_kernel",
             "bound": "hbm",
             "achieved": achieved,
             "peak": peak,
@@ -1023,13 +1026,14 @@ def main():
             "frac": achieved / peak,
             "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": pos_kernel_bytes,
-            "traffic": profile_traffic("ps_positions_random_box_1000"),
+            "traffic": profile_traffic("ps_positions_staged_random_box_1000"),
         },
         "clocks": clocks,
         # per step, this library's own kernels: neighbour list (assign, fill,
         # count, write), direction keys and segments, neighbourhood tables
-        # (count, fill), fused spherical expansion, power spectrum values /
-        # positions / strain; beside them 11 CUB sort / scan kernels
+        # (count, fill), fused spherical expansion, power spectrum values,
+        # positions rows (staged) and centre rows (own positions rows and
+        # strain); beside them 11 CUB sort / scan kernels
         "gpu_launches": 12 * args.steps,
     }
     if not args.no_chosen_forms:
