@@ -277,10 +277,12 @@ OutputPlan plan_power_spectrum(const Neighborhoods& nh, const Hypers& h, const G
 
 void fill_power_spectrum_labels(const Neighborhoods& nh, const GradientOptions& g, OutputPlan& plan) {
     const int64_t N = nh.n_atoms;
+    const int S = nh.n_species;
     const int32_t nb = (int32_t)plan.blocks.size();
     // labels, written in place: every slot knows its sample row and its first
     // gradient row, so centres fill their rows independently
     std::vector<int32_t*> sample_w(nb), grad_w(nb);
+#pragma omp parallel for schedule(static)
     for (int32_t k = 0; k < nb; k++) {
         auto& bp = plan.blocks[k];
         bp.samples.names = {"system", "atom"};
@@ -292,23 +294,54 @@ void fill_power_spectrum_labels(const Neighborhoods& nh, const GradientOptions& 
             grad_w[k] = bp.gradient_samples.values.data();
         }
     }
-#pragma omp parallel for schedule(static)
-    for (int64_t c = 0; c < N; c++) {
-        const int32_t sys = nh.atom_system[c];
-        for (int64_t s = plan.slot_offset[c]; s < plan.slot_offset[c + 1]; s++) {
-            const PsKeySlot& slot = plan.slots[s];
-            int32_t* w = sample_w[slot.block] + 2 * (size_t)slot.sample;
-            w[0] = sys;
-            w[1] = nh.atom_local[c];
+#pragma omp parallel
+    {
+        // per centre: the write position of every slot's next gradient row,
+        // and the slots of each neighbour species
+        std::vector<int32_t*> w;
+        std::vector<int32_t> by_species, n_by_species(S);
+#pragma omp for schedule(static)
+        for (int64_t c = 0; c < N; c++) {
+            const int32_t sys = nh.atom_system[c];
+            const int64_t s0 = plan.slot_offset[c], ns = plan.slot_offset[c + 1] - s0;
+            for (int64_t i = 0; i < ns; i++) {
+                const PsKeySlot& slot = plan.slots[s0 + i];
+                int32_t* sw = sample_w[slot.block] + 2 * (size_t)slot.sample;
+                sw[0] = sys;
+                sw[1] = nh.atom_local[c];
+            }
             if (!g.positions) continue;
-            int32_t* gw = grad_w[slot.block] + 3 * (size_t)plan.slot_row[s];
+            w.resize(ns);
+            by_species.resize((size_t)S * ns);
+            std::fill(n_by_species.begin(), n_by_species.end(), 0);
+            for (int64_t i = 0; i < ns; i++) {
+                const PsKeySlot& slot = plan.slots[s0 + i];
+                w[i] = grad_w[slot.block] + 3 * (size_t)plan.slot_row[s0 + i];
+                by_species[(size_t)slot.a * ns + n_by_species[slot.a]++] = (int32_t)i;
+                if (slot.b != slot.a) by_species[(size_t)slot.b * ns + n_by_species[slot.b]++] = (int32_t)i;
+            }
+            // entries in atom order: each row goes to the end of its slots' rows
             for (int64_t e = nh.entry_offset[c]; e < nh.entry_offset[c + 1]; e++) {
                 const PsEntry& en = nh.entries[e];
-                if (en.atom != (int32_t)c && en.species != slot.a && en.species != slot.b) continue;
-                gw[0] = slot.sample;
-                gw[1] = sys;
-                gw[2] = nh.atom_local[en.atom];
-                gw += 3;
+                const int32_t local = nh.atom_local[en.atom];
+                if (en.atom == (int32_t)c) {
+                    for (int64_t i = 0; i < ns; i++) {
+                        int32_t* gw = w[i];
+                        gw[0] = plan.slots[s0 + i].sample;
+                        gw[1] = sys;
+                        gw[2] = local;
+                        w[i] = gw + 3;
+                    }
+                    continue;
+                }
+                for (int j = 0; j < n_by_species[en.species]; j++) {
+                    const int32_t i = by_species[(size_t)en.species * ns + j];
+                    int32_t* gw = w[i];
+                    gw[0] = plan.slots[s0 + i].sample;
+                    gw[1] = sys;
+                    gw[2] = local;
+                    w[i] = gw + 3;
+                }
             }
         }
     }
