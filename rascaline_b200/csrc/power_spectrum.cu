@@ -295,7 +295,7 @@ __device__ __forceinline__ void positions_row(const PsArgs& a, int lane, int K, 
 // 8 x 8 x 4): lane t holds A[t / 4][t % 4] and B[t % 4][t / 4] and the two
 // outputs D[t / 4][2 (t % 4) + {0, 1}]
 __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d[0]), "+d"(d[1])
                  : "d"(a), "d"(b));
 }
@@ -522,6 +522,7 @@ constexpr int STG_CHUNK = 64;
 constexpr int STG_SPLIT = 2;
 constexpr int STG_MAX_SPECIES = 10;
 constexpr int STG_MAX_SLOTS = STG_MAX_SPECIES * (STG_MAX_SPECIES + 1) / 2;
+constexpr int STG_MAX_STEPS = 5;
 constexpr int STG_G_PAD = 32;  // doubles after an unpadded gradient buffer, read by the padded last m step
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
@@ -611,7 +612,11 @@ __device__ __forceinline__ void stg_row(int lane, int lmax, int nmax, int64_t n_
         double acc[3][2];
 #pragma unroll
         for (int x = 0; x < 3; x++) acc[x][0] = acc[x][1] = 0.0;
-        for (int st = 0; st < steps; st++) {
+        // at most STG_MAX_STEPS steps per l (lmax <= 9: the launch condition),
+        // unrolled so that the fragment loads of later steps are issued early
+#pragma unroll
+        for (int st = 0; st < STG_MAX_STEPS; st++) {
+            if (st >= steps) break;
             double g[3];
             if (N8) {
                 const double* gp = g0 + (step + st) * 32;
