@@ -828,6 +828,7 @@ __global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(
 // the self gradients, the strain / cell rows three components of the 3 x 3
 // gradients at a time.
 constexpr int CR_MAX_STEPS = 5;
+constexpr int CR_SPLIT = 2;
 
 __device__ __forceinline__ void centre_row(int lane, int lmax, int nmax, int K, int64_t n_props,
                                            const double* __restrict__ da, const double* __restrict__ db,
@@ -895,15 +896,17 @@ __device__ __forceinline__ void centre_row(int lane, int lmax, int nmax, int K, 
 // The centre's rows, on the side stream beside the staged positions kernel:
 // its own positions-gradient rows (CR_SELF; featomic's
 // sum_m c_b dself_a + c_a dself_b) and its strain / cell rows (CR_STRAIN,
-// CR_CELL; three passes of three components).  One CTA per centre with the
+// CR_CELL; three passes of three components).  CR_SPLIT CTAs per centre with the
 // coefficients in fragment order in shared memory; items (slot, kind, pass)
-// are spread over the warps.
+// are spread over their warps.
 constexpr int CR_SELF = 1, CR_STRAIN = 2, CR_CELL = 4;
 
 __global__ void __launch_bounds__(128) ps_centre_rows_kernel(PsArgs a, int kinds) {
     extern __shared__ __align__(16) double cr_smem[];
     __shared__ int64_t self_entry;
-    const int64_t c = blockIdx.x;
+    // CR_SPLIT CTAs per centre share its items
+    const int64_t c = blockIdx.x / CR_SPLIT;
+    const int part = (int)(blockIdx.x - c * CR_SPLIT);
     const int S = a.n_species, L = a.lmax, N = a.nmax;
     const int K = (L + 1) * (L + 1) * N;
     const int P = 32 * stg_steps(L);
@@ -945,7 +948,7 @@ __global__ void __launch_bounds__(128) ps_centre_rows_kernel(PsArgs a, int kinds
     const int n_self = (kinds & CR_SELF) && self_entry >= 0 ? 1 : 0;
     const int n_strain = (kinds & CR_STRAIN) ? 3 : 0, n_cell = (kinds & CR_CELL) ? 3 : 0;
     const int per_slot = n_self + n_strain + n_cell;
-    for (int it = warp; it < ns * per_slot; it += nwarps) {
+    for (int it = part * nwarps + warp; it < ns * per_slot; it += CR_SPLIT * nwarps) {
         const int si = it / per_slot;
         int kind = it - si * per_slot;
         const PsKeySlot slot = a.slots[s0 + si];
@@ -1063,7 +1066,7 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
     const size_t cr_bytes = sizeof(double) * ((size_t)args.n_species * 32 * stg_steps(args.lmax) + 2 * (args.lmax + 1));
     const int kinds = (staged ? CR_SELF : 0) | (strain ? CR_STRAIN : 0) | (cell ? CR_CELL : 0);
     if (dmma_rows && cr_bytes <= 200 * 1024 && kinds != 0 && (staged || !positions)) {
-        ps_centre_rows_kernel<<<(unsigned)args.n_centres, 128, cr_bytes, side>>>(args, kinds);
+        ps_centre_rows_kernel<<<(unsigned)(CR_SPLIT * args.n_centres), 128, cr_bytes, side>>>(args, kinds);
         CUDA_CHECK(cudaGetLastError());
     } else {
         if (staged) throw std::logic_error("the centres' own rows need ps_centre_rows_kernel");
