@@ -177,8 +177,10 @@ void BatchPlan::run_dense(const double* positions, const float* weights, const f
         if (!d_values_scratch_) CUDA_CHECK(cudaMalloc(&d_values_scratch_, sizeof(float) * (size_t)(n_atoms_ * kp)));
         vals = d_values_scratch_;
     }
-    auto st = engine_.forward_dense(32, systems_, positions, species_, vals, n_atoms_ * kp, stream);
-    if ((weights || grad_values) && (grad_positions || grad_strain)) {
+    const bool backward = (weights || grad_values) && (grad_positions || grad_strain);
+    auto st = engine_.forward_dense(32, systems_, positions, species_, vals, n_atoms_ * kp, stream,
+                                    /*expansion=*/false, /*backward_follows=*/backward);
+    if (backward) {
         float* gp = grad_positions;
         if (!gp) {
             if (!d_grad_scratch_) CUDA_CHECK(cudaMalloc(&d_grad_scratch_, sizeof(float) * 3 * (size_t)n_atoms_));

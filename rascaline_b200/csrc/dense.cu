@@ -834,7 +834,8 @@ void launch_dense_forward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t s
         if (a.marks) CUDA_CHECK(cudaEventRecord(a.marks[k], stream));
     };
     mark(0);
-    launch_features<T, false>(a, n_pairs, stream);
+    if (a.gradient_features) launch_features<T, true>(a, n_pairs, stream);
+    else launch_features<T, false>(a, n_pairs, stream);
     mark(1);
     if (a.n_atoms == 0) {
         mark(2);
@@ -915,7 +916,7 @@ void launch_dense_backward(const DenseArgs<T>& a, int64_t n_pairs, cudaStream_t 
         else dense_pair_adjoint_fused<T, 16><<<blocks, threads, 0, stream>>>(a, n_pairs);
         CUDA_CHECK(cudaGetLastError());
     } else if (n_pairs > 0) {
-        launch_features<T, true>(a, n_pairs, stream);
+        if (!a.gradient_features) launch_features<T, true>(a, n_pairs, stream);
         const int warps = 8;
         dense_pair_adjoint<T><<<(unsigned)((n_pairs + warps - 1) / warps), 32 * warps, 0, stream>>>(a, n_pairs);
         CUDA_CHECK(cudaGetLastError());

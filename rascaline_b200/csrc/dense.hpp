@@ -21,6 +21,9 @@ class RadialSurrogate;
 template <typename T>
 struct DenseArgs {
     int lmax, nmax, n_species, n_keys, K;
+    // forward: compute the pair features with their derivatives (layout with
+    // gradients); backward: `features` already holds them
+    bool gradient_features = false;
     int64_t n_atoms, n_props, n_systems;
     FeatureLayout layout;
     DevicePairs pairs;
@@ -78,6 +81,10 @@ struct DenseState {
     int32_t* dir_code = nullptr;
     int64_t* d_atom_offset = nullptr;
     void* coef = nullptr;
+    // pair features with their derivatives, computed by the forward pass when
+    // the caller announced a backward pass that recomputes them otherwise
+    // (FP32 with the learned radial surrogate); the backward reads them
+    void* features_grad = nullptr;
 
     DenseState() = default;
     DenseState(const DenseState&) = delete;

@@ -943,7 +943,7 @@ void Engine::dense_args(const DenseState& st, bool grad, DenseArgs<T>& a) {
 std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<HostSystem>& systems,
                                                   const double* d_positions, const std::vector<int32_t>& species,
                                                   void* values, int64_t values_count, cudaStream_t stream,
-                                                  bool expansion) {
+                                                  bool expansion, bool backward_follows) {
     if (precision != 32 && precision != 64) throw invalid_parameter("precision must be 32 or 64");
     upload_tables();
     const std::shared_ptr<RadialSurrogate> hold = surrogate_.lock();
@@ -1036,8 +1036,14 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
     st->coef = st->alloc(T_size * (size_t)n_atoms * S * st->K);
     int32_t* status = arena_.alloc<int32_t>("dense.status", 1);
     CUDA_CHECK(cudaMemsetAsync(status, 0, sizeof(int32_t), stream));
-    const FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), false);
-    void* features = arena_.alloc_bytes("dense.features", T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride);
+    // with the learned surrogate, the FP32 backward recomputes the pair
+    // features with their derivatives; when the caller announces a backward
+    // pass, the forward computes them once and leaves them in the state
+    const bool keep = backward_follows && precision == 32 && active_surrogate_ != nullptr && !expansion;
+    const FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), keep);
+    const size_t feature_bytes = T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride;
+    void* features = keep ? st->alloc(feature_bytes) : arena_.alloc_bytes("dense.features", feature_bytes);
+    if (keep) st->features_grad = features;
     cudaEvent_t* marks = dense_marks();
     if (precision == 64) {
         DenseArgs<double> a;
@@ -1049,7 +1055,8 @@ std::unique_ptr<DenseState> Engine::forward_dense(int precision, std::vector<Hos
         launch_dense_forward<double>(a, P, stream);
     } else {
         DenseArgs<float> a;
-        dense_args(*st, false, a);
+        dense_args(*st, keep, a);
+        a.gradient_features = keep;
         a.marks = marks;
         a.features = (float*)features;
         a.values = expansion ? nullptr : (float*)values;
@@ -1124,7 +1131,11 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
     const size_t T_size = st.precision == 64 ? 8 : 4;
     const int64_t P = st.n_pairs;
     const FeatureLayout layout = FeatureLayout::make(h_.max_angular, h_.nmax(), true);
-    void* features = arena_.alloc_bytes("dense.features_grad", T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride);
+    // the forward's features with derivatives when it kept them (and the
+    // surrogate that made them is still the active radial integral)
+    const bool kept = st.features_grad != nullptr && active_surrogate_ != nullptr;
+    void* features = kept ? st.features_grad
+                          : arena_.alloc_bytes("dense.features_grad", T_size * (size_t)std::max<int64_t>(P, 1) * layout.stride);
     void* grad_coef = coefficients ? const_cast<void*>(grad_values)
                                    : arena_.alloc_bytes("dense.grad_coef", T_size * (size_t)st.n_atoms * st.n_species * st.K);
     void* pair_grad = arena_.alloc_bytes("dense.pair_grad", T_size * 3 * (size_t)std::max<int64_t>(P, 1));
@@ -1149,6 +1160,7 @@ void Engine::backward_dense(DenseState& st, const void* grad_values, void* grad_
     } else {
         DenseArgs<float> a;
         dense_args(st, true, a);
+        a.gradient_features = kept;
         a.marks = marks;
         a.features = (float*)features;
         a.grad_values = (const float*)grad_values;

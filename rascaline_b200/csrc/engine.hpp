@@ -358,7 +358,7 @@ class Engine {
     std::unique_ptr<DenseState> forward_dense(int precision, std::vector<HostSystem>& systems,
                                               const double* d_positions, const std::vector<int32_t>& species,
                                               void* values, int64_t values_count, cudaStream_t stream,
-                                              bool expansion = false);
+                                              bool expansion = false, bool backward_follows = false);
     // dL/dpositions [n_atoms][3], and when not null dL/dstrain and dL/dcell
     // [n_systems][3][3], all device buffers of the forward precision
     // `by_species`: grad_values holds one dL/dP row per species (the weights

@@ -602,10 +602,10 @@ __global__ void __launch_bounds__(256) by_pair_kernel(ByPairArgs a) {
     const int64_t row0 = a.dir_row0[d], row1 = a.dir_row1[d];
     const int64_t grow = GRAD ? a.dir_grow[d] : 0;
     const bool same_atom = a.pairs.first[p] == a.pairs.second[p];
-    double fg = 0.0, r = 1.0, u[3] = {0.0, 0.0, 0.0}, vd[3] = {0.0, 0.0, 0.0}, sd[3] = {0.0, 0.0, 0.0};
+    double fg = 0.0, rinv = 1.0, u[3] = {0.0, 0.0, 0.0}, vd[3] = {0.0, 0.0, 0.0}, sd[3] = {0.0, 0.0, 0.0};
     if (GRAD) {
         fg = F[1];
-        r = F[2];
+        rinv = 1.0 / F[2];  // multiplied into the angular term, as in se_fused_kernel
 #pragma unroll
         for (int x = 0; x < 3; x++) {
             u[x] = F[3 + x];
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(256) by_pair_kernel(ByPairArgs a) {
 #pragma unroll
         for (int x = 0; x < 3; x++) {
             const double dY = F[L.off_dy + x * L.L2 + lm];
-            g[x] = fg * u[x] * Rv * Yv + f * dR * u[x] * Yv + f * Rv * dY / r;
+            g[x] = fg * u[x] * Rv * Yv + f * dR * u[x] * Yv + f * Rv * dY * rinv;
             if (inv) g[x] *= -m1;
         }
         if (POS && !same_atom) {
