@@ -225,3 +225,42 @@ def test_freed_surrogate_falls_back_to_the_spline():
     del calc2
     s2._calculator = None
     del s2
+
+
+def test_batched_pipeline_with_surrogate_keeps_the_pair_features(trained):
+    # The batch's dense pipeline asks for forces, so its forward pass computes
+    # the surrogate's pair features with their derivatives once and its
+    # backward reuses them.  Values and forces must agree with the dense
+    # forward + backward, whose backward evaluates the network again
+    # (tolerance 1e-4 of the largest force: the two sum dL/dc in different
+    # orders in FP32).
+    from rascaline_b200.torch_api import Batch, dense_backward, dense_power_spectrum
+    calc, s, _ = trained
+    mols = workloads.molecules(24, seed=11)
+    positions = np.concatenate([m["positions"] for m in mols])
+    types = np.concatenate([m["types"] for m in mols]).astype(np.int32)
+    sizes = np.array([len(m["types"]) for m in mols])
+    species = [1, 6, 7, 8]
+    batch = Batch(calc, sizes, types, species)
+    rng = np.random.default_rng(3)
+    W = rng.normal(0.0, 1.0 / np.sqrt(batch.n_keys * batch.n_properties),
+                   size=(len(species), batch.n_keys, batch.n_properties))
+    weights = torch.as_tensor(W, dtype=torch.float32, device="cuda").contiguous()
+    pos = torch.as_tensor(positions, device="cuda")
+    out = batch.outputs()
+    batch.config = {"warps": 4, "chunk": 32, "layout": 1, "ctas_per_sm": 2, "pipeline": 1}
+    s.attach()
+    try:
+        batch.run(pos, out, weights=weights)
+        values, state = dense_power_spectrum(calc, pos, types, np.zeros((len(mols), 9)), sizes, 32, species)
+        G = torch.as_tensor(W[np.searchsorted(species, types)], dtype=torch.float32, device="cuda")
+        grad, _, _ = dense_backward(state, G, len(mols), strain=False, cell=False)
+        torch.cuda.synchronize()
+    finally:
+        s.attach(False)
+
+    def rel(a, b):
+        return float((a.double() - b.double()).abs().max() / b.double().abs().max())
+
+    assert rel(out["values"], values) <= 1e-6
+    assert rel(out["gradients"], grad) <= 1e-4
