@@ -1102,17 +1102,14 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
 }
 
 // One centre's S-way merge of its (centre, species) segments of directions,
-// by the other atom's index (plan.cpp build_neighborhoods): counts the unique
-// neighbours (FILL false) or writes them with their prefix counts (FILL true)
+// by the other atom's index (plan.cpp build_neighborhoods): writes its unique
+// neighbours and itself with their prefix counts, one thread
 constexpr int NB_MAX_SPECIES = 64;
 
-template <bool FILL>
 __device__ void neighborhoods_merge(int64_t c, const int32_t* __restrict__ first, const int32_t* __restrict__ second,
                                     const int32_t* __restrict__ atom_species, const int32_t* __restrict__ dir,
-                                    const int64_t* __restrict__ seg, int S, int64_t* __restrict__ counts,
-                                    const int64_t* __restrict__ offsets, PsEntry* __restrict__ entries,
-                                    int32_t* __restrict__ entry_cum, int32_t* __restrict__ species_count,
-                                    uint8_t* __restrict__ species_mask) {
+                                    const int64_t* __restrict__ seg, int S, const int64_t* __restrict__ offsets,
+                                    PsEntry* __restrict__ entries, int32_t* __restrict__ entry_cum) {
     int64_t pos[NB_MAX_SPECIES], end[NB_MAX_SPECIES];
     int32_t head[NB_MAX_SPECIES], cum[NB_MAX_SPECIES + 1];
     const int sc = atom_species[c];
@@ -1129,14 +1126,12 @@ __device__ void neighborhoods_merge(int64_t c, const int32_t* __restrict__ first
         cum[t] = 0;
     }
     cum[S] = 0;
-    const int64_t base = FILL ? offsets[c] : 0;
+    const int64_t base = offsets[c];
     int64_t n = 0;
     auto emit = [&](int32_t atom, int32_t species, int32_t d0, int32_t d1) {
-        if (FILL) {
-            entries[base + n] = PsEntry{atom, species, d0, d1};
-            int32_t* w = entry_cum + (base + n) * (S + 1);
-            for (int t = 0; t <= S; t++) w[t] = cum[t];
-        }
+        entries[base + n] = PsEntry{atom, species, d0, d1};
+        int32_t* w = entry_cum + (base + n) * (S + 1);
+        for (int t = 0; t <= S; t++) w[t] = cum[t];
         n++;
     };
     bool self_done = false;
@@ -1171,13 +1166,6 @@ __device__ void neighborhoods_merge(int64_t c, const int32_t* __restrict__ first
         emit(best_atom, best, (int32_t)d0, (int32_t)d);
         cum[best]++;
     }
-    if (!FILL) {
-        counts[c] = n;
-        for (int t = 0; t < S; t++) {
-            species_count[c * S + t] = cum[t];
-            species_mask[c * S + t] = (end[t] > seg[c * S + t] || t == sc) ? 1 : 0;
-        }
-    }
 }
 
 // The filling half, a warp per centre: the centre's directions (other atom
@@ -1186,7 +1174,7 @@ __device__ void neighborhoods_merge(int64_t c, const int32_t* __restrict__ first
 // entry, whose place in the centre's list is the number of such entries with
 // a smaller atom index (plus the centre's own entry when that comes first),
 // and whose prefix count of species t the number of them in segment t.  The
-// same entries and prefix counts as neighborhoods_merge<true>, which takes
+// same entries and prefix counts as neighborhoods_merge, which takes
 // the centres with more than NB_WARP_DIRS directions.
 constexpr int NB_WARP_DIRS = 256;
 constexpr int NB_FILL_WARPS = 4;
@@ -1205,8 +1193,7 @@ __global__ void __launch_bounds__(NB_FILL_WARPS * 32)
     const int64_t b = seg[c * S], n = seg[c * S + S] - b;
     if (n > NB_WARP_DIRS) {
         if (lane == 0)
-            neighborhoods_merge<true>(c, first, second, atom_species, dir, seg, S, nullptr, offsets, entries,
-                                      entry_cum, nullptr, nullptr);
+            neighborhoods_merge(c, first, second, atom_species, dir, seg, S, offsets, entries, entry_cum);
         return;
     }
     int32_t* other = other_s[warp];
@@ -1263,12 +1250,13 @@ __global__ void __launch_bounds__(NB_FILL_WARPS * 32)
     }
 }
 
-// The counting half of neighborhoods_merge, a warp per centre: within a
+// The counting half, a warp per centre: within a
 // (centre, species) segment the other atoms come in increasing order with the
 // periodic images of one atom adjacent, so the unique neighbours of that
 // species are the directions whose other atom differs from the previous
 // direction's and is not the centre.  Writes the same counts, species counts
-// and species masks as neighborhoods_merge<false>.
+// and species masks as the merge would (one unique neighbour per run of
+// adjacent images, the centre's own images excluded).
 __global__ void neighborhoods_count_kernel(const int32_t* __restrict__ first, const int32_t* __restrict__ second,
                                            const int32_t* __restrict__ atom_species, const int32_t* __restrict__ dir,
                                            const int64_t* __restrict__ seg, int S, int64_t n_atoms,

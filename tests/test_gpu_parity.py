@@ -206,6 +206,14 @@ def test_power_spectrum_many_radial_functions(oracle):
     check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(4.0, 9, 2), systems, ("positions", "strain"))
 
 
+def test_dense_neighbourhoods(oracle):
+    # 314 to 329 neighbours per centre within 8.5 A of the 216-atom lattice: more
+    # than the 256 directions the warp-per-centre neighbourhood tables hold,
+    # so these centres take the serial merge
+    systems = [workloads.sc_lattice(seed=1)]
+    check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(8.5, 3, 2), systems, ("positions",))
+
+
 def test_strain_and_cell_without_positions(oracle):
     systems = [workloads.random_box(90, seed=22)]
     check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(4.5, 7, 5), systems, ("strain", "cell"))
