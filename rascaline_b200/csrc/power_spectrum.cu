@@ -899,7 +899,41 @@ __device__ __forceinline__ void centre_row(int lane, int lmax, int nmax, int K, 
 // CR_CELL; three passes of three components).  CR_SPLIT CTAs per centre with the
 // coefficients in fragment order in shared memory; items (slot, kind, pass)
 // are spread over their warps.
-constexpr int CR_SELF = 1, CR_STRAIN = 2, CR_CELL = 4;
+constexpr int CR_SELF = 1, CR_STRAIN = 2, CR_CELL = 4, CR_VALUES = 8;
+
+// the values row of one centre and slot (a, b): per l the 8 x 8 tile
+// sum_m c_a[l m][n1] c_b[l m][n2] from the fragment-ordered coefficients
+__device__ __forceinline__ void values_row(int lane, int lmax, int nmax, const double* __restrict__ cf, int P,
+                                           const double* __restrict__ scales, int a, int b, double* __restrict__ out) {
+    const int tm = lane & 3, tn = lane >> 2;
+    const double* ca = cf + a * P + lane;
+    const double* cb = cf + b * P + lane;
+    const int N = nmax;
+    const bool vec = N == 8 && ((((uintptr_t)out) & 15) == 0);
+    int step = 0;
+    for (int l = 0; l <= lmax; l++) {
+        const int steps = (2 * l + 1 + 3) >> 2;
+        double acc[2] = {0.0, 0.0};
+#pragma unroll
+        for (int st = 0; st < CR_MAX_STEPS; st++) {
+            if (st >= steps) break;
+            dmma_8x8x4(acc, ca[(step + st) * 32], cb[(step + st) * 32]);
+        }
+        step += steps;
+        const double scale = scales[l];
+        const int n2 = 2 * tm;
+        if (vec) {
+            double2 w;
+            w.x = acc[0] * scale;
+            w.y = acc[1] * scale;
+            __stcs(reinterpret_cast<double2*>(out + (int64_t)l * 64 + tn * 8 + n2), w);
+        } else if (tn < N) {
+            double* o = out + (int64_t)l * N * N + tn * N + n2;
+            if (n2 < N) __stcs(o, acc[0] * scale);
+            if (n2 + 1 < N) __stcs(o + 1, acc[1] * scale);
+        }
+    }
+}
 
 __global__ void __launch_bounds__(128) ps_centre_rows_kernel(PsArgs a, int kinds) {
     extern __shared__ __align__(16) double cr_smem[];
@@ -945,14 +979,20 @@ __global__ void __launch_bounds__(128) ps_centre_rows_kernel(PsArgs a, int kinds
     const int ns = (int)(a.slot_offset[c + 1] - s0);
     // per slot: the self row (if requested and the centre's entry exists),
     // then 3 strain passes, then 3 cell passes
-    const int n_self = (kinds & CR_SELF) && self_entry >= 0 ? 1 : 0;
+    const int n_values = (kinds & CR_VALUES) ? 1 : 0, n_self = (kinds & CR_SELF) && self_entry >= 0 ? 1 : 0;
     const int n_strain = (kinds & CR_STRAIN) ? 3 : 0, n_cell = (kinds & CR_CELL) ? 3 : 0;
-    const int per_slot = n_self + n_strain + n_cell;
+    const int per_slot = n_values + n_self + n_strain + n_cell;
     for (int it = part * nwarps + warp; it < ns * per_slot; it += CR_SPLIT * nwarps) {
         const int si = it / per_slot;
         int kind = it - si * per_slot;
         const PsKeySlot slot = a.slots[s0 + si];
         const double* scales = scale_s + (slot.a != slot.b ? L + 1 : 0);
+        if (kind < n_values) {
+            values_row(lane, L, N, cf, P, scales, slot.a, slot.b,
+                       a.out + a.off_values[slot.block] + (int64_t)slot.sample * a.n_props);
+            continue;
+        }
+        kind -= n_values;
         const double *da, *db;
         double* out;
         if (kind < n_self) {
@@ -1053,19 +1093,22 @@ void launch_all(const PsArgs& args, bool values, bool positions, bool strain, bo
     CUDA_CHECK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
     CUDA_CHECK(cudaEventRecord(fork, stream));
     CUDA_CHECK(cudaStreamWaitEvent(side, fork, 0));
-    if (values) {
-        ps_values_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args);
-        CUDA_CHECK(cudaGetLastError());
-    }
-    if (events.after_values) CUDA_CHECK(cudaEventRecord(events.after_values, side));
-    // nmax <= 8, lmax <= 8: the staged positions kernel, and the centres'
-    // own positions rows with the strain / cell rows in ps_centre_rows_kernel
+    // nmax <= 8, lmax <= 9: the staged positions kernel, and the values rows
+    // with the centres' own positions rows and the strain / cell rows in
+    // ps_centre_rows_kernel (values alone keep ps_values_kernel)
     const StgLayout stg = stg_layout(args.n_species, args.lmax, args.nmax);
     const bool dmma_rows = args.nmax <= 8 && (2 * args.lmax + 1 + 3) / 4 <= CR_MAX_STEPS;
     const bool staged = positions && dmma_rows && args.n_species <= STG_MAX_SPECIES && stg.bytes <= 200 * 1024;
     const size_t cr_bytes = sizeof(double) * ((size_t)args.n_species * 32 * stg_steps(args.lmax) + 2 * (args.lmax + 1));
-    const int kinds = (staged ? CR_SELF : 0) | (strain ? CR_STRAIN : 0) | (cell ? CR_CELL : 0);
-    if (dmma_rows && cr_bytes <= 200 * 1024 && kinds != 0 && (staged || !positions)) {
+    const int gradient_kinds = (staged ? CR_SELF : 0) | (strain ? CR_STRAIN : 0) | (cell ? CR_CELL : 0);
+    const bool centre_rows = dmma_rows && cr_bytes <= 200 * 1024 && gradient_kinds != 0 && (staged || !positions);
+    const int kinds = gradient_kinds | (values ? CR_VALUES : 0);
+    if (values && !centre_rows) {
+        ps_values_kernel<MAXN><<<(unsigned)args.n_centres, threads, coef_bytes, side>>>(args);
+        CUDA_CHECK(cudaGetLastError());
+    }
+    if (events.after_values) CUDA_CHECK(cudaEventRecord(events.after_values, side));
+    if (centre_rows) {
         ps_centre_rows_kernel<<<(unsigned)(CR_SPLIT * args.n_centres), 128, cr_bytes, side>>>(args, kinds);
         CUDA_CHECK(cudaGetLastError());
     } else {
