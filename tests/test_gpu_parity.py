@@ -214,6 +214,14 @@ def test_dense_neighbourhoods(oracle):
     check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(8.5, 3, 2), systems, ("positions",))
 
 
+def test_many_species(oracle):
+    # more than 10 atomic types: the positions rows take the per-warp kernel,
+    # the strain rows ps_strain_cell_kernel and the values ps_values_kernel
+    species = (1, 3, 5, 6, 7, 8, 9, 11, 12, 14, 15)
+    systems = [workloads.random_box(70, density=0.12, species=species, seed=23)]
+    check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(4.0, 3, 2), systems, ("positions", "strain"))
+
+
 def test_strain_and_cell_without_positions(oracle):
     systems = [workloads.random_box(90, seed=22)]
     check_against_oracle(oracle, "soap_power_spectrum", workloads.hypers(4.5, 7, 5), systems, ("strain", "cell"))
