@@ -500,8 +500,8 @@ __global__ void __launch_bounds__(POS_WARPS * 32, POS_MIN_BLOCKS) ps_positions_k
 // warps share, in shared memory:
 //   * the centre's coefficients of every species in DMMA fragment order,
 //     zero-padded to 4 m and 8 n per l (so that padding contributes nothing);
-//   * a ring of three pair-gradient buffers filled by cp.async two entries
-//     ahead of the one being computed.  For nmax = 8 a buffer holds
+//   * two pair-gradient buffers, the next entry's filled by cp.async while
+//     the current one is computed.  For nmax = 8 a buffer holds
 //     [3][step][4 m][8 n] (m padded to 4 per l like the coefficients, the
 //     padding kept at zero), with the 16-byte chunks of the rows m = 2, 3 of
 //     each step swapped pairwise, so that a fragment load is one offset per
@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(POS_WARPS * 32, POS_MIN_BLOCKS) ps_positions_k
 // take the CUDA-core rows with global operands; the centre's own rows are
 // written by ps_centre_rows_kernel on the side stream.
 constexpr int STG_WARPS = 4;
-constexpr int STG_RING = 3;
+constexpr int STG_RING = 2;
 constexpr int STG_CHUNK = 64;
 constexpr int STG_SPLIT = 2;
 constexpr int STG_MAX_SPECIES = 10;
@@ -788,13 +788,12 @@ __global__ void __launch_bounds__(STG_WARPS * 32, 4) ps_positions_staged_kernel(
             cp_async_commit();
         };
         issue(0);
-        issue(1);
         for (int k = 0; k < nc; k++) {
-            cp_async_wait<1>();
+            cp_async_wait<0>();
             // entry k's gradient is visible to every warp, and every warp is
             // done with entry k - 1, whose buffer the next issue reuses
             __syncthreads();
-            issue(k + 2);
+            issue(k + 1);
             const PsEntry entry = meta_entry[k];
             if (entry.atom == (int32_t)c) continue;  // the centre's own rows: ps_centre_rows_kernel
             const int32_t* cum = meta_cum + k * (S + 1);
